@@ -1,0 +1,340 @@
+/* SPDX-License-Identifier: Apache-2.0
+ *
+ * nepheline_b200: the physics world step's solver stage (the graph-coloured
+ * soft-step contact and joint solver) on one NVIDIA B200, behind a plain C ABI.
+ *
+ * The entry points replace the reference engine's
+ *
+ *     NphResult phys_solve(NphPhysicsWorld *w, f32 dt, NphJobSystem *js);
+ *
+ * (engine/physics/src/world_internal.h:791, defined at engine/physics/src/solver.c:961,
+ * called once per step from nph_physics_world_step at engine/physics/src/world.c:346).
+ * The reference passes its whole world; this ABI passes the part of it the solver
+ * stage reads and writes, as flat arrays of plain records (the "world view"):
+ *
+ *   - the awake bodies, in the world's awake-list order (world_internal.h:600), which is
+ *     the solver-body order of solver.c:967-973;
+ *   - the bodies a constraint names that have no solver slot (static bodies, sleeping
+ *     kinematic ones), read-only;
+ *   - the touching contacts of the constraint graph, in colour order (colours 0..23, then
+ *     the overflow: the order build_groups lays out, solver.c:810-843), each colour's
+ *     contacts in its list order (world_internal.h:363-367);
+ *   - the graph's joints, in the same colour order (build_step_joints, solver.c:793-806).
+ *
+ * Every record is updated in place with what phys_solve writes back into the world:
+ * body velocities, rotation, centre, origin, sleep time, cleared force and torque
+ * (finalize_body, solver.c:304-349); contact points' impulses, approach speeds and the
+ * HIT flag (store_group, solver.c:475-499); joints' accumulated impulses.
+ *
+ * Result codes have the values of the reference's NphResult (engine/core/include/
+ * nepheline/core/result.h:16-36), so a caller can return them as they are.
+ *
+ * Threading: one thread owns a solver object. Calls are synchronous (they return after
+ * the device-to-host copy), as phys_solve returns after its stages, except the
+ * *_async device-resident calls, which enqueue on the solver's stream.
+ */
+#ifndef NEPHELINE_B200_H
+#define NEPHELINE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define NPH_GPU_API __attribute__((visibility("default")))
+#else
+#define NPH_GPU_API
+#endif
+
+/* ------------------------------------------------------------------------------------
+ * Constants (the reference's values)
+ * ---------------------------------------------------------------------------------- */
+
+#define NPH_GPU_NULL 0xFFFFFFFFu
+#define NPH_GPU_MAX_POINTS 4u        /* NPH_PHYSICS_MANIFOLD_MAX_POINTS, collide.h:64 */
+#define NPH_GPU_COLORS 24u           /* PHYS_GRAPH_COLORS, world_internal.h:359 */
+#define NPH_GPU_DYNAMIC_COLORS 20u   /* PHYS_GRAPH_DYNAMIC_COLORS, world_internal.h:360 */
+#define NPH_GPU_OVERFLOW 24u         /* PHYS_GRAPH_OVERFLOW, world_internal.h:361 */
+#define NPH_GPU_COLOR_SLOTS 25u      /* colours 0..23 and the overflow */
+
+/* Result codes: the values of NphResult (core/result.h:16-36). */
+typedef int32_t NphGpuResult;
+#define NPH_GPU_OK 0
+#define NPH_GPU_OUT_OF_MEMORY 1
+#define NPH_GPU_INVALID_ARGUMENT 2
+#define NPH_GPU_UNSUPPORTED 8
+#define NPH_GPU_DEVICE_LOST 17
+#define NPH_GPU_INVALID_STATE 18
+#define NPH_GPU_UNKNOWN 19
+
+/* Body types (NphPhysicsBodyType, body.h). */
+#define NPH_GPU_BODY_STATIC 0u
+#define NPH_GPU_BODY_KINEMATIC 1u
+#define NPH_GPU_BODY_DYNAMIC 2u
+
+/* Body flag bits the solver stage reads (PHYS_BODY_*, world_internal.h:59-69). */
+#define NPH_GPU_BODY_ENABLE_SLEEP (1u << 1)
+#define NPH_GPU_BODY_GYROSCOPIC (1u << 2)
+#define NPH_GPU_BODY_BULLET (1u << 5)
+
+/* Lock bits (NPH_PHYSICS_LOCK_*, body.h). */
+#define NPH_GPU_LOCK_LINEAR_X (1u << 0)
+#define NPH_GPU_LOCK_LINEAR_Y (1u << 1)
+#define NPH_GPU_LOCK_LINEAR_Z (1u << 2)
+#define NPH_GPU_LOCK_ANGULAR_X (1u << 3)
+#define NPH_GPU_LOCK_ANGULAR_Y (1u << 4)
+#define NPH_GPU_LOCK_ANGULAR_Z (1u << 5)
+
+/* Contact flag bits the solver stage reads and writes (PHYS_CONTACT_*,
+ * world_internal.h:207-213). */
+#define NPH_GPU_CONTACT_HIT (1u << 4)
+
+/* Constraint bits of nph_gpu_graph_color. */
+#define NPH_GPU_CONSTRAINT_A_DYNAMIC 1u
+#define NPH_GPU_CONSTRAINT_B_DYNAMIC 2u
+#define NPH_GPU_CONSTRAINT_JOINT 4u
+
+/* Joint types (NphPhysicsJointType, joint.h). The device solver runs ball and hinge
+ * joints; the world's other types are refused with NPH_GPU_UNSUPPORTED. */
+#define NPH_GPU_JOINT_BALL 0u
+#define NPH_GPU_JOINT_HINGE 1u
+
+/* Solvers (NphPhysicsSolver, world.h). The device solver runs the soft step. */
+#define NPH_GPU_SOLVER_SOFT_STEP 0u
+
+/* ------------------------------------------------------------------------------------
+ * Records
+ * ---------------------------------------------------------------------------------- */
+
+/* The world settings the solver stage reads: NphPhysicsWorldDesc (world.h:104-143),
+ * defaults at world.c:85-104. */
+typedef struct NphGpuWorldParams {
+    float gravity[3];
+    uint32_t solver; /* NPH_GPU_SOLVER_SOFT_STEP */
+    uint32_t substeps;
+    float contact_hertz; /* 0: an eighth of the substep rate (solver.c:996-997) */
+    float contact_damping_ratio;
+    float contact_push_max_velocity;
+    float restitution_threshold;
+    float max_linear_speed;
+    float joint_hertz; /* 0: a quarter of the substep rate (solver.c:998) */
+    float joint_damping_ratio;
+    uint32_t enable_continuous; /* must be 0: continuous collision stays on the host */
+} NphGpuWorldParams;
+
+/* A body, as PhysBody (world_internal.h:71-107) holds what the solver stage reads.
+ * Matrices are column-major, as NphMat3 (m[col * 3 + row]). Quaternions are x, y, z, w. */
+typedef struct NphGpuBody {
+    double center[3];           /* centre of mass, world; in and out */
+    double origin[3];           /* the body frame's origin; out */
+    float rotation[4];          /* in and out */
+    float local_center[3];      /* centre of mass in the body frame */
+    float linear_velocity[3];   /* in and out */
+    float angular_velocity[3];  /* in and out */
+    float force[3];             /* in; zero after the step */
+    float torque[3];            /* in; zero after the step */
+    float inertia[9];           /* about the centre of mass, body axes */
+    float inv_inertia[9];
+    float inv_mass;
+    float linear_damping;
+    float angular_damping;
+    float gravity_scale;
+    float sleep_threshold;
+    float sleep_time;           /* in and out */
+    float max_extent;
+    uint32_t type;              /* NPH_GPU_BODY_* */
+    uint32_t flags;             /* NPH_GPU_BODY_* bits */
+    uint32_t locks;             /* NPH_GPU_LOCK_* bits */
+    uint32_t pad;
+} NphGpuBody;
+
+/* A manifold point, as PhysContactPoint (world_internal.h:196-205). */
+typedef struct NphGpuContactPoint {
+    float anchor_a[3];          /* from A's centre of mass, world axes */
+    float anchor_b[3];          /* from B's */
+    float separation;
+    float normal_impulse;       /* in (warm start) and out */
+    float max_normal_impulse;   /* out: the largest this step */
+    float tangent_impulse[3];   /* in and out: world vector */
+    float relative_velocity;    /* out: normal approach speed at the step's start */
+    uint32_t id;                /* the narrow phase's feature id: passed through */
+} NphGpuContactPoint;
+
+/* A touching contact (one manifold), as PhysContact (world_internal.h:229-253).
+ * `body_a` and `body_b` index the view's bodies: below `body_count` an awake body,
+ * from `body_count` on the fixed body `index - body_count`. */
+typedef struct NphGpuContact {
+    uint32_t body_a;
+    uint32_t body_b;
+    uint32_t flags;             /* NPH_GPU_CONTACT_HIT: in and out */
+    uint32_t point_count;       /* 1..4 */
+    float normal[3];            /* from A to B */
+    float friction;
+    float restitution;
+    uint32_t pad[3];
+    NphGpuContactPoint points[NPH_GPU_MAX_POINTS];
+} NphGpuContact;
+
+/* Ball joint settings (NphPhysicsBallJoint, joint.h). */
+typedef struct NphGpuBallJoint {
+    uint32_t enable_swing_limit;
+    float swing_y;
+    float swing_z;
+    uint32_t enable_twist_limit;
+    float twist_lower;
+    float twist_upper;
+    float friction_torque;
+    float pad[3];
+} NphGpuBallJoint;
+
+/* Hinge joint settings (NphPhysicsHingeJoint, joint.h). */
+typedef struct NphGpuHingeJoint {
+    uint32_t enable_limit;
+    float lower;
+    float upper;
+    uint32_t enable_motor;
+    float motor_speed;
+    float max_motor_torque;
+    uint32_t enable_spring;
+    float spring_hertz;
+    float spring_damping_ratio;
+    float spring_target;
+} NphGpuHingeJoint;
+
+/* A joint of the constraint graph, as PhysJoint (world_internal.h:280-330): its frames
+ * in the bodies' frames, its settings, and its accumulated impulses (in and out). */
+typedef struct NphGpuJoint {
+    uint32_t type;              /* NPH_GPU_JOINT_BALL or NPH_GPU_JOINT_HINGE */
+    uint32_t body_a;            /* as NphGpuContact */
+    uint32_t body_b;
+    uint32_t pad0;
+    float frame_a_position[3];  /* in body A's frame (its origin) */
+    float frame_a_rotation[4];
+    float frame_b_position[3];
+    float frame_b_rotation[4];
+    union {
+        NphGpuBallJoint ball;
+        NphGpuHingeJoint hinge;
+    } u;
+    float linear_impulse[3];
+    float angular_impulse[3];
+    float friction_impulse[3];
+    float lower_impulse;
+    float upper_impulse;
+    float swing_impulse;
+    float motor_impulse;
+    float spring_impulse;
+} NphGpuJoint;
+
+/* The solver stage's part of a world. The arrays are the caller's; a solve updates
+ * `bodies`, `contacts` and `joints` in place. */
+typedef struct NphGpuWorldView {
+    NphGpuBody *bodies;                 /* awake bodies, awake-list order */
+    uint32_t body_count;
+    uint32_t fixed_count;
+    const NphGpuBody *fixed_bodies;     /* bodies without a solver slot, read only */
+    NphGpuContact *contacts;            /* colour order */
+    uint32_t contact_count;
+    uint32_t joint_count;
+    NphGpuJoint *joints;                /* colour order */
+    uint32_t contact_color_counts[NPH_GPU_COLOR_SLOTS]; /* colours 0..23, then the overflow */
+    uint32_t joint_color_counts[NPH_GPU_COLOR_SLOTS];
+} NphGpuWorldView;
+
+/* What a step reports (a subset of NphPhysicsStats, world.h:250-278). */
+typedef struct NphGpuStepStats {
+    uint32_t colors_used;           /* colours holding contacts or joints */
+    uint32_t overflow_contacts;
+    uint32_t overflow_joints;
+    uint32_t launches;              /* device kernels launched per step */
+    float device_ms;                /* device time of the last step (CUDA events) */
+    float upload_ms;                /* host->device of the last phys_solve call */
+    float download_ms;              /* device->host of the last phys_solve call */
+    uint32_t error_word;            /* device error flags of the last step (0: none) */
+} NphGpuStepStats;
+
+/* ------------------------------------------------------------------------------------
+ * The solver object
+ * ---------------------------------------------------------------------------------- */
+
+typedef struct NphGpuSolver NphGpuSolver;
+
+typedef struct NphGpuSolverDesc {
+    int32_t device;            /* CUDA ordinal */
+    void *stream;              /* a cudaStream_t to launch on, or NULL for the solver's own */
+    uint32_t use_graph;        /* 1: replay each step's launches as one CUDA graph */
+    uint32_t body_capacity;    /* initial device capacities (grown between steps) */
+    uint32_t contact_capacity;
+    uint32_t joint_capacity;
+} NphGpuSolverDesc;
+
+/* Creates a solver on `desc->device`. Device buffers are sized to the capacities and grow
+ * only between steps, so a steady state allocates nothing (as the world's arrays,
+ * world.h:37-43). */
+NPH_GPU_API NphGpuResult nph_gpu_solver_create(const NphGpuSolverDesc *desc, NphGpuSolver **out);
+NPH_GPU_API void nph_gpu_solver_destroy(NphGpuSolver *solver);
+
+/* The drop-in for phys_solve (solver.c:961-1105): uploads the view, runs the stage list
+ * (prepare bodies, prepare contacts and joints; per substep integrate velocities, warm
+ * start, solve, integrate positions, relax, each constraint pass colour by colour with the
+ * overflow first; then restitution, store, finalize) and writes the results back into the
+ * view's arrays. Returns NPH_GPU_INVALID_ARGUMENT for a malformed view (an index out of
+ * range, a point count outside 1..4, colour counts that do not add up), NPH_GPU_UNSUPPORTED
+ * for a setting the device solver does not run (another solver, continuous collision, a
+ * joint type other than ball and hinge), NPH_GPU_OUT_OF_MEMORY when the device buffers
+ * cannot grow (the view is then untouched: the step did not happen), and
+ * NPH_GPU_DEVICE_LOST when a device wait gave up or the device reported an error. */
+NPH_GPU_API NphGpuResult nph_gpu_phys_solve(NphGpuSolver *solver, const NphGpuWorldParams *params,
+                                            float dt, NphGpuWorldView *view);
+
+/* Device-resident stepping: the view's records are uploaded once, stepped `steps` times on
+ * the device (each step the whole solver stage over the resident records: the manifolds'
+ * geometry stays as uploaded, the bodies and impulses carry over), and read back when the
+ * caller asks. upload/download are synchronous; step_async enqueues on the solver's stream. */
+NPH_GPU_API NphGpuResult nph_gpu_world_upload(NphGpuSolver *solver, const NphGpuWorldView *view);
+NPH_GPU_API NphGpuResult nph_gpu_world_step_async(NphGpuSolver *solver,
+                                                  const NphGpuWorldParams *params, float dt,
+                                                  uint32_t steps);
+NPH_GPU_API NphGpuResult nph_gpu_world_download(NphGpuSolver *solver, NphGpuWorldView *view);
+NPH_GPU_API NphGpuResult nph_gpu_solver_synchronize(NphGpuSolver *solver);
+NPH_GPU_API NphGpuResult nph_gpu_solver_stats(const NphGpuSolver *solver, NphGpuStepStats *out);
+/* The stream the solver launches on (a cudaStream_t). */
+NPH_GPU_API void *nph_gpu_solver_stream(const NphGpuSolver *solver);
+
+/* Test hook: the iteration limit of every bounded device wait (0 restores the default). A
+ * limit of 1 makes the waits give up at once, so the error path can be tested without
+ * hanging a device. */
+NPH_GPU_API void nph_gpu_solver_set_wait_limit(NphGpuSolver *solver, uint32_t limit);
+
+/* ------------------------------------------------------------------------------------
+ * The constraint graph's colouring on the device
+ * ---------------------------------------------------------------------------------- */
+
+/* Colours `count` constraints inserted in order into an empty constraint graph, as the
+ * reference's phys_graph_add / phys_graph_add_joint do one at a time (graph_pick_color,
+ * island.c:34-56; graph_set_bodies, island.c:58-75): a pair of dynamic bodies takes the
+ * first of colours 0..19 free for both, a constraint with one dynamic body the first of
+ * colours 1..23 free for it, and the rest overflow (NPH_GPU_OVERFLOW). `body_a`/`body_b`
+ * are body slots below `body_slots`; `dynamic_bits` bit 0 says A is dynamic, bit 1 B, and
+ * bit 2 that the constraint is a joint (joints and contacts share the colours' body sets,
+ * but each colour keeps a contact list and a joint list: island.c:77-88, 106-118). Writes
+ * each constraint's colour and its slot in its colour's list of its kind (the list order
+ * is the insertion order). The result equals the sequential first-fit bit for bit. */
+NPH_GPU_API NphGpuResult nph_gpu_graph_color(NphGpuSolver *solver, const uint32_t *body_a,
+                                             const uint32_t *body_b, const uint8_t *dynamic_bits,
+                                             uint32_t count, uint32_t body_slots,
+                                             uint32_t *out_color, uint32_t *out_slot);
+
+/* ------------------------------------------------------------------------------------
+ * Version
+ * ---------------------------------------------------------------------------------- */
+
+NPH_GPU_API const char *nph_gpu_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NEPHELINE_B200_H */

@@ -1,0 +1,241 @@
+"""Record layouts of include/nepheline_b200.h as numpy dtypes and ctypes structures.
+
+The world view's arrays are numpy structured arrays with exactly the C structs' layout,
+so a view built here is passed to the C ABI without copying. `check_layout` compares the
+sizes with the ones the shared library reports.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+NULL = 0xFFFFFFFF
+MAX_POINTS = 4
+COLORS = 24
+DYNAMIC_COLORS = 20
+OVERFLOW = 24
+COLOR_SLOTS = 25
+
+OK = 0
+OUT_OF_MEMORY = 1
+INVALID_ARGUMENT = 2
+UNSUPPORTED = 8
+DEVICE_LOST = 17
+INVALID_STATE = 18
+UNKNOWN = 19
+RESULT_NAMES = {
+    OK: "OK", OUT_OF_MEMORY: "OUT_OF_MEMORY", INVALID_ARGUMENT: "INVALID_ARGUMENT",
+    UNSUPPORTED: "UNSUPPORTED", DEVICE_LOST: "DEVICE_LOST", INVALID_STATE: "INVALID_STATE",
+    UNKNOWN: "UNKNOWN",
+}
+
+BODY_STATIC = 0
+BODY_KINEMATIC = 1
+BODY_DYNAMIC = 2
+BODY_ENABLE_SLEEP = 1 << 1
+BODY_GYROSCOPIC = 1 << 2
+BODY_BULLET = 1 << 5
+CONTACT_HIT = 1 << 4
+CONSTRAINT_A_DYNAMIC = 1
+CONSTRAINT_B_DYNAMIC = 2
+CONSTRAINT_JOINT = 4
+JOINT_BALL = 0
+JOINT_HINGE = 1
+SOLVER_SOFT_STEP = 0
+
+BODY_DTYPE = np.dtype([
+    ("center", "<f8", 3), ("origin", "<f8", 3), ("rotation", "<f4", 4),
+    ("local_center", "<f4", 3), ("linear_velocity", "<f4", 3), ("angular_velocity", "<f4", 3),
+    ("force", "<f4", 3), ("torque", "<f4", 3), ("inertia", "<f4", 9), ("inv_inertia", "<f4", 9),
+    ("inv_mass", "<f4"), ("linear_damping", "<f4"), ("angular_damping", "<f4"),
+    ("gravity_scale", "<f4"), ("sleep_threshold", "<f4"), ("sleep_time", "<f4"),
+    ("max_extent", "<f4"), ("type", "<u4"), ("flags", "<u4"), ("locks", "<u4"), ("pad", "<u4"),
+], align=True)
+
+POINT_DTYPE = np.dtype([
+    ("anchor_a", "<f4", 3), ("anchor_b", "<f4", 3), ("separation", "<f4"),
+    ("normal_impulse", "<f4"), ("max_normal_impulse", "<f4"), ("tangent_impulse", "<f4", 3),
+    ("relative_velocity", "<f4"), ("id", "<u4"),
+], align=True)
+
+CONTACT_DTYPE = np.dtype([
+    ("body_a", "<u4"), ("body_b", "<u4"), ("flags", "<u4"), ("point_count", "<u4"),
+    ("normal", "<f4", 3), ("friction", "<f4"), ("restitution", "<f4"), ("pad", "<u4", 3),
+    ("points", POINT_DTYPE, MAX_POINTS),
+], align=True)
+
+# The settings union: ball and hinge fields overlay the same 40 bytes.
+_BALL = [("enable_swing_limit", "<u4", 0), ("swing_y", "<f4", 4), ("swing_z", "<f4", 8),
+         ("enable_twist_limit", "<u4", 12), ("twist_lower", "<f4", 16),
+         ("twist_upper", "<f4", 20), ("friction_torque", "<f4", 24)]
+_HINGE = [("enable_limit", "<u4", 0), ("lower", "<f4", 4), ("upper", "<f4", 8),
+          ("enable_motor", "<u4", 12), ("motor_speed", "<f4", 16),
+          ("max_motor_torque", "<f4", 20), ("enable_spring", "<u4", 24),
+          ("spring_hertz", "<f4", 28), ("spring_damping_ratio", "<f4", 32),
+          ("spring_target", "<f4", 36)]
+_SETTINGS_BASE = 72
+
+
+def _joint_dtype() -> np.dtype:
+    names, formats, offsets = [], [], []
+
+    def add(name, fmt, off):
+        names.append(name)
+        formats.append(fmt)
+        offsets.append(off)
+
+    add("type", "<u4", 0)
+    add("body_a", "<u4", 4)
+    add("body_b", "<u4", 8)
+    add("pad0", "<u4", 12)
+    add("frame_a_position", ("<f4", 3), 16)
+    add("frame_a_rotation", ("<f4", 4), 28)
+    add("frame_b_position", ("<f4", 3), 44)
+    add("frame_b_rotation", ("<f4", 4), 56)
+    add("settings", ("<u4", 10), _SETTINGS_BASE)
+    for name, fmt, off in _BALL:
+        add("ball_" + name, fmt, _SETTINGS_BASE + off)
+    for name, fmt, off in _HINGE:
+        add("hinge_" + name, fmt, _SETTINGS_BASE + off)
+    add("linear_impulse", ("<f4", 3), 112)
+    add("angular_impulse", ("<f4", 3), 124)
+    add("friction_impulse", ("<f4", 3), 136)
+    add("lower_impulse", "<f4", 148)
+    add("upper_impulse", "<f4", 152)
+    add("swing_impulse", "<f4", 156)
+    add("motor_impulse", "<f4", 160)
+    add("spring_impulse", "<f4", 164)
+    return np.dtype({"names": names, "formats": formats, "offsets": offsets, "itemsize": 168})
+
+
+JOINT_DTYPE = _joint_dtype()
+
+
+class WorldParams(ctypes.Structure):
+    """NphGpuWorldParams: the world settings the solver stage reads (world.h:104-143)."""
+
+    _fields_ = [
+        ("gravity", ctypes.c_float * 3), ("solver", ctypes.c_uint32),
+        ("substeps", ctypes.c_uint32), ("contact_hertz", ctypes.c_float),
+        ("contact_damping_ratio", ctypes.c_float), ("contact_push_max_velocity", ctypes.c_float),
+        ("restitution_threshold", ctypes.c_float), ("max_linear_speed", ctypes.c_float),
+        ("joint_hertz", ctypes.c_float), ("joint_damping_ratio", ctypes.c_float),
+        ("enable_continuous", ctypes.c_uint32),
+    ]
+
+    @classmethod
+    def default(cls, **overrides) -> "WorldParams":
+        """The reference's defaults (world.c:85-104), continuous collision off."""
+        p = cls()
+        p.gravity[:] = (0.0, -9.81, 0.0)
+        p.solver = SOLVER_SOFT_STEP
+        p.substeps = 4
+        p.contact_hertz = 0.0
+        p.contact_damping_ratio = 10.0
+        p.contact_push_max_velocity = 3.0
+        p.restitution_threshold = 1.0
+        p.max_linear_speed = 400.0
+        p.joint_hertz = 0.0
+        p.joint_damping_ratio = 2.0
+        p.enable_continuous = 0
+        for k, v in overrides.items():
+            if k == "gravity":
+                p.gravity[:] = v
+            else:
+                setattr(p, k, v)
+        return p
+
+
+class WorldView(ctypes.Structure):
+    """NphGpuWorldView: pointers into numpy record arrays, updated in place by a solve."""
+
+    _fields_ = [
+        ("bodies", ctypes.c_void_p), ("body_count", ctypes.c_uint32),
+        ("fixed_count", ctypes.c_uint32), ("fixed_bodies", ctypes.c_void_p),
+        ("contacts", ctypes.c_void_p), ("contact_count", ctypes.c_uint32),
+        ("joint_count", ctypes.c_uint32), ("joints", ctypes.c_void_p),
+        ("contact_color_counts", ctypes.c_uint32 * COLOR_SLOTS),
+        ("joint_color_counts", ctypes.c_uint32 * COLOR_SLOTS),
+    ]
+
+
+class StepStats(ctypes.Structure):
+    _fields_ = [
+        ("colors_used", ctypes.c_uint32), ("overflow_contacts", ctypes.c_uint32),
+        ("overflow_joints", ctypes.c_uint32), ("launches", ctypes.c_uint32),
+        ("device_ms", ctypes.c_float), ("upload_ms", ctypes.c_float),
+        ("download_ms", ctypes.c_float), ("error_word", ctypes.c_uint32),
+    ]
+
+
+class SolverDesc(ctypes.Structure):
+    _fields_ = [
+        ("device", ctypes.c_int32), ("stream", ctypes.c_void_p), ("use_graph", ctypes.c_uint32),
+        ("body_capacity", ctypes.c_uint32), ("contact_capacity", ctypes.c_uint32),
+        ("joint_capacity", ctypes.c_uint32),
+    ]
+
+
+def _ptr(a: np.ndarray | None) -> int | None:
+    if a is None or len(a) == 0:
+        return None
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data
+
+
+class View:
+    """A world view: the solver stage's records as numpy arrays plus the colour tables.
+
+    bodies:  awake bodies (BODY_DTYPE), solver order
+    fixed:   bodies without a solver slot (BODY_DTYPE), read only
+    contacts: CONTACT_DTYPE in colour order (colours 0..23, then the overflow)
+    joints:  JOINT_DTYPE in colour order
+    contact_color_counts / joint_color_counts: 25 counts each
+    """
+
+    def __init__(self, bodies, fixed, contacts, joints, contact_color_counts,
+                 joint_color_counts):
+        self.bodies = np.ascontiguousarray(bodies, dtype=BODY_DTYPE)
+        self.fixed = np.ascontiguousarray(fixed if fixed is not None else
+                                          np.zeros(0, BODY_DTYPE), dtype=BODY_DTYPE)
+        self.contacts = np.ascontiguousarray(contacts, dtype=CONTACT_DTYPE)
+        self.joints = np.ascontiguousarray(joints if joints is not None else
+                                           np.zeros(0, JOINT_DTYPE), dtype=JOINT_DTYPE)
+        self.contact_color_counts = np.asarray(contact_color_counts, dtype=np.uint32).copy()
+        self.joint_color_counts = np.asarray(joint_color_counts, dtype=np.uint32).copy()
+        assert self.contact_color_counts.shape == (COLOR_SLOTS,)
+        assert self.joint_color_counts.shape == (COLOR_SLOTS,)
+
+    def copy(self) -> "View":
+        return View(self.bodies.copy(), self.fixed.copy(), self.contacts.copy(),
+                    self.joints.copy(), self.contact_color_counts, self.joint_color_counts)
+
+    def c_view(self) -> WorldView:
+        v = WorldView()
+        v.bodies = _ptr(self.bodies)
+        v.body_count = len(self.bodies)
+        v.fixed_bodies = _ptr(self.fixed)
+        v.fixed_count = len(self.fixed)
+        v.contacts = _ptr(self.contacts)
+        v.contact_count = len(self.contacts)
+        v.joints = _ptr(self.joints)
+        v.joint_count = len(self.joints)
+        v.contact_color_counts[:] = [int(x) for x in self.contact_color_counts]
+        v.joint_color_counts[:] = [int(x) for x in self.joint_color_counts]
+        return v
+
+    @property
+    def colors_used(self) -> int:
+        return int(np.count_nonzero((self.contact_color_counts[:COLORS] > 0)
+                                    | (self.joint_color_counts[:COLORS] > 0)))
+
+    @property
+    def manifold_points(self) -> int:
+        return int(self.contacts["point_count"].sum())
+
+
+def layout_sizes() -> dict:
+    return {"body": BODY_DTYPE.itemsize, "point": POINT_DTYPE.itemsize,
+            "contact": CONTACT_DTYPE.itemsize, "joint": JOINT_DTYPE.itemsize,
+            "params": ctypes.sizeof(WorldParams), "view": ctypes.sizeof(WorldView)}

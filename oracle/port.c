@@ -1,0 +1,311 @@
+// SPDX-License-Identifier: Apache-2.0
+//
+// TEST INFRASTRUCTURE (the oracle), never the product: the CPU restatement of the reference's
+// solver stage (port_impl.h) instantiated in FP32 (bit-exact with the reference, checked
+// against oracle/_ref/libnphref.so) and in FP64 (the error baseline), with the write-back of
+// phys_solve's results into the view: finalize_body (solver.c:304-349), store_group
+// (solver.c:475-499), the joints' impulses, and the driven joints' sleep reset of
+// post_finalize (solver.c:851-857).
+
+#include "nepheline_b200.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define PORT_API __attribute__((visibility("default")))
+
+#define REAL float
+#define SUF _f32
+#define SQRT sqrtf
+#define ATAN2 atan2f
+#define ABS fabsf
+#include "port_impl.h"
+#undef REAL
+#undef SUF
+#undef SQRT
+#undef ATAN2
+#undef ABS
+
+#define REAL double
+#define SUF _f64
+#define SQRT sqrt
+#define ATAN2 atan2
+#define ABS fabs
+#include "port_impl.h"
+#undef REAL
+#undef SUF
+#undef SQRT
+#undef ATAN2
+#undef ABS
+
+// Checks what the reference asserts or relies on: indices in range, 1..4 points, colour
+// counts that add up, supported joint types and settings.
+static int check_view(const NphGpuWorldParams *wp, const NphGpuWorldView *v)
+{
+    if (wp == NULL || v == NULL || wp->substeps == 0U || wp->solver != NPH_GPU_SOLVER_SOFT_STEP) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    const unsigned total = v->body_count + v->fixed_count;
+    unsigned nc = 0U;
+    unsigned nj = 0U;
+    for (unsigned c = 0U; c < NPH_GPU_COLOR_SLOTS; ++c) {
+        nc += v->contact_color_counts[c];
+        nj += v->joint_color_counts[c];
+    }
+    if (nc != v->contact_count || nj != v->joint_count) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    for (unsigned i = 0U; i < v->contact_count; ++i) {
+        const NphGpuContact *c = &v->contacts[i];
+        if (c->body_a >= total || c->body_b >= total || c->point_count < 1U ||
+            c->point_count > NPH_GPU_MAX_POINTS) {
+            return NPH_GPU_INVALID_ARGUMENT;
+        }
+    }
+    for (unsigned i = 0U; i < v->joint_count; ++i) {
+        const NphGpuJoint *j = &v->joints[i];
+        if (j->body_a >= total || j->body_b >= total) {
+            return NPH_GPU_INVALID_ARGUMENT;
+        }
+        if (j->type != NPH_GPU_JOINT_BALL && j->type != NPH_GPU_JOINT_HINGE) {
+            return NPH_GPU_UNSUPPORTED;
+        }
+    }
+    if (wp->enable_continuous != 0U) {
+        return NPH_GPU_UNSUPPORTED;
+    }
+    return NPH_GPU_OK;
+}
+
+static int joint_is_driven(const NphGpuJoint *j)
+{
+    return j->type == NPH_GPU_JOINT_HINGE && j->u.hinge.enable_motor != 0U &&
+           j->u.hinge.motor_speed != 0.0F && j->u.hinge.max_motor_torque > 0.0F;
+}
+
+// The FP32 solve, in place on the view, as the device library's nph_gpu_phys_solve.
+PORT_API int nph_port32_solve(const NphGpuWorldParams *wp, float dt, NphGpuWorldView *v)
+{
+    const int bad = check_view(wp, v);
+    if (bad != NPH_GPU_OK) {
+        return bad;
+    }
+    Result_f32 r;
+    const int res = run_f32(wp, dt, v, &r);
+    if (res != NPH_GPU_OK) {
+        return res;
+    }
+    // finalize_body (solver.c:304-349). Recomputed from the FP32 prepare: q0 is the record's.
+    for (unsigned i = 0U; i < r.n; ++i) {
+        NphGpuBody *b = &v->bodies[i];
+        const Body_f32 *sb = &r.bodies[i];
+        const Q4_f32 q0 = q4_load_f32(b->rotation);
+        b->linear_velocity[0] = sb->v.x;
+        b->linear_velocity[1] = sb->v.y;
+        b->linear_velocity[2] = sb->v.z;
+        b->angular_velocity[0] = sb->w.x;
+        b->angular_velocity[1] = sb->w.y;
+        b->angular_velocity[2] = sb->w.z;
+        const Q4_f32 q = q_normalize_f32(q_mul_f32(sb->dq, q0));
+        b->rotation[0] = q.x;
+        b->rotation[1] = q.y;
+        b->rotation[2] = q.z;
+        b->rotation[3] = q.w;
+        b->center[0] = b->center[0] + (double)sb->dp.x;
+        b->center[1] = b->center[1] + (double)sb->dp.y;
+        b->center[2] = b->center[2] + (double)sb->dp.z;
+        const V3_f32 rc = rotate_f32(q, v3_load_f32(b->local_center));
+        b->origin[0] = b->center[0] + (double)(-rc.x);
+        b->origin[1] = b->center[1] + (double)(-rc.y);
+        b->origin[2] = b->center[2] + (double)(-rc.z);
+        memset(b->force, 0, sizeof b->force);
+        memset(b->torque, 0, sizeof b->torque);
+        const float speed = max_f32(length_f32(sb->v), b->max_extent * length_f32(sb->w));
+        if ((b->flags & NPH_GPU_BODY_ENABLE_SLEEP) == 0U || speed > b->sleep_threshold) {
+            b->sleep_time = 0.0F;
+        } else {
+            b->sleep_time += dt;
+        }
+    }
+    // store_group (solver.c:475-499).
+    for (unsigned i = 0U; i < v->contact_count; ++i) {
+        NphGpuContact *c = &v->contacts[i];
+        const Manifold_f32 *m = &r.m[i];
+        c->flags = m->impacted ? (c->flags | NPH_GPU_CONTACT_HIT) : (c->flags & ~NPH_GPU_CONTACT_HIT);
+        for (unsigned k = 0U; k < c->point_count; ++k) {
+            const Point_f32 *p = &m->p[k];
+            NphGpuContactPoint *cp = &c->points[k];
+            cp->normal_impulse = p->normal_impulse;
+            cp->max_normal_impulse = p->max_normal_impulse;
+            cp->relative_velocity = p->relative_velocity;
+            const V3_f32 t = add_f32(scale_f32(m->t1, p->tangent_impulse[0]),
+                                     scale_f32(m->t2, p->tangent_impulse[1]));
+            cp->tangent_impulse[0] = t.x;
+            cp->tangent_impulse[1] = t.y;
+            cp->tangent_impulse[2] = t.z;
+        }
+    }
+    for (unsigned i = 0U; i < v->joint_count; ++i) {
+        NphGpuJoint *jr = &v->joints[i];
+        const Joint_f32 *j = &r.j[i];
+        jr->linear_impulse[0] = j->linear_impulse.x;
+        jr->linear_impulse[1] = j->linear_impulse.y;
+        jr->linear_impulse[2] = j->linear_impulse.z;
+        jr->angular_impulse[0] = j->angular_impulse.x;
+        jr->angular_impulse[1] = j->angular_impulse.y;
+        jr->angular_impulse[2] = j->angular_impulse.z;
+        jr->friction_impulse[0] = j->friction_impulse.x;
+        jr->friction_impulse[1] = j->friction_impulse.y;
+        jr->friction_impulse[2] = j->friction_impulse.z;
+        jr->lower_impulse = j->lower_impulse;
+        jr->upper_impulse = j->upper_impulse;
+        jr->swing_impulse = j->swing_impulse;
+        jr->motor_impulse = j->motor_impulse;
+        jr->spring_impulse = j->spring_impulse;
+    }
+    // post_finalize (solver.c:851-857): a driven joint keeps its bodies awake.
+    for (unsigned i = 0U; i < v->joint_count; ++i) {
+        const NphGpuJoint *jr = &v->joints[i];
+        if (joint_is_driven(jr)) {
+            if (jr->body_a < v->body_count) {
+                v->bodies[jr->body_a].sleep_time = 0.0F;
+            }
+            if (jr->body_b < v->body_count) {
+                v->bodies[jr->body_b].sleep_time = 0.0F;
+            }
+        }
+    }
+    free(r.bodies);
+    free(r.m);
+    free(r.j);
+    return NPH_GPU_OK;
+}
+
+// What the FP64 step returns: the same results as the FP32 write-back, in double.
+typedef struct NphPort64Out {
+    double *linear_velocity;       // 3 per body
+    double *angular_velocity;      // 3 per body
+    double *rotation;              // 4 per body
+    double *center;                // 3 per body
+    double *normal_impulse;        // 4 per contact
+    double *max_normal_impulse;    // 4 per contact
+    double *tangent_impulse;       // 12 per contact (world)
+    double *relative_velocity;     // 4 per contact
+    double *joint_linear_impulse;  // 3 per joint
+    double *joint_angular_impulse; // 3 per joint
+} NphPort64Out;
+
+// The FP64 re-run of the same step: the view is read only.
+PORT_API int nph_port64_solve(const NphGpuWorldParams *wp, float dt, const NphGpuWorldView *v,
+                              NphPort64Out *out)
+{
+    const int bad = check_view(wp, v);
+    if (bad != NPH_GPU_OK) {
+        return bad;
+    }
+    Result_f64 r;
+    const int res = run_f64(wp, dt, v, &r);
+    if (res != NPH_GPU_OK) {
+        return res;
+    }
+    for (unsigned i = 0U; i < r.n; ++i) {
+        const NphGpuBody *b = &v->bodies[i];
+        const Body_f64 *sb = &r.bodies[i];
+        const Q4_f64 q = q_normalize_f64(q_mul_f64(sb->dq, q4_load_f64(b->rotation)));
+        const double vv[3] = {sb->v.x, sb->v.y, sb->v.z};
+        const double ww[3] = {sb->w.x, sb->w.y, sb->w.z};
+        const double qq[4] = {q.x, q.y, q.z, q.w};
+        const double cc[3] = {b->center[0] + sb->dp.x, b->center[1] + sb->dp.y,
+                              b->center[2] + sb->dp.z};
+        memcpy(&out->linear_velocity[3 * i], vv, sizeof vv);
+        memcpy(&out->angular_velocity[3 * i], ww, sizeof ww);
+        memcpy(&out->rotation[4 * i], qq, sizeof qq);
+        memcpy(&out->center[3 * i], cc, sizeof cc);
+    }
+    for (unsigned i = 0U; i < v->contact_count; ++i) {
+        const Manifold_f64 *m = &r.m[i];
+        for (unsigned k = 0U; k < 4U; ++k) {
+            const Point_f64 *p = &m->p[k];
+            const int has = k < m->point_count;
+            out->normal_impulse[4 * i + k] = has ? p->normal_impulse : 0.0;
+            out->max_normal_impulse[4 * i + k] = has ? p->max_normal_impulse : 0.0;
+            out->relative_velocity[4 * i + k] = has ? p->relative_velocity : 0.0;
+            const V3_f64 t = add_f64(scale_f64(m->t1, p->tangent_impulse[0]),
+                                     scale_f64(m->t2, p->tangent_impulse[1]));
+            out->tangent_impulse[12 * i + 3 * k + 0] = has ? t.x : 0.0;
+            out->tangent_impulse[12 * i + 3 * k + 1] = has ? t.y : 0.0;
+            out->tangent_impulse[12 * i + 3 * k + 2] = has ? t.z : 0.0;
+        }
+    }
+    for (unsigned i = 0U; i < v->joint_count; ++i) {
+        const Joint_f64 *j = &r.j[i];
+        out->joint_linear_impulse[3 * i + 0] = j->linear_impulse.x;
+        out->joint_linear_impulse[3 * i + 1] = j->linear_impulse.y;
+        out->joint_linear_impulse[3 * i + 2] = j->linear_impulse.z;
+        out->joint_angular_impulse[3 * i + 0] = j->angular_impulse.x;
+        out->joint_angular_impulse[3 * i + 1] = j->angular_impulse.y;
+        out->joint_angular_impulse[3 * i + 2] = j->angular_impulse.z;
+    }
+    free(r.bodies);
+    free(r.m);
+    free(r.j);
+    return NPH_GPU_OK;
+}
+
+// Sequential first-fit colouring of constraints inserted in order into an empty graph
+// (graph_pick_color, island.c:34-56; graph_set_bodies, island.c:58-75), with each
+// constraint's slot in its colour's list: its contact list, or its joint list for a
+// constraint whose bit 2 of `dynamic_bits` is set (island.c:77-88, 106-118).
+PORT_API int nph_port_graph_color(const unsigned *body_a, const unsigned *body_b,
+                                  const unsigned char *dynamic_bits, unsigned count,
+                                  unsigned body_slots, unsigned *out_color, unsigned *out_slot)
+{
+    const size_t words = ((size_t)body_slots + 63U) / 64U;
+    unsigned long long *bits =
+        (unsigned long long *)calloc(words * NPH_GPU_COLORS + 1U, sizeof(unsigned long long));
+    if (bits == NULL) {
+        return NPH_GPU_OUT_OF_MEMORY;
+    }
+    unsigned lens[2][NPH_GPU_COLOR_SLOTS]; // the colours' contact lists and joint lists
+    memset(lens, 0, sizeof lens);
+#define TEST(c, b) ((bits[(size_t)(c) * words + (b) / 64U] >> ((b) % 64U)) & 1ULL)
+#define SET(c, b) (bits[(size_t)(c) * words + (b) / 64U] |= 1ULL << ((b) % 64U))
+    for (unsigned i = 0U; i < count; ++i) {
+        const unsigned a = body_a[i];
+        const unsigned b = body_b[i];
+        const int da = (dynamic_bits[i] & 1U) != 0U;
+        const int db = (dynamic_bits[i] & 2U) != 0U;
+        unsigned color = NPH_GPU_OVERFLOW;
+        if (da && db) {
+            for (unsigned k = 0U; k < NPH_GPU_DYNAMIC_COLORS; ++k) {
+                if (!TEST(k, a) && !TEST(k, b)) {
+                    color = k;
+                    break;
+                }
+            }
+        } else {
+            const unsigned body = da ? a : b;
+            for (unsigned k = 1U; k < NPH_GPU_COLORS; ++k) {
+                if (!TEST(k, body)) {
+                    color = k;
+                    break;
+                }
+            }
+        }
+        if (color != NPH_GPU_OVERFLOW) {
+            if (da) {
+                SET(color, a);
+            }
+            if (db) {
+                SET(color, b);
+            }
+        }
+        out_color[i] = color;
+        out_slot[i] = lens[(dynamic_bits[i] & 4U) != 0U ? 1 : 0][color]++;
+    }
+#undef TEST
+#undef SET
+    free(bits);
+    return NPH_GPU_OK;
+}

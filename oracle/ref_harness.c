@@ -1,0 +1,779 @@
+// SPDX-License-Identifier: Apache-2.0
+//
+// TEST INFRASTRUCTURE (the oracle), never the product: a white-box harness around the
+// reference engine's physics, compiled together with the reference's own sources
+// (oracle/Makefile) into oracle/_ref/libnphref.so. Only the tests, the smoke check and the
+// bench's CPU-baseline leg load it.
+//
+// It builds reference worlds (bodies and shapes through the public API; joints through
+// nph_physics_joint_create; synthetic manifolds injected into the world's contact array
+// and coloured by the reference's own phys_graph_add, island.c:77), runs the reference's
+// stages one by one (phys_update_pairs, phys_collide, phys_solve; world.c:332-346), and
+// converts between the world and the solver-stage view of include/nepheline_b200.h:
+//
+//   export  the solver stage's inputs and outputs as NphGpuWorldView records, in the
+//           reference's solver order (awake list; colours 0..23, then the overflow);
+//   import  a view solved elsewhere back into the world, with what the reference's
+//           finalize pass does beside the solver arithmetic (phys_body_refresh_boxes,
+//           solver.c:351-369; growing the proxies of moved shapes, solver.c:867-878).
+//
+// All arithmetic of the step is the reference's: the harness only copies fields.
+
+#include <nepheline/core/alloc.h>
+#include <nepheline/core/hash.h>
+#include <nepheline/jobs/jobs.h>
+#include <nepheline/physics/body.h>
+#include <nepheline/physics/joint.h>
+#include <nepheline/physics/shape.h>
+#include <nepheline/physics/world.h>
+
+#include "world_internal.h"
+
+#include "nepheline_b200.h"
+
+#include <stdlib.h>
+#include <string.h>
+
+#define REF_API __attribute__((visibility("default")))
+
+enum { REF_CONSTRAINT_JOINT = 0, REF_CONSTRAINT_CONTACT = 1 };
+
+typedef struct RefWorld {
+    NphPhysicsWorld *w;
+    NphJobSystem *js;
+    NphPhysicsBody *bodies; // by creation index
+    u32 body_count;
+    u32 body_cap;
+    u32 *kinds; // insertion order of constraints: kind and record index
+    u32 *records;
+    u32 constraint_count;
+    u32 constraint_cap;
+    u32 *fixed_of_slot; // per body slot: its fixed-body index in the last view, or PHYS_NULL
+    u32 fixed_cap;
+    u32 *fixed_slots; // per fixed-body index: its body slot
+} RefWorld;
+
+static void *grow(void *p, u32 *cap, u32 need, size_t elem)
+{
+    if (need <= *cap) {
+        return p;
+    }
+    u32 c = *cap > 0U ? *cap : 64U;
+    while (c < need) {
+        c *= 2U;
+    }
+    void *q = realloc(p, (size_t)c * elem);
+    if (q == NULL) {
+        abort();
+    }
+    *cap = c;
+    return q;
+}
+
+REF_API RefWorld *nphref_world_create(const NphGpuWorldParams *p, u32 enable_sleep, u32 workers)
+{
+    NphPhysicsWorldDesc d = nph_physics_world_desc_default();
+    d.alloc = nph_allocator_system();
+    d.gravity = nph_vec3(p->gravity[0], p->gravity[1], p->gravity[2]);
+    d.solver = NPH_PHYSICS_SOLVER_SOFT_STEP;
+    d.substeps = p->substeps;
+    d.contact_hertz = p->contact_hertz;
+    d.contact_damping_ratio = p->contact_damping_ratio;
+    d.contact_push_max_velocity = p->contact_push_max_velocity;
+    d.restitution_threshold = p->restitution_threshold;
+    d.max_linear_speed = p->max_linear_speed;
+    d.joint_hertz = p->joint_hertz;
+    d.joint_damping_ratio = p->joint_damping_ratio;
+    d.enable_continuous = p->enable_continuous != 0U ? 1 : 0;
+    d.enable_sleep = enable_sleep != 0U ? 1 : 0;
+    RefWorld *r = (RefWorld *)calloc(1, sizeof *r);
+    if (r == NULL || nph_physics_world_create(&d, &r->w) != NPH_RESULT_OK) {
+        free(r);
+        return NULL;
+    }
+    if (workers != 0U) {
+        NphJobSystemDesc jd;
+        memset(&jd, 0, sizeof jd);
+        jd.alloc = nph_allocator_system();
+        jd.worker_count = workers == PHYS_NULL ? 0U : workers; // 0: logical cores - 1
+        jd.pinning = NPH_JOB_PIN_NEVER;
+        if (nph_job_system_create(&jd, &r->js) != NPH_RESULT_OK) {
+            r->js = NULL;
+        }
+    }
+    return r;
+}
+
+REF_API void nphref_world_destroy(RefWorld *r)
+{
+    if (r == NULL) {
+        return;
+    }
+    nph_physics_world_destroy(r->w);
+    if (r->js != NULL) {
+        nph_job_system_destroy(r->js);
+    }
+    free(r->bodies);
+    free(r->kinds);
+    free(r->records);
+    free(r->fixed_of_slot);
+    free(r->fixed_slots);
+    free(r);
+}
+
+REF_API u32 nphref_worker_count(const RefWorld *r)
+{
+    return r->js != NULL ? nph_job_system_worker_count(r->js) : 0U;
+}
+
+// The white-box knob of the reference's determinism tests (world_internal.h:653).
+REF_API void nphref_force_participants(RefWorld *r, u32 participants)
+{
+    r->w->forced_participants = participants;
+}
+
+static u32 push_body(RefWorld *r, NphPhysicsBody b)
+{
+    r->bodies = (NphPhysicsBody *)grow(r->bodies, &r->body_cap, r->body_count + 1U, sizeof *r->bodies);
+    r->bodies[r->body_count] = b;
+    return r->body_count++;
+}
+
+static void push_constraint(RefWorld *r, u32 kind, u32 record)
+{
+    u32 cap = r->constraint_cap;
+    r->kinds = (u32 *)grow(r->kinds, &cap, r->constraint_count + 1U, sizeof(u32));
+    cap = r->constraint_cap;
+    r->records = (u32 *)grow(r->records, &cap, r->constraint_count + 1U, sizeof(u32));
+    r->constraint_cap = cap;
+    r->kinds[r->constraint_count] = kind;
+    r->records[r->constraint_count] = record;
+    r->constraint_count += 1U;
+}
+
+// shape: 0 none, 1 box (dims = half extents), 2 sphere (dims[0] = radius), 3 capsule
+// (dims[0] = half height, dims[1] = radius). flags: bit 0 gyroscopic, bit 1 sleep enabled,
+// bit 2 bullet. Returns the body's creation index, or PHYS_NULL.
+REF_API u32 nphref_add_body(RefWorld *r, u32 type, const f64 position[3], const f32 rotation[4],
+                            const f32 velocity[3], const f32 angular_velocity[3], u32 shape,
+                            const f32 dims[3], f32 density, f32 friction, f32 restitution,
+                            u32 flags)
+{
+    NphPhysicsBodyDesc bd = nph_physics_body_desc_default();
+    bd.type = (NphPhysicsBodyType)type;
+    bd.position = nph_dvec3(position[0], position[1], position[2]);
+    bd.rotation = nph_quat(rotation[0], rotation[1], rotation[2], rotation[3]);
+    bd.linear_velocity = nph_vec3(velocity[0], velocity[1], velocity[2]);
+    bd.angular_velocity = nph_vec3(angular_velocity[0], angular_velocity[1], angular_velocity[2]);
+    bd.gyroscopic = (flags & 1U) != 0U ? 1 : 0;
+    bd.enable_sleep = (flags & 2U) != 0U ? 1 : 0;
+    bd.bullet = (flags & 4U) != 0U ? 1 : 0;
+    NphPhysicsBody b;
+    if (nph_physics_body_create(r->w, &bd, &b) != NPH_RESULT_OK) {
+        return PHYS_NULL;
+    }
+    if (shape != 0U) {
+        NphPhysicsGeometry g;
+        if (shape == 1U) {
+            g = nph_physics_geometry_box(nph_vec3(dims[0], dims[1], dims[2]));
+        } else if (shape == 2U) {
+            g = nph_physics_geometry_sphere(dims[0]);
+        } else {
+            g = nph_physics_geometry_capsule(dims[0], dims[1]);
+        }
+        NphPhysicsShapeDesc sd = nph_physics_shape_desc_default(g);
+        sd.density = density;
+        sd.friction = friction;
+        sd.restitution = restitution;
+        NphPhysicsShape s;
+        if (nph_physics_shape_create(r->w, b, &sd, &s) != NPH_RESULT_OK) {
+            return PHYS_NULL;
+        }
+    }
+    return push_body(r, b);
+}
+
+// Sets a shapeless body's mass, centre of mass (body frame) and inertia (column-major).
+REF_API void nphref_set_mass(RefWorld *r, u32 body, f32 mass, const f32 center[3],
+                             const f32 inertia[9])
+{
+    NphPhysicsMassData m;
+    memset(&m, 0, sizeof m);
+    m.mass = mass;
+    m.center = nph_vec3(center[0], center[1], center[2]);
+    memcpy(&m.inertia, inertia, sizeof m.inertia);
+    nph_physics_body_set_mass_data(r->w, r->bodies[body], &m);
+}
+
+// A joint between two bodies given by creation index; the record's body fields are ignored.
+REF_API u32 nphref_add_joint(RefWorld *r, const NphGpuJoint *j, u32 body_a, u32 body_b)
+{
+    NphPhysicsJointDesc d = nph_physics_joint_desc_default((NphPhysicsJointType)j->type,
+                                                           r->bodies[body_a], r->bodies[body_b]);
+    d.frame_a.position = nph_vec3(j->frame_a_position[0], j->frame_a_position[1],
+                                  j->frame_a_position[2]);
+    d.frame_a.rotation = nph_quat(j->frame_a_rotation[0], j->frame_a_rotation[1],
+                                  j->frame_a_rotation[2], j->frame_a_rotation[3]);
+    d.frame_b.position = nph_vec3(j->frame_b_position[0], j->frame_b_position[1],
+                                  j->frame_b_position[2]);
+    d.frame_b.rotation = nph_quat(j->frame_b_rotation[0], j->frame_b_rotation[1],
+                                  j->frame_b_rotation[2], j->frame_b_rotation[3]);
+    if (j->type == NPH_GPU_JOINT_BALL) {
+        d.ball.enable_swing_limit = (b32)j->u.ball.enable_swing_limit;
+        d.ball.swing_y = j->u.ball.swing_y;
+        d.ball.swing_z = j->u.ball.swing_z;
+        d.ball.enable_twist_limit = (b32)j->u.ball.enable_twist_limit;
+        d.ball.twist_lower = j->u.ball.twist_lower;
+        d.ball.twist_upper = j->u.ball.twist_upper;
+        d.ball.friction_torque = j->u.ball.friction_torque;
+    } else if (j->type == NPH_GPU_JOINT_HINGE) {
+        d.hinge.enable_limit = (b32)j->u.hinge.enable_limit;
+        d.hinge.lower = j->u.hinge.lower;
+        d.hinge.upper = j->u.hinge.upper;
+        d.hinge.enable_motor = (b32)j->u.hinge.enable_motor;
+        d.hinge.motor_speed = j->u.hinge.motor_speed;
+        d.hinge.max_motor_torque = j->u.hinge.max_motor_torque;
+        d.hinge.enable_spring = (b32)j->u.hinge.enable_spring;
+        d.hinge.spring_hertz = j->u.hinge.spring_hertz;
+        d.hinge.spring_damping_ratio = j->u.hinge.spring_damping_ratio;
+        d.hinge.spring_target = j->u.hinge.spring_target;
+    }
+    NphPhysicsJoint out;
+    if (nph_physics_joint_create(r->w, &d, &out) != NPH_RESULT_OK) {
+        return PHYS_NULL;
+    }
+    const u32 slot = phys_handle_slot(out.value);
+    push_constraint(r, REF_CONSTRAINT_JOINT, slot);
+    return slot;
+}
+
+// A touching manifold between two bodies (creation indices in the record's body fields),
+// placed in the world's contact array and added to the constraint graph by the reference's
+// phys_graph_add (island.c:77). For solver-only scenes: the bodies have no shapes, so no
+// narrow phase ever replaces the manifold.
+REF_API u32 nphref_inject_contact(RefWorld *r, const NphGpuContact *in)
+{
+    NphPhysicsWorld *w = r->w;
+    PhysContact *c = NPH_ARRAY_PUSH_SLOT(&w->contacts);
+    if (c == NULL) {
+        return PHYS_NULL;
+    }
+    const u32 index = w->contacts.len - 1U;
+    memset(c, 0, sizeof *c);
+    c->shape_a = 0U;
+    c->shape_b = 0U;
+    c->body_a = phys_handle_slot(r->bodies[in->body_a].value);
+    c->body_b = phys_handle_slot(r->bodies[in->body_b].value);
+    c->flags = PHYS_CONTACT_TOUCHING | (in->flags & NPH_GPU_CONTACT_HIT);
+    c->parent = PHYS_NULL;
+    c->child = PHYS_NULL;
+    c->prev[0] = c->prev[1] = PHYS_NULL;
+    c->next[0] = c->next[1] = PHYS_NULL;
+    c->color = PHYS_NULL;
+    c->color_slot = PHYS_NULL;
+    c->island = PHYS_NULL;
+    c->island_prev = PHYS_NULL;
+    c->island_next = PHYS_NULL;
+    c->awake_slot = PHYS_NULL;
+    c->friction = in->friction;
+    c->restitution = in->restitution;
+    c->normal = nph_vec3(in->normal[0], in->normal[1], in->normal[2]);
+    c->point_count = in->point_count;
+    for (u32 k = 0U; k < in->point_count; ++k) {
+        const NphGpuContactPoint *p = &in->points[k];
+        PhysContactPoint *q = &c->points[k];
+        q->anchor_a = nph_vec3(p->anchor_a[0], p->anchor_a[1], p->anchor_a[2]);
+        q->anchor_b = nph_vec3(p->anchor_b[0], p->anchor_b[1], p->anchor_b[2]);
+        q->separation = p->separation;
+        q->id = p->id;
+        q->normal_impulse = p->normal_impulse;
+        q->max_normal_impulse = p->max_normal_impulse;
+        q->tangent_impulse = nph_vec3(p->tangent_impulse[0], p->tangent_impulse[1],
+                                      p->tangent_impulse[2]);
+        q->relative_velocity = p->relative_velocity;
+    }
+    if (phys_graph_add(w, index) != NPH_RESULT_OK) {
+        return PHYS_NULL;
+    }
+    push_constraint(r, REF_CONSTRAINT_CONTACT, index);
+    return index;
+}
+
+// The world step's stages before and after the solver (world.c:332-339, 355-366).
+REF_API int nphref_collide(RefWorld *r)
+{
+    NphResult res = phys_update_pairs(r->w, r->js);
+    if (res == NPH_RESULT_OK) {
+        res = phys_collide(r->w, r->js);
+    }
+    return (int)res;
+}
+
+REF_API int nphref_solve(RefWorld *r, f32 dt)
+{
+    r->w->step_dt = dt;
+    return (int)phys_solve(r->w, dt, r->js);
+}
+
+REF_API int nphref_finish(RefWorld *r)
+{
+    NphResult res = phys_island_merge_pending(r->w);
+    if (res == NPH_RESULT_OK && r->w->desc.enable_sleep != 0) {
+        res = phys_island_sleep_and_split(r->w);
+    }
+    return (int)res;
+}
+
+REF_API int nphref_step(RefWorld *r, f32 dt)
+{
+    return (int)nph_physics_world_step(r->w, dt, r->js);
+}
+
+REF_API u64 nphref_hash(const RefWorld *r)
+{
+    return nph_physics_world_hash(r->w);
+}
+
+REF_API double nphref_last_solve_ms(const RefWorld *r)
+{
+    return r->w->stats.solve_ms;
+}
+
+REF_API u32 nphref_body_count(const RefWorld *r)
+{
+    return r->body_count;
+}
+
+// A body's state by creation index: centre, origin, rotation, velocities, sleep time, flags.
+REF_API void nphref_body_state(const RefWorld *r, u32 body, f64 center[3], f64 origin[3],
+                               f32 rotation[4], f32 v[3], f32 w[3], f32 *sleep_time, u32 *flags)
+{
+    const PhysBody *b = phys_body(r->w, r->bodies[body]);
+    center[0] = b->center.x;
+    center[1] = b->center.y;
+    center[2] = b->center.z;
+    origin[0] = b->origin.x;
+    origin[1] = b->origin.y;
+    origin[2] = b->origin.z;
+    memcpy(rotation, &b->rotation, sizeof(f32) * 4U);
+    memcpy(v, &b->linear_velocity, sizeof(f32) * 3U);
+    memcpy(w, &b->angular_velocity, sizeof(f32) * 3U);
+    *sleep_time = b->sleep_time;
+    *flags = b->flags;
+}
+
+// ---------------------------------------------------------------------------
+// The colouring, in insertion order
+// ---------------------------------------------------------------------------
+
+REF_API u32 nphref_constraint_count(const RefWorld *r)
+{
+    return r->constraint_count;
+}
+
+// Per constraint in insertion order: its bodies' slots, which are dynamic (bit 0 A, bit 1 B),
+// and the colour and slot the reference gave it (PHYS_GRAPH_OVERFLOW = 24).
+REF_API void nphref_constraints(const RefWorld *r, u32 *body_a, u32 *body_b, u8 *dynamic_bits,
+                                u32 *color, u32 *slot)
+{
+    const NphPhysicsWorld *w = r->w;
+    for (u32 i = 0U; i < r->constraint_count; ++i) {
+        u32 a;
+        u32 b;
+        if (r->kinds[i] == REF_CONSTRAINT_JOINT) {
+            const PhysJoint *j = &w->joints.data[r->records[i]];
+            a = j->body_a;
+            b = j->body_b;
+            color[i] = j->color;
+            slot[i] = j->color_slot;
+        } else {
+            const PhysContact *c = &w->contacts.data[r->records[i]];
+            a = c->body_a;
+            b = c->body_b;
+            color[i] = c->color;
+            slot[i] = c->color_slot;
+        }
+        body_a[i] = a;
+        body_b[i] = b;
+        dynamic_bits[i] = (u8)((w->bodies.data[a].type == NPH_PHYSICS_BODY_DYNAMIC ? 1U : 0U) |
+                               (w->bodies.data[b].type == NPH_PHYSICS_BODY_DYNAMIC ? 2U : 0U));
+    }
+}
+
+REF_API u32 nphref_body_slots(const RefWorld *r)
+{
+    return r->w->bodies.len;
+}
+
+// ---------------------------------------------------------------------------
+// World <-> view
+// ---------------------------------------------------------------------------
+
+static const NphArrayU32 *contact_list(const NphPhysicsWorld *w, u32 c)
+{
+    return c == PHYS_GRAPH_OVERFLOW ? &w->overflow : &w->colors[c].contacts;
+}
+
+static const NphArrayU32 *joint_list(const NphPhysicsWorld *w, u32 c)
+{
+    return c == PHYS_GRAPH_OVERFLOW ? &w->overflow_joints : &w->colors[c].joints;
+}
+
+static void body_record(const PhysBody *b, NphGpuBody *o)
+{
+    memset(o, 0, sizeof *o);
+    o->center[0] = b->center.x;
+    o->center[1] = b->center.y;
+    o->center[2] = b->center.z;
+    o->origin[0] = b->origin.x;
+    o->origin[1] = b->origin.y;
+    o->origin[2] = b->origin.z;
+    memcpy(o->rotation, &b->rotation, sizeof o->rotation);
+    memcpy(o->local_center, &b->local_center, sizeof o->local_center);
+    memcpy(o->linear_velocity, &b->linear_velocity, sizeof o->linear_velocity);
+    memcpy(o->angular_velocity, &b->angular_velocity, sizeof o->angular_velocity);
+    memcpy(o->force, &b->force, sizeof o->force);
+    memcpy(o->torque, &b->torque, sizeof o->torque);
+    memcpy(o->inertia, &b->inertia, sizeof o->inertia);
+    memcpy(o->inv_inertia, &b->inv_inertia, sizeof o->inv_inertia);
+    o->inv_mass = b->inv_mass;
+    o->linear_damping = b->linear_damping;
+    o->angular_damping = b->angular_damping;
+    o->gravity_scale = b->gravity_scale;
+    o->sleep_threshold = b->sleep_threshold;
+    o->sleep_time = b->sleep_time;
+    o->max_extent = b->max_extent;
+    o->type = b->type;
+    o->flags = b->flags;
+    o->locks = b->locks;
+}
+
+// The view index of body slot `slot`: its awake slot, or a fixed body's index after them.
+static u32 view_index(RefWorld *r, u32 slot, u32 *fixed_count)
+{
+    const PhysBody *b = &r->w->bodies.data[slot];
+    if (b->awake_slot != PHYS_NULL) {
+        return b->awake_slot;
+    }
+    if (r->fixed_of_slot[slot] == PHYS_NULL) {
+        r->fixed_slots[*fixed_count] = slot;
+        r->fixed_of_slot[slot] = (*fixed_count)++;
+    }
+    return r->w->awake_bodies.len + r->fixed_of_slot[slot];
+}
+
+static void map_fixed(RefWorld *r, u32 *fixed_count)
+{
+    const NphPhysicsWorld *w = r->w;
+    u32 cap = r->fixed_cap;
+    r->fixed_of_slot = (u32 *)grow(r->fixed_of_slot, &cap, w->bodies.len + 1U, sizeof(u32));
+    cap = r->fixed_cap;
+    r->fixed_slots = (u32 *)grow(r->fixed_slots, &cap, w->bodies.len + 1U, sizeof(u32));
+    r->fixed_cap = cap;
+    for (u32 i = 0U; i < w->bodies.len; ++i) {
+        r->fixed_of_slot[i] = PHYS_NULL;
+    }
+    *fixed_count = 0U;
+    for (u32 c = 0U; c <= PHYS_GRAPH_COLORS; ++c) {
+        const NphArrayU32 *list = contact_list(w, c);
+        for (u32 i = 0U; i < list->len; ++i) {
+            const PhysContact *ct = &w->contacts.data[list->data[i]];
+            (void)view_index(r, ct->body_a, fixed_count);
+            (void)view_index(r, ct->body_b, fixed_count);
+        }
+        const NphArrayU32 *jl = joint_list(w, c);
+        for (u32 i = 0U; i < jl->len; ++i) {
+            const PhysJoint *j = &w->joints.data[jl->data[i]];
+            (void)view_index(r, j->body_a, fixed_count);
+            (void)view_index(r, j->body_b, fixed_count);
+        }
+    }
+}
+
+// The sizes a view of the world needs.
+REF_API void nphref_view_sizes(RefWorld *r, u32 *bodies, u32 *fixed, u32 *contacts, u32 *joints)
+{
+    const NphPhysicsWorld *w = r->w;
+    map_fixed(r, fixed);
+    *bodies = w->awake_bodies.len;
+    u32 nc = 0U;
+    u32 nj = 0U;
+    for (u32 c = 0U; c <= PHYS_GRAPH_COLORS; ++c) {
+        nc += contact_list(w, c)->len;
+        nj += joint_list(w, c)->len;
+    }
+    *contacts = nc;
+    *joints = nj;
+}
+
+static void contact_record(RefWorld *r, const PhysContact *c, NphGpuContact *o, u32 *fixed_count)
+{
+    memset(o, 0, sizeof *o);
+    o->body_a = view_index(r, c->body_a, fixed_count);
+    o->body_b = view_index(r, c->body_b, fixed_count);
+    o->flags = c->flags & PHYS_CONTACT_HIT;
+    o->point_count = c->point_count;
+    memcpy(o->normal, &c->normal, sizeof o->normal);
+    o->friction = c->friction;
+    o->restitution = c->restitution;
+    for (u32 k = 0U; k < c->point_count; ++k) {
+        const PhysContactPoint *p = &c->points[k];
+        NphGpuContactPoint *q = &o->points[k];
+        memcpy(q->anchor_a, &p->anchor_a, sizeof q->anchor_a);
+        memcpy(q->anchor_b, &p->anchor_b, sizeof q->anchor_b);
+        q->separation = p->separation;
+        q->normal_impulse = p->normal_impulse;
+        q->max_normal_impulse = p->max_normal_impulse;
+        memcpy(q->tangent_impulse, &p->tangent_impulse, sizeof q->tangent_impulse);
+        q->relative_velocity = p->relative_velocity;
+        q->id = p->id;
+    }
+}
+
+static void joint_record(RefWorld *r, const PhysJoint *j, NphGpuJoint *o, u32 *fixed_count)
+{
+    memset(o, 0, sizeof *o);
+    o->type = j->type;
+    o->body_a = view_index(r, j->body_a, fixed_count);
+    o->body_b = view_index(r, j->body_b, fixed_count);
+    memcpy(o->frame_a_position, &j->frame_a.position, sizeof o->frame_a_position);
+    memcpy(o->frame_a_rotation, &j->frame_a.rotation, sizeof o->frame_a_rotation);
+    memcpy(o->frame_b_position, &j->frame_b.position, sizeof o->frame_b_position);
+    memcpy(o->frame_b_rotation, &j->frame_b.rotation, sizeof o->frame_b_rotation);
+    if (j->type == NPH_PHYSICS_JOINT_BALL) {
+        o->u.ball.enable_swing_limit = (u32)j->ball.enable_swing_limit;
+        o->u.ball.swing_y = j->ball.swing_y;
+        o->u.ball.swing_z = j->ball.swing_z;
+        o->u.ball.enable_twist_limit = (u32)j->ball.enable_twist_limit;
+        o->u.ball.twist_lower = j->ball.twist_lower;
+        o->u.ball.twist_upper = j->ball.twist_upper;
+        o->u.ball.friction_torque = j->ball.friction_torque;
+    } else if (j->type == NPH_PHYSICS_JOINT_HINGE) {
+        o->u.hinge.enable_limit = (u32)j->hinge.enable_limit;
+        o->u.hinge.lower = j->hinge.lower;
+        o->u.hinge.upper = j->hinge.upper;
+        o->u.hinge.enable_motor = (u32)j->hinge.enable_motor;
+        o->u.hinge.motor_speed = j->hinge.motor_speed;
+        o->u.hinge.max_motor_torque = j->hinge.max_motor_torque;
+        o->u.hinge.enable_spring = (u32)j->hinge.enable_spring;
+        o->u.hinge.spring_hertz = j->hinge.spring_hertz;
+        o->u.hinge.spring_damping_ratio = j->hinge.spring_damping_ratio;
+        o->u.hinge.spring_target = j->hinge.spring_target;
+    }
+    memcpy(o->linear_impulse, &j->linear_impulse, sizeof o->linear_impulse);
+    memcpy(o->angular_impulse, &j->angular_impulse, sizeof o->angular_impulse);
+    memcpy(o->friction_impulse, &j->friction_impulse, sizeof o->friction_impulse);
+    o->lower_impulse = j->lower_impulse;
+    o->upper_impulse = j->upper_impulse;
+    o->swing_impulse = j->swing_impulse;
+    o->motor_impulse = j->motor_impulse;
+    o->spring_impulse = j->spring_impulse;
+}
+
+// Fills a view whose arrays the caller sized by nphref_view_sizes.
+REF_API int nphref_export(RefWorld *r, NphGpuWorldView *v)
+{
+    const NphPhysicsWorld *w = r->w;
+    u32 fixed = 0U;
+    map_fixed(r, &fixed);
+    v->body_count = w->awake_bodies.len;
+    for (u32 i = 0U; i < w->awake_bodies.len; ++i) {
+        body_record(&w->bodies.data[w->awake_bodies.data[i]], &v->bodies[i]);
+    }
+    v->fixed_count = fixed;
+    for (u32 i = 0U; i < fixed; ++i) {
+        body_record(&w->bodies.data[r->fixed_slots[i]], (NphGpuBody *)&v->fixed_bodies[i]);
+    }
+    u32 nc = 0U;
+    u32 nj = 0U;
+    u32 again = fixed;
+    for (u32 c = 0U; c <= PHYS_GRAPH_COLORS; ++c) {
+        const NphArrayU32 *list = contact_list(w, c);
+        v->contact_color_counts[c] = list->len;
+        for (u32 i = 0U; i < list->len; ++i) {
+            contact_record(r, &w->contacts.data[list->data[i]], &v->contacts[nc++], &again);
+        }
+        const NphArrayU32 *jl = joint_list(w, c);
+        v->joint_color_counts[c] = jl->len;
+        for (u32 i = 0U; i < jl->len; ++i) {
+            joint_record(r, &w->joints.data[jl->data[i]], &v->joints[nj++], &again);
+        }
+    }
+    v->contact_count = nc;
+    v->joint_count = nj;
+    return again == fixed ? 0 : 1;
+}
+
+// Writes a solved view back into the world: what phys_solve's stages write
+// (finalize_body, store_group, the joints' impulses), then the finalize pass's box refresh
+// and the growth of moved proxies (solver.c:351-369, 867-878). The view must have been
+// exported from this world since its last change.
+REF_API int nphref_import(RefWorld *r, const NphGpuWorldView *v, f32 dt)
+{
+    NphPhysicsWorld *w = r->w;
+    if (v->body_count != w->awake_bodies.len) {
+        return (int)NPH_RESULT_INVALID_STATE;
+    }
+    for (u32 i = 0U; i < v->body_count; ++i) {
+        PhysBody *b = &w->bodies.data[w->awake_bodies.data[i]];
+        const NphGpuBody *o = &v->bodies[i];
+        b->center = nph_dvec3(o->center[0], o->center[1], o->center[2]);
+        b->origin = nph_dvec3(o->origin[0], o->origin[1], o->origin[2]);
+        memcpy(&b->rotation, o->rotation, sizeof o->rotation);
+        memcpy(&b->linear_velocity, o->linear_velocity, sizeof o->linear_velocity);
+        memcpy(&b->angular_velocity, o->angular_velocity, sizeof o->angular_velocity);
+        b->force = nph_vec3_zero();
+        b->torque = nph_vec3_zero();
+        b->sleep_time = o->sleep_time;
+        phys_body_refresh_boxes(w, b);
+    }
+    u32 nc = 0U;
+    u32 nj = 0U;
+    for (u32 c = 0U; c <= PHYS_GRAPH_COLORS; ++c) {
+        const NphArrayU32 *list = contact_list(w, c);
+        for (u32 i = 0U; i < list->len; ++i) {
+            PhysContact *ct = &w->contacts.data[list->data[i]];
+            const NphGpuContact *o = &v->contacts[nc++];
+            ct->flags = (ct->flags & ~(u32)PHYS_CONTACT_HIT) | (o->flags & PHYS_CONTACT_HIT);
+            for (u32 k = 0U; k < ct->point_count; ++k) {
+                PhysContactPoint *p = &ct->points[k];
+                p->normal_impulse = o->points[k].normal_impulse;
+                p->max_normal_impulse = o->points[k].max_normal_impulse;
+                p->relative_velocity = o->points[k].relative_velocity;
+                memcpy(&p->tangent_impulse, o->points[k].tangent_impulse,
+                       sizeof o->points[k].tangent_impulse);
+            }
+        }
+        const NphArrayU32 *jl = joint_list(w, c);
+        for (u32 i = 0U; i < jl->len; ++i) {
+            PhysJoint *j = &w->joints.data[jl->data[i]];
+            const NphGpuJoint *o = &v->joints[nj++];
+            memcpy(&j->linear_impulse, o->linear_impulse, sizeof o->linear_impulse);
+            memcpy(&j->angular_impulse, o->angular_impulse, sizeof o->angular_impulse);
+            memcpy(&j->friction_impulse, o->friction_impulse, sizeof o->friction_impulse);
+            j->lower_impulse = o->lower_impulse;
+            j->upper_impulse = o->upper_impulse;
+            j->swing_impulse = o->swing_impulse;
+            j->motor_impulse = o->motor_impulse;
+            j->spring_impulse = o->spring_impulse;
+        }
+    }
+    w->last_substep = dt / (f32)w->desc.substeps;
+    for (u32 i = 0U; i < w->awake_bodies.len; ++i) {
+        PhysBody *b = &w->bodies.data[w->awake_bodies.data[i]];
+        if ((b->flags & PHYS_BODY_ENLARGED) == 0U) {
+            continue;
+        }
+        b->flags &= ~(u32)PHYS_BODY_ENLARGED;
+        for (u32 s = b->shape_head; s != PHYS_NULL; s = w->shapes.data[s].next) {
+            PhysShape *shape = &w->shapes.data[s];
+            if ((shape->flags & PHYS_SHAPE_ENLARGED) != 0U) {
+                shape->flags &= ~(u32)PHYS_SHAPE_ENLARGED;
+                nph_aabb_tree_enlarge_proxy(&w->trees[shape->tree], shape->proxy,
+                                            shape->fat_aabb);
+                const NphResult res = phys_move_buffer_push(w, s);
+                if (res != NPH_RESULT_OK) {
+                    return (int)res;
+                }
+            }
+        }
+    }
+    return 0;
+}
+
+// The world's statistics the scenes report.
+REF_API void nphref_stats(const RefWorld *r, u32 *touching, u32 *points, u32 *colors_used,
+                          u32 *overflow, u32 *awake)
+{
+    const NphPhysicsStats s = nph_physics_world_stats(r->w);
+    *touching = s.touching_contacts;
+    *points = s.manifold_points;
+    *colors_used = s.colors_used;
+    *overflow = s.overflow_constraints;
+    *awake = s.awake_bodies;
+}
+
+// ---------------------------------------------------------------------------
+// Bulk scene building (solver-only scenes of shapeless bodies)
+// ---------------------------------------------------------------------------
+
+// Dynamic (or the record's type) shapeless bodies at the records' centres, with the records'
+// rotation, velocities, damping, gravity scale, sleep settings and mass properties (`mass`
+// per body; the record's inertia, column-major, and local centre). Returns the first
+// creation index, or PHYS_NULL.
+REF_API u32 nphref_add_shapeless_bodies(RefWorld *r, u32 n, const NphGpuBody *recs,
+                                        const f32 *mass)
+{
+    const u32 first = r->body_count;
+    for (u32 i = 0U; i < n; ++i) {
+        const NphGpuBody *o = &recs[i];
+        NphPhysicsBodyDesc bd = nph_physics_body_desc_default();
+        bd.type = (NphPhysicsBodyType)o->type;
+        const NphQuat q = nph_quat(o->rotation[0], o->rotation[1], o->rotation[2], o->rotation[3]);
+        const NphVec3 lc = nph_vec3(o->local_center[0], o->local_center[1], o->local_center[2]);
+        bd.position = nph_dvec3_add_vec3(nph_dvec3(o->center[0], o->center[1], o->center[2]),
+                                         nph_vec3_neg(nph_quat_rotate(q, lc)));
+        bd.rotation = q;
+        bd.linear_velocity = nph_vec3(o->linear_velocity[0], o->linear_velocity[1],
+                                      o->linear_velocity[2]);
+        bd.angular_velocity = nph_vec3(o->angular_velocity[0], o->angular_velocity[1],
+                                       o->angular_velocity[2]);
+        bd.linear_damping = o->linear_damping;
+        bd.angular_damping = o->angular_damping;
+        bd.gravity_scale = o->gravity_scale;
+        bd.sleep_threshold = o->sleep_threshold;
+        bd.locks = o->locks;
+        bd.enable_sleep = (o->flags & NPH_GPU_BODY_ENABLE_SLEEP) != 0U ? 1 : 0;
+        bd.gyroscopic = (o->flags & NPH_GPU_BODY_GYROSCOPIC) != 0U ? 1 : 0;
+        bd.bullet = (o->flags & NPH_GPU_BODY_BULLET) != 0U ? 1 : 0;
+        NphPhysicsBody b;
+        if (nph_physics_body_create(r->w, &bd, &b) != NPH_RESULT_OK) {
+            return PHYS_NULL;
+        }
+        const u32 index = push_body(r, b);
+        if (o->type == NPH_GPU_BODY_DYNAMIC) {
+            nphref_set_mass(r, index, mass[i], o->local_center, o->inertia);
+        }
+        if (o->force[0] != 0.0F || o->force[1] != 0.0F || o->force[2] != 0.0F) {
+            nph_physics_body_apply_force_at_center(
+                r->w, b, nph_vec3(o->force[0], o->force[1], o->force[2]));
+        }
+        if (o->torque[0] != 0.0F || o->torque[1] != 0.0F || o->torque[2] != 0.0F) {
+            nph_physics_body_apply_torque(r->w, b,
+                                          nph_vec3(o->torque[0], o->torque[1], o->torque[2]));
+        }
+    }
+    return first;
+}
+
+// Joints in insertion order; the records' body fields are creation indices.
+REF_API u32 nphref_add_joints(RefWorld *r, u32 n, const NphGpuJoint *recs)
+{
+    for (u32 i = 0U; i < n; ++i) {
+        if (nphref_add_joint(r, &recs[i], recs[i].body_a, recs[i].body_b) == PHYS_NULL) {
+            return PHYS_NULL;
+        }
+    }
+    return n;
+}
+
+// Manifolds in insertion order; the records' body fields are creation indices.
+REF_API u32 nphref_inject_contacts(RefWorld *r, u32 n, const NphGpuContact *recs)
+{
+    if (NPH_ARRAY_RESERVE(&r->w->contacts, r->w->contacts.len + n) != NPH_RESULT_OK) {
+        return PHYS_NULL;
+    }
+    for (u32 i = 0U; i < n; ++i) {
+        if (nphref_inject_contact(r, &recs[i]) == PHYS_NULL) {
+            return PHYS_NULL;
+        }
+    }
+    return n;
+}
+
+// Sets every dynamic awake body's velocities (by creation index) between steps.
+REF_API void nphref_set_velocity(RefWorld *r, u32 body, const f32 v[3], const f32 w[3])
+{
+    nph_physics_body_set_linear_velocity(r->w, r->bodies[body], nph_vec3(v[0], v[1], v[2]));
+    nph_physics_body_set_angular_velocity(r->w, r->bodies[body], nph_vec3(w[0], w[1], w[2]));
+}

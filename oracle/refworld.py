@@ -1,0 +1,317 @@
+"""TEST INFRASTRUCTURE (the oracle), never the product.
+
+Python bindings for the two checkers built by oracle/Makefile:
+
+  RefWorld  the reference engine's own physics (oracle/_ref/libnphref.so, compiled from the
+            reference's sources) driven white-box: scene building, its stages one by one,
+            and conversion of its world to and from the solver-stage view.
+  port32 / port64 / port_graph_color
+            this project's CPU restatement of the solver stage (oracle/_build/
+            liboracle_port.so): FP32 (bit-exact with the reference) and FP64 (the error
+            baseline), and the sequential first-fit colouring.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import this module.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+from nepheline_b200 import abi
+
+HERE = Path(__file__).resolve().parent
+REF_LIB = HERE / "_ref" / "libnphref.so"
+PORT_LIB = HERE / "_build" / "liboracle_port.so"
+
+_u32 = ctypes.c_uint32
+_f32 = ctypes.c_float
+_vp = ctypes.c_void_p
+_ref = None
+_port = None
+
+
+def ref_available() -> bool:
+    return REF_LIB.exists()
+
+
+def _ref_lib():
+    global _ref
+    if _ref is None:
+        lib = ctypes.CDLL(str(REF_LIB))
+        sig = {
+            "nphref_world_create": (_vp, [ctypes.POINTER(abi.WorldParams), _u32, _u32]),
+            "nphref_world_destroy": (None, [_vp]),
+            "nphref_worker_count": (_u32, [_vp]),
+            "nphref_force_participants": (None, [_vp, _u32]),
+            "nphref_add_body": (_u32, [_vp, _u32, _vp, _vp, _vp, _vp, _u32, _vp, _f32, _f32,
+                                       _f32, _u32]),
+            "nphref_set_mass": (None, [_vp, _u32, _f32, _vp, _vp]),
+            "nphref_add_shapeless_bodies": (_u32, [_vp, _u32, _vp, _vp]),
+            "nphref_add_joints": (_u32, [_vp, _u32, _vp]),
+            "nphref_inject_contacts": (_u32, [_vp, _u32, _vp]),
+            "nphref_collide": (ctypes.c_int, [_vp]),
+            "nphref_solve": (ctypes.c_int, [_vp, _f32]),
+            "nphref_finish": (ctypes.c_int, [_vp]),
+            "nphref_step": (ctypes.c_int, [_vp, _f32]),
+            "nphref_hash": (ctypes.c_uint64, [_vp]),
+            "nphref_last_solve_ms": (ctypes.c_double, [_vp]),
+            "nphref_body_count": (_u32, [_vp]),
+            "nphref_body_state": (None, [_vp, _u32, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+            "nphref_constraint_count": (_u32, [_vp]),
+            "nphref_constraints": (None, [_vp, _vp, _vp, _vp, _vp, _vp]),
+            "nphref_body_slots": (_u32, [_vp]),
+            "nphref_view_sizes": (None, [_vp, _vp, _vp, _vp, _vp]),
+            "nphref_export": (ctypes.c_int, [_vp, ctypes.POINTER(abi.WorldView)]),
+            "nphref_import": (ctypes.c_int, [_vp, ctypes.POINTER(abi.WorldView), _f32]),
+            "nphref_stats": (None, [_vp, _vp, _vp, _vp, _vp, _vp]),
+            "nphref_set_velocity": (None, [_vp, _u32, _vp, _vp]),
+        }
+        for name, (res, args) in sig.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _ref = lib
+    return _ref
+
+
+def _port_lib():
+    global _port
+    if _port is None:
+        lib = ctypes.CDLL(str(PORT_LIB))
+        lib.nph_port32_solve.restype = ctypes.c_int
+        lib.nph_port32_solve.argtypes = [ctypes.POINTER(abi.WorldParams), _f32,
+                                         ctypes.POINTER(abi.WorldView)]
+        lib.nph_port64_solve.restype = ctypes.c_int
+        lib.nph_port64_solve.argtypes = [ctypes.POINTER(abi.WorldParams), _f32,
+                                         ctypes.POINTER(abi.WorldView), _vp]
+        lib.nph_port_graph_color.restype = ctypes.c_int
+        lib.nph_port_graph_color.argtypes = [_vp, _vp, _vp, _u32, _u32, _vp, _vp]
+        _port = lib
+    return _port
+
+
+def _p(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+class RefWorld:
+    """A reference world (engine/physics) built and stepped through the harness."""
+
+    def __init__(self, params: abi.WorldParams | None = None, enable_sleep: bool = False,
+                 workers: int = 0):
+        """workers: 0 no job system; n > 0 a job system of n workers; -1 the reference's
+        default (logical cores - 1)."""
+        self.params = params if params is not None else abi.WorldParams.default()
+        lib = _ref_lib()
+        w = abi.NULL if workers < 0 else workers
+        self._h = lib.nphref_world_create(ctypes.byref(self.params), int(enable_sleep), w)
+        if not self._h:
+            raise RuntimeError("reference world creation failed")
+        self.lib = lib
+
+    def close(self):
+        if self._h:
+            self.lib.nphref_world_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def workers(self) -> int:
+        return int(self.lib.nphref_worker_count(self._h))
+
+    def force_participants(self, n: int):
+        self.lib.nphref_force_participants(self._h, n)
+
+    # -- scene building -------------------------------------------------------------
+    def add_body(self, type_, position, rotation=(0, 0, 0, 1), velocity=(0, 0, 0),
+                 angular_velocity=(0, 0, 0), shape=0, dims=(0, 0, 0), density=1000.0,
+                 friction=0.6, restitution=0.0, gyroscopic=True, enable_sleep=True,
+                 bullet=False) -> int:
+        pos = np.asarray(position, np.float64)
+        rot = np.asarray(rotation, np.float32)
+        v = np.asarray(velocity, np.float32)
+        w = np.asarray(angular_velocity, np.float32)
+        d = np.asarray(dims, np.float32)
+        flags = (1 if gyroscopic else 0) | (2 if enable_sleep else 0) | (4 if bullet else 0)
+        idx = self.lib.nphref_add_body(self._h, type_, _p(pos), _p(rot), _p(v), _p(w), shape,
+                                       _p(d), density, friction, restitution, flags)
+        if idx == abi.NULL:
+            raise RuntimeError("reference body creation failed")
+        return int(idx)
+
+    def add_box(self, position, half=(0.5, 0.5, 0.5), type_=abi.BODY_DYNAMIC, **kw) -> int:
+        return self.add_body(type_, position, shape=1, dims=half, **kw)
+
+    def add_sphere(self, position, radius, type_=abi.BODY_DYNAMIC, **kw) -> int:
+        return self.add_body(type_, position, shape=2, dims=(radius, 0, 0), **kw)
+
+    def add_capsule(self, position, half_height, radius, type_=abi.BODY_DYNAMIC, **kw) -> int:
+        return self.add_body(type_, position, shape=3, dims=(half_height, radius, 0), **kw)
+
+    def add_ground(self, top=0.0, friction=0.6) -> int:
+        """A static slab whose top face is y = top (test_world_support.h:64-68)."""
+        return self.add_box((0.0, top - 1.0, 0.0), half=(50.0, 1.0, 50.0),
+                            type_=abi.BODY_STATIC, friction=friction)
+
+    def add_shapeless_bodies(self, records: np.ndarray, mass: np.ndarray) -> int:
+        records = np.ascontiguousarray(records, abi.BODY_DTYPE)
+        mass = np.ascontiguousarray(mass, np.float32)
+        first = self.lib.nphref_add_shapeless_bodies(self._h, len(records), _p(records), _p(mass))
+        if first == abi.NULL:
+            raise RuntimeError("reference body creation failed")
+        return int(first)
+
+    def add_joints(self, records: np.ndarray):
+        records = np.ascontiguousarray(records, abi.JOINT_DTYPE)
+        if len(records) and self.lib.nphref_add_joints(self._h, len(records), _p(records)) == abi.NULL:
+            raise RuntimeError("reference joint creation failed")
+
+    def inject_contacts(self, records: np.ndarray):
+        records = np.ascontiguousarray(records, abi.CONTACT_DTYPE)
+        if len(records) and self.lib.nphref_inject_contacts(self._h, len(records),
+                                                            _p(records)) == abi.NULL:
+            raise RuntimeError("reference contact injection failed")
+
+    # -- stages -----------------------------------------------------------------------
+    def collide(self):
+        r = self.lib.nphref_collide(self._h)
+        if r != 0:
+            raise RuntimeError(f"reference collide failed: {r}")
+
+    def solve(self, dt: float) -> float:
+        r = self.lib.nphref_solve(self._h, dt)
+        if r != 0:
+            raise RuntimeError(f"reference phys_solve failed: {r}")
+        return 0.0
+
+    def finish(self):
+        r = self.lib.nphref_finish(self._h)
+        if r != 0:
+            raise RuntimeError(f"reference island stage failed: {r}")
+
+    def step(self, dt: float):
+        r = self.lib.nphref_step(self._h, dt)
+        if r != 0:
+            raise RuntimeError(f"reference world step failed: {r}")
+
+    def hash(self) -> int:
+        return int(self.lib.nphref_hash(self._h))
+
+    @property
+    def last_solve_ms(self) -> float:
+        return float(self.lib.nphref_last_solve_ms(self._h))
+
+    def body_state(self, body: int) -> dict:
+        c = np.zeros(3, np.float64)
+        o = np.zeros(3, np.float64)
+        q = np.zeros(4, np.float32)
+        v = np.zeros(3, np.float32)
+        w = np.zeros(3, np.float32)
+        st = ctypes.c_float()
+        fl = ctypes.c_uint32()
+        self.lib.nphref_body_state(self._h, body, _p(c), _p(o), _p(q), _p(v), _p(w),
+                                   ctypes.addressof(st), ctypes.addressof(fl))
+        return {"center": c, "origin": o, "rotation": q, "v": v, "w": w,
+                "sleep_time": st.value, "flags": fl.value}
+
+    def stats(self) -> dict:
+        vals = [ctypes.c_uint32() for _ in range(5)]
+        self.lib.nphref_stats(self._h, *[ctypes.addressof(x) for x in vals])
+        keys = ["touching", "points", "colors_used", "overflow", "awake"]
+        return {k: int(x.value) for k, x in zip(keys, vals)}
+
+    # -- the colouring ----------------------------------------------------------------
+    def constraints(self) -> dict:
+        n = int(self.lib.nphref_constraint_count(self._h))
+        a = np.zeros(n, np.uint32)
+        b = np.zeros(n, np.uint32)
+        d = np.zeros(n, np.uint8)
+        c = np.zeros(n, np.uint32)
+        s = np.zeros(n, np.uint32)
+        if n:
+            self.lib.nphref_constraints(self._h, _p(a), _p(b), _p(d), _p(c), _p(s))
+        return {"body_a": a, "body_b": b, "dynamic_bits": d, "color": c, "slot": s,
+                "body_slots": int(self.lib.nphref_body_slots(self._h))}
+
+    # -- world <-> view ---------------------------------------------------------------
+    def export_view(self) -> abi.View:
+        sizes = [ctypes.c_uint32() for _ in range(4)]
+        self.lib.nphref_view_sizes(self._h, *[ctypes.addressof(x) for x in sizes])
+        nb, nf, nc, nj = (int(x.value) for x in sizes)
+        view = abi.View(np.zeros(nb, abi.BODY_DTYPE), np.zeros(nf, abi.BODY_DTYPE),
+                        np.zeros(nc, abi.CONTACT_DTYPE), np.zeros(nj, abi.JOINT_DTYPE),
+                        np.zeros(abi.COLOR_SLOTS, np.uint32), np.zeros(abi.COLOR_SLOTS, np.uint32))
+        cv = view.c_view()
+        r = self.lib.nphref_export(self._h, ctypes.byref(cv))
+        if r != 0:
+            raise RuntimeError("reference export found bodies outside the first mapping")
+        view.contact_color_counts[:] = np.frombuffer(cv.contact_color_counts, np.uint32)
+        view.joint_color_counts[:] = np.frombuffer(cv.joint_color_counts, np.uint32)
+        return view
+
+    def import_view(self, view: abi.View, dt: float):
+        cv = view.c_view()
+        r = self.lib.nphref_import(self._h, ctypes.byref(cv), dt)
+        if r != 0:
+            raise RuntimeError(f"reference import failed: {r}")
+
+
+# ------------------------------------------------------------------------------------
+# The CPU restatement
+# ------------------------------------------------------------------------------------
+
+def port32(view: abi.View, params: abi.WorldParams, dt: float) -> abi.View:
+    """FP32 solve of a copy of `view` (the reference's arithmetic, one manifold at a time)."""
+    out = view.copy()
+    cv = out.c_view()
+    r = _port_lib().nph_port32_solve(ctypes.byref(params), dt, ctypes.byref(cv))
+    if r != 0:
+        raise RuntimeError(f"port32 failed: {abi.RESULT_NAMES.get(r, r)}")
+    return out
+
+
+def port32_result(view: abi.View, params: abi.WorldParams, dt: float) -> int:
+    cv = view.copy().c_view()
+    return int(_port_lib().nph_port32_solve(ctypes.byref(params), dt, ctypes.byref(cv)))
+
+
+def port64(view: abi.View, params: abi.WorldParams, dt: float) -> dict:
+    """FP64 re-run of the same step: the error baseline. Returns float64 arrays."""
+    nb, nc, nj = len(view.bodies), len(view.contacts), len(view.joints)
+    out = {
+        "linear_velocity": np.zeros((nb, 3)), "angular_velocity": np.zeros((nb, 3)),
+        "rotation": np.zeros((nb, 4)), "center": np.zeros((nb, 3)),
+        "normal_impulse": np.zeros((nc, 4)), "max_normal_impulse": np.zeros((nc, 4)),
+        "tangent_impulse": np.zeros((nc, 4, 3)), "relative_velocity": np.zeros((nc, 4)),
+        "joint_linear_impulse": np.zeros((nj, 3)), "joint_angular_impulse": np.zeros((nj, 3)),
+    }
+    order = ["linear_velocity", "angular_velocity", "rotation", "center", "normal_impulse",
+             "max_normal_impulse", "tangent_impulse", "relative_velocity",
+             "joint_linear_impulse", "joint_angular_impulse"]
+    ptrs = (ctypes.c_void_p * len(order))(*[out[k].ctypes.data for k in order])
+    cv = view.c_view()
+    r = _port_lib().nph_port64_solve(ctypes.byref(params), dt, ctypes.byref(cv), ptrs)
+    if r != 0:
+        raise RuntimeError(f"port64 failed: {abi.RESULT_NAMES.get(r, r)}")
+    return out
+
+
+def port_graph_color(body_a, body_b, dynamic_bits, body_slots) -> tuple[np.ndarray, np.ndarray]:
+    a = np.ascontiguousarray(body_a, np.uint32)
+    b = np.ascontiguousarray(body_b, np.uint32)
+    d = np.ascontiguousarray(dynamic_bits, np.uint8)
+    n = len(a)
+    color = np.zeros(n, np.uint32)
+    slot = np.zeros(n, np.uint32)
+    r = _port_lib().nph_port_graph_color(_p(a), _p(b), _p(d), n, body_slots, _p(color), _p(slot))
+    if r != 0:
+        raise RuntimeError("port colouring failed")
+    return color, slot
