@@ -1,0 +1,377 @@
+#!/usr/bin/env python3
+"""Throughput of the solver stage: contact-solves/s on the 1M-body synthetic constraint graph.
+
+Workload (the metric's configuration): a 128^3 lattice of unit boxes (1,048,576 dynamic
+bodies), one 4-point manifold per neighbour pair (6,242,304 manifolds), ball or hinge joints
+on 10 % of the pairs, soft step, 4 substeps, dt 1/60, seeded. A step is one whole solver
+stage (phys_solve) over the device-resident world: prepare, 4 x (integrate, warm start,
+solve, integrate, relax) over every colour, restitution, store, finalize. One contact-solve
+is one manifold in one solve or relax pass: 2 x substeps x manifolds per step.
+
+  value   device time of K resident steps (CUDA events on the solver's stream, max over ranks)
+  e2e     the same metric through the drop-in call nph_gpu_phys_solve on pinned host
+          records: host->device upload, the step, device->host download, every step
+  roofline the dominant kernel (the solve pass) against the measured HBM bandwidth
+  cpu_baseline the reference's own phys_solve (oracle/_ref, built from its sources) on the
+          host's cores, on a bounded sample of the same workload
+
+With --impl reference the reference's phys_solve on its job system (all host cores) is
+timed on this configuration instead (rank 0 only).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "contact-solves/s @1M bodies"
+UNIT = "contact-solves/s"
+DT = 1.0 / 60.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="nepheline_b200")
+    ap.add_argument("--edge", type=int, default=128, help="lattice edge (128: 1,048,576 bodies)")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+class Clocks:
+    """nvidia-smi samples of the SM clock and throttle reasons during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(n_gpus: int):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl" if os.environ.get("NPH_BENCH_GLOO") is None else "gloo",
+                                timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return rank, world, local, pg
+
+
+def max_over_ranks(pg, value: float) -> float:
+    if pg is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def build_view(edge: int, seed: int, solver):
+    from nepheline_b200 import scenes
+    sc = scenes.lattice_graph(edge, seed=seed, joint_fraction=0.1)
+    a, b, d = sc.constraint_arrays()
+    color, slot = solver.graph_color(a, b, d, len(sc.bodies))
+    return sc, sc.to_view(color, slot)
+
+
+def pinned_copy(view):
+    """The view's records in page-locked host memory (the e2e path's host buffers)."""
+    import torch
+
+    from nepheline_b200 import abi
+
+    def pin(a):
+        t = torch.empty(a.nbytes, dtype=torch.uint8, pin_memory=True)
+        out = t.numpy().view(a.dtype)
+        out[...] = a
+        return out, t
+
+    b, tb = pin(view.bodies)
+    c, tc = pin(view.contacts)
+    j, tj = pin(view.joints)
+    v = abi.View(b, view.fixed, c, j, view.contact_color_counts, view.joint_color_counts)
+    v._keep = (tb, tc, tj)
+    return v
+
+
+def reference_sample(edge: int, steps: int, warmup: int, workers: int) -> dict:
+    """The reference's phys_solve on its job system over an edge^3 sample of the lattice."""
+    from nepheline_b200 import abi
+    from tests import ref_scenes
+    params = abi.WorldParams.default()
+    w, sc = ref_scenes.lattice(edge=edge, seed=0, joint_fraction=0.1, params=params,
+                               workers=workers)
+    for _ in range(warmup):
+        w.solve(DT)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        w.solve(DT)
+    sec = (time.perf_counter() - t0) / max(steps, 1)
+    threads = w.workers + 1 if w.workers > 0 else 1
+    manifolds = len(sc.contacts)
+    w.close()
+    return {"value": 8.0 * manifolds / sec, "ms_per_step": 1e3 * sec, "threads": threads,
+            "manifolds": manifolds, "bodies": len(sc.bodies), "edge": edge}
+
+
+def cpu_model() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import refworld
+    if not refworld.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/libnphref.so was not built (reference sources absent)"}))
+        return 0
+    cores = os.cpu_count() or 1
+    # The full workload when the run fits a few minutes on this host, else a smaller lattice:
+    # about 0.6 s per step for 64^3 on 8 cores, scaling with the volume and the cores.
+    est = 0.6 * (args.edge / 64.0) ** 3 * (8.0 / cores)
+    edge = args.edge
+    while edge > 16 and est * (args.steps + args.warmup) > 150.0:
+        edge = int(edge * 0.8)
+        est = 0.6 * (edge / 64.0) ** 3 * (8.0 / cores)
+    r = reference_sample(edge, args.steps, args.warmup, workers=-1)
+    sample = (f"{edge}^3 lattice ({r['bodies']} bodies, {r['manifolds']} manifolds), "
+              f"{args.steps} timed steps after {args.warmup}; {cpu_model()}")
+    out = {
+        "impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "synthetic constraint graph, 128^3 lattice", "edge": args.edge,
+                   "sample_edge": edge, "substeps": 4, "dt": DT},
+        "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["threads"],
+                         "kind": "reference", "sample": sample},
+        "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+
+    from nepheline_b200 import abi
+    from nepheline_b200.solver import Solver
+
+    rank, world, local, pg = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    stream = torch.cuda.current_stream()
+    solver = Solver(device=local, stream=stream.cuda_stream)
+    params = abi.WorldParams.default()
+    sc, view = build_view(args.edge, seed=rank, solver=solver)
+    manifolds = len(view.contacts)
+    solves_per_step = 2 * params.substeps * manifolds
+
+    # Device-resident steps.
+    solver.upload(view)
+    solver.step_async(params, DT, args.warmup)
+    torch.cuda.synchronize()
+    barrier(pg)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        solver.step_async(params, DT, args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    barrier(pg)
+    ms = max_over_ranks(pg, ms)
+    stats = solver.stats()
+    value = world * solves_per_step / (ms * 1e-3)
+
+    # The dominant kernel, timed launch by launch on the same stream.
+    prof = [solver.profile_step(params, DT) for _ in range(3)]
+    kinds = {}
+    for p in prof:
+        for k in p:
+            d = kinds.setdefault(k["name"], {"launches": 0, "total_ms": 0.0, "bytes": 0.0,
+                                             "units": 0})
+            d["launches"] += k["launches"]
+            d["total_ms"] += k["total_ms"]
+            d["bytes"] += k["algorithmic_bytes"]
+            d["units"] += k["units"]
+    top = max(kinds.items(), key=lambda kv: kv[1]["total_ms"])
+    pk = peaks()
+    per_launch_ms = top[1]["total_ms"] / top[1]["launches"]
+    per_launch_bytes = top[1]["bytes"] / top[1]["launches"]
+    achieved = per_launch_bytes / (per_launch_ms * 1e-3) / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "solve_traffic.json"
+    if tf.exists():
+        try:
+            traffic = json.loads(tf.read_text()).get("bytes_per_launch_at_full_size")
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / pk["hbm_gbs"], "traffic": traffic, "kernel": top[0],
+                "peak_source": pk["source"], "launches_per_step": top[1]["launches"] // 3,
+                "ms_per_launch": per_launch_ms, "algorithmic_bytes_per_launch": per_launch_bytes,
+                "kernel_share": top[1]["total_ms"] / sum(v["total_ms"] for v in kinds.values())}
+
+    # End to end through the drop-in call on pinned host records.
+    pv = pinned_copy(view)
+    h2d = pv.bodies.nbytes + pv.contacts.nbytes + pv.joints.nbytes + pv.fixed.nbytes
+    d2h = pv.bodies.nbytes + pv.contacts.nbytes + pv.joints.nbytes
+    solver.phys_solve(pv, params, DT)
+    torch.cuda.synchronize()
+    barrier(pg)
+    s0 = torch.cuda.Event(enable_timing=True)
+    s1 = torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    s0.record(stream)
+    for _ in range(args.e2e_steps):
+        solver.phys_solve(pv, params, DT)
+    s1.record(stream)
+    torch.cuda.synchronize()
+    wall = (time.perf_counter() - t0) / args.e2e_steps
+    e2e_ms = max(s0.elapsed_time(s1) / args.e2e_steps, wall * 1e3)
+    e2e_ms = max_over_ranks(pg, e2e_ms)
+    e2e_value = world * solves_per_step / (e2e_ms * 1e-3)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import refworld
+        if refworld.ref_available():
+            r = reference_sample(64, steps=8, warmup=1, workers=-1)
+            cpu = {"value": r["value"], "unit": UNIT, "cores": r["threads"], "kind": "reference",
+                   "sample": f"64^3 lattice ({r['bodies']} bodies, {r['manifolds']} manifolds), "
+                             f"8 steps of the reference phys_solve on its job system; {cpu_model()}"}
+        else:
+            from oracle.refworld import port32
+            from nepheline_b200 import scenes
+            small = scenes.lattice_graph(32, seed=0)
+            c, s = scenes.host_color(small)
+            v = small.to_view(c, s)
+            t0 = time.perf_counter()
+            for _ in range(3):
+                v = port32(v, params, DT)
+            sec = (time.perf_counter() - t0) / 3
+            cpu = {"value": 8.0 * len(small.contacts) / sec, "unit": UNIT, "cores": 1,
+                   "kind": "port", "sample": "32^3 lattice, 3 steps of the FP32 restatement"}
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "synthetic constraint graph, 128^3 lattice" if args.edge == 128
+                       else f"synthetic constraint graph, {args.edge}^3 lattice",
+                       "bodies": len(view.bodies), "manifolds": manifolds,
+                       "joints": len(view.joints), "colors": view.colors_used, "substeps": 4,
+                       "dt": DT, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (about 2 GB of manifold rows per step)"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms},
+            "gpu_launches": int(stats.launches) * args.steps,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+            "points_solved_per_s": value * 4,
+            "kernels": {k: {"launches": v["launches"] // 3, "ms": v["total_ms"] / 3}
+                        for k, v in kinds.items()},
+        }
+        print(json.dumps(out))
+    solver.close()
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -303,10 +303,27 @@ NPH_GPU_API NphGpuResult nph_gpu_solver_stats(const NphGpuSolver *solver, NphGpu
 /* The stream the solver launches on (a cudaStream_t). */
 NPH_GPU_API void *nph_gpu_solver_stream(const NphGpuSolver *solver);
 
-/* Test hook: the iteration limit of every bounded device wait (0 restores the default). A
- * limit of 1 makes the waits give up at once, so the error path can be tested without
- * hanging a device. */
-NPH_GPU_API void nph_gpu_solver_set_wait_limit(NphGpuSolver *solver, uint32_t limit);
+/* One kind of kernel in a profiled step. */
+typedef struct NphGpuKernelTime {
+    char name[32];
+    uint32_t launches;
+    uint32_t pad;
+    uint64_t units;              /* manifolds, joints or bodies processed over the launches */
+    double total_ms;             /* summed device time of the launches (CUDA events) */
+    double algorithmic_bytes;    /* the reference data model's live bytes over the launches */
+} NphGpuKernelTime;
+
+/* One step of the uploaded world with every launch issued directly and bracketed by CUDA
+ * events on the solver's stream, reported per kind of kernel (at most `capacity` kinds;
+ * `*count` receives how many). The step is a real step: the world advances. The
+ * algorithmic bytes use the reference data model's per-unit figures (a manifold solve pass
+ * 224 + 148 per point bytes, relax 212 + 148 per point, warm start 120 per point, prepare 936,
+ * store 160, restitution check 40; a body's prepare 368, each integration 84, finalize 200;
+ * a joint pass 330). */
+NPH_GPU_API NphGpuResult nph_gpu_world_profile_step(NphGpuSolver *solver,
+                                                    const NphGpuWorldParams *params, float dt,
+                                                    NphGpuKernelTime *out, uint32_t capacity,
+                                                    uint32_t *count);
 
 /* ------------------------------------------------------------------------------------
  * The constraint graph's colouring on the device

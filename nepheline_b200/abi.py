@@ -169,6 +169,16 @@ class StepStats(ctypes.Structure):
     ]
 
 
+class KernelTime(ctypes.Structure):
+    """NphGpuKernelTime: one kind of kernel in a profiled step."""
+
+    _fields_ = [
+        ("name", ctypes.c_char * 32), ("launches", ctypes.c_uint32), ("pad", ctypes.c_uint32),
+        ("units", ctypes.c_uint64), ("total_ms", ctypes.c_double),
+        ("algorithmic_bytes", ctypes.c_double),
+    ]
+
+
 class SolverDesc(ctypes.Structure):
     _fields_ = [
         ("device", ctypes.c_int32), ("stream", ctypes.c_void_p), ("use_graph", ctypes.c_uint32),

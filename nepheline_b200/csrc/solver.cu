@@ -1,0 +1,1037 @@
+// SPDX-License-Identifier: Apache-2.0
+//
+// The solver stage on the device for one world of any size: the reference's stage list
+// (phys_solve, engine/physics/src/solver.c:961-1105) as kernels, one launch per stage and
+// colour, replayed as one CUDA graph per step:
+//
+//   prepare bodies; prepare joints and contacts;
+//   per substep: integrate velocities, warm start, solve, integrate positions, relax
+//     (each constraint pass: the overflow serially in list order, then colours 0..23, each
+//      colour's joints and contacts in one launch: push_contact_pass, solver.c:774-789);
+//   restitution (contacts only); store; finalize; the driven joints' sleep reset.
+//
+// The reference's lockstep thread claiming (solver.c:628-713) becomes kernel boundaries:
+// every stage's writes are visible to the next launch on the stream.
+
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "nepheline_b200.h"
+
+#include "bodies.cuh"
+#include "contacts.cuh"
+#include "joints.cuh"
+
+namespace nph {
+
+constexpr uint32_t kBlock = 256;
+
+struct ColorTable {
+    uint32_t cfirst[NPH_GPU_COLOR_SLOTS];
+    uint32_t ccount[NPH_GPU_COLOR_SLOTS];
+};
+
+enum Pass : int { kWarm = 0, kSolve = 1, kRelax = 2, kRestitution = 3 };
+
+// ------------------------------------------------------------------------------------
+// Kernels
+// ------------------------------------------------------------------------------------
+
+__global__ void __launch_bounds__(kBlock) k_prepare_bodies(BodyArrays B, const NphGpuBody *bodies,
+                                                           uint32_t n, StepConsts K)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        prepare_body(B, i, bodies[i], K);
+    } else if (i == n) {
+        prepare_dummy(B, n);
+    }
+}
+
+// The largest point count of the eight-lane group holding manifold g (build_groups,
+// solver.c:810-843: a colour's list in eights, the overflow one per group).
+__device__ uint32_t group_points(const NphGpuContact *contacts, uint32_t g, const ColorTable &T,
+                                 uint32_t &color)
+{
+    uint32_t c = 0;
+    while (c + 1u < NPH_GPU_COLOR_SLOTS && g >= T.cfirst[c] + T.ccount[c]) {
+        ++c;
+    }
+    const uint32_t per = c == NPH_GPU_OVERFLOW ? 1u : 8u;
+    const uint32_t start = T.cfirst[c] + ((g - T.cfirst[c]) / per) * per;
+    const uint32_t end = min(start + per, T.cfirst[c] + T.ccount[c]);
+    uint32_t gp = 0;
+    for (uint32_t q = start; q < end; ++q) {
+        const uint32_t pc = contacts[q].point_count;
+        gp = pc <= NPH_GPU_MAX_POINTS && pc > gp ? pc : gp;
+    }
+    color = c;
+    return gp;
+}
+
+__global__ void __launch_bounds__(kBlock)
+k_prepare_constraints(DevSolver S, const NphGpuContact *contacts, const NphGpuJoint *joints,
+                      const NphGpuBody *bodies, const NphGpuBody *fixed, uint32_t n, uint32_t nf,
+                      uint32_t m, uint32_t nj, uint32_t jblocks, ColorTable T, float h,
+                      uint32_t *err, uint32_t *color_points)
+{
+    const uint32_t total = n + nf;
+    if (blockIdx.x < jblocks) {
+        const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+        if (j >= nj) {
+            return;
+        }
+        const NphGpuJoint &jr = joints[j];
+        if (jr.body_a >= total || jr.body_b >= total ||
+            (jr.type != NPH_GPU_JOINT_BALL && jr.type != NPH_GPU_JOINT_HINGE)) {
+            atomicOr(err, kErrBadJoint);
+            // Inert: both ends the dummy, no impulse, nothing written.
+            for (uint32_t r = 0; r < kJointRows; ++r) {
+                S.jw[r * S.jcap + j] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+            S.jw[kJrFrameA * S.jcap + j] = make_float4(0.f, 0.f, 0.f, 1.f);
+            S.jw[kJrFrameB * S.jcap + j] = make_float4(0.f, 0.f, 0.f, 1.f);
+            S.jw[kJrHead * S.jcap + j] = make_float4(__uint_as_float(n), __uint_as_float(n), 0.f, 0.f);
+            return;
+        }
+        const NphGpuBody &a = jr.body_a < n ? bodies[jr.body_a] : fixed[jr.body_a - n];
+        const NphGpuBody &b = jr.body_b < n ? bodies[jr.body_b] : fixed[jr.body_b - n];
+        prepare_joint(S, j, jr, a, b, jr.body_a < n ? jr.body_a : n, jr.body_b < n ? jr.body_b : n, h);
+        return;
+    }
+    const uint32_t g = (blockIdx.x - jblocks) * blockDim.x + threadIdx.x;
+    if (g >= m) {
+        return;
+    }
+    const NphGpuContact &c = contacts[g];
+    if (c.body_a >= total || c.body_b >= total) {
+        atomicOr(err, kErrBadIndex);
+        S.hdr[g] = make_uint4(n, n, 0u, 0u);
+        return;
+    }
+    if (c.point_count < 1u || c.point_count > NPH_GPU_MAX_POINTS) {
+        atomicOr(err, kErrBadPoints);
+        S.hdr[g] = make_uint4(n, n, 0u, 0u);
+        return;
+    }
+    const NphGpuBody &a = c.body_a < n ? bodies[c.body_a] : fixed[c.body_a - n];
+    const NphGpuBody &b = c.body_b < n ? bodies[c.body_b] : fixed[c.body_b - n];
+    S.nrm[g] = make_float4(c.normal[0], c.normal[1], c.normal[2], c.friction);
+    S.rest[g] = c.restitution;
+    uint32_t color = 0;
+    const uint32_t gp = group_points(contacts, g, T, color);
+    prepare_manifold(S, g, c, a, b, c.body_a < n ? c.body_a : n, c.body_b < n ? c.body_b : n, gp);
+    atomicAdd(&color_points[color], c.point_count);
+}
+
+template <int P>
+__device__ __forceinline__ void joint_op(const DevSolver &S, uint32_t j, const StepConsts &K)
+{
+    if (P == kWarm) {
+        warm_joint(S, j);
+    } else if (P == kSolve) {
+        solve_joint<true>(S, j, K);
+    } else if (P == kRelax) {
+        solve_joint<false>(S, j, K);
+    }
+}
+
+template <int P>
+__device__ __forceinline__ void contact_op(const DevSolver &S, uint32_t g, const StepConsts &K)
+{
+    if (P == kWarm) {
+        warm_manifold(S, g);
+    } else if (P == kSolve) {
+        solve_manifold<true>(S, g, K);
+    } else if (P == kRelax) {
+        solve_manifold<false>(S, g, K);
+    } else {
+        restitution_manifold(S, g, K);
+    }
+}
+
+// One colour of one constraint pass: its joints' blocks, then its contacts'.
+template <int P>
+__global__ void __launch_bounds__(kBlock)
+k_pass(DevSolver S, uint32_t cfirst, uint32_t ccount, uint32_t jfirst, uint32_t jcount,
+       uint32_t jblocks, StepConsts K)
+{
+    if (blockIdx.x < jblocks) {
+        const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+        if (j < jcount) {
+            joint_op<P>(S, jfirst + j, K);
+        }
+        return;
+    }
+    const uint32_t g = (blockIdx.x - jblocks) * blockDim.x + threadIdx.x;
+    if (g < ccount) {
+        contact_op<P>(S, cfirst + g, K);
+    }
+}
+
+// The overflow: its joints, then its contacts, one at a time in list order (they may share
+// bodies; solver.c:778-782 runs them as one block each).
+template <int P>
+__global__ void k_overflow(DevSolver S, uint32_t cfirst, uint32_t ccount, uint32_t jfirst,
+                           uint32_t jcount, StepConsts K)
+{
+    if (threadIdx.x != 0 || blockIdx.x != 0) {
+        return;
+    }
+    if (P != kRestitution) {
+        for (uint32_t j = 0; j < jcount; ++j) {
+            joint_op<P>(S, jfirst + j, K);
+        }
+    }
+    for (uint32_t g = 0; g < ccount; ++g) {
+        contact_op<P>(S, cfirst + g, K);
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_integrate_velocity(BodyArrays B, uint32_t n, float h)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        integrate_velocity(B, i, h);
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) k_integrate_position(BodyArrays B, uint32_t n, float h)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        integrate_position(B, i, h);
+    }
+}
+
+// store_group (solver.c:475-499), the joints' impulses, and finalize_body (solver.c:304-324).
+__global__ void __launch_bounds__(kBlock)
+k_store_finalize(DevSolver S, BodyArrays B, NphGpuContact *contacts, uint32_t m,
+                 NphGpuJoint *joints, uint32_t nj, NphGpuBody *bodies, uint32_t n, float dt)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) {
+        store_manifold(S, i, contacts[i]);
+        return;
+    }
+    i -= m;
+    if (i < nj) {
+        store_joint(S, i, joints[i]);
+        return;
+    }
+    i -= nj;
+    if (i < n) {
+        finalize_body(B, i, bodies[i], dt);
+    }
+}
+
+// post_finalize, solver.c:851-857: a driven joint's bodies stay awake.
+__global__ void __launch_bounds__(kBlock) k_driven(DevSolver S, NphGpuBody *bodies, uint32_t n,
+                                                   uint32_t nj)
+{
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nj) {
+        return;
+    }
+    uint32_t sa, sb, flags;
+    joint_head(S, j, sa, sb, flags);
+    if ((flags & kJDriven) != 0u) {
+        if (sa < n) {
+            bodies[sa].sleep_time = 0.0f;
+        }
+        if (sb < n) {
+            bodies[sb].sleep_time = 0.0f;
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------
+// Host side
+// ------------------------------------------------------------------------------------
+
+static uint32_t blocks_for(uint64_t count) { return (uint32_t)((count + kBlock - 1) / kBlock); }
+
+// solver.c:48-65 on the host, in FP32 as the reference.
+static Soft host_make_soft(float hertz, float zeta, float h)
+{
+    if (hertz <= 0.0f) {
+        return Soft{0.0f, 1.0f, 0.0f};
+    }
+    const float omega = 2.0f * 3.14159265f * hertz;
+    const float a1 = 2.0f * zeta + h * omega;
+    const float a2 = h * omega * a1;
+    const float a3 = 1.0f / (1.0f + a2);
+    return Soft{omega / a1, a2 * a3, a3};
+}
+
+static float minf_ref(float a, float b) { return a < b ? a : b; }
+
+// phys_solve's step constants, solver.c:985-1006 (soft step).
+StepConsts make_step_consts(const NphGpuWorldParams &p, float dt)
+{
+    StepConsts K;
+    std::memset(&K, 0, sizeof K);
+    K.dt = dt;
+    K.h = dt / (float)p.substeps;
+    K.inv_h = 1.0f / K.h;
+    K.push_max = p.contact_push_max_velocity;
+    K.restitution_threshold = p.restitution_threshold;
+    const float contact_hertz = p.contact_hertz > 0.0f ? p.contact_hertz : 0.125f * K.inv_h;
+    const float joint_hertz = p.joint_hertz > 0.0f ? p.joint_hertz : 0.25f * K.inv_h;
+    const float hertz = minf_ref(contact_hertz, 0.25f * K.inv_h);
+    K.contact_soft = host_make_soft(hertz, p.contact_damping_ratio, K.h);
+    K.static_soft = host_make_soft(2.0f * hertz, p.contact_damping_ratio, K.h);
+    K.joint_soft = host_make_soft(minf_ref(joint_hertz, 0.25f * K.inv_h), p.joint_damping_ratio, K.h);
+    const float max_rotation = 0.25f * 3.14159265f * K.inv_h;
+    K.max_angular_speed_sq = max_rotation * max_rotation;
+    K.max_linear_speed_sq = p.max_linear_speed * p.max_linear_speed;
+    K.gravity[0] = p.gravity[0];
+    K.gravity[1] = p.gravity[1];
+    K.gravity[2] = p.gravity[2];
+    return K;
+}
+
+} // namespace nph
+
+using namespace nph;
+
+struct NphGpuSolver {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    bool use_graph = true;
+    // Capacities of the device arrays.
+    uint32_t bcap = 0, fcap = 0, mcap = 0, jcap = 0;
+    // Records (device copies of the view's arrays).
+    NphGpuBody *d_bodies = nullptr;
+    NphGpuBody *d_fixed = nullptr;
+    NphGpuContact *d_contacts = nullptr;
+    NphGpuJoint *d_joints = nullptr;
+    // Solver state.
+    float4 *vel = nullptr, *pos = nullptr, *prm = nullptr, *itg = nullptr;
+    uint4 *hdr = nullptr;
+    float4 *nrm = nullptr;
+    float *rest = nullptr;
+    float4 *pa = nullptr, *pb = nullptr, *pt = nullptr, *pi = nullptr;
+    float4 *jw = nullptr;
+    uint32_t *d_err = nullptr;     // [0] error bits, [1..25] points per colour slot
+    uint32_t *h_err = nullptr;     // pinned copy of the same 26 words
+    // Per-launch timing of a profiled step.
+    struct Mark {
+        int kind;
+        uint64_t units;
+        double bytes;
+        cudaEvent_t a, b;
+    };
+    std::vector<Mark> *marks = nullptr;
+    std::vector<cudaEvent_t> event_pool;
+    size_t events_used = 0;
+    // The uploaded world.
+    bool uploaded = false;
+    uint32_t n = 0, nf = 0, m = 0, nj = 0;
+    uint32_t ccount[NPH_GPU_COLOR_SLOTS] = {}, jcount[NPH_GPU_COLOR_SLOTS] = {};
+    uint32_t cfirst[NPH_GPU_COLOR_SLOTS] = {}, jfirst[NPH_GPU_COLOR_SLOTS] = {};
+    uint32_t driven = 0;
+    // The step graph and what it was captured for.
+    cudaGraphExec_t graph = nullptr;
+    StepConsts graph_consts{};
+    uint32_t graph_substeps = 0;
+    bool graph_valid = false;
+    cudaEvent_t ev[6] = {};
+    NphGpuStepStats stats{};
+    uint32_t launches = 0;
+};
+
+namespace {
+
+template <typename T> void dfree(T *&p)
+{
+    if (p != nullptr) {
+        cudaFree(p);
+        p = nullptr;
+    }
+}
+
+template <typename T> bool dalloc(T *&p, size_t count)
+{
+    dfree(p);
+    if (count == 0) {
+        count = 1;
+    }
+    return cudaMalloc((void **)&p, count * sizeof(T)) == cudaSuccess;
+}
+
+void drop_graph(NphGpuSolver *s)
+{
+    if (s->graph != nullptr) {
+        cudaGraphExecDestroy(s->graph);
+        s->graph = nullptr;
+    }
+    s->graph_valid = false;
+}
+
+// Grows the device arrays to hold the view (between steps only).
+NphGpuResult ensure_capacity(NphGpuSolver *s, uint32_t n, uint32_t nf, uint32_t m, uint32_t nj)
+{
+    bool ok = true;
+    if (n + 1u > s->bcap) {
+        const uint32_t cap = n + 1u + (n + 1u) / 8u;
+        ok = ok && dalloc(s->d_bodies, cap) && dalloc(s->vel, 2ull * cap) &&
+             dalloc(s->pos, 2ull * cap) && dalloc(s->prm, 3ull * cap) && dalloc(s->itg, 6ull * cap);
+        s->bcap = ok ? cap : 0;
+    }
+    if (ok && nf > s->fcap) {
+        const uint32_t cap = nf + nf / 8u + 1u;
+        ok = dalloc(s->d_fixed, cap);
+        s->fcap = ok ? cap : 0;
+    }
+    if (ok && m > s->mcap) {
+        const uint32_t cap = m + m / 8u + 1u;
+        ok = dalloc(s->d_contacts, cap) && dalloc(s->hdr, cap) && dalloc(s->nrm, cap) &&
+             dalloc(s->rest, cap) && dalloc(s->pa, 4ull * cap) && dalloc(s->pb, 4ull * cap) &&
+             dalloc(s->pt, 4ull * cap) && dalloc(s->pi, 4ull * cap);
+        s->mcap = ok ? cap : 0;
+    }
+    if (ok && nj > s->jcap) {
+        const uint32_t cap = nj + nj / 8u + 1u;
+        ok = dalloc(s->d_joints, cap) && dalloc(s->jw, (size_t)kJointRows * cap);
+        s->jcap = ok ? cap : 0;
+    }
+    if (!ok) {
+        s->uploaded = false;
+        drop_graph(s);
+        cudaGetLastError();
+        return NPH_GPU_OUT_OF_MEMORY;
+    }
+    return NPH_GPU_OK;
+}
+
+DevSolver dev_solver(const NphGpuSolver *s)
+{
+    DevSolver S;
+    S.vel = s->vel;
+    S.pos = s->pos;
+    S.prm = s->prm;
+    S.hdr = s->hdr;
+    S.nrm = s->nrm;
+    S.rest = s->rest;
+    S.pa = s->pa;
+    S.pb = s->pb;
+    S.pt = s->pt;
+    S.pi = s->pi;
+    S.mcap = s->mcap;
+    S.jw = s->jw;
+    S.jcap = s->jcap;
+    return S;
+}
+
+BodyArrays body_arrays(const NphGpuSolver *s)
+{
+    return BodyArrays{s->vel, s->pos, s->prm, s->itg};
+}
+
+// Kernel kinds of a profiled step, and the reference data model's live bytes per unit.
+enum Kind : int {
+    kKPrepareBodies = 0,
+    kKPrepareConstraints,
+    kKIntegrateVelocity,
+    kKWarm,
+    kKSolve,
+    kKIntegratePosition,
+    kKRelax,
+    kKRestitution,
+    kKStoreFinalize,
+    kKOverflow,
+    kKDriven,
+    kKinds
+};
+const char *const kKindNames[kKinds] = {"prepare_bodies", "prepare_constraints", "integrate_velocity",
+                                        "warm_start", "solve", "integrate_position", "relax",
+                                        "restitution", "store_finalize", "overflow", "driven"};
+
+cudaEvent_t next_event(NphGpuSolver *s)
+{
+    if (s->events_used == s->event_pool.size()) {
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        s->event_pool.push_back(e);
+    }
+    return s->event_pool[s->events_used++];
+}
+
+void mark_begin(NphGpuSolver *s, int kind, uint64_t units, double bytes)
+{
+    if (s->marks == nullptr) {
+        return;
+    }
+    NphGpuSolver::Mark m{kind, units, bytes, next_event(s), next_event(s)};
+    cudaEventRecord(m.a, s->stream);
+    s->marks->push_back(m);
+}
+
+void mark_end(NphGpuSolver *s)
+{
+    if (s->marks != nullptr) {
+        cudaEventRecord(s->marks->back().b, s->stream);
+    }
+}
+
+// Points per colour slot (filled by the last prepare), for the byte counts.
+uint64_t color_points(const NphGpuSolver *s, uint32_t c) { return s->h_err[1 + c]; }
+
+template <int P> void enqueue_pass(NphGpuSolver *s, const StepConsts &K)
+{
+    const DevSolver S = dev_solver(s);
+    const uint32_t o = NPH_GPU_OVERFLOW;
+    const uint32_t oj = P == kRestitution ? 0u : s->jcount[o];
+    const int kind = P == kWarm ? kKWarm : P == kSolve ? kKSolve : P == kRelax ? kKRelax : kKRestitution;
+    auto bytes = [&](uint32_t c, uint32_t jc) -> double {
+        const double m = s->ccount[c];
+        const double pts = s->marks != nullptr ? (double)color_points(s, c) : 4.0 * m;
+        switch (P) {
+        case kWarm: return 120.0 * pts + 330.0 * jc;
+        case kSolve: return 224.0 * m + 148.0 * pts + 330.0 * jc;
+        case kRelax: return 212.0 * m + 148.0 * pts + 330.0 * jc;
+        default: return 40.0 * m;
+        }
+    };
+    if (s->ccount[o] > 0u || oj > 0u) {
+        mark_begin(s, kKOverflow, (uint64_t)s->ccount[o] + oj, bytes(o, oj));
+        k_overflow<P><<<1, 32, 0, s->stream>>>(S, s->cfirst[o], s->ccount[o], s->jfirst[o], oj, K);
+        mark_end(s);
+        s->launches++;
+    }
+    for (uint32_t c = 0; c < NPH_GPU_COLORS; ++c) {
+        const uint32_t jc = P == kRestitution ? 0u : s->jcount[c];
+        const uint32_t cc = s->ccount[c];
+        if (jc == 0u && cc == 0u) {
+            continue;
+        }
+        const uint32_t jb = blocks_for(jc);
+        mark_begin(s, kind, (uint64_t)cc + jc, bytes(c, jc));
+        k_pass<P><<<jb + blocks_for(cc), kBlock, 0, s->stream>>>(S, s->cfirst[c], cc, s->jfirst[c], jc,
+                                                                 jb, K);
+        mark_end(s);
+        s->launches++;
+    }
+}
+
+// One step's launches on the solver's stream (the stage list, solver.c:1032-1067).
+void enqueue_step(NphGpuSolver *s, const StepConsts &K, uint32_t substeps)
+{
+    const DevSolver S = dev_solver(s);
+    const BodyArrays B = body_arrays(s);
+    const double n = s->n;
+    s->launches = 0;
+    mark_begin(s, kKPrepareBodies, s->n, 368.0 * n);
+    k_prepare_bodies<<<blocks_for(s->n + 1u), kBlock, 0, s->stream>>>(B, s->d_bodies, s->n, K);
+    mark_end(s);
+    s->launches++;
+    ColorTable T;
+    std::memcpy(T.cfirst, s->cfirst, sizeof T.cfirst);
+    std::memcpy(T.ccount, s->ccount, sizeof T.ccount);
+    const uint32_t jb = blocks_for(s->nj);
+    if (s->m + s->nj > 0u) {
+        cudaMemsetAsync(s->d_err + 1, 0, NPH_GPU_COLOR_SLOTS * sizeof(uint32_t), s->stream);
+        mark_begin(s, kKPrepareConstraints, (uint64_t)s->m + s->nj, 936.0 * s->m + 330.0 * s->nj);
+        k_prepare_constraints<<<jb + blocks_for(s->m), kBlock, 0, s->stream>>>(
+            S, s->d_contacts, s->d_joints, s->d_bodies, s->d_fixed, s->n, s->nf, s->m, s->nj, jb, T,
+            K.h, s->d_err, s->d_err + 1);
+        mark_end(s);
+        s->launches++;
+    }
+    for (uint32_t sub = 0; sub < substeps; ++sub) {
+        mark_begin(s, kKIntegrateVelocity, s->n, 84.0 * n);
+        k_integrate_velocity<<<blocks_for(s->n), kBlock, 0, s->stream>>>(B, s->n, K.h);
+        mark_end(s);
+        enqueue_pass<kWarm>(s, K);
+        enqueue_pass<kSolve>(s, K);
+        mark_begin(s, kKIntegratePosition, s->n, 84.0 * n);
+        k_integrate_position<<<blocks_for(s->n), kBlock, 0, s->stream>>>(B, s->n, K.h);
+        mark_end(s);
+        enqueue_pass<kRelax>(s, K);
+        s->launches += 2;
+    }
+    enqueue_pass<kRestitution>(s, K);
+    mark_begin(s, kKStoreFinalize, (uint64_t)s->m + s->nj + s->n, 160.0 * s->m + 330.0 * s->nj + 200.0 * n);
+    k_store_finalize<<<blocks_for((uint64_t)s->m + s->nj + s->n), kBlock, 0, s->stream>>>(
+        S, B, s->d_contacts, s->m, s->d_joints, s->nj, s->d_bodies, s->n, K.dt);
+    mark_end(s);
+    s->launches++;
+    if (s->driven > 0u) {
+        mark_begin(s, kKDriven, s->nj, 0.0);
+        k_driven<<<blocks_for(s->nj), kBlock, 0, s->stream>>>(S, s->d_bodies, s->n, s->nj);
+        mark_end(s);
+        s->launches++;
+    }
+}
+
+NphGpuResult check_cuda(cudaError_t e)
+{
+    if (e == cudaSuccess) {
+        return NPH_GPU_OK;
+    }
+    if (e == cudaErrorMemoryAllocation) {
+        return NPH_GPU_OUT_OF_MEMORY;
+    }
+    return NPH_GPU_DEVICE_LOST;
+}
+
+// Replays (capturing first if needed) one step as a graph, or launches it directly.
+NphGpuResult launch_step(NphGpuSolver *s, const StepConsts &K, uint32_t substeps)
+{
+    if (!s->use_graph) {
+        enqueue_step(s, K, substeps);
+        return check_cuda(cudaGetLastError());
+    }
+    if (!s->graph_valid || s->graph_substeps != substeps ||
+        std::memcmp(&s->graph_consts, &K, sizeof K) != 0) {
+        drop_graph(s);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) {
+            return check_cuda(e);
+        }
+        enqueue_step(s, K, substeps);
+        e = cudaStreamEndCapture(s->stream, &g);
+        if (e != cudaSuccess) {
+            return check_cuda(e);
+        }
+        e = cudaGraphInstantiate(&s->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            s->graph = nullptr;
+            return check_cuda(e);
+        }
+        s->graph_consts = K;
+        s->graph_substeps = substeps;
+        s->graph_valid = true;
+    }
+    return check_cuda(cudaGraphLaunch(s->graph, s->stream));
+}
+
+NphGpuResult validate_params(const NphGpuWorldParams *p, float dt)
+{
+    if (p == nullptr || !(dt > 0.0f) || p->substeps == 0u || p->substeps > 64u) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    if (p->solver != NPH_GPU_SOLVER_SOFT_STEP || p->enable_continuous != 0u) {
+        return NPH_GPU_UNSUPPORTED;
+    }
+    return NPH_GPU_OK;
+}
+
+NphGpuResult validate_view(const NphGpuWorldView *v)
+{
+    if (v == nullptr) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    uint64_t nc = 0, nj = 0;
+    for (uint32_t c = 0; c < NPH_GPU_COLOR_SLOTS; ++c) {
+        nc += v->contact_color_counts[c];
+        nj += v->joint_color_counts[c];
+    }
+    if (nc != v->contact_count || nj != v->joint_count) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    if ((v->body_count > 0 && v->bodies == nullptr) || (v->fixed_count > 0 && v->fixed_bodies == nullptr) ||
+        (v->contact_count > 0 && v->contacts == nullptr) || (v->joint_count > 0 && v->joints == nullptr)) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    if ((uint64_t)v->body_count + v->fixed_count >= 0xFFFFFFF0ull) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    return NPH_GPU_OK;
+}
+
+NphGpuResult upload(NphGpuSolver *s, const NphGpuWorldView *v)
+{
+    NphGpuResult r = validate_view(v);
+    if (r != NPH_GPU_OK) {
+        return r;
+    }
+    // The joint types first: a refused view leaves the solver as it was.
+    uint32_t driven = 0;
+    for (uint32_t j = 0; j < v->joint_count; ++j) {
+        const NphGpuJoint &jr = v->joints[j];
+        if (jr.type != NPH_GPU_JOINT_BALL && jr.type != NPH_GPU_JOINT_HINGE) {
+            return NPH_GPU_UNSUPPORTED;
+        }
+        driven += (jr.type == NPH_GPU_JOINT_HINGE && jr.u.hinge.enable_motor != 0u &&
+                   jr.u.hinge.motor_speed != 0.0f && jr.u.hinge.max_motor_torque > 0.0f)
+                      ? 1u
+                      : 0u;
+    }
+    r = ensure_capacity(s, v->body_count, v->fixed_count, v->contact_count, v->joint_count);
+    if (r != NPH_GPU_OK) {
+        return r;
+    }
+    const bool same_shape = s->uploaded && s->n == v->body_count && s->nf == v->fixed_count &&
+                            s->m == v->contact_count && s->nj == v->joint_count &&
+                            std::memcmp(s->ccount, v->contact_color_counts, sizeof s->ccount) == 0 &&
+                            std::memcmp(s->jcount, v->joint_color_counts, sizeof s->jcount) == 0;
+    s->n = v->body_count;
+    s->nf = v->fixed_count;
+    s->m = v->contact_count;
+    s->nj = v->joint_count;
+    uint32_t cf = 0, jf = 0;
+    for (uint32_t c = 0; c < NPH_GPU_COLOR_SLOTS; ++c) {
+        s->ccount[c] = v->contact_color_counts[c];
+        s->jcount[c] = v->joint_color_counts[c];
+        s->cfirst[c] = cf;
+        s->jfirst[c] = jf;
+        cf += s->ccount[c];
+        jf += s->jcount[c];
+    }
+    if (!same_shape || driven != s->driven) {
+        drop_graph(s);
+    }
+    s->driven = driven;
+    cudaMemcpyAsync(s->d_bodies, v->bodies, sizeof(NphGpuBody) * s->n, cudaMemcpyHostToDevice, s->stream);
+    if (s->nf > 0) {
+        cudaMemcpyAsync(s->d_fixed, v->fixed_bodies, sizeof(NphGpuBody) * s->nf, cudaMemcpyHostToDevice,
+                        s->stream);
+    }
+    if (s->m > 0) {
+        cudaMemcpyAsync(s->d_contacts, v->contacts, sizeof(NphGpuContact) * s->m, cudaMemcpyHostToDevice,
+                        s->stream);
+    }
+    if (s->nj > 0) {
+        cudaMemcpyAsync(s->d_joints, v->joints, sizeof(NphGpuJoint) * s->nj, cudaMemcpyHostToDevice,
+                        s->stream);
+    }
+    cudaMemsetAsync(s->d_err, 0, 32 * sizeof(uint32_t), s->stream);
+    s->uploaded = true;
+    return check_cuda(cudaGetLastError());
+}
+
+NphGpuResult download(NphGpuSolver *s, NphGpuWorldView *v)
+{
+    if (!s->uploaded || v == nullptr || v->body_count != s->n || v->contact_count != s->m ||
+        v->joint_count != s->nj) {
+        return NPH_GPU_INVALID_STATE;
+    }
+    cudaMemcpyAsync(v->bodies, s->d_bodies, sizeof(NphGpuBody) * s->n, cudaMemcpyDeviceToHost, s->stream);
+    if (s->m > 0) {
+        cudaMemcpyAsync(v->contacts, s->d_contacts, sizeof(NphGpuContact) * s->m, cudaMemcpyDeviceToHost,
+                        s->stream);
+    }
+    if (s->nj > 0) {
+        cudaMemcpyAsync(v->joints, s->d_joints, sizeof(NphGpuJoint) * s->nj, cudaMemcpyDeviceToHost,
+                        s->stream);
+    }
+    return check_cuda(cudaStreamSynchronize(s->stream));
+}
+
+NphGpuResult read_error(NphGpuSolver *s)
+{
+    cudaMemcpyAsync(s->h_err, s->d_err, 32 * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream);
+    const NphGpuResult r = check_cuda(cudaStreamSynchronize(s->stream));
+    if (r != NPH_GPU_OK) {
+        return r;
+    }
+    s->stats.error_word = *s->h_err;
+    return *s->h_err != 0u ? NPH_GPU_INVALID_ARGUMENT : NPH_GPU_OK;
+}
+
+void fill_stats(NphGpuSolver *s)
+{
+    uint32_t used = 0;
+    for (uint32_t c = 0; c < NPH_GPU_COLORS; ++c) {
+        used += (s->ccount[c] > 0u || s->jcount[c] > 0u) ? 1u : 0u;
+    }
+    s->stats.colors_used = used;
+    s->stats.overflow_contacts = s->ccount[NPH_GPU_OVERFLOW];
+    s->stats.overflow_joints = s->jcount[NPH_GPU_OVERFLOW];
+    s->stats.launches = s->launches;
+}
+
+} // namespace
+
+// ------------------------------------------------------------------------------------
+// The C ABI
+// ------------------------------------------------------------------------------------
+
+extern "C" {
+
+NPH_GPU_API NphGpuResult nph_gpu_solver_create(const NphGpuSolverDesc *desc, NphGpuSolver **out)
+{
+    if (out == nullptr) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    *out = nullptr;
+    NphGpuSolverDesc d{};
+    if (desc != nullptr) {
+        d = *desc;
+    } else {
+        d.use_graph = 1;
+    }
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return NPH_GPU_DEVICE_LOST;
+    }
+    if (d.device < 0 || d.device >= count) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    NphGpuSolver *s = new (std::nothrow) NphGpuSolver();
+    if (s == nullptr) {
+        return NPH_GPU_OUT_OF_MEMORY;
+    }
+    s->device = d.device;
+    s->use_graph = d.use_graph != 0u;
+    if (cudaSetDevice(d.device) != cudaSuccess) {
+        delete s;
+        return NPH_GPU_DEVICE_LOST;
+    }
+    if (d.stream != nullptr) {
+        s->stream = (cudaStream_t)d.stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete s;
+            return NPH_GPU_DEVICE_LOST;
+        }
+        s->own_stream = true;
+    }
+    bool ok = dalloc(s->d_err, 32) && cudaMallocHost((void **)&s->h_err, 32 * sizeof(uint32_t)) == cudaSuccess;
+    for (auto &e : s->ev) {
+        ok = ok && cudaEventCreate(&e) == cudaSuccess;
+    }
+    if (ok) {
+        ok = ensure_capacity(s, d.body_capacity, 0, d.contact_capacity, d.joint_capacity) == NPH_GPU_OK;
+    }
+    if (!ok) {
+        nph_gpu_solver_destroy(s);
+        return NPH_GPU_OUT_OF_MEMORY;
+    }
+    *out = s;
+    return NPH_GPU_OK;
+}
+
+NPH_GPU_API void nph_gpu_solver_destroy(NphGpuSolver *s)
+{
+    if (s == nullptr) {
+        return;
+    }
+    cudaSetDevice(s->device);
+    if (s->stream != nullptr) {
+        cudaStreamSynchronize(s->stream);
+    }
+    drop_graph(s);
+    dfree(s->d_bodies);
+    dfree(s->d_fixed);
+    dfree(s->d_contacts);
+    dfree(s->d_joints);
+    dfree(s->vel);
+    dfree(s->pos);
+    dfree(s->prm);
+    dfree(s->itg);
+    dfree(s->hdr);
+    dfree(s->nrm);
+    dfree(s->rest);
+    dfree(s->pa);
+    dfree(s->pb);
+    dfree(s->pt);
+    dfree(s->pi);
+    dfree(s->jw);
+    dfree(s->d_err);
+    if (s->h_err != nullptr) {
+        cudaFreeHost(s->h_err);
+    }
+    for (auto &e : s->ev) {
+        if (e != nullptr) {
+            cudaEventDestroy(e);
+        }
+    }
+    for (auto &e : s->event_pool) {
+        cudaEventDestroy(e);
+    }
+    if (s->own_stream && s->stream != nullptr) {
+        cudaStreamDestroy(s->stream);
+    }
+    delete s;
+}
+
+NPH_GPU_API NphGpuResult nph_gpu_world_upload(NphGpuSolver *s, const NphGpuWorldView *view)
+{
+    if (s == nullptr) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    cudaSetDevice(s->device);
+    NphGpuResult r = upload(s, view);
+    if (r == NPH_GPU_OK) {
+        r = check_cuda(cudaStreamSynchronize(s->stream));
+    }
+    return r;
+}
+
+NPH_GPU_API NphGpuResult nph_gpu_world_step_async(NphGpuSolver *s, const NphGpuWorldParams *params,
+                                                  float dt, uint32_t steps)
+{
+    if (s == nullptr) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    NphGpuResult r = validate_params(params, dt);
+    if (r != NPH_GPU_OK) {
+        return r;
+    }
+    if (!s->uploaded) {
+        return NPH_GPU_INVALID_STATE;
+    }
+    cudaSetDevice(s->device);
+    const StepConsts K = make_step_consts(*params, dt);
+    for (uint32_t i = 0; i < steps && r == NPH_GPU_OK; ++i) {
+        r = launch_step(s, K, params->substeps);
+    }
+    fill_stats(s);
+    return r;
+}
+
+NPH_GPU_API NphGpuResult nph_gpu_world_download(NphGpuSolver *s, NphGpuWorldView *view)
+{
+    if (s == nullptr) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    cudaSetDevice(s->device);
+    NphGpuResult r = read_error(s);
+    if (r != NPH_GPU_OK) {
+        return r;
+    }
+    return download(s, view);
+}
+
+NPH_GPU_API NphGpuResult nph_gpu_solver_synchronize(NphGpuSolver *s)
+{
+    if (s == nullptr) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    cudaSetDevice(s->device);
+    return check_cuda(cudaStreamSynchronize(s->stream));
+}
+
+NPH_GPU_API NphGpuResult nph_gpu_phys_solve(NphGpuSolver *s, const NphGpuWorldParams *params, float dt,
+                                            NphGpuWorldView *view)
+{
+    if (s == nullptr) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    NphGpuResult r = validate_params(params, dt);
+    if (r != NPH_GPU_OK) {
+        return r;
+    }
+    cudaSetDevice(s->device);
+    if (view != nullptr && view->body_count == 0u) {
+        return validate_view(view); // phys_solve with no awake body does nothing (solver.c:963-966)
+    }
+    cudaEventRecord(s->ev[0], s->stream);
+    r = upload(s, view);
+    if (r != NPH_GPU_OK) {
+        return r;
+    }
+    cudaEventRecord(s->ev[1], s->stream);
+    const StepConsts K = make_step_consts(*params, dt);
+    r = launch_step(s, K, params->substeps);
+    if (r != NPH_GPU_OK) {
+        return r;
+    }
+    cudaEventRecord(s->ev[2], s->stream);
+    r = read_error(s);
+    if (r != NPH_GPU_OK) {
+        return r; // the view is untouched: the step did not happen
+    }
+    cudaEventRecord(s->ev[3], s->stream);
+    r = download(s, view);
+    if (r != NPH_GPU_OK) {
+        return r;
+    }
+    cudaEventRecord(s->ev[4], s->stream);
+    cudaEventSynchronize(s->ev[4]);
+    cudaEventElapsedTime(&s->stats.upload_ms, s->ev[0], s->ev[1]);
+    cudaEventElapsedTime(&s->stats.device_ms, s->ev[1], s->ev[2]);
+    cudaEventElapsedTime(&s->stats.download_ms, s->ev[3], s->ev[4]);
+    fill_stats(s);
+    return NPH_GPU_OK;
+}
+
+NPH_GPU_API NphGpuResult nph_gpu_world_profile_step(NphGpuSolver *s, const NphGpuWorldParams *params,
+                                                    float dt, NphGpuKernelTime *out, uint32_t capacity,
+                                                    uint32_t *count)
+{
+    if (s == nullptr || out == nullptr || count == nullptr) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    NphGpuResult r = validate_params(params, dt);
+    if (r != NPH_GPU_OK) {
+        return r;
+    }
+    if (!s->uploaded) {
+        return NPH_GPU_INVALID_STATE;
+    }
+    cudaSetDevice(s->device);
+    // The points per colour of the last prepare: run one prepare's worth first when needed.
+    r = read_error(s);
+    if (r != NPH_GPU_OK) {
+        return r;
+    }
+    const StepConsts K = make_step_consts(*params, dt);
+    std::vector<NphGpuSolver::Mark> marks;
+    marks.reserve(1024);
+    s->marks = &marks;
+    s->events_used = 0;
+    enqueue_step(s, K, params->substeps);
+    s->marks = nullptr;
+    r = check_cuda(cudaStreamSynchronize(s->stream));
+    if (r != NPH_GPU_OK) {
+        return r;
+    }
+    NphGpuKernelTime kinds[kKinds];
+    std::memset(kinds, 0, sizeof kinds);
+    for (const auto &m : marks) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, m.a, m.b);
+        NphGpuKernelTime &k = kinds[m.kind];
+        k.launches += 1;
+        k.units += m.units;
+        k.total_ms += ms;
+        k.algorithmic_bytes += m.bytes;
+    }
+    uint32_t n = 0;
+    for (int k = 0; k < kKinds; ++k) {
+        if (kinds[k].launches == 0) {
+            continue;
+        }
+        if (n < capacity) {
+            out[n] = kinds[k];
+            std::strncpy(out[n].name, kKindNames[k], sizeof out[n].name - 1);
+        }
+        ++n;
+    }
+    *count = n < capacity ? n : capacity;
+    fill_stats(s);
+    return NPH_GPU_OK;
+}
+
+NPH_GPU_API NphGpuResult nph_gpu_solver_stats(const NphGpuSolver *s, NphGpuStepStats *out)
+{
+    if (s == nullptr || out == nullptr) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    *out = s->stats;
+    return NPH_GPU_OK;
+}
+
+NPH_GPU_API void *nph_gpu_solver_stream(const NphGpuSolver *s)
+{
+    return s != nullptr ? (void *)s->stream : nullptr;
+}
+
+NPH_GPU_API const char *nph_gpu_version(void)
+{
+    return "nepheline_b200 0.1.0 (sm_100a)";
+}
+
+} // extern "C"

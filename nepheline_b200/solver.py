@@ -1,0 +1,154 @@
+"""ctypes binding of the C ABI (include/nepheline_b200.h).
+
+Loads lib/libnepheline_b200.so and fails loudly when it is missing: there is no other
+implementation of the solver stage in this package.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+from . import abi
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "libnepheline_b200.so"
+_lib = None
+
+_u32 = ctypes.c_uint32
+_vp = ctypes.c_void_p
+
+
+class SolverError(RuntimeError):
+    def __init__(self, code: int, what: str):
+        super().__init__(f"{what}: {abi.RESULT_NAMES.get(code, code)}")
+        self.code = code
+
+
+def lib() -> ctypes.CDLL:
+    """The shared library, with its signatures declared."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with python -m nepheline_b200.build")
+    L = ctypes.CDLL(str(LIB_PATH))
+    P = ctypes.POINTER
+    sig = {
+        "nph_gpu_solver_create": (ctypes.c_int32, [P(abi.SolverDesc), P(_vp)]),
+        "nph_gpu_solver_destroy": (None, [_vp]),
+        "nph_gpu_phys_solve": (ctypes.c_int32, [_vp, P(abi.WorldParams), ctypes.c_float,
+                                                P(abi.WorldView)]),
+        "nph_gpu_world_upload": (ctypes.c_int32, [_vp, P(abi.WorldView)]),
+        "nph_gpu_world_step_async": (ctypes.c_int32, [_vp, P(abi.WorldParams), ctypes.c_float,
+                                                      _u32]),
+        "nph_gpu_world_download": (ctypes.c_int32, [_vp, P(abi.WorldView)]),
+        "nph_gpu_solver_synchronize": (ctypes.c_int32, [_vp]),
+        "nph_gpu_solver_stats": (ctypes.c_int32, [_vp, P(abi.StepStats)]),
+        "nph_gpu_solver_stream": (_vp, [_vp]),
+        "nph_gpu_graph_color": (ctypes.c_int32, [_vp, _vp, _vp, _vp, _u32, _u32, _vp, _vp]),
+        "nph_gpu_version": (ctypes.c_char_p, []),
+        "nph_gpu_world_profile_step": (ctypes.c_int32, [_vp, P(abi.WorldParams), ctypes.c_float,
+                                                        P(abi.KernelTime), _u32, P(_u32)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def _check(code: int, what: str):
+    if code != abi.OK:
+        raise SolverError(code, what)
+
+
+class Solver:
+    """One device solver (NphGpuSolver): owns its device buffers and stream."""
+
+    def __init__(self, device: int = 0, stream: int | None = None, use_graph: bool = True,
+                 body_capacity: int = 0, contact_capacity: int = 0, joint_capacity: int = 0):
+        L = lib()
+        d = abi.SolverDesc()
+        d.device = device
+        d.stream = stream
+        d.use_graph = 1 if use_graph else 0
+        d.body_capacity = body_capacity
+        d.contact_capacity = contact_capacity
+        d.joint_capacity = joint_capacity
+        h = _vp()
+        _check(L.nph_gpu_solver_create(ctypes.byref(d), ctypes.byref(h)), "nph_gpu_solver_create")
+        self._h = h
+        self.L = L
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.L.nph_gpu_solver_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self) -> int:
+        return int(self.L.nph_gpu_solver_stream(self._h) or 0)
+
+    def phys_solve(self, view: abi.View, params: abi.WorldParams, dt: float) -> None:
+        """The drop-in for phys_solve: solves `view` in place."""
+        cv = view.c_view()
+        _check(self.L.nph_gpu_phys_solve(self._h, ctypes.byref(params), dt, ctypes.byref(cv)),
+               "nph_gpu_phys_solve")
+
+    def phys_solve_code(self, view: abi.View, params: abi.WorldParams, dt: float) -> int:
+        cv = view.c_view()
+        return int(self.L.nph_gpu_phys_solve(self._h, ctypes.byref(params), dt, ctypes.byref(cv)))
+
+    def upload(self, view: abi.View) -> None:
+        cv = view.c_view()
+        _check(self.L.nph_gpu_world_upload(self._h, ctypes.byref(cv)), "nph_gpu_world_upload")
+
+    def step_async(self, params: abi.WorldParams, dt: float, steps: int = 1) -> None:
+        _check(self.L.nph_gpu_world_step_async(self._h, ctypes.byref(params), dt, steps),
+               "nph_gpu_world_step_async")
+
+    def download(self, view: abi.View) -> None:
+        cv = view.c_view()
+        _check(self.L.nph_gpu_world_download(self._h, ctypes.byref(cv)), "nph_gpu_world_download")
+
+    def synchronize(self) -> None:
+        _check(self.L.nph_gpu_solver_synchronize(self._h), "nph_gpu_solver_synchronize")
+
+    def stats(self) -> abi.StepStats:
+        st = abi.StepStats()
+        _check(self.L.nph_gpu_solver_stats(self._h, ctypes.byref(st)), "nph_gpu_solver_stats")
+        return st
+
+    def profile_step(self, params: abi.WorldParams, dt: float) -> list[dict]:
+        """One resident step with every launch timed (CUDA events), per kind of kernel."""
+        arr = (abi.KernelTime * 32)()
+        n = _u32()
+        _check(self.L.nph_gpu_world_profile_step(self._h, ctypes.byref(params), dt, arr, 32,
+                                                 ctypes.byref(n)), "nph_gpu_world_profile_step")
+        return [{"name": arr[i].name.decode(), "launches": arr[i].launches,
+                 "units": arr[i].units, "total_ms": arr[i].total_ms,
+                 "algorithmic_bytes": arr[i].algorithmic_bytes} for i in range(n.value)]
+
+    def graph_color(self, body_a, body_b, dynamic_bits, body_slots: int):
+        """Device colouring of constraints in insertion order (graph_pick_color)."""
+        a = np.ascontiguousarray(body_a, np.uint32)
+        b = np.ascontiguousarray(body_b, np.uint32)
+        d = np.ascontiguousarray(dynamic_bits, np.uint8)
+        color = np.zeros(len(a), np.uint32)
+        slot = np.zeros(len(a), np.uint32)
+        _check(self.L.nph_gpu_graph_color(self._h, a.ctypes.data, b.ctypes.data, d.ctypes.data,
+                                          len(a), body_slots, color.ctypes.data,
+                                          slot.ctypes.data), "nph_gpu_graph_color")
+        return color, slot
+
+
+def version() -> str:
+    return lib().nph_gpu_version().decode()

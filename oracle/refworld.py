@@ -279,7 +279,9 @@ def port32(view: abi.View, params: abi.WorldParams, dt: float) -> abi.View:
 
 
 def port32_result(view: abi.View, params: abi.WorldParams, dt: float) -> int:
-    cv = view.copy().c_view()
+    """The result code of an FP32 solve of a copy of `view`."""
+    work = view.copy()  # kept alive across the call: the C view points into its arrays
+    cv = work.c_view()
     return int(_port_lib().nph_port32_solve(ctypes.byref(params), dt, ctypes.byref(cv)))
 
 

@@ -1,0 +1,147 @@
+"""Scenes built in the reference engine (through the oracle harness) for the parity tests.
+
+Each builder returns a RefWorld whose full world step (pairs, narrow phase, solver, islands)
+is the reference's; the tests cut it at the solver stage (collide, export the view, solve
+both ways, compare, finish).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from nepheline_b200 import abi, scenes
+
+
+def pyramid(rows: int = 20, jitter: float = 1e-3, seed: int = 1, params=None, workers: int = 0):
+    """The box pyramid: row r holds rows - r unit boxes at x = (j - (n-1)/2) * 1.05,
+    y = 0.5 + r (benchmarks/physics/bench_physics.c:1233-1252), +-jitter in x and z, on a
+    static ground slab whose top is y = 0 (test_world_support.h:64-68)."""
+    from oracle.refworld import RefWorld
+    rng = np.random.default_rng(seed)
+    w = RefWorld(params or abi.WorldParams.default(), enable_sleep=False, workers=workers)
+    w.add_ground(0.0)
+    for row in range(rows):
+        n = rows - row
+        for j in range(n):
+            dx, dz = (rng.uniform(-jitter, jitter, 2) if jitter > 0 else (0.0, 0.0))
+            w.add_box(((j - (n - 1) / 2) * 1.05 + dx, 0.5 + row, dz))
+    return w
+
+
+def sphere_pour(count: int = 512, seed: int = 2, extent: float = 12.0, params=None,
+                workers: int = 0):
+    """Spheres of radius 0.5 with density U[500, 2000], friction U[0.2, 0.9], restitution
+    U[0, 0.3], at seeded non-overlapping lattice sites of a box above the ground."""
+    from oracle.refworld import RefWorld
+    rng = np.random.default_rng(seed)
+    w = RefWorld(params or abi.WorldParams.default(), enable_sleep=False, workers=workers)
+    w.add_ground(0.0, friction=0.6)
+    side = int(np.ceil(count ** (1.0 / 3.0)))
+    spacing = max(1.05, extent / side)
+    sites = np.stack(np.meshgrid(np.arange(side), np.arange(side), np.arange(side),
+                                 indexing="ij"), -1).reshape(-1, 3)[:count]
+    rng.shuffle(sites)
+    for s in sites:
+        p = (s - side / 2) * spacing
+        p[1] = 0.6 + s[1] * spacing
+        p[[0, 2]] += rng.uniform(-0.02, 0.02, 2)
+        w.add_sphere(tuple(p), 0.5, density=float(rng.uniform(500, 2000)),
+                     friction=float(rng.uniform(0.2, 0.9)),
+                     restitution=float(rng.uniform(0.0, 0.3)),
+                     velocity=tuple(rng.uniform(-1.0, 1.0, 3) + np.array([0, -2.0, 0])))
+    return w
+
+
+def box_pile(count: int = 60, seed: int = 3, params=None, workers: int = 0):
+    """Boxes of half extents U[0.2, 1.0] at random orientations dropped on the ground."""
+    from oracle.refworld import RefWorld
+    rng = np.random.default_rng(seed)
+    w = RefWorld(params or abi.WorldParams.default(), enable_sleep=False, workers=workers)
+    w.add_ground(0.0)
+    side = int(np.ceil(np.sqrt(count)))
+    for i in range(count):
+        half = rng.uniform(0.2, 1.0, 3)
+        q = rng.normal(size=4)
+        q /= np.linalg.norm(q)
+        x, z = (i % side) * 2.2 - side, (i // side) * 2.2 - side
+        w.add_box((x, 1.5 + 2.0 * (i % 3), z), half=tuple(half), rotation=tuple(q))
+    return w
+
+
+_S = 0.70710678
+
+
+def _qmul(a, b):
+    ax, ay, az, aw = a
+    bx, by, bz, bw = b
+    return (aw * bx + ax * bw + ay * bz - az * by, aw * by - ax * bz + ay * bw + az * bx,
+            aw * bz + ax * by - ay * bx + az * bw, aw * bw - ax * bx - ay * by - az * bz)
+
+
+_RZ90 = (0.0, 0.0, _S, _S)
+_RX90 = (_S, 0.0, 0.0, _S)
+
+
+def hinge_chain(links: int = 12, seed: int = 4, params=None, limits=True, motor=True, spring=True):
+    """A chain of capsules on hinge joints hanging from a static anchor, with limits, a motor
+    and a spring on alternating links, and a ball-jointed tail with a cone, twist limits and
+    friction: every ball and hinge row of the joint solver."""
+    from oracle.refworld import RefWorld
+    rng = np.random.default_rng(seed)
+    w = RefWorld(params or abi.WorldParams.default(), enable_sleep=False)
+    anchor = w.add_body(abi.BODY_STATIC, (0.0, 10.0, 0.0))
+    bodies = [anchor]
+    for i in range(links):
+        b = w.add_capsule((0.5 + i * 1.0, 10.0, 0.0), 0.25, 0.25, rotation=_RZ90,
+                          velocity=tuple(rng.uniform(-0.5, 0.5, 3)))
+        bodies.append(b)
+    joints = np.zeros(links, abi.JOINT_DTYPE)
+    for i in range(links):
+        j = joints[i]
+        ball = i >= links - 3
+        j["type"] = abi.JOINT_BALL if ball else abi.JOINT_HINGE
+        # Anchor at x = i (the previous link's end), frames with X along world z.
+        j["frame_a_position"] = (0.0, 0.0, 0.0) if i == 0 else (0.0, -0.5, 0.0)
+        j["frame_b_position"] = (0.0, 0.5, 0.0)
+        # Frame X along world z on both sides: link rotation Rz(90) times Rx(90) on a link,
+        # the product itself on the static anchor.
+        j["frame_a_rotation"] = _qmul(_RZ90, _RX90) if i == 0 else _RX90
+        j["frame_b_rotation"] = _RX90
+        if ball:
+            j["ball_enable_swing_limit"] = 1
+            j["ball_swing_y"] = 0.6
+            j["ball_swing_z"] = 0.4
+            j["ball_enable_twist_limit"] = 1
+            j["ball_twist_lower"] = -0.3
+            j["ball_twist_upper"] = 0.3
+            j["ball_friction_torque"] = 0.5
+        else:
+            if limits and i % 3 == 0:
+                j["hinge_enable_limit"] = 1
+                j["hinge_lower"] = -0.4
+                j["hinge_upper"] = 0.4
+            if motor and i % 3 == 1:
+                j["hinge_enable_motor"] = 1
+                j["hinge_motor_speed"] = 1.5
+                j["hinge_max_motor_torque"] = 20.0
+            if spring and i % 3 == 2:
+                j["hinge_enable_spring"] = 1
+                j["hinge_spring_hertz"] = 2.0
+                j["hinge_spring_damping_ratio"] = 0.3
+                j["hinge_spring_target"] = 0.2
+        j["body_a"] = bodies[i]
+        j["body_b"] = bodies[i + 1]
+    w.add_joints(joints)
+    return w
+
+
+def lattice(edge: int = 6, seed: int = 3, joint_fraction: float = 0.1, params=None,
+            workers: int = 0):
+    """The synthetic constraint graph in the reference: shapeless bodies, joints created,
+    manifolds injected in insertion order (coloured by the reference's phys_graph_add)."""
+    from oracle.refworld import RefWorld
+    sc = scenes.lattice_graph(edge, seed=seed, joint_fraction=joint_fraction)
+    w = RefWorld(params or abi.WorldParams.default(), enable_sleep=False, workers=workers)
+    w.add_shapeless_bodies(sc.bodies, sc.mass)
+    w.add_joints(sc.joints)
+    w.inject_contacts(sc.contacts)
+    return w, sc

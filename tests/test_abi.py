@@ -1,0 +1,60 @@
+"""The C ABI on the CPU: record layouts agree with the header, and the shared library loads
+and exports every entry point include/nepheline_b200.h declares (no device calls)."""
+from __future__ import annotations
+
+import re
+import subprocess
+from pathlib import Path
+
+import pytest
+
+from nepheline_b200 import abi
+
+ROOT = Path(__file__).resolve().parent.parent
+HEADER = ROOT / "include" / "nepheline_b200.h"
+
+
+def declared_entry_points() -> list[str]:
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"NPH_GPU_API\s+[\w\s\*]+?\b(nph_gpu_\w+)\s*\(", text)))
+
+
+def test_header_declares_the_entry_points():
+    names = declared_entry_points()
+    for n in ("nph_gpu_solver_create", "nph_gpu_phys_solve", "nph_gpu_graph_color",
+              "nph_gpu_world_upload", "nph_gpu_world_step_async", "nph_gpu_world_download"):
+        assert n in names
+
+
+def test_record_layouts_match_the_header(tmp_path):
+    src = tmp_path / "sizes.c"
+    src.write_text(
+        '#include <stdio.h>\n#include <stddef.h>\n#include "nepheline_b200.h"\n'
+        'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\\n",'
+        'sizeof(NphGpuBody),sizeof(NphGpuContactPoint),sizeof(NphGpuContact),'
+        'sizeof(NphGpuJoint),sizeof(NphGpuWorldParams),sizeof(NphGpuWorldView),'
+        'offsetof(NphGpuJoint,linear_impulse),offsetof(NphGpuContact,points),'
+        'sizeof(NphGpuKernelTime));return 0;}\n')
+    exe = tmp_path / "sizes"
+    subprocess.run(["gcc", f"-I{HEADER.parent}", str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True,
+                                          check=True).stdout.split()]
+    sz = abi.layout_sizes()
+    import ctypes
+    assert got == [sz["body"], sz["point"], sz["contact"], sz["joint"], sz["params"], sz["view"],
+                   abi.JOINT_DTYPE.fields["linear_impulse"][1],
+                   abi.CONTACT_DTYPE.fields["points"][1], ctypes.sizeof(abi.KernelTime)]
+
+
+def test_library_exports_every_declared_entry_point():
+    from nepheline_b200 import solver
+    if not solver.LIB_PATH.exists():
+        pytest.skip("library not built")
+    out = subprocess.run(["nm", "-D", "--defined-only", str(solver.LIB_PATH)],
+                         capture_output=True, text=True, check=True).stdout
+    exported = set(re.findall(r"\bT (nph_gpu_\w+)", out))
+    missing = [n for n in declared_entry_points() if n not in exported]
+    assert not missing, missing
+    lib = solver.lib()  # loads with its signatures, no device needed
+    assert "sm_100a" in solver.version()
+    del lib
