@@ -1,9 +1,11 @@
 #!/usr/bin/env python3
 """Throughput of the solver stage: contact-solves/s on the 1M-body synthetic constraint graph.
 
-Workload (the metric's configuration): a 128^3 lattice of unit boxes (1,048,576 dynamic
-bodies), one 4-point manifold per neighbour pair (6,242,304 manifolds), ball or hinge joints
-on 10 % of the pairs, soft step, 4 substeps, dt 1/60, seeded. A step is one whole solver
+Workload (the metric's configuration): a 128 x 128 x 64 lattice of unit boxes at 1 m spacing
+(exactly 1,048,576 dynamic bodies; the configuration's "128^3" would be 2,097,152, so the
+body count it names decides), one 4-point manifold per neighbour pair (3,112,960 manifolds),
+ball or hinge joints on 10 % of the pairs, soft step, 4 substeps, dt 1/60, seeded.
+--dims 128,128,128 runs the 2,097,152-body cube. A step is one whole solver
 stage (phys_solve) over the device-resident world: prepare, 4 x (integrate, warm start,
 solve, integrate, relax) over every colour, restitution, store, finalize. One contact-solve
 is one manifold in one solve or relax pass: 2 x substeps x manifolds per step.
@@ -45,7 +47,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="nepheline_b200")
-    ap.add_argument("--edge", type=int, default=128, help="lattice edge (128: 1,048,576 bodies)")
+    ap.add_argument("--dims", default="128,128,64",
+                    help="lattice bodies per axis (128,128,64: 1,048,576 bodies)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -143,9 +146,9 @@ def barrier(pg):
         pg.barrier()
 
 
-def build_view(edge: int, seed: int, solver):
+def build_view(dims, seed: int, solver):
     from nepheline_b200 import scenes
-    sc = scenes.lattice_graph(edge, seed=seed, joint_fraction=0.1)
+    sc = scenes.lattice_graph(dims, seed=seed, joint_fraction=0.1)
     a, b, d = sc.constraint_arrays()
     color, slot = solver.graph_color(a, b, d, len(sc.bodies))
     return sc, sc.to_view(color, slot)
@@ -171,13 +174,12 @@ def pinned_copy(view):
     return v
 
 
-def reference_sample(edge: int, steps: int, warmup: int, workers: int) -> dict:
-    """The reference's phys_solve on its job system over an edge^3 sample of the lattice."""
+def reference_sample(dims, steps: int, warmup: int, workers: int) -> dict:
+    """The reference's phys_solve on its job system over a dims lattice (the same scene)."""
     from nepheline_b200 import abi
-    from tests import ref_scenes
+    from oracle.refworld import lattice_world
     params = abi.WorldParams.default()
-    w, sc = ref_scenes.lattice(edge=edge, seed=0, joint_fraction=0.1, params=params,
-                               workers=workers)
+    w, sc = lattice_world(dims, seed=0, joint_fraction=0.1, params=params, workers=workers)
     for _ in range(warmup):
         w.solve(DT)
     t0 = time.perf_counter()
@@ -188,7 +190,7 @@ def reference_sample(edge: int, steps: int, warmup: int, workers: int) -> dict:
     manifolds = len(sc.contacts)
     w.close()
     return {"value": 8.0 * manifolds / sec, "ms_per_step": 1e3 * sec, "threads": threads,
-            "manifolds": manifolds, "bodies": len(sc.bodies), "edge": edge}
+            "manifolds": manifolds, "bodies": len(sc.bodies), "dims": tuple(dims)}
 
 
 def cpu_model() -> str:
@@ -211,30 +213,37 @@ def run_reference(args):
                           "oracle/_ref/libnphref.so was not built (reference sources absent)"}))
         return 0
     cores = os.cpu_count() or 1
-    # The full workload when the run fits a few minutes on this host, else a smaller lattice:
-    # about 0.6 s per step for 64^3 on 8 cores, scaling with the volume and the cores.
-    est = 0.6 * (args.edge / 64.0) ** 3 * (8.0 / cores)
-    edge = args.edge
-    while edge > 16 and est * (args.steps + args.warmup) > 150.0:
-        edge = int(edge * 0.8)
-        est = 0.6 * (edge / 64.0) ** 3 * (8.0 / cores)
-    r = reference_sample(edge, args.steps, args.warmup, workers=-1)
-    sample = (f"{edge}^3 lattice ({r['bodies']} bodies, {r['manifolds']} manifolds), "
-              f"{args.steps} timed steps after {args.warmup}; {cpu_model()}")
+    dims = [int(x) for x in args.dims.split(",")]
+    # The full workload when the run fits a few minutes on this host, else a thinner slab of
+    # the same lattice: about 0.6 s per step per 262,144 bodies on 8 cores.
+    def est(d):
+        return 0.6 * (d[0] * d[1] * d[2] / 262144.0) * (8.0 / cores)
+    sample = list(dims)
+    while sample[2] > 4 and est(sample) * (args.steps + args.warmup) > 150.0:
+        sample[2] = max(4, int(sample[2] * 0.75))
+    r = reference_sample(sample, args.steps, args.warmup, workers=-1)
+    sample_txt = (f"{sample[0]}x{sample[1]}x{sample[2]} lattice ({r['bodies']} bodies, "
+                  f"{r['manifolds']} manifolds), {args.steps} timed steps after {args.warmup}; "
+                  f"{cpu_model()}")
     out = {
         "impl": "reference", "metric": METRIC, "value": r["value"], "unit": UNIT,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "synthetic constraint graph, 128^3 lattice", "edge": args.edge,
-                   "sample_edge": edge, "substeps": 4, "dt": DT},
+        "config": {"workload": workload_name(dims), "dims": dims, "sample_dims": sample,
+                   "substeps": 4, "dt": DT},
         "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["threads"],
-                         "kind": "reference", "sample": sample},
+                         "kind": "reference", "sample": sample_txt},
         "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out))
     return 0
+
+
+def workload_name(dims) -> str:
+    n = dims[0] * dims[1] * dims[2]
+    return f"synthetic constraint graph, {dims[0]}x{dims[1]}x{dims[2]} lattice, {n} bodies"
 
 
 def main():
@@ -248,10 +257,13 @@ def main():
 
     rank, world, local, pg = dist_setup(args.gpus)
     torch.cuda.set_device(local)
-    stream = torch.cuda.current_stream()
-    solver = Solver(device=local, stream=stream.cuda_stream)
+    dims = [int(x) for x in args.dims.split(",")]
+    solver = Solver(device=local)
+    # The solver launches on its own stream: the events are recorded on that stream.
+    stream = torch.cuda.ExternalStream(solver.stream, device=local)
     params = abi.WorldParams.default()
-    sc, view = build_view(args.edge, seed=rank, solver=solver)
+    clk = Clocks(local).__enter__()
+    sc, view = build_view(dims, seed=rank, solver=solver)
     manifolds = len(view.contacts)
     solves_per_step = 2 * params.substeps * manifolds
 
@@ -262,12 +274,14 @@ def main():
     barrier(pg)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    with Clocks(local) as clk:
-        torch.cuda.synchronize()
-        e0.record(stream)
-        solver.step_async(params, DT, args.steps)
-        e1.record(stream)
-        torch.cuda.synchronize()
+    clk.lines.clear()  # keep only the samples of the timed region
+    torch.cuda.synchronize()
+    e0.record(stream)
+    solver.step_async(params, DT, args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = clk.summary()
+    clk.__exit__(None, None, None)
     ms = e0.elapsed_time(e1) / args.steps
     barrier(pg)
     ms = max_over_ranks(pg, ms)
@@ -327,10 +341,11 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import refworld
         if refworld.ref_available():
-            r = reference_sample(64, steps=8, warmup=1, workers=-1)
+            r = reference_sample((128, 128, 16), steps=8, warmup=1, workers=-1)
             cpu = {"value": r["value"], "unit": UNIT, "cores": r["threads"], "kind": "reference",
-                   "sample": f"64^3 lattice ({r['bodies']} bodies, {r['manifolds']} manifolds), "
-                             f"8 steps of the reference phys_solve on its job system; {cpu_model()}"}
+                   "sample": f"128x128x16 slab of the lattice ({r['bodies']} bodies, "
+                             f"{r['manifolds']} manifolds), 8 steps of the reference phys_solve "
+                             f"on its job system; {cpu_model()}"}
         else:
             from oracle.refworld import port32
             from nepheline_b200 import scenes
@@ -350,8 +365,7 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": "synthetic constraint graph, 128^3 lattice" if args.edge == 128
-                       else f"synthetic constraint graph, {args.edge}^3 lattice",
+            "config": {"workload": workload_name(dims),
                        "bodies": len(view.bodies), "manifolds": manifolds,
                        "joints": len(view.joints), "colors": view.colors_used, "substeps": 4,
                        "dt": DT, "parallelism": f"replicas x{world}",
@@ -361,7 +375,7 @@ def main():
             "gpu_launches": int(stats.launches) * args.steps,
             "roofline": roofline,
             "cpu_baseline": cpu,
-            "clocks": clk.summary(),
+            "clocks": clocks,
             "points_solved_per_s": value * 4,
             "kernels": {k: {"launches": v["launches"] // 3, "ms": v["total_ms"] / 3}
                         for k, v in kinds.items()},

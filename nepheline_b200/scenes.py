@@ -1,8 +1,8 @@
 """Seeded synthetic workloads for the solver stage, as world-view records.
 
-`lattice_graph` is the 1M-body synthetic constraint graph the solver is benchmarked on
-(a 128^3 lattice of unit boxes at 1 m spacing, one 4-point manifold per neighbour pair,
-an extra 10 % of the pairs jointed), at any edge length. It returns the bodies, and the
+`lattice_graph` is the synthetic constraint graph the solver is benchmarked on (a lattice
+of unit boxes at 1 m spacing, one 4-point manifold per neighbour pair, an extra 10 % of the
+pairs jointed; 128 x 128 x 64 is the 1,048,576-body configuration), at any size. It returns the bodies, and the
 constraints in their insertion order (joints, then contacts, each in lexicographic pair
 order: x-axis pairs, then y, then z), with body fields that are body indices. The same
 scene feeds the reference solver (bodies created and manifolds injected in that order)
@@ -123,9 +123,11 @@ class SolverScene:
         return abi.View(self.bodies.copy(), self.fixed, contacts, joints, ccounts, jcounts)
 
 
-def lattice_graph(edge: int = 128, seed: int = 0, joint_fraction: float = 0.1,
-                  max_tilt_deg: float = 5.0, max_penetration: float = 0.02) -> SolverScene:
-    """The synthetic constraint graph: an edge^3 lattice of unit boxes at 1 m spacing.
+def lattice_graph(edge: int | tuple[int, int, int] = 128, seed: int = 0,
+                  joint_fraction: float = 0.1, max_tilt_deg: float = 5.0,
+                  max_penetration: float = 0.02) -> SolverScene:
+    """The synthetic constraint graph: a lattice of unit boxes at 1 m spacing, `edge` bodies
+    along each axis (or (nx, ny, nz)).
 
     Mass log-uniform in 0.1-100 kg, unit-box inertia scaled by mass (m/6, isotropic). Each
     6-neighbour pair carries one 4-point manifold: normal the lattice axis tilted by up to
@@ -135,12 +137,12 @@ def lattice_graph(edge: int = 128, seed: int = 0, joint_fraction: float = 0.1,
     centre. Bodies start at rest with zero warm-start impulses.
     """
     rng = np.random.default_rng(seed)
-    n = edge
-    nb = n ** 3
+    nx, ny, nz = (edge, edge, edge) if isinstance(edge, int) else tuple(edge)
+    nb = nx * ny * nz
     idx = np.arange(nb, dtype=np.int64)
-    x = idx % n
-    y = (idx // n) % n
-    z = idx // (n * n)
+    x = idx % nx
+    y = (idx // nx) % ny
+    z = idx // (nx * ny)
     bodies = body_records(nb)
     bodies["center"][:, 0] = x
     bodies["center"][:, 1] = y
@@ -156,9 +158,10 @@ def lattice_graph(edge: int = 128, seed: int = 0, joint_fraction: float = 0.1,
 
     pairs_a, pairs_b, axes = [], [], []
     coords = (x, y, z)
-    strides = (1, n, n * n)
+    dims = (nx, ny, nz)
+    strides = (1, nx, nx * ny)
     for axis in range(3):
-        sel = idx[coords[axis] < n - 1]
+        sel = idx[coords[axis] < dims[axis] - 1]
         pairs_a.append(sel)
         pairs_b.append(sel + strides[axis])
         axes.append(np.full(len(sel), axis, np.int64))

@@ -317,3 +317,15 @@ def port_graph_color(body_a, body_b, dynamic_bits, body_slots) -> tuple[np.ndarr
     if r != 0:
         raise RuntimeError("port colouring failed")
     return color, slot
+
+
+def lattice_world(dims, seed: int = 0, joint_fraction: float = 0.1, params=None, workers: int = 0):
+    """The synthetic constraint graph in the reference: shapeless bodies created, joints made,
+    manifolds injected in insertion order (coloured by the reference's phys_graph_add)."""
+    from nepheline_b200 import scenes
+    sc = scenes.lattice_graph(dims, seed=seed, joint_fraction=joint_fraction)
+    w = RefWorld(params or abi.WorldParams.default(), enable_sleep=False, workers=workers)
+    w.add_shapeless_bodies(sc.bodies, sc.mass)
+    w.add_joints(sc.joints)
+    w.inject_contacts(sc.contacts)
+    return w, sc

@@ -138,10 +138,6 @@ def lattice(edge: int = 6, seed: int = 3, joint_fraction: float = 0.1, params=No
             workers: int = 0):
     """The synthetic constraint graph in the reference: shapeless bodies, joints created,
     manifolds injected in insertion order (coloured by the reference's phys_graph_add)."""
-    from oracle.refworld import RefWorld
-    sc = scenes.lattice_graph(edge, seed=seed, joint_fraction=joint_fraction)
-    w = RefWorld(params or abi.WorldParams.default(), enable_sleep=False, workers=workers)
-    w.add_shapeless_bodies(sc.bodies, sc.mass)
-    w.add_joints(sc.joints)
-    w.inject_contacts(sc.contacts)
-    return w, sc
+    from oracle.refworld import lattice_world
+    return lattice_world(edge, seed=seed, joint_fraction=joint_fraction, params=params,
+                         workers=workers)
