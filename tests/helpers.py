@@ -66,3 +66,17 @@ def max_rel_err(a: abi.View, b: abi.View, floor: float = 1e-6) -> dict:
             continue
         out[k] = float(np.max(np.abs(x - y) / np.maximum(np.abs(y), floor)))
     return out
+
+
+def max_normwise_err(a: abi.View, b: abi.View) -> dict:
+    """Per field, max |a - b| over the field's largest magnitude in b (relative to the
+    field's scale: the error measure of rows whose angle goes through atan2f)."""
+    fa, fb = _fields(a), _fields(b)
+    out = {}
+    for k in fa:
+        x, y = np.asarray(fa[k], np.float64), np.asarray(fb[k], np.float64)
+        if x.size == 0:
+            continue
+        scale = np.max(np.abs(y))
+        out[k] = float(np.max(np.abs(x - y)) / scale) if scale > 0 else float(np.max(np.abs(x)))
+    return out

@@ -4,8 +4,10 @@ Every scene is cut at the solver stage: the reference's world exports the solver
 view; the device solves a copy through nph_gpu_phys_solve; the reference's own phys_solve
 (or the CPU restatement pinned to it) solves the same input. Outputs must agree value for
 value (IEEE equality, so +0 and -0 are equal), except the joint rows whose angle goes
-through atan2f, which agree within 1e-5 relative (the device's atan2f is not the host C
-library's).
+through atan2f (hinge limits and springs, ball cones and twists), which agree within 1e-5 of
+each field's scale: the device's atan2f is not the host C library's (glibc 2.39's atan2f is
+not correctly rounded either: it differs from the correctly rounded value in about a fifth of
+random inputs), so one step's angle may differ in its last bit.
 """
 from __future__ import annotations
 
@@ -43,7 +45,7 @@ def cut_and_compare(solver, w, steps, params, dt=DT, every=1, exact=True):
             assert not bad, f"step {s}: {bad}"
             worst_bits = min(worst_bits, helpers.bitwise_fraction(dev, ref))
         else:
-            err = helpers.max_rel_err(dev, ref, floor=1e-3)
+            err = helpers.max_normwise_err(dev, ref)
             assert max(err.values()) < ANGLE_TOL, f"step {s}: {err}"
     return worst_bits
 
