@@ -64,6 +64,7 @@ typedef int32_t NphGpuResult;
 #define NPH_GPU_OK 0
 #define NPH_GPU_OUT_OF_MEMORY 1
 #define NPH_GPU_INVALID_ARGUMENT 2
+#define NPH_GPU_TOO_LARGE 7 /* NPH_RESULT_OVERFLOW: beyond a fixed capacity */
 #define NPH_GPU_UNSUPPORTED 8
 #define NPH_GPU_DEVICE_LOST 17
 #define NPH_GPU_INVALID_STATE 18
@@ -343,6 +344,27 @@ NPH_GPU_API NphGpuResult nph_gpu_graph_color(NphGpuSolver *solver, const uint32_
                                              const uint32_t *body_b, const uint8_t *dynamic_bits,
                                              uint32_t count, uint32_t body_slots,
                                              uint32_t *out_color, uint32_t *out_slot);
+
+/* The same colouring without allocating anything: no counterpart in the reference. For
+ * callers that may not allocate device memory while they run (an engine that reserves its
+ * memory up front, a fixed per-frame budget, an allocator owned by another runtime). Its
+ * scratch is one fixed device array of NPH_GPU_GRAPH_COLOR_STATIC_SCRATCH_BYTES that every
+ * GPU loading this library holds until exit; inputs and outputs are the caller's host
+ * arrays, as in nph_gpu_graph_color. At most NPH_GPU_GRAPH_COLOR_STATIC_MAX_CONSTRAINTS
+ * constraints over NPH_GPU_GRAPH_COLOR_STATIC_MAX_BODY_SLOTS body slots: larger inputs
+ * return NPH_GPU_TOO_LARGE. Runs on the current device, on `stream` (a cudaStream_t, NULL for
+ * the default stream). The first call on a device looks the array's address up and should
+ * come before any stream capture. All calls share the one array: calls that overlap on the
+ * GPU (other threads, other streams of the device) race and must be serialised by the
+ * caller. The result equals nph_gpu_graph_color's. */
+#define NPH_GPU_GRAPH_COLOR_STATIC_MAX_CONSTRAINTS 131072u
+#define NPH_GPU_GRAPH_COLOR_STATIC_MAX_BODY_SLOTS 131072u
+#define NPH_GPU_GRAPH_COLOR_STATIC_SCRATCH_BYTES (8u << 20)
+NPH_GPU_API NphGpuResult nph_gpu_graph_color_static(void *stream, const uint32_t *body_a,
+                                                    const uint32_t *body_b,
+                                                    const uint8_t *dynamic_bits, uint32_t count,
+                                                    uint32_t body_slots, uint32_t *out_color,
+                                                    uint32_t *out_slot);
 
 /* ------------------------------------------------------------------------------------
  * Version

@@ -25,6 +25,7 @@
 
 #include <cub/cub.cuh>
 
+#include <atomic>
 #include <cstdint>
 #include <cstring>
 #include <new>
@@ -299,6 +300,187 @@ NPH_GPU_API NphGpuResult nph_gpu_graph_color(NphGpuSolver *solver, const uint32_
     }
     cudaFree(base);
     return result;
+}
+
+} // extern "C"
+
+// ------------------------------------------------------------------------------------
+// The colouring without allocation
+//
+// For callers that may not allocate device memory once they run: an engine that reserves
+// all of its device memory up front, a frame loop with a fixed memory budget, a process
+// whose allocator is owned by another runtime, code recorded into work that must not
+// allocate. The scratch the colouring needs lives in one file-scope device array of fixed
+// size, which every GPU that loads this library holds until the process exits. The host
+// cannot use the array's name as a device address (in host code it names a host-side
+// stand-in), so the first call on each device asks the runtime for the address once, with
+// that device current, and keeps it.
+// ------------------------------------------------------------------------------------
+
+namespace {
+
+constexpr uint32_t kStaticMaxConstraints = NPH_GPU_GRAPH_COLOR_STATIC_MAX_CONSTRAINTS;
+constexpr uint32_t kStaticMaxBodySlots = NPH_GPU_GRAPH_COLOR_STATIC_MAX_BODY_SLOTS;
+constexpr size_t kStaticScratchBytes = (size_t)NPH_GPU_GRAPH_COLOR_STATIC_SCRATCH_BYTES;
+constexpr int kMaxDevices = 64;
+
+__device__ __align__(256) unsigned char g_color_scratch[kStaticScratchBytes];
+
+struct StaticScratch {
+    std::atomic<int> state[kMaxDevices]; // 0 unset, 1 being set, 2 set
+    void *ptr[kMaxDevices];
+};
+StaticScratch g_static;
+
+// The device address of g_color_scratch on the current device (first call: looked up).
+NphGpuResult static_scratch(int device, unsigned char **out)
+{
+    if (device < 0 || device >= kMaxDevices) {
+        return NPH_GPU_UNSUPPORTED;
+    }
+    int expected = 0;
+    if (g_static.state[device].compare_exchange_strong(expected, 1)) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_color_scratch);
+        if (e != cudaSuccess || p == nullptr) {
+            cudaGetLastError();
+            g_static.state[device].store(0);
+            return NPH_GPU_DEVICE_LOST;
+        }
+        g_static.ptr[device] = p;
+        g_static.state[device].store(2);
+    }
+    while (g_static.state[device].load() != 2) {
+        if (g_static.state[device].load() == 0) {
+            return NPH_GPU_DEVICE_LOST; // another thread's lookup failed
+        }
+    }
+    *out = (unsigned char *)g_static.ptr[device];
+    return NPH_GPU_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+NPH_GPU_API NphGpuResult nph_gpu_graph_color_static(void *stream, const uint32_t *body_a,
+                                                    const uint32_t *body_b,
+                                                    const uint8_t *dynamic_bits, uint32_t count,
+                                                    uint32_t body_slots, uint32_t *out_color,
+                                                    uint32_t *out_slot)
+{
+    if (count > 0 && (body_a == nullptr || body_b == nullptr || dynamic_bits == nullptr ||
+                      out_color == nullptr || out_slot == nullptr)) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    if (count > kStaticMaxConstraints || body_slots > kStaticMaxBodySlots) {
+        return NPH_GPU_TOO_LARGE;
+    }
+    if (count == 0) {
+        return NPH_GPU_OK;
+    }
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) {
+        cudaGetLastError();
+        return NPH_GPU_DEVICE_LOST;
+    }
+    unsigned char *base = nullptr;
+    NphGpuResult result = static_scratch(device, &base);
+    if (result != NPH_GPU_OK) {
+        return result;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    // The sort's and the scan's temporary storage, for these sizes, must fit what is left.
+    size_t sort_bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (const uint8_t *)nullptr, (uint8_t *)nullptr,
+                                    (const uint32_t *)nullptr, (uint32_t *)nullptr, (int)count, 0, 6);
+    size_t scan_bytes = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (const uint32_t *)nullptr, (uint32_t *)nullptr,
+                                  (int)body_slots + 1);
+    const size_t n = count;
+    const size_t slots = (size_t)body_slots + 1u;
+    char *cur = (char *)base;
+    uint32_t *d_a = carve<uint32_t>(cur, n);
+    uint32_t *d_b = carve<uint32_t>(cur, n);
+    uint32_t *d_color = carve<uint32_t>(cur, n);
+    uint32_t *d_slot = carve<uint32_t>(cur, n);
+    uint8_t *d_dyn = carve<uint8_t>(cur, n);
+    uint8_t *c0 = carve<uint8_t>(cur, n);
+    uint8_t *c1 = carve<uint8_t>(cur, n);
+    uint8_t *keys = carve<uint8_t>(cur, n);
+    uint8_t *keys_sorted = carve<uint8_t>(cur, n);
+    uint32_t *index = carve<uint32_t>(cur, n);
+    uint32_t *index_sorted = carve<uint32_t>(cur, n);
+    uint32_t *degree = carve<uint32_t>(cur, slots);
+    uint32_t *offsets = carve<uint32_t>(cur, slots);
+    uint32_t *cursor = carve<uint32_t>(cur, slots);
+    uint32_t *incident = carve<uint32_t>(cur, 2 * n);
+    uint32_t *counters = carve<uint32_t>(cur, 64);
+    void *sort_tmp = carve<char>(cur, sort_bytes);
+    void *scan_tmp = carve<char>(cur, scan_bytes);
+    if ((size_t)(cur - (char *)base) > kStaticScratchBytes) {
+        return NPH_GPU_TOO_LARGE;
+    }
+
+    // The array keeps the last call's contents: what must start at zero is cleared here.
+    uint32_t host_counters[2] = {0, 0};
+    cudaMemcpyAsync(d_a, body_a, n * 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d_b, body_b, n * 4, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(d_dyn, dynamic_bits, n, cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(degree, 0, slots * 4, st);
+    cudaMemsetAsync(counters, 0, 64 * 4, st);
+    k_check_and_count<<<blocks_for(n), kBlock, 0, st>>>(d_a, d_b, d_dyn, count, body_slots, degree,
+                                                        counters);
+    cub::DeviceScan::ExclusiveSum(scan_tmp, scan_bytes, degree, offsets, (int)body_slots + 1, st);
+    cudaMemcpyAsync(cursor, offsets, slots * 4, cudaMemcpyDeviceToDevice, st);
+    cudaMemcpyAsync(&host_counters[0], counters, 4, cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) {
+        cudaGetLastError();
+        return NPH_GPU_DEVICE_LOST;
+    }
+    if (host_counters[0] != 0u) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    k_fill<<<blocks_for(n), kBlock, 0, st>>>(d_a, d_b, d_dyn, count, cursor, incident);
+    cudaMemsetAsync(c0, kOverflow, n, st);
+    uint8_t *in = c0;
+    uint8_t *out = c1;
+    uint64_t rounds = 0;
+    for (;;) {
+        cudaMemsetAsync(counters + 1, 0, 4, st);
+        for (uint32_t r = 0; r < kRoundsPerCheck; ++r) {
+            k_round<<<blocks_for(n), kBlock, 0, st>>>(d_a, d_b, d_dyn, count, offsets, incident, in, out,
+                                                     counters + 1);
+            uint8_t *t = in;
+            in = out;
+            out = t;
+        }
+        rounds += kRoundsPerCheck;
+        cudaMemcpyAsync(&host_counters[1], counters + 1, 4, cudaMemcpyDeviceToHost, st);
+        if (cudaStreamSynchronize(st) != cudaSuccess) {
+            cudaGetLastError();
+            return NPH_GPU_DEVICE_LOST;
+        }
+        if (host_counters[1] == 0u) {
+            break;
+        }
+        if (rounds > (uint64_t)count + 2u * kRoundsPerCheck) {
+            return NPH_GPU_UNKNOWN;
+        }
+    }
+    uint32_t *buckets = counters + 2;
+    k_keys<<<blocks_for(n), kBlock, 0, st>>>(in, d_dyn, count, keys, index, buckets);
+    cub::DeviceRadixSort::SortPairs(sort_tmp, sort_bytes, keys, keys_sorted, index, index_sorted,
+                                    (int)count, 0, 6, st);
+    k_slots<<<blocks_for(n), kBlock, 0, st>>>(keys_sorted, index_sorted, count, buckets, in, d_color,
+                                              d_slot);
+    cudaMemcpyAsync(out_color, d_color, n * 4, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(out_slot, d_slot, n * 4, cudaMemcpyDeviceToHost, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) {
+        cudaGetLastError();
+        return NPH_GPU_DEVICE_LOST;
+    }
+    return NPH_GPU_OK;
 }
 
 } // extern "C"
