@@ -267,8 +267,9 @@ def main():
     manifolds = len(view.contacts)
     solves_per_step = 2 * params.substeps * manifolds
 
-    # Device-resident steps.
+    # Device-resident steps: the autotuner's timed steps, then the warm-up.
     solver.upload(view)
+    tuned = solver.autotune(params, DT, rounds=1)
     solver.step_async(params, DT, args.warmup)
     torch.cuda.synchronize()
     barrier(pg)
@@ -369,6 +370,7 @@ def main():
                        "bodies": len(view.bodies), "manifolds": manifolds,
                        "joints": len(view.joints), "colors": view.colors_used, "substeps": 4,
                        "dt": DT, "parallelism": f"replicas x{world}",
+                       "pass_configs": tuned,
                        "l2": "inputs larger than L2 (about 2 GB of manifold rows per step)"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms},

@@ -326,6 +326,82 @@ NPH_GPU_API NphGpuResult nph_gpu_world_profile_step(NphGpuSolver *solver,
                                                     NphGpuKernelTime *out, uint32_t capacity,
                                                     uint32_t *count);
 
+/* The constraint passes' launch configuration (threads per block and register budget), per
+ * pass kind: 0 warm start, 1 solve, 2 relax, 3 restitution; `config` below
+ * nph_gpu_pass_config_count(). Results do not depend on it. */
+NPH_GPU_API NphGpuResult nph_gpu_solver_set_pass_config(NphGpuSolver *solver, uint32_t pass,
+                                                        uint32_t config);
+NPH_GPU_API uint32_t nph_gpu_pass_config_count(void);
+
+/* The autotuner: times every pass configuration on the uploaded world (`rounds` timed steps
+ * each, after one untimed step) and keeps the fastest per pass kind, written to chosen[4]
+ * when not NULL. Each timed step is a real step: the world advances. */
+NPH_GPU_API NphGpuResult nph_gpu_solver_autotune(NphGpuSolver *solver,
+                                                 const NphGpuWorldParams *params, float dt,
+                                                 uint32_t rounds, uint32_t *chosen);
+
+/* ------------------------------------------------------------------------------------
+ * Batched worlds: many independent worlds of uneven size in one persistent launch
+ * ---------------------------------------------------------------------------------------
+ * The reference steps one world per nph_physics_world_step; this steps a batch of worlds
+ * with the same settings, each as phys_solve would, in one kernel launch per step: each
+ * block takes a whole world at a time from a queue sorted by size and runs its stage list
+ * with block barriers between stages and colours. A world solved in a batch gives the same
+ * bits as the world solved alone by nph_gpu_phys_solve. */
+
+typedef struct NphGpuBatch NphGpuBatch;
+
+/* What the batch autotuner chose. */
+typedef struct NphGpuBatchTuning {
+    uint32_t config;            /* below nph_gpu_batch_config_count() */
+    uint32_t threads;           /* threads per block */
+    uint32_t shared_velocities; /* 1: a world's body velocities in shared memory */
+    float ms_per_step;
+} NphGpuBatchTuning;
+
+typedef struct NphGpuBatchInfo {
+    uint32_t worlds;
+    uint32_t config;
+    uint64_t bodies;
+    uint64_t manifolds;
+    uint64_t joints;
+    uint32_t threads;
+    uint32_t shared_velocities;
+    uint32_t blocks_per_sm;
+    uint32_t pad;
+} NphGpuBatchInfo;
+
+NPH_GPU_API NphGpuResult nph_gpu_batch_create(const NphGpuSolverDesc *desc, NphGpuBatch **out);
+NPH_GPU_API void nph_gpu_batch_destroy(NphGpuBatch *batch);
+NPH_GPU_API void *nph_gpu_batch_stream(const NphGpuBatch *batch);
+/* Uploads `count` world views (device arrays sized to the batch). Refuses as
+ * nph_gpu_phys_solve does. */
+NPH_GPU_API NphGpuResult nph_gpu_batch_upload(NphGpuBatch *batch, const NphGpuWorldView *worlds,
+                                              uint32_t count);
+/* `steps` steps of every uploaded world, enqueued on the batch's stream (one CUDA graph launch
+ * per step). */
+NPH_GPU_API NphGpuResult nph_gpu_batch_step_async(NphGpuBatch *batch,
+                                                  const NphGpuWorldParams *params, float dt,
+                                                  uint32_t steps);
+/* Writes every world's results back into its view (the same views, in the same order). */
+NPH_GPU_API NphGpuResult nph_gpu_batch_download(NphGpuBatch *batch, NphGpuWorldView *worlds,
+                                                uint32_t count);
+/* Upload, one step, download: phys_solve for each of `count` worlds. */
+NPH_GPU_API NphGpuResult nph_gpu_phys_solve_worlds(NphGpuBatch *batch,
+                                                   const NphGpuWorldParams *params, float dt,
+                                                   NphGpuWorldView *worlds, uint32_t count);
+/* The launch configuration (threads per block) and whether velocities live in shared memory.
+ * Results do not depend on either. */
+NPH_GPU_API NphGpuResult nph_gpu_batch_set_config(NphGpuBatch *batch, uint32_t config,
+                                                  uint32_t shared_velocities);
+NPH_GPU_API uint32_t nph_gpu_batch_config_count(void);
+/* The batch autotuner: times every configuration on the uploaded worlds (`rounds` timed steps
+ * each after an untimed one; the worlds advance) and keeps the fastest. */
+NPH_GPU_API NphGpuResult nph_gpu_batch_autotune(NphGpuBatch *batch,
+                                                const NphGpuWorldParams *params, float dt,
+                                                uint32_t rounds, NphGpuBatchTuning *out);
+NPH_GPU_API NphGpuResult nph_gpu_batch_info(const NphGpuBatch *batch, NphGpuBatchInfo *out);
+
 /* ------------------------------------------------------------------------------------
  * The constraint graph's colouring on the device
  * ---------------------------------------------------------------------------------- */

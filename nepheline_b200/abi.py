@@ -179,6 +179,19 @@ class KernelTime(ctypes.Structure):
     ]
 
 
+class BatchTuning(ctypes.Structure):
+    _fields_ = [("config", ctypes.c_uint32), ("threads", ctypes.c_uint32),
+                ("shared_velocities", ctypes.c_uint32), ("ms_per_step", ctypes.c_float)]
+
+
+class BatchInfo(ctypes.Structure):
+    _fields_ = [("worlds", ctypes.c_uint32), ("config", ctypes.c_uint32),
+                ("bodies", ctypes.c_uint64), ("manifolds", ctypes.c_uint64),
+                ("joints", ctypes.c_uint64), ("threads", ctypes.c_uint32),
+                ("shared_velocities", ctypes.c_uint32), ("blocks_per_sm", ctypes.c_uint32),
+                ("pad", ctypes.c_uint32)]
+
+
 class SolverDesc(ctypes.Structure):
     _fields_ = [
         ("device", ctypes.c_int32), ("stream", ctypes.c_void_p), ("use_graph", ctypes.c_uint32),

@@ -10,6 +10,7 @@
 //   0 linear_accel.xyz, linear_damping      1 angular_accel.xyz, angular_damping
 //   2 q0 (the rotation at the step's start)  3 inertia_local c0, max_angular_speed_sq
 //   4 inertia_local c1, max_linear_speed_sq 5 inertia_local c2, flags | locks << 8
+// and prm[3i + 1].w is 1 for a dynamic body (the constraints' prepare reads it there).
 #pragma once
 
 #include "layout.cuh"
@@ -95,7 +96,7 @@ NPH_D void prepare_body(const BodyArrays &B, uint32_t i, const NphGpuBody &b, co
         inv_mass = b.inv_mass;
     }
     B.prm[3u * i + 0u] = f4(ii.c0, inv_mass);
-    B.prm[3u * i + 1u] = f4(ii.c1, 0.f);
+    B.prm[3u * i + 1u] = f4(ii.c1, (flags & kParamDynamic) != 0u ? 1.f : 0.f);
     B.prm[3u * i + 2u] = f4(ii.c2, 0.f);
     B.itg[6u * i + 0u] = f4(la, ld);
     B.itg[6u * i + 1u] = f4(aa, ad);

@@ -95,16 +95,13 @@ NPH_D Sides load_sides(const float4 *prm, uint32_t ia, uint32_t ib, uint32_t bit
 // Prepare: prepare_group (solver.c:394-473) and the prepare kernel (solver_impl.h:276-385)
 // ---------------------------------------------------------------------------------------
 
-// `c` is the manifold's record; `rec_a`/`rec_b` its bodies' records; `ia`/`ib` their solver
-// slots (the dummy for bodies without one). Writes the manifold's rows at lane g.
-NPH_D void prepare_manifold(const DevSolver &S, uint32_t g, const NphGpuContact &c,
-                            const NphGpuBody &rec_a, const NphGpuBody &rec_b, uint32_t ia,
-                            uint32_t ib, uint32_t group_points)
+// `c` is the manifold's record; `ia`/`ib` its bodies' solver slots (the dummy for bodies
+// without one), `dyn_a`/`dyn_b` whether they are dynamic and `ma`/`mb` their inverse masses
+// (zero unless dynamic). Writes the manifold's rows at lane g.
+NPH_D void prepare_manifold(const DevSolver &S, uint32_t g, const NphGpuContact &c, uint32_t ia,
+                            uint32_t ib, bool dyn_a, bool dyn_b, float ma, float mb,
+                            uint32_t group_points)
 {
-    const bool dyn_a = rec_a.type == NPH_GPU_BODY_DYNAMIC;
-    const bool dyn_b = rec_b.type == NPH_GPU_BODY_DYNAMIC;
-    const float ma = dyn_a ? rec_a.inv_mass : 0.0f;
-    const float mb = dyn_b ? rec_b.inv_mass : 0.0f;
     float unused;
     // prm holds zeros for a body that is not dynamic and for the dummy: dyn ? params : zero.
     const M3 ii_a = dyn_a ? load_inv_inertia(S.prm, ia, &unused) : m_zero();
@@ -170,15 +167,27 @@ NPH_D void prepare_manifold(const DevSolver &S, uint32_t g, const NphGpuContact 
 NPH_D void warm_manifold(const DevSolver &S, uint32_t g)
 {
     uint4 hdr = S.hdr[g];
+    const V3 n = v3(S.nrm[g]);
     const uint32_t bits = hdr.z;
     const uint32_t pc = bits & kHdrPointsMask;
     if (pc == 0u) {
         return;
     }
+    // Every load of the manifold at once: the rows, the bodies, their inertia.
+    V3 ra[4], rb[4];
+    float4 im[4];
+#pragma unroll
+    for (uint32_t k = 0; k < 4u; ++k) {
+        if (k < pc) {
+            const uint32_t row = k * S.mcap + g;
+            ra[k] = v3(S.pa[row]);
+            rb[k] = v3(S.pb[row]);
+            im[k] = S.pi[row];
+        }
+    }
     const Sides sd = load_sides(S.prm, hdr.x, hdr.y, bits);
     BodyState a = load_state(S.vel, hdr.x);
     BodyState b = load_state(S.vel, hdr.y);
-    const V3 n = v3(S.nrm[g]);
     const V3 t1 = perpendicular(n);
     const V3 t2 = cross(n, t1);
     if ((bits & kHdrImpacted) != 0u) {
@@ -186,38 +195,38 @@ NPH_D void warm_manifold(const DevSolver &S, uint32_t g)
         // pushes no point apart faster than it already moves apart.
         BodyState a1 = a;
         BodyState b1 = b;
-        for (uint32_t k = 0; k < pc; ++k) {
-            const uint32_t row = k * S.mcap + g;
-            const V3 ra = v3(S.pa[row]);
-            const V3 rb = v3(S.pb[row]);
-            const float4 im = S.pi[row];
-            apply2(sd, a1, b1, im.x, n, ra, rb);
-            apply2(sd, a1, b1, im.z, t1, ra, rb);
-            apply2(sd, a1, b1, im.w, t2, ra, rb);
+#pragma unroll
+        for (uint32_t k = 0; k < 4u; ++k) {
+            if (k < pc) {
+                apply2(sd, a1, b1, im[k].x, n, ra[k], rb[k]);
+                apply2(sd, a1, b1, im[k].z, t1, ra[k], rb[k]);
+                apply2(sd, a1, b1, im[k].w, t2, ra[k], rb[k]);
+            }
         }
         float share = 1.0f;
         const uint32_t gp = (bits >> kHdrGroupShift) & kHdrPointsMask;
-        for (uint32_t k = 0; k < gp; ++k) {
-            V3 ra = v3(0.0f, 0.0f, 0.0f);
-            V3 rb = v3(0.0f, 0.0f, 0.0f);
-            if (k < pc) {
-                ra = v3(S.pa[k * S.mcap + g]);
-                rb = v3(S.pb[k * S.mcap + g]);
+#pragma unroll
+        for (uint32_t k = 0; k < 4u; ++k) {
+            if (k < gp) {
+                // Points of the group this lane lacks have zero anchors.
+                const V3 za = k < pc ? ra[k] : v3(0.0f, 0.0f, 0.0f);
+                const V3 zb = k < pc ? rb[k] : v3(0.0f, 0.0f, 0.0f);
+                const float before = dot(rel_vel(a, b, za, zb), n);
+                const float after = dot(rel_vel(a1, b1, za, zb), n);
+                const float allowed = fmax_ref(before, 0.0f);
+                const bool pushed = after > allowed;
+                const float part = (allowed - before) / (pushed ? after - before : 1.0f);
+                share = fmin_ref(share, pushed ? part : 1.0f);
             }
-            const float before = dot(rel_vel(a, b, ra, rb), n);
-            const float after = dot(rel_vel(a1, b1, ra, rb), n);
-            const float allowed = fmax_ref(before, 0.0f);
-            const bool pushed = after > allowed;
-            const float part = (allowed - before) / (pushed ? after - before : 1.0f);
-            share = fmin_ref(share, pushed ? part : 1.0f);
         }
-        for (uint32_t k = 0; k < pc; ++k) {
-            const uint32_t row = k * S.mcap + g;
-            float4 im = S.pi[row];
-            im.x = im.x * share;
-            im.z = im.z * share;
-            im.w = im.w * share;
-            S.pi[row] = im;
+#pragma unroll
+        for (uint32_t k = 0; k < 4u; ++k) {
+            if (k < pc) {
+                im[k].x = im[k].x * share;
+                im[k].z = im[k].z * share;
+                im[k].w = im[k].w * share;
+                S.pi[k * S.mcap + g] = im[k];
+            }
         }
         hdr.z = bits & ~kHdrImpacted;
         S.hdr[g] = hdr;
@@ -225,13 +234,9 @@ NPH_D void warm_manifold(const DevSolver &S, uint32_t g)
 #pragma unroll
     for (uint32_t k = 0; k < 4u; ++k) {
         if (k < pc) {
-            const uint32_t row = k * S.mcap + g;
-            const V3 ra = v3(S.pa[row]);
-            const V3 rb = v3(S.pb[row]);
-            const float4 im = S.pi[row];
-            apply2(sd, a, b, im.x, n, ra, rb);
-            apply2(sd, a, b, im.z, t1, ra, rb);
-            apply2(sd, a, b, im.w, t2, ra, rb);
+            apply2(sd, a, b, im[k].x, n, ra[k], rb[k]);
+            apply2(sd, a, b, im[k].z, t1, ra[k], rb[k]);
+            apply2(sd, a, b, im[k].w, t2, ra[k], rb[k]);
         }
     }
     if (sd.wa) {
@@ -267,33 +272,38 @@ NPH_D void normal_row(float s, float inv_h, float soft_bias, float min_bias, flo
     impulse_scale = apart ? 0.0f : soft_impulse;
 }
 
-// solver_impl.h:400-421.
+// solver_impl.h:400-421. The reference computes every branch of every lane and selects;
+// here only the selected branch is computed, with the same operations, so the results are the
+// same bits: inside the circle the impulse stands, past it without slip it is scaled to the
+// circle, and sliding it blends towards opposing the slip.
 NPH_D void friction_circle(float vt1, float vt2, float limit, float &new1, float &new2)
 {
     const float len = sqrtf(new1 * new1 + new2 * new2);
-    const bool over = len > limit;
+    if (!(len > limit)) {
+        return;
+    }
     const float slip = sqrtf(vt1 * vt1 + vt2 * vt2);
-    const bool sliding = over && slip > 0.0f;
-    const float r = limit / (over ? len : 1.0f);
-    const float stop_share = r / (over ? len : 1.0f);
-    const float slip_share = (1.0f - r) / (sliding ? slip : 1.0f);
+    const float r = limit / len;
+    if (!(slip > 0.0f)) {
+        new1 = new1 * r;
+        new2 = new2 * r;
+        return;
+    }
+    const float stop_share = r / len;
+    const float slip_share = (1.0f - r) / slip;
     const float d1 = stop_share * new1 - slip_share * vt1;
     const float d2 = stop_share * new2 - slip_share * vt2;
     const float dlen = sqrtf(d1 * d1 + d2 * d2);
-    const float to_edge = limit / (sliding ? dlen : 1.0f);
-    if (sliding) {
-        new1 = d1 * to_edge;
-        new2 = d2 * to_edge;
-    } else if (over) {
-        new1 = new1 * r;
-        new2 = new2 * r;
-    }
+    const float to_edge = limit / dlen;
+    new1 = d1 * to_edge;
+    new2 = d2 * to_edge;
 }
 
 template <bool kUseBias>
 NPH_D void solve_manifold(const DevSolver &S, uint32_t g, const StepConsts &K)
 {
     const uint4 hdr = S.hdr[g];
+    const float4 nf = S.nrm[g];
     const uint32_t bits = hdr.z;
     const uint32_t pc = bits & kHdrPointsMask;
     if (pc == 0u) {
@@ -304,7 +314,6 @@ NPH_D void solve_manifold(const DevSolver &S, uint32_t g, const StepConsts &K)
     BodyState b = load_state(S.vel, hdr.y);
     const BodyPose pa_ = load_pose(S.pos, hdr.x);
     const BodyPose pb_ = load_pose(S.pos, hdr.y);
-    const float4 nf = S.nrm[g];
     const V3 n = v3(nf);
     const float friction = nf.w;
     const Soft soft = (bits & kHdrStaticSoft) != 0u ? K.static_soft : K.contact_soft;
@@ -315,7 +324,7 @@ NPH_D void solve_manifold(const DevSolver &S, uint32_t g, const StepConsts &K)
 
     V3 ra[4], rb[4];
     float adj[4], nm[4];
-    float4 im[4];
+    float4 im[4], tm[4];
 #pragma unroll
     for (uint32_t k = 0; k < 4u; ++k) {
         if (k < pc) {
@@ -327,6 +336,7 @@ NPH_D void solve_manifold(const DevSolver &S, uint32_t g, const StepConsts &K)
             rb[k] = v3(B);
             nm[k] = B.w;
             im[k] = S.pi[row];
+            tm[k] = S.pt[row];
         }
     }
 #pragma unroll
@@ -381,14 +391,13 @@ NPH_D void solve_manifold(const DevSolver &S, uint32_t g, const StepConsts &K)
 #pragma unroll
     for (uint32_t k = 0; k < 4u; ++k) {
         if (k < pc) {
-            const float4 tm = S.pt[k * S.mcap + g];
             const V3 dv = rel_vel(a, b, ra[k], rb[k]);
             const float vt1 = dot(dv, t1);
             const float vt2 = dot(dv, t2);
             const float old1 = im[k].z;
             const float old2 = im[k].w;
-            float new1 = old1 - (tm.x * vt1 + tm.y * vt2);
-            float new2 = old2 - (tm.y * vt1 + tm.z * vt2);
+            float new1 = old1 - (tm[k].x * vt1 + tm[k].y * vt2);
+            float new2 = old2 - (tm[k].y * vt1 + tm[k].z * vt2);
             friction_circle(vt1, vt2, friction * im[k].x, new1, new2);
             im[k].z = new1;
             im[k].w = new2;

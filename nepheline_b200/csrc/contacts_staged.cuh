@@ -1,0 +1,269 @@
+// SPDX-License-Identifier: Apache-2.0
+//
+// The warm start, solve and relax rows of contacts.cuh with their loads staged through shared
+// memory: after the manifold's header, each lane issues every load it needs (its point rows
+// and its two bodies' velocities, displacements and inertia) as asynchronous 16-byte copies
+// into its own column of the block's tile, waits for them once, and computes from the tile.
+// The copies hold no registers while in flight, so a lane keeps all of its loads in flight at
+// once whatever its register budget. The tile is [slot][lane]: a warp's 32 lanes read 512
+// contiguous bytes per slot, free of bank conflicts. The arithmetic is contacts.cuh's, in
+// its order: the staged and unstaged passes give the same bits.
+#pragma once
+
+#include <cuda_pipeline_primitives.h>
+
+#include "contacts.cuh"
+
+namespace nph {
+
+// Tile slots: per point k, 4k + {0 pa, 1 pb, 2 pi, 3 pt}; then the bodies.
+constexpr uint32_t kSlotVa = 16, kSlotWa = 17, kSlotVb = 18, kSlotWb = 19;
+constexpr uint32_t kSlotDpa = 20, kSlotDqa = 21, kSlotDpb = 22, kSlotDqb = 23;
+constexpr uint32_t kSlotIa = 24, kSlotIb = 27; // three columns each
+constexpr uint32_t kSlots = 30;
+
+template <uint32_t kLanes> struct Tile {
+    float4 *base;
+    uint32_t lane;
+    NPH_D float4 *at(uint32_t slot) const { return base + slot * kLanes + lane; }
+    NPH_D float4 get(uint32_t slot) const { return *at(slot); }
+};
+
+NPH_D void copy16(float4 *dst, const float4 *src) { __pipeline_memcpy_async(dst, src, 16); }
+
+// Issues the manifold's loads into the lane's column: the rows of its own points (pt only
+// when `tangents`), the velocities of both bodies, their displacements and rotations when
+// `poses`, and the inertia of the sides that take results.
+template <uint32_t kLanes>
+NPH_D void stage_manifold(const DevSolver &S, uint32_t g, uint4 hdr, const Tile<kLanes> &T,
+                          bool tangents, bool poses)
+{
+    const uint32_t bits = hdr.z;
+    const uint32_t pc = bits & kHdrPointsMask;
+#pragma unroll
+    for (uint32_t k = 0; k < 4u; ++k) {
+        if (k < pc) {
+            const uint32_t row = k * S.mcap + g;
+            copy16(T.at(4u * k + 0u), &S.pa[row]);
+            copy16(T.at(4u * k + 1u), &S.pb[row]);
+            copy16(T.at(4u * k + 2u), &S.pi[row]);
+            if (tangents) {
+                copy16(T.at(4u * k + 3u), &S.pt[row]);
+            }
+        }
+    }
+    copy16(T.at(kSlotVa), &S.vel[2u * hdr.x]);
+    copy16(T.at(kSlotWa), &S.vel[2u * hdr.x + 1u]);
+    copy16(T.at(kSlotVb), &S.vel[2u * hdr.y]);
+    copy16(T.at(kSlotWb), &S.vel[2u * hdr.y + 1u]);
+    if (poses) {
+        copy16(T.at(kSlotDpa), &S.pos[2u * hdr.x]);
+        copy16(T.at(kSlotDqa), &S.pos[2u * hdr.x + 1u]);
+        copy16(T.at(kSlotDpb), &S.pos[2u * hdr.y]);
+        copy16(T.at(kSlotDqb), &S.pos[2u * hdr.y + 1u]);
+    }
+    if ((bits & kHdrWriteA) != 0u) {
+        copy16(T.at(kSlotIa + 0u), &S.prm[3u * hdr.x + 0u]);
+        copy16(T.at(kSlotIa + 1u), &S.prm[3u * hdr.x + 1u]);
+        copy16(T.at(kSlotIa + 2u), &S.prm[3u * hdr.x + 2u]);
+    }
+    if ((bits & kHdrWriteB) != 0u) {
+        copy16(T.at(kSlotIb + 0u), &S.prm[3u * hdr.y + 0u]);
+        copy16(T.at(kSlotIb + 1u), &S.prm[3u * hdr.y + 1u]);
+        copy16(T.at(kSlotIb + 2u), &S.prm[3u * hdr.y + 2u]);
+    }
+    __pipeline_commit();
+    __pipeline_wait_prior(0);
+}
+
+template <uint32_t kLanes> NPH_D Sides staged_sides(const Tile<kLanes> &T, uint32_t bits)
+{
+    Sides s;
+    s.wa = (bits & kHdrWriteA) != 0u;
+    s.wb = (bits & kHdrWriteB) != 0u;
+    s.ma = 0.0f;
+    s.mb = 0.0f;
+    s.ia = m_zero();
+    s.ib = m_zero();
+    if (s.wa) {
+        const float4 c0 = T.get(kSlotIa), c1 = T.get(kSlotIa + 1u), c2 = T.get(kSlotIa + 2u);
+        s.ma = c0.w;
+        s.ia = M3{v3(c0), v3(c1), v3(c2)};
+    }
+    if (s.wb) {
+        const float4 c0 = T.get(kSlotIb), c1 = T.get(kSlotIb + 1u), c2 = T.get(kSlotIb + 2u);
+        s.mb = c0.w;
+        s.ib = M3{v3(c0), v3(c1), v3(c2)};
+    }
+    return s;
+}
+
+// warm_manifold (solver_impl.h:181-258) on the staged loads.
+template <uint32_t kLanes>
+NPH_D void warm_manifold_staged(const DevSolver &S, uint32_t g, const Tile<kLanes> &T)
+{
+    uint4 hdr = S.hdr[g];
+    const V3 n = v3(S.nrm[g]);
+    const uint32_t bits = hdr.z;
+    const uint32_t pc = bits & kHdrPointsMask;
+    if (pc == 0u) {
+        return;
+    }
+    stage_manifold(S, g, hdr, T, false, false);
+    const Sides sd = staged_sides(T, bits);
+    BodyState a = BodyState{v3(T.get(kSlotVa)), v3(T.get(kSlotWa))};
+    BodyState b = BodyState{v3(T.get(kSlotVb)), v3(T.get(kSlotWb))};
+    const V3 t1 = perpendicular(n);
+    const V3 t2 = cross(n, t1);
+    if ((bits & kHdrImpacted) != 0u) {
+        BodyState a1 = a;
+        BodyState b1 = b;
+        for (uint32_t k = 0; k < pc; ++k) {
+            const V3 ra = v3(T.get(4u * k)), rb = v3(T.get(4u * k + 1u));
+            const float4 im = T.get(4u * k + 2u);
+            apply2(sd, a1, b1, im.x, n, ra, rb);
+            apply2(sd, a1, b1, im.z, t1, ra, rb);
+            apply2(sd, a1, b1, im.w, t2, ra, rb);
+        }
+        float share = 1.0f;
+        const uint32_t gp = (bits >> kHdrGroupShift) & kHdrPointsMask;
+        for (uint32_t k = 0; k < gp; ++k) {
+            const V3 ra = k < pc ? v3(T.get(4u * k)) : v3(0.0f, 0.0f, 0.0f);
+            const V3 rb = k < pc ? v3(T.get(4u * k + 1u)) : v3(0.0f, 0.0f, 0.0f);
+            const float before = dot(rel_vel(a, b, ra, rb), n);
+            const float after = dot(rel_vel(a1, b1, ra, rb), n);
+            const float allowed = fmax_ref(before, 0.0f);
+            const bool pushed = after > allowed;
+            const float part = (allowed - before) / (pushed ? after - before : 1.0f);
+            share = fmin_ref(share, pushed ? part : 1.0f);
+        }
+        for (uint32_t k = 0; k < pc; ++k) {
+            float4 im = T.get(4u * k + 2u);
+            im.x = im.x * share;
+            im.z = im.z * share;
+            im.w = im.w * share;
+            *T.at(4u * k + 2u) = im;
+            S.pi[k * S.mcap + g] = im;
+        }
+        hdr.z = bits & ~kHdrImpacted;
+        S.hdr[g] = hdr;
+    }
+    for (uint32_t k = 0; k < pc; ++k) {
+        const V3 ra = v3(T.get(4u * k)), rb = v3(T.get(4u * k + 1u));
+        const float4 im = T.get(4u * k + 2u);
+        apply2(sd, a, b, im.x, n, ra, rb);
+        apply2(sd, a, b, im.z, t1, ra, rb);
+        apply2(sd, a, b, im.w, t2, ra, rb);
+    }
+    if (sd.wa) {
+        store_state(S.vel, hdr.x, a);
+    }
+    if (sd.wb) {
+        store_state(S.vel, hdr.y, b);
+    }
+}
+
+// solve_manifold (solver_impl.h:484-602) on the staged loads.
+template <bool kUseBias, uint32_t kLanes>
+NPH_D void solve_manifold_staged(const DevSolver &S, uint32_t g, const StepConsts &K,
+                                 const Tile<kLanes> &T)
+{
+    const uint4 hdr = S.hdr[g];
+    const float4 nf = S.nrm[g];
+    const uint32_t bits = hdr.z;
+    const uint32_t pc = bits & kHdrPointsMask;
+    if (pc == 0u) {
+        return;
+    }
+    stage_manifold(S, g, hdr, T, true, true);
+    const Sides sd = staged_sides(T, bits);
+    BodyState a = BodyState{v3(T.get(kSlotVa)), v3(T.get(kSlotWa))};
+    BodyState b = BodyState{v3(T.get(kSlotVb)), v3(T.get(kSlotWb))};
+    const BodyPose pa_ = BodyPose{v3(T.get(kSlotDpa)), q4(T.get(kSlotDqa))};
+    const BodyPose pb_ = BodyPose{v3(T.get(kSlotDpb)), q4(T.get(kSlotDqb))};
+    const V3 n = v3(nf);
+    const float friction = nf.w;
+    const Soft soft = (bits & kHdrStaticSoft) != 0u ? K.static_soft : K.contact_soft;
+    const float soft_bias = kUseBias ? soft.bias_rate : 0.0f;
+    const float soft_mass = kUseBias ? soft.mass_scale : 1.0f;
+    const float soft_impulse = kUseBias ? soft.impulse_scale : 0.0f;
+    const float min_bias = -K.push_max;
+    for (uint32_t k = 0; k < pc; ++k) {
+        const float4 A = T.get(4u * k), B = T.get(4u * k + 1u);
+        float4 im = T.get(4u * k + 2u);
+        const V3 ra = v3(A), rb = v3(B);
+        float bias, mass_scale, impulse_scale;
+        normal_row(separation(pa_, pb_, ra, rb, A.w, n), K.inv_h, soft_bias, min_bias, soft_mass,
+                   soft_impulse, bias, mass_scale, impulse_scale);
+        const float vn = dot(rel_vel(a, b, ra, rb), n);
+        const float row = B.w * mass_scale;
+        const float acc = im.x;
+        const float impulse = -(row * (vn + bias)) - impulse_scale * acc;
+        const float total = fmax_ref(acc + impulse, 0.0f);
+        const float delta = total - acc;
+        im.x = total;
+        im.y = fmax_ref(im.y, total);
+        *T.at(4u * k + 2u) = im;
+        apply2(sd, a, b, delta, n, ra, rb);
+    }
+    const uint32_t gp = (bits >> kHdrGroupShift) & kHdrPointsMask;
+    if (gp > 1u && (bits & kHdrImpact) != 0u) {
+        float row_bias[4], row_mass[4], row_soft[4];
+#pragma unroll
+        for (uint32_t k = 0; k < 4u; ++k) {
+            if (k < pc) {
+                const float4 A = T.get(4u * k), B = T.get(4u * k + 1u);
+                float mass_scale;
+                normal_row(separation(pa_, pb_, v3(A), v3(B), A.w, n), K.inv_h, soft_bias, min_bias,
+                           soft_mass, soft_impulse, row_bias[k], mass_scale, row_soft[k]);
+                row_mass[k] = B.w * mass_scale;
+            }
+        }
+        for (uint32_t sweep = 0; sweep < 7u; ++sweep) {
+#pragma unroll
+            for (uint32_t k = 0; k < 4u; ++k) {
+                if (k < pc) {
+                    const V3 ra = v3(T.get(4u * k)), rb = v3(T.get(4u * k + 1u));
+                    float4 im = T.get(4u * k + 2u);
+                    const float vn = dot(rel_vel(a, b, ra, rb), n);
+                    const float acc = im.x;
+                    const float impulse = -(row_mass[k] * (vn + row_bias[k])) - row_soft[k] * acc;
+                    const float total = fmax_ref(acc + impulse, 0.0f);
+                    const float delta = total - acc;
+                    im.x = total;
+                    im.y = fmax_ref(im.y, total);
+                    *T.at(4u * k + 2u) = im;
+                    apply2(sd, a, b, delta, n, ra, rb);
+                }
+            }
+        }
+    }
+    const V3 t1 = perpendicular(n);
+    const V3 t2 = cross(n, t1);
+    for (uint32_t k = 0; k < pc; ++k) {
+        const V3 ra = v3(T.get(4u * k)), rb = v3(T.get(4u * k + 1u));
+        const float4 tm = T.get(4u * k + 3u);
+        float4 im = T.get(4u * k + 2u);
+        const V3 dv = rel_vel(a, b, ra, rb);
+        const float vt1 = dot(dv, t1);
+        const float vt2 = dot(dv, t2);
+        const float old1 = im.z;
+        const float old2 = im.w;
+        float new1 = old1 - (tm.x * vt1 + tm.y * vt2);
+        float new2 = old2 - (tm.y * vt1 + tm.z * vt2);
+        friction_circle(vt1, vt2, friction * im.x, new1, new2);
+        im.z = new1;
+        im.w = new2;
+        S.pi[k * S.mcap + g] = im;
+        apply2(sd, a, b, new1 - old1, t1, ra, rb);
+        apply2(sd, a, b, new2 - old2, t2, ra, rb);
+    }
+    if (sd.wa) {
+        store_state(S.vel, hdr.x, a);
+    }
+    if (sd.wb) {
+        store_state(S.vel, hdr.y, b);
+    }
+}
+
+} // namespace nph

@@ -6,9 +6,10 @@
 // lock (264-336), each ending in the point block (207-230). The reference keeps joints
 // scalar, so every formula here is its scalar formula in its order. Joints of a colour share
 // no dynamic body with each other or with the colour's contacts, so a colour's joints run
-// in parallel. The angle of a hinge limit or spring and of a ball cone or twist limit uses
-// the device's atan2f, which is not bit-identical to the host C library's: those rows match
-// the reference within floating-point tolerance, the others bit for bit.
+// in parallel. The angle of a hinge limit or spring and of a ball cone or twist limit is the
+// correctly rounded FP32 arctangent (the double-precision atan2 rounded once to FP32): the
+// reference's is the host C library's atan2f, which is not correctly rounded, so those rows
+// match the reference within floating-point tolerance, the others bit for bit.
 #pragma once
 
 #include "layout.cuh"
@@ -52,6 +53,9 @@ NPH_D float axial_mass(const JointBodies &jb, V3 axis)
     return k > 0.0f ? 1.0f / k : 0.0f;
 }
 
+// atan2(y, x) rounded once to FP32 from the double-precision value.
+NPH_D float atan2_rn(float y, float x) { return (float)atan2((double)y, (double)x); }
+
 // joint_solver.c:77-84.
 NPH_D float twist_angle(Q4 qa, Q4 qb)
 {
@@ -59,7 +63,7 @@ NPH_D float twist_angle(Q4 qa, Q4 qb)
     if (r.w < 0.0f) {
         r = Q4{-r.x, -r.y, -r.z, -r.w};
     }
-    return 2.0f * atan2f(r.x, r.w);
+    return 2.0f * atan2_rn(r.x, r.w);
 }
 
 // joint_solver.c:86-96.
@@ -440,7 +444,7 @@ NPH_D void solve_joint(const DevSolver &S, uint32_t j, const StepConsts &K)
                 const float ey = local.y / set_a.x;
                 const float ez = local.z / set_a.y;
                 const float limit = 1.0f / sqrtf(ey * ey + ez * ez);
-                const float phi = atan2f(sin_phi, dot(xa, xb));
+                const float phi = atan2_rn(sin_phi, dot(xa, xb));
                 solve_angular_limit(jb, axis, limit - phi, fric.w, K, kUseBias);
             }
         }

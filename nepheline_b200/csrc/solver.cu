@@ -17,6 +17,7 @@
 
 #include <cstdio>
 #include <cstdlib>
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -24,6 +25,7 @@
 
 #include "bodies.cuh"
 #include "contacts.cuh"
+#include "contacts_staged.cuh"
 #include "joints.cuh"
 
 namespace nph {
@@ -41,20 +43,58 @@ enum Pass : int { kWarm = 0, kSolve = 1, kRelax = 2, kRestitution = 3 };
 // Kernels
 // ------------------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(kBlock) k_prepare_bodies(BodyArrays B, const NphGpuBody *bodies,
+// Record staging: a block copies its records between global and shared memory with 16- or
+// 8-byte accesses covering whole cache lines, and the threads work on the shared copies.
+constexpr uint32_t kStage = 128;
+
+template <typename V, typename Rec>
+__device__ __forceinline__ void stage_in(const Rec *src, uint32_t count, Rec *dst)
+{
+    const V *s = reinterpret_cast<const V *>(src);
+    V *d = reinterpret_cast<V *>(dst);
+    const uint32_t words = (uint32_t)(count * sizeof(Rec) / sizeof(V));
+    for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) {
+        d[i] = s[i];
+    }
+}
+
+template <typename V, typename Rec>
+__device__ __forceinline__ void stage_out(const Rec *src, uint32_t count, Rec *dst)
+{
+    const V *s = reinterpret_cast<const V *>(src);
+    V *d = reinterpret_cast<V *>(dst);
+    const uint32_t words = (uint32_t)(count * sizeof(Rec) / sizeof(V));
+    for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) {
+        d[i] = s[i];
+    }
+}
+
+static_assert(sizeof(NphGpuBody) % 16 == 0, "body records stage in 16-byte words");
+static_assert(sizeof(NphGpuContact) % 16 == 0, "contact records stage in 16-byte words");
+static_assert(sizeof(NphGpuJoint) % 8 == 0, "joint records stage in 8-byte words");
+
+__global__ void __launch_bounds__(kStage) k_prepare_bodies(BodyArrays B, const NphGpuBody *bodies,
                                                            uint32_t n, StepConsts K)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) {
-        prepare_body(B, i, bodies[i], K);
-    } else if (i == n) {
+    __shared__ NphGpuBody rec[kStage];
+    const uint32_t first = blockIdx.x * kStage;
+    if (first < n) {
+        const uint32_t count = min(kStage, n - first);
+        stage_in<uint4>(bodies + first, count, rec);
+        __syncthreads();
+        if (threadIdx.x < count) {
+            prepare_body(B, first + threadIdx.x, rec[threadIdx.x], K);
+        }
+    }
+    if (first + threadIdx.x == n) {
         prepare_dummy(B, n);
     }
 }
 
 // The largest point count of the eight-lane group holding manifold g (build_groups,
-// solver.c:810-843: a colour's list in eights, the overflow one per group).
-__device__ uint32_t group_points(const NphGpuContact *contacts, uint32_t g, const ColorTable &T,
+// solver.c:810-843: a colour's list in eights, the overflow one per group), and g's colour.
+__device__ uint32_t group_points(const NphGpuContact *contacts, const NphGpuContact *staged,
+                                 uint32_t first, uint32_t count, uint32_t g, const ColorTable &T,
                                  uint32_t &color)
 {
     uint32_t c = 0;
@@ -66,66 +106,102 @@ __device__ uint32_t group_points(const NphGpuContact *contacts, uint32_t g, cons
     const uint32_t end = min(start + per, T.cfirst[c] + T.ccount[c]);
     uint32_t gp = 0;
     for (uint32_t q = start; q < end; ++q) {
-        const uint32_t pc = contacts[q].point_count;
+        const uint32_t pc = q >= first && q < first + count ? staged[q - first].point_count
+                                                            : contacts[q].point_count;
         gp = pc <= NPH_GPU_MAX_POINTS && pc > gp ? pc : gp;
     }
     color = c;
     return gp;
 }
 
-__global__ void __launch_bounds__(kBlock)
-k_prepare_constraints(DevSolver S, const NphGpuContact *contacts, const NphGpuJoint *joints,
-                      const NphGpuBody *bodies, const NphGpuBody *fixed, uint32_t n, uint32_t nf,
-                      uint32_t m, uint32_t nj, uint32_t jblocks, ColorTable T, float h,
-                      uint32_t *err, uint32_t *color_points)
+// Whether a view index is a dynamic body, and its inverse mass (zero unless dynamic).
+__device__ __forceinline__ void body_kind(const float4 *prm, const NphGpuBody *fixed, uint32_t n,
+                                          uint32_t index, bool &dyn, float &inv_mass)
 {
+    if (index < n) {
+        dyn = prm[3u * index + 1u].w != 0.0f;
+        inv_mass = prm[3u * index].w;
+    } else {
+        const NphGpuBody &f = fixed[index - n];
+        dyn = f.type == NPH_GPU_BODY_DYNAMIC;
+        inv_mass = dyn ? f.inv_mass : 0.0f;
+    }
+}
+
+__global__ void __launch_bounds__(kStage)
+k_prepare_contacts(DevSolver S, const NphGpuContact *contacts, const NphGpuBody *fixed, uint32_t n,
+                   uint32_t nf, uint32_t m, ColorTable T, uint32_t *err, uint32_t *color_points)
+{
+    __shared__ NphGpuContact rec[kStage];
+    __shared__ uint32_t points[NPH_GPU_COLOR_SLOTS];
+    const uint32_t first = blockIdx.x * kStage;
+    const uint32_t count = min(kStage, m - first);
+    if (threadIdx.x < NPH_GPU_COLOR_SLOTS) {
+        points[threadIdx.x] = 0u;
+    }
+    stage_in<uint4>(contacts + first, count, rec);
+    __syncthreads();
+    const uint32_t g = first + threadIdx.x;
     const uint32_t total = n + nf;
-    if (blockIdx.x < jblocks) {
-        const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-        if (j >= nj) {
-            return;
+    if (threadIdx.x < count) {
+        const NphGpuContact &c = rec[threadIdx.x];
+        if (c.body_a >= total || c.body_b >= total) {
+            atomicOr(err, kErrBadIndex);
+            S.hdr[g] = make_uint4(n, n, 0u, 0u);
+        } else if (c.point_count < 1u || c.point_count > NPH_GPU_MAX_POINTS) {
+            atomicOr(err, kErrBadPoints);
+            S.hdr[g] = make_uint4(n, n, 0u, 0u);
+        } else {
+            bool dyn_a, dyn_b;
+            float ma, mb;
+            body_kind(S.prm, fixed, n, c.body_a, dyn_a, ma);
+            body_kind(S.prm, fixed, n, c.body_b, dyn_b, mb);
+            S.nrm[g] = make_float4(c.normal[0], c.normal[1], c.normal[2], c.friction);
+            S.rest[g] = c.restitution;
+            uint32_t color = 0;
+            const uint32_t gp = group_points(contacts, rec, first, count, g, T, color);
+            prepare_manifold(S, g, c, c.body_a < n ? c.body_a : n, c.body_b < n ? c.body_b : n,
+                             dyn_a, dyn_b, ma, mb, gp);
+            atomicAdd(&points[color], c.point_count);
         }
-        const NphGpuJoint &jr = joints[j];
-        if (jr.body_a >= total || jr.body_b >= total ||
-            (jr.type != NPH_GPU_JOINT_BALL && jr.type != NPH_GPU_JOINT_HINGE)) {
-            atomicOr(err, kErrBadJoint);
-            // Inert: both ends the dummy, no impulse, nothing written.
-            for (uint32_t r = 0; r < kJointRows; ++r) {
-                S.jw[r * S.jcap + j] = make_float4(0.f, 0.f, 0.f, 0.f);
-            }
-            S.jw[kJrFrameA * S.jcap + j] = make_float4(0.f, 0.f, 0.f, 1.f);
-            S.jw[kJrFrameB * S.jcap + j] = make_float4(0.f, 0.f, 0.f, 1.f);
-            S.jw[kJrHead * S.jcap + j] = make_float4(__uint_as_float(n), __uint_as_float(n), 0.f, 0.f);
-            return;
+    }
+    // The points per colour (the byte counts of a profiled step): one global add per block.
+    __syncthreads();
+    if (threadIdx.x < NPH_GPU_COLOR_SLOTS && points[threadIdx.x] != 0u) {
+        atomicAdd(&color_points[threadIdx.x], points[threadIdx.x]);
+    }
+}
+
+__global__ void __launch_bounds__(kStage)
+k_prepare_joints(DevSolver S, const NphGpuJoint *joints, const NphGpuBody *bodies,
+                 const NphGpuBody *fixed, uint32_t n, uint32_t nf, uint32_t nj, float h, uint32_t *err)
+{
+    __shared__ NphGpuJoint rec[kStage];
+    const uint32_t first = blockIdx.x * kStage;
+    const uint32_t count = min(kStage, nj - first);
+    stage_in<uint2>(joints + first, count, rec);
+    __syncthreads();
+    if (threadIdx.x >= count) {
+        return;
+    }
+    const uint32_t j = first + threadIdx.x;
+    const uint32_t total = n + nf;
+    const NphGpuJoint &jr = rec[threadIdx.x];
+    if (jr.body_a >= total || jr.body_b >= total ||
+        (jr.type != NPH_GPU_JOINT_BALL && jr.type != NPH_GPU_JOINT_HINGE)) {
+        atomicOr(err, kErrBadJoint);
+        // Inert: both ends the dummy, no impulse, nothing written.
+        for (uint32_t r = 0; r < kJointRows; ++r) {
+            S.jw[r * S.jcap + j] = make_float4(0.f, 0.f, 0.f, 0.f);
         }
-        const NphGpuBody &a = jr.body_a < n ? bodies[jr.body_a] : fixed[jr.body_a - n];
-        const NphGpuBody &b = jr.body_b < n ? bodies[jr.body_b] : fixed[jr.body_b - n];
-        prepare_joint(S, j, jr, a, b, jr.body_a < n ? jr.body_a : n, jr.body_b < n ? jr.body_b : n, h);
+        S.jw[kJrFrameA * S.jcap + j] = make_float4(0.f, 0.f, 0.f, 1.f);
+        S.jw[kJrFrameB * S.jcap + j] = make_float4(0.f, 0.f, 0.f, 1.f);
+        S.jw[kJrHead * S.jcap + j] = make_float4(__uint_as_float(n), __uint_as_float(n), 0.f, 0.f);
         return;
     }
-    const uint32_t g = (blockIdx.x - jblocks) * blockDim.x + threadIdx.x;
-    if (g >= m) {
-        return;
-    }
-    const NphGpuContact &c = contacts[g];
-    if (c.body_a >= total || c.body_b >= total) {
-        atomicOr(err, kErrBadIndex);
-        S.hdr[g] = make_uint4(n, n, 0u, 0u);
-        return;
-    }
-    if (c.point_count < 1u || c.point_count > NPH_GPU_MAX_POINTS) {
-        atomicOr(err, kErrBadPoints);
-        S.hdr[g] = make_uint4(n, n, 0u, 0u);
-        return;
-    }
-    const NphGpuBody &a = c.body_a < n ? bodies[c.body_a] : fixed[c.body_a - n];
-    const NphGpuBody &b = c.body_b < n ? bodies[c.body_b] : fixed[c.body_b - n];
-    S.nrm[g] = make_float4(c.normal[0], c.normal[1], c.normal[2], c.friction);
-    S.rest[g] = c.restitution;
-    uint32_t color = 0;
-    const uint32_t gp = group_points(contacts, g, T, color);
-    prepare_manifold(S, g, c, a, b, c.body_a < n ? c.body_a : n, c.body_b < n ? c.body_b : n, gp);
-    atomicAdd(&color_points[color], c.point_count);
+    const NphGpuBody &a = jr.body_a < n ? bodies[jr.body_a] : fixed[jr.body_a - n];
+    const NphGpuBody &b = jr.body_b < n ? bodies[jr.body_b] : fixed[jr.body_b - n];
+    prepare_joint(S, j, jr, a, b, jr.body_a < n ? jr.body_a : n, jr.body_b < n ? jr.body_b : n, h);
 }
 
 template <int P>
@@ -154,23 +230,87 @@ __device__ __forceinline__ void contact_op(const DevSolver &S, uint32_t g, const
     }
 }
 
-// One colour of one constraint pass: its joints' blocks, then its contacts'.
-template <int P>
-__global__ void __launch_bounds__(kBlock)
-k_pass(DevSolver S, uint32_t cfirst, uint32_t ccount, uint32_t jfirst, uint32_t jcount,
-       uint32_t jblocks, StepConsts K)
+// One colour of one constraint pass: its joints' blocks, then its contacts'. Instantiated
+// for several block sizes and register budgets (the pass configurations the autotuner picks
+// from).
+template <int P, int kThreads, int kMinBlocks>
+__global__ void __launch_bounds__(kThreads, kMinBlocks)
+k_pass(DevSolver S, uint32_t cfirst, uint32_t ccount, StepConsts K)
 {
-    if (blockIdx.x < jblocks) {
-        const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-        if (j < jcount) {
-            joint_op<P>(S, jfirst + j, K);
-        }
-        return;
-    }
-    const uint32_t g = (blockIdx.x - jblocks) * blockDim.x + threadIdx.x;
+    const uint32_t g = blockIdx.x * kThreads + threadIdx.x;
     if (g < ccount) {
         contact_op<P>(S, cfirst + g, K);
     }
+}
+
+// One colour's joints in one constraint pass. A colour's joints share no dynamic body with its
+// contacts, so the two kernels run side by side.
+template <int P>
+__global__ void __launch_bounds__(kBlock) k_joint_pass(DevSolver S, uint32_t jfirst, uint32_t jcount,
+                                                       StepConsts K)
+{
+    const uint32_t j = blockIdx.x * kBlock + threadIdx.x;
+    if (j < jcount) {
+        joint_op<P>(S, jfirst + j, K);
+    }
+}
+
+// The same pass with the manifold's loads staged through shared memory (contacts_staged.cuh).
+template <int P, uint32_t kLanes, int kMinBlocks>
+__global__ void __launch_bounds__(kLanes, kMinBlocks)
+k_pass_staged(DevSolver S, uint32_t cfirst, uint32_t ccount, StepConsts K)
+{
+    extern __shared__ float4 tile[];
+    const uint32_t g = blockIdx.x * kLanes + threadIdx.x;
+    if (g >= ccount) {
+        return;
+    }
+    const Tile<kLanes> T{tile, threadIdx.x};
+    if (P == kWarm) {
+        warm_manifold_staged(S, cfirst + g, T);
+    } else if (P == kSolve) {
+        solve_manifold_staged<true>(S, cfirst + g, K, T);
+    } else if (P == kRelax) {
+        solve_manifold_staged<false>(S, cfirst + g, K, T);
+    } else {
+        restitution_manifold(S, cfirst + g, K);
+    }
+}
+
+// The pass configurations: threads per block and the blocks per SM the register budget
+// allows (65,536 registers / (threads x blocks)); the last two stage the loads through
+// shared memory (kSlots x threads x 16 bytes per block).
+struct PassConfig {
+    uint32_t threads, min_blocks, staged;
+};
+constexpr PassConfig kPassConfigs[] = {{256, 1, 0}, {256, 2, 0}, {128, 4, 0}, {256, 3, 0},
+                                       {64, 6, 1},  {64, 7, 1},  {128, 3, 1}, {32, 14, 1}};
+constexpr uint32_t kPassConfigCount = sizeof(kPassConfigs) / sizeof(kPassConfigs[0]);
+
+template <int P>
+void launch_pass(uint32_t config, uint32_t cc, cudaStream_t st, const DevSolver &S, uint32_t cfirst,
+                 const StepConsts &K)
+{
+    const uint32_t t = kPassConfigs[config].threads;
+    const uint32_t grid = (cc + t - 1) / t;
+    const size_t tile = kPassConfigs[config].staged ? (size_t)kSlots * t * sizeof(float4) : 0;
+    switch (config) {
+    case 0: k_pass<P, 256, 1><<<grid, 256, 0, st>>>(S, cfirst, cc, K); break;
+    case 1: k_pass<P, 256, 2><<<grid, 256, 0, st>>>(S, cfirst, cc, K); break;
+    case 2: k_pass<P, 128, 4><<<grid, 128, 0, st>>>(S, cfirst, cc, K); break;
+    case 3: k_pass<P, 256, 3><<<grid, 256, 0, st>>>(S, cfirst, cc, K); break;
+    case 4: k_pass_staged<P, 64, 6><<<grid, 64, tile, st>>>(S, cfirst, cc, K); break;
+    case 5: k_pass_staged<P, 64, 7><<<grid, 64, tile, st>>>(S, cfirst, cc, K); break;
+    case 6: k_pass_staged<P, 128, 3><<<grid, 128, tile, st>>>(S, cfirst, cc, K); break;
+    default: k_pass_staged<P, 32, 14><<<grid, 32, tile, st>>>(S, cfirst, cc, K); break;
+    }
+}
+
+// The staged kernels with tiles above the default 48 KiB of dynamic shared memory.
+template <int P> void allow_tiles()
+{
+    cudaFuncSetAttribute(k_pass_staged<P, 128, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(kSlots * 128 * sizeof(float4)));
 }
 
 // The overflow: its joints, then its contacts, one at a time in list order (they may share
@@ -208,25 +348,51 @@ __global__ void __launch_bounds__(kBlock) k_integrate_position(BodyArrays B, uin
     }
 }
 
-// store_group (solver.c:475-499), the joints' impulses, and finalize_body (solver.c:304-324).
-__global__ void __launch_bounds__(kBlock)
-k_store_finalize(DevSolver S, BodyArrays B, NphGpuContact *contacts, uint32_t m,
-                 NphGpuJoint *joints, uint32_t nj, NphGpuBody *bodies, uint32_t n, float dt)
+// store_group (solver.c:475-499) on staged records.
+__global__ void __launch_bounds__(kStage) k_store_contacts(DevSolver S, NphGpuContact *contacts,
+                                                           uint32_t m)
 {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < m) {
-        store_manifold(S, i, contacts[i]);
-        return;
+    __shared__ NphGpuContact rec[kStage];
+    const uint32_t first = blockIdx.x * kStage;
+    const uint32_t count = min(kStage, m - first);
+    stage_in<uint4>(contacts + first, count, rec);
+    __syncthreads();
+    if (threadIdx.x < count) {
+        store_manifold(S, first + threadIdx.x, rec[threadIdx.x]);
     }
-    i -= m;
-    if (i < nj) {
-        store_joint(S, i, joints[i]);
-        return;
+    __syncthreads();
+    stage_out<uint4>(rec, count, contacts + first);
+}
+
+// The joints' accumulated impulses back into their records.
+__global__ void __launch_bounds__(kStage) k_store_joints(DevSolver S, NphGpuJoint *joints, uint32_t nj)
+{
+    __shared__ NphGpuJoint rec[kStage];
+    const uint32_t first = blockIdx.x * kStage;
+    const uint32_t count = min(kStage, nj - first);
+    stage_in<uint2>(joints + first, count, rec);
+    __syncthreads();
+    if (threadIdx.x < count) {
+        store_joint(S, first + threadIdx.x, rec[threadIdx.x]);
     }
-    i -= nj;
-    if (i < n) {
-        finalize_body(B, i, bodies[i], dt);
+    __syncthreads();
+    stage_out<uint2>(rec, count, joints + first);
+}
+
+// finalize_body, solver.c:304-324, on staged records.
+__global__ void __launch_bounds__(kStage) k_finalize(BodyArrays B, NphGpuBody *bodies, uint32_t n,
+                                                     float dt)
+{
+    __shared__ NphGpuBody rec[kStage];
+    const uint32_t first = blockIdx.x * kStage;
+    const uint32_t count = min(kStage, n - first);
+    stage_in<uint4>(bodies + first, count, rec);
+    __syncthreads();
+    if (threadIdx.x < count) {
+        finalize_body(B, first + threadIdx.x, rec[threadIdx.x], dt);
     }
+    __syncthreads();
+    stage_out<uint4>(rec, count, bodies + first);
 }
 
 // post_finalize, solver.c:851-857: a driven joint's bodies stay awake.
@@ -254,6 +420,7 @@ __global__ void __launch_bounds__(kBlock) k_driven(DevSolver S, NphGpuBody *bodi
 // ------------------------------------------------------------------------------------
 
 static uint32_t blocks_for(uint64_t count) { return (uint32_t)((count + kBlock - 1) / kBlock); }
+static uint32_t stage_blocks(uint64_t count) { return (uint32_t)((count + kStage - 1) / kStage); }
 
 // solver.c:48-65 on the host, in FP32 as the reference.
 static Soft host_make_soft(float hertz, float zeta, float h)
@@ -303,6 +470,8 @@ struct NphGpuSolver {
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    cudaStream_t side = nullptr; // a colour's joints run here beside its contacts
+    cudaEvent_t fork_event = nullptr, join_event = nullptr;
     bool use_graph = true;
     // Capacities of the device arrays.
     uint32_t bcap = 0, fcap = 0, mcap = 0, jcap = 0;
@@ -312,6 +481,7 @@ struct NphGpuSolver {
     NphGpuContact *d_contacts = nullptr;
     NphGpuJoint *d_joints = nullptr;
     // Solver state.
+    float4 *body_rows = nullptr; // vel | pos | prm
     float4 *vel = nullptr, *pos = nullptr, *prm = nullptr, *itg = nullptr;
     uint4 *hdr = nullptr;
     float4 *nrm = nullptr;
@@ -336,6 +506,8 @@ struct NphGpuSolver {
     uint32_t ccount[NPH_GPU_COLOR_SLOTS] = {}, jcount[NPH_GPU_COLOR_SLOTS] = {};
     uint32_t cfirst[NPH_GPU_COLOR_SLOTS] = {}, jfirst[NPH_GPU_COLOR_SLOTS] = {};
     uint32_t driven = 0;
+    // Pass configuration per pass kind (warm, solve, relax, restitution).
+    uint32_t pass_config[4] = {2, 7, 7, 0};
     // The step graph and what it was captured for.
     cudaGraphExec_t graph = nullptr;
     StepConsts graph_consts{};
@@ -380,8 +552,14 @@ NphGpuResult ensure_capacity(NphGpuSolver *s, uint32_t n, uint32_t nf, uint32_t 
     bool ok = true;
     if (n + 1u > s->bcap) {
         const uint32_t cap = n + 1u + (n + 1u) / 8u;
-        ok = ok && dalloc(s->d_bodies, cap) && dalloc(s->vel, 2ull * cap) &&
-             dalloc(s->pos, 2ull * cap) && dalloc(s->prm, 3ull * cap) && dalloc(s->itg, 6ull * cap);
+        // vel, pos and prm in one allocation: the body rows the constraint passes gather.
+        ok = ok && dalloc(s->d_bodies, cap) && dalloc(s->body_rows, 7ull * cap) &&
+             dalloc(s->itg, 6ull * cap);
+        if (ok) {
+            s->vel = s->body_rows;
+            s->pos = s->body_rows + 2ull * cap;
+            s->prm = s->body_rows + 4ull * cap;
+        }
         s->bcap = ok ? cap : 0;
     }
     if (ok && nf > s->fcap) {
@@ -447,11 +625,13 @@ enum Kind : int {
     kKStoreFinalize,
     kKOverflow,
     kKDriven,
+    kKJoints,
     kKinds
 };
 const char *const kKindNames[kKinds] = {"prepare_bodies", "prepare_constraints", "integrate_velocity",
                                         "warm_start", "solve", "integrate_position", "relax",
-                                        "restitution", "store_finalize", "overflow", "driven"};
+                                        "restitution", "store_finalize", "overflow", "driven",
+                                        "joints"};
 
 cudaEvent_t next_event(NphGpuSolver *s)
 {
@@ -511,12 +691,31 @@ template <int P> void enqueue_pass(NphGpuSolver *s, const StepConsts &K)
         if (jc == 0u && cc == 0u) {
             continue;
         }
-        const uint32_t jb = blocks_for(jc);
-        mark_begin(s, kind, (uint64_t)cc + jc, bytes(c, jc));
-        k_pass<P><<<jb + blocks_for(cc), kBlock, 0, s->stream>>>(S, s->cfirst[c], cc, s->jfirst[c], jc,
-                                                                 jb, K);
-        mark_end(s);
-        s->launches++;
+        // The colour's joints beside its contacts: forked to the side stream and joined back
+        // (sequential on the solver's stream when a profiled step times each launch).
+        const bool fork = jc > 0u && cc > 0u && s->marks == nullptr;
+        if (jc > 0u) {
+            cudaStream_t js = s->stream;
+            if (fork) {
+                cudaEventRecord(s->fork_event, s->stream);
+                cudaStreamWaitEvent(s->side, s->fork_event, 0);
+                js = s->side;
+            }
+            mark_begin(s, kKJoints, jc, 330.0 * jc);
+            k_joint_pass<P><<<blocks_for(jc), kBlock, 0, js>>>(S, s->jfirst[c], jc, K);
+            mark_end(s);
+            s->launches++;
+        }
+        if (cc > 0u) {
+            mark_begin(s, kind, cc, bytes(c, 0u));
+            launch_pass<P>(s->pass_config[P], cc, s->stream, S, s->cfirst[c], K);
+            mark_end(s);
+            s->launches++;
+        }
+        if (fork) {
+            cudaEventRecord(s->join_event, s->side);
+            cudaStreamWaitEvent(s->stream, s->join_event, 0);
+        }
     }
 }
 
@@ -528,19 +727,24 @@ void enqueue_step(NphGpuSolver *s, const StepConsts &K, uint32_t substeps)
     const double n = s->n;
     s->launches = 0;
     mark_begin(s, kKPrepareBodies, s->n, 368.0 * n);
-    k_prepare_bodies<<<blocks_for(s->n + 1u), kBlock, 0, s->stream>>>(B, s->d_bodies, s->n, K);
+    k_prepare_bodies<<<stage_blocks(s->n + 1u), kStage, 0, s->stream>>>(B, s->d_bodies, s->n, K);
     mark_end(s);
     s->launches++;
     ColorTable T;
     std::memcpy(T.cfirst, s->cfirst, sizeof T.cfirst);
     std::memcpy(T.ccount, s->ccount, sizeof T.ccount);
-    const uint32_t jb = blocks_for(s->nj);
-    if (s->m + s->nj > 0u) {
-        cudaMemsetAsync(s->d_err + 1, 0, NPH_GPU_COLOR_SLOTS * sizeof(uint32_t), s->stream);
-        mark_begin(s, kKPrepareConstraints, (uint64_t)s->m + s->nj, 936.0 * s->m + 330.0 * s->nj);
-        k_prepare_constraints<<<jb + blocks_for(s->m), kBlock, 0, s->stream>>>(
-            S, s->d_contacts, s->d_joints, s->d_bodies, s->d_fixed, s->n, s->nf, s->m, s->nj, jb, T,
-            K.h, s->d_err, s->d_err + 1);
+    cudaMemsetAsync(s->d_err + 1, 0, NPH_GPU_COLOR_SLOTS * sizeof(uint32_t), s->stream);
+    if (s->nj > 0u) {
+        mark_begin(s, kKPrepareConstraints, s->nj, 330.0 * s->nj);
+        k_prepare_joints<<<stage_blocks(s->nj), kStage, 0, s->stream>>>(
+            S, s->d_joints, s->d_bodies, s->d_fixed, s->n, s->nf, s->nj, K.h, s->d_err);
+        mark_end(s);
+        s->launches++;
+    }
+    if (s->m > 0u) {
+        mark_begin(s, kKPrepareConstraints, s->m, 936.0 * s->m);
+        k_prepare_contacts<<<stage_blocks(s->m), kStage, 0, s->stream>>>(
+            S, s->d_contacts, s->d_fixed, s->n, s->nf, s->m, T, s->d_err, s->d_err + 1);
         mark_end(s);
         s->launches++;
     }
@@ -557,9 +761,20 @@ void enqueue_step(NphGpuSolver *s, const StepConsts &K, uint32_t substeps)
         s->launches += 2;
     }
     enqueue_pass<kRestitution>(s, K);
-    mark_begin(s, kKStoreFinalize, (uint64_t)s->m + s->nj + s->n, 160.0 * s->m + 330.0 * s->nj + 200.0 * n);
-    k_store_finalize<<<blocks_for((uint64_t)s->m + s->nj + s->n), kBlock, 0, s->stream>>>(
-        S, B, s->d_contacts, s->m, s->d_joints, s->nj, s->d_bodies, s->n, K.dt);
+    if (s->m > 0u) {
+        mark_begin(s, kKStoreFinalize, s->m, 160.0 * s->m);
+        k_store_contacts<<<stage_blocks(s->m), kStage, 0, s->stream>>>(S, s->d_contacts, s->m);
+        mark_end(s);
+        s->launches++;
+    }
+    if (s->nj > 0u) {
+        mark_begin(s, kKStoreFinalize, s->nj, 330.0 * s->nj);
+        k_store_joints<<<stage_blocks(s->nj), kStage, 0, s->stream>>>(S, s->d_joints, s->nj);
+        mark_end(s);
+        s->launches++;
+    }
+    mark_begin(s, kKStoreFinalize, s->n, 200.0 * n);
+    k_finalize<<<stage_blocks(s->n), kStage, 0, s->stream>>>(B, s->d_bodies, s->n, K.dt);
     mark_end(s);
     s->launches++;
     if (s->driven > 0u) {
@@ -797,13 +1012,20 @@ NPH_GPU_API NphGpuResult nph_gpu_solver_create(const NphGpuSolverDesc *desc, Nph
         }
         s->own_stream = true;
     }
-    bool ok = dalloc(s->d_err, 32) && cudaMallocHost((void **)&s->h_err, 32 * sizeof(uint32_t)) == cudaSuccess;
+    bool ok = cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&s->fork_event, cudaEventDisableTiming) == cudaSuccess &&
+              cudaEventCreateWithFlags(&s->join_event, cudaEventDisableTiming) == cudaSuccess &&
+              dalloc(s->d_err, 32) && cudaMallocHost((void **)&s->h_err, 32 * sizeof(uint32_t)) == cudaSuccess;
     for (auto &e : s->ev) {
         ok = ok && cudaEventCreate(&e) == cudaSuccess;
     }
     if (ok) {
         ok = ensure_capacity(s, d.body_capacity, 0, d.contact_capacity, d.joint_capacity) == NPH_GPU_OK;
     }
+    allow_tiles<kWarm>();
+    allow_tiles<kSolve>();
+    allow_tiles<kRelax>();
+    allow_tiles<kRestitution>();
     if (!ok) {
         nph_gpu_solver_destroy(s);
         return NPH_GPU_OUT_OF_MEMORY;
@@ -826,9 +1048,8 @@ NPH_GPU_API void nph_gpu_solver_destroy(NphGpuSolver *s)
     dfree(s->d_fixed);
     dfree(s->d_contacts);
     dfree(s->d_joints);
-    dfree(s->vel);
-    dfree(s->pos);
-    dfree(s->prm);
+    dfree(s->body_rows);
+    s->vel = s->pos = s->prm = nullptr;
     dfree(s->itg);
     dfree(s->hdr);
     dfree(s->nrm);
@@ -849,6 +1070,16 @@ NPH_GPU_API void nph_gpu_solver_destroy(NphGpuSolver *s)
     }
     for (auto &e : s->event_pool) {
         cudaEventDestroy(e);
+    }
+    if (s->fork_event != nullptr) {
+        cudaEventDestroy(s->fork_event);
+    }
+    if (s->join_event != nullptr) {
+        cudaEventDestroy(s->join_event);
+    }
+    if (s->side != nullptr) {
+        cudaStreamSynchronize(s->side);
+        cudaStreamDestroy(s->side);
     }
     if (s->own_stream && s->stream != nullptr) {
         cudaStreamDestroy(s->stream);
@@ -1012,6 +1243,90 @@ NPH_GPU_API NphGpuResult nph_gpu_world_profile_step(NphGpuSolver *s, const NphGp
     }
     *count = n < capacity ? n : capacity;
     fill_stats(s);
+    return NPH_GPU_OK;
+}
+
+NPH_GPU_API NphGpuResult nph_gpu_solver_set_pass_config(NphGpuSolver *s, uint32_t pass,
+                                                         uint32_t config)
+{
+    if (s == nullptr || pass >= 4u || config >= kPassConfigCount) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    if (s->pass_config[pass] != config) {
+        s->pass_config[pass] = config;
+        drop_graph(s);
+    }
+    return NPH_GPU_OK;
+}
+
+NPH_GPU_API uint32_t nph_gpu_pass_config_count(void) { return kPassConfigCount; }
+
+NPH_GPU_API NphGpuResult nph_gpu_solver_autotune(NphGpuSolver *s, const NphGpuWorldParams *params,
+                                                 float dt, uint32_t rounds, uint32_t *chosen)
+{
+    if (s == nullptr) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    NphGpuResult r = validate_params(params, dt);
+    if (r != NPH_GPU_OK) {
+        return r;
+    }
+    if (!s->uploaded) {
+        return NPH_GPU_INVALID_STATE;
+    }
+    cudaSetDevice(s->device);
+    const StepConsts K = make_step_consts(*params, dt);
+    const int kinds[4] = {kKWarm, kKSolve, kKRelax, kKRestitution};
+    double best_ms[4];
+    uint32_t best[4];
+    for (uint32_t p = 0; p < 4; ++p) {
+        best_ms[p] = 1e300;
+        best[p] = s->pass_config[p];
+    }
+    rounds = rounds == 0u ? 1u : rounds;
+    for (uint32_t c = 0; c < kPassConfigCount; ++c) {
+        for (uint32_t p = 0; p < 4; ++p) {
+            s->pass_config[p] = c;
+        }
+        double ms[4] = {0.0, 0.0, 0.0, 0.0};
+        for (uint32_t round = 0; round <= rounds; ++round) {
+            std::vector<NphGpuSolver::Mark> marks;
+            marks.reserve(1024);
+            s->marks = &marks;
+            s->events_used = 0;
+            enqueue_step(s, K, params->substeps);
+            s->marks = nullptr;
+            r = check_cuda(cudaStreamSynchronize(s->stream));
+            if (r != NPH_GPU_OK) {
+                return r;
+            }
+            if (round == 0u) {
+                continue; // the first step of a configuration warms its kernels
+            }
+            for (const auto &m : marks) {
+                float t = 0.0f;
+                cudaEventElapsedTime(&t, m.a, m.b);
+                for (uint32_t p = 0; p < 4; ++p) {
+                    if (m.kind == kinds[p]) {
+                        ms[p] += t;
+                    }
+                }
+            }
+        }
+        for (uint32_t p = 0; p < 4; ++p) {
+            if (ms[p] < best_ms[p]) {
+                best_ms[p] = ms[p];
+                best[p] = c;
+            }
+        }
+    }
+    for (uint32_t p = 0; p < 4; ++p) {
+        s->pass_config[p] = best[p];
+        if (chosen != nullptr) {
+            chosen[p] = best[p];
+        }
+    }
+    drop_graph(s);
     return NPH_GPU_OK;
 }
 

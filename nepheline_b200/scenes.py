@@ -246,3 +246,236 @@ def host_color(scene: SolverScene) -> tuple[np.ndarray, np.ndarray]:
         slot[i] = lens[kind, c]
         lens[kind, c] += 1
     return color, slot
+
+
+# ---------------------------------------------------------------------------------------
+# Batched worlds: box pyramids, sphere piles and capsule chains on hinges
+# ---------------------------------------------------------------------------------------
+
+_DENSITY = 1000.0
+
+
+def _ground() -> np.ndarray:
+    g = np.zeros(1, abi.BODY_DTYPE)
+    g["rotation"][:, 3] = 1.0
+    g["type"] = abi.BODY_STATIC
+    g["center"][:, 1] = -1.0
+    g["origin"][:, 1] = -1.0
+    return g
+
+
+class _WorldBuilder:
+    """Bodies resting on a ground (the world's one fixed body, index n), with their manifolds
+    and joints in insertion order; all shapes' contacts computed analytically at rest."""
+
+    def __init__(self, rng):
+        self.rng = rng
+        self.centers: list = []
+        self.mass: list = []
+        self.inertia: list = []
+        self.extent: list = []
+        self.contacts: list = []
+        self.joints: list = []
+        self.x = 0.0  # next free x on the ground
+
+    def body(self, center, mass, inertia_diag, extent) -> int:
+        self.centers.append(center)
+        self.mass.append(mass)
+        self.inertia.append(inertia_diag)
+        self.extent.append(extent)
+        return len(self.centers) - 1
+
+    GROUND = -1  # resolved to the fixed body's index at the end
+
+    def pyramid(self, rows: int):
+        """Unit boxes, row r holding rows - r boxes at 1.05 m spacing."""
+        m = _DENSITY
+        ids = {}
+        for r in range(rows):
+            cnt = rows - r
+            for j in range(cnt):
+                x = self.x + (j - (cnt - 1) / 2) * 1.05
+                ids[(r, j)] = self.body((x, 0.5 + r - 0.005 * r, 0.0), m, (m / 6,) * 3, 0.866)
+        half = 0.5
+        for r in range(rows):
+            cnt = rows - r
+            for j in range(cnt):
+                b = ids[(r, j)]
+                if r == 0:
+                    corners_b = [(-half, -half, -half), (half, -half, -half), (half, -half, half),
+                                 (-half, -half, half)]
+                    cx, cy, cz = self.centers[b]
+                    # A is the ground (centre y = -1): anchors from its centre.
+                    pa = [(cx + p[0], cy + p[1] + 1.0, cz + p[2]) for p in corners_b]
+                    self.contacts.append((self.GROUND, b, (0, 1, 0), pa, corners_b, -0.005, 0.6))
+                else:
+                    for dj in (0, 1):
+                        a = ids[(r - 1, j + dj)]
+                        ax = self.centers[a][0]
+                        bx = self.centers[b][0]
+                        lo = max(ax, bx) - half + abs(ax - bx) * 0.0
+                        x0, x1 = max(ax - half, bx - half), min(ax + half, bx + half)
+                        dy = self.centers[b][1] - self.centers[a][1]
+                        pts_world = [(x0, -half), (x1, -half), (x1, half), (x0, half)]
+                        pa = [(px - ax, half, pz) for px, pz in pts_world]
+                        pb = [(px - bx, half - dy, pz) for px, pz in pts_world]
+                        self.contacts.append((a, b, (0, 1, 0), pa, pb, -0.005, 0.6))
+        self.x += rows * 1.05 + 2.0
+
+    def pile(self, columns: int, height: int):
+        """Spheres of radius 0.5 stacked in columns (one-point manifolds)."""
+        r = 0.5
+        m = _DENSITY * 4.0 / 3.0 * np.pi * r ** 3
+        for c in range(columns):
+            x = self.x + c * 1.1
+            prev = None
+            for h in range(height):
+                y = r + h * (2 * r - 0.004)
+                b = self.body((x, y, 0.0), m, (0.4 * m * r * r,) * 3, r)
+                if prev is None:
+                    self.contacts.append((self.GROUND, b, (0, 1, 0), [(x, 1.0 + y - r, 0.0)],
+                                          [(0.0, -r, 0.0)], -0.002, 0.5, 0.2))
+                else:
+                    self.contacts.append((prev, b, (0, 1, 0), [(0.0, r, 0.0)], [(0.0, -r, 0.0)],
+                                          -0.004, 0.5, 0.2))
+                prev = b
+        self.x += columns * 1.1 + 2.0
+
+    def chain(self, links: int):
+        """Capsules (radius 0.25, 1 m long) lying along x on hinges about z at their ends."""
+        rad, half_len = 0.25, 0.25
+        m = _DENSITY * (np.pi * rad * rad * 2 * half_len + 4.0 / 3.0 * np.pi * rad ** 3)
+        ix = m * (0.5 * rad * rad)
+        iy = m * (0.25 * rad * rad + (2 * half_len + rad) ** 2 / 12.0)
+        prev = None
+        for k in range(links):
+            x = self.x + 0.5 + k * 1.0
+            b = self.body((x, rad - 0.002, 0.0), m, (ix, iy, iy), 0.5)
+            cx, cy, cz = self.centers[b]
+            pb = [(-half_len, -rad, 0.0), (half_len, -rad, 0.0)]
+            pa = [(cx + p[0], cy + p[1] + 1.0, cz) for p in pb]
+            self.contacts.append((self.GROUND, b, (0, 1, 0), pa, pb, -0.002, 0.7))
+            if prev is not None:
+                j = np.zeros(1, abi.JOINT_DTYPE)
+                j["type"] = abi.JOINT_HINGE
+                j["body_a"] = prev
+                j["body_b"] = b
+                j["frame_a_position"] = (0.5, 0.0, 0.0)
+                j["frame_b_position"] = (-0.5, 0.0, 0.0)
+                s = np.sqrt(0.5)
+                j["frame_a_rotation"] = (0.0, -s, 0.0, s)  # frame X along world z
+                j["frame_b_rotation"] = (0.0, -s, 0.0, s)
+                self.joints.append(j)
+            prev = b
+        self.x += links * 1.0 + 2.0
+
+    def scene(self) -> "SolverScene":
+        n = len(self.centers)
+        bodies = body_records(n)
+        bodies["center"] = np.asarray(self.centers, np.float64)
+        bodies["origin"] = bodies["center"]
+        mass = np.asarray(self.mass, np.float32)
+        inertia = np.zeros((n, 9), np.float32)
+        diag = np.asarray(self.inertia, np.float32)
+        inertia[:, 0], inertia[:, 4], inertia[:, 8] = diag[:, 0], diag[:, 1], diag[:, 2]
+        set_mass(bodies, mass, inertia)
+        bodies["max_extent"] = np.asarray(self.extent, np.float32)
+        m = len(self.contacts)
+        contacts = np.zeros(m, abi.CONTACT_DTYPE)
+        if m:
+            a = np.array([c[0] for c in self.contacts], np.int64)
+            contacts["body_a"] = np.where(a == self.GROUND, n, a)
+            contacts["body_b"] = [c[1] for c in self.contacts]
+            contacts["normal"] = np.array([c[2] for c in self.contacts], np.float32)
+            counts = np.array([len(c[3]) for c in self.contacts], np.uint32)
+            contacts["point_count"] = counts
+            contacts["friction"] = [c[6] for c in self.contacts]
+            contacts["restitution"] = [c[7] if len(c) > 7 else 0.0 for c in self.contacts]
+            pa = np.zeros((m, 4, 3), np.float32)
+            pb = np.zeros((m, 4, 3), np.float32)
+            sep = np.zeros((m, 4), np.float32)
+            for i, c in enumerate(self.contacts):
+                k = len(c[3])
+                pa[i, :k] = c[3]
+                pb[i, :k] = c[4]
+                sep[i, :k] = c[5]
+            pts = contacts["points"]
+            pts["anchor_a"] = pa
+            pts["anchor_b"] = pb
+            pts["separation"] = sep
+            pts["id"] = np.arange(4, dtype=np.uint32)[None, :]
+        joints = np.concatenate(self.joints) if self.joints else np.zeros(0, abi.JOINT_DTYPE)
+        return SolverScene(bodies=bodies, mass=mass, joints=joints, contacts=contacts,
+                           fixed=_ground())
+
+
+def mixed_world(bodies: int, seed: int) -> SolverScene:
+    """One world of about `bodies` bodies: a seeded mix of box pyramids, sphere piles and
+    capsule chains on hinges, resting on a ground."""
+    rng = np.random.default_rng(seed)
+    wb = _WorldBuilder(rng)
+    share = rng.dirichlet((1.0, 1.0, 1.0))
+    want = [int(round(bodies * s)) for s in share]
+    while sum(want) < bodies:
+        want[int(rng.integers(0, 3))] += 1
+    # Pyramids: rows with rows (rows + 1) / 2 <= the share.
+    left = want[0]
+    while left >= 3:
+        rows = int(min(20, max(2, np.floor((np.sqrt(8 * left + 1) - 1) / 2))))
+        wb.pyramid(rows)
+        left -= rows * (rows + 1) // 2
+    left += want[1]
+    while left >= 1:
+        h = int(min(left, rng.integers(1, 8)))
+        cols = max(1, min(left // h, int(rng.integers(1, 16))))
+        wb.pile(cols, h)
+        left -= cols * h
+    left = want[2]
+    while left >= 2:
+        links = int(min(left, rng.integers(2, 40)))
+        wb.chain(links)
+        left -= links
+    if not wb.centers:
+        wb.pile(1, 1)
+    return wb.scene()
+
+
+def color_scenes(solver, scs: list) -> list:
+    """Colours many disjoint scenes in one device call and lays each out as its own view:
+    disjoint worlds colour as they would alone, and each world's list slots are its own."""
+    offs = np.cumsum([0] + [len(s.bodies) + (0 if s.fixed is None else len(s.fixed)) for s in scs])
+    aa, bb, dd, world, kind = [], [], [], [], []
+    for w, s in enumerate(scs):
+        a, b, d = s.constraint_arrays()
+        aa.append(a + offs[w])
+        bb.append(b + offs[w])
+        dd.append(d)
+        world.append(np.full(len(a), w, np.int64))
+    a = np.concatenate(aa).astype(np.uint32)
+    b = np.concatenate(bb).astype(np.uint32)
+    d = np.concatenate(dd).astype(np.uint8)
+    world = np.concatenate(world)
+    color, _ = solver.graph_color(a, b, d, int(offs[-1]))
+    # Slots per (world, kind, colour) in insertion order.
+    key = (world * 2 + (d >> 2 & 1)) * abi.COLOR_SLOTS + color
+    order = np.argsort(key, kind="stable")
+    sorted_key = key[order]
+    starts = np.r_[0, np.flatnonzero(np.diff(sorted_key)) + 1]
+    rank = np.arange(len(key)) - np.repeat(starts, np.diff(np.r_[starts, len(key)]))
+    slot = np.empty(len(key), np.uint32)
+    slot[order] = rank
+    views = []
+    first = 0
+    for s in scs:
+        cnt = s.constraint_count
+        views.append(s.to_view(color[first:first + cnt], slot[first:first + cnt]))
+        first += cnt
+    return views
+
+
+def batched_worlds(count: int = 4096, seed: int = 0, min_bodies: int = 8,
+                   max_bodies: int = 4096) -> list:
+    """`count` worlds with body counts log-uniform in [min_bodies, max_bodies]."""
+    rng = np.random.default_rng(seed)
+    sizes = np.round(np.exp(rng.uniform(np.log(min_bodies), np.log(max_bodies), count))).astype(int)
+    return [mixed_world(int(n), seed * 1_000_003 + i) for i, n in enumerate(sizes)]

@@ -50,6 +50,24 @@ def lib() -> ctypes.CDLL:
         "nph_gpu_version": (ctypes.c_char_p, []),
         "nph_gpu_world_profile_step": (ctypes.c_int32, [_vp, P(abi.WorldParams), ctypes.c_float,
                                                         P(abi.KernelTime), _u32, P(_u32)]),
+        "nph_gpu_solver_set_pass_config": (ctypes.c_int32, [_vp, _u32, _u32]),
+        "nph_gpu_batch_create": (ctypes.c_int32, [P(abi.SolverDesc), P(_vp)]),
+        "nph_gpu_batch_destroy": (None, [_vp]),
+        "nph_gpu_batch_stream": (_vp, [_vp]),
+        "nph_gpu_batch_upload": (ctypes.c_int32, [_vp, P(abi.WorldView), _u32]),
+        "nph_gpu_batch_step_async": (ctypes.c_int32, [_vp, P(abi.WorldParams), ctypes.c_float,
+                                                      _u32]),
+        "nph_gpu_batch_download": (ctypes.c_int32, [_vp, P(abi.WorldView), _u32]),
+        "nph_gpu_phys_solve_worlds": (ctypes.c_int32, [_vp, P(abi.WorldParams), ctypes.c_float,
+                                                       P(abi.WorldView), _u32]),
+        "nph_gpu_batch_set_config": (ctypes.c_int32, [_vp, _u32, _u32]),
+        "nph_gpu_batch_config_count": (_u32, []),
+        "nph_gpu_batch_autotune": (ctypes.c_int32, [_vp, P(abi.WorldParams), ctypes.c_float,
+                                                    _u32, P(abi.BatchTuning)]),
+        "nph_gpu_batch_info": (ctypes.c_int32, [_vp, P(abi.BatchInfo)]),
+        "nph_gpu_pass_config_count": (_u32, []),
+        "nph_gpu_solver_autotune": (ctypes.c_int32, [_vp, P(abi.WorldParams), ctypes.c_float,
+                                                     _u32, P(_u32)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -137,6 +155,17 @@ class Solver:
                  "units": arr[i].units, "total_ms": arr[i].total_ms,
                  "algorithmic_bytes": arr[i].algorithmic_bytes} for i in range(n.value)]
 
+    def set_pass_config(self, pass_kind: int, config: int) -> None:
+        _check(self.L.nph_gpu_solver_set_pass_config(self._h, pass_kind, config),
+               "nph_gpu_solver_set_pass_config")
+
+    def autotune(self, params: abi.WorldParams, dt: float, rounds: int = 1) -> list[int]:
+        """Picks the fastest launch configuration per pass kind on the uploaded world."""
+        chosen = (_u32 * 4)()
+        _check(self.L.nph_gpu_solver_autotune(self._h, ctypes.byref(params), dt, rounds, chosen),
+               "nph_gpu_solver_autotune")
+        return list(chosen)
+
     def graph_color(self, body_a, body_b, dynamic_bits, body_slots: int):
         """Device colouring of constraints in insertion order (graph_pick_color)."""
         a = np.ascontiguousarray(body_a, np.uint32)
@@ -148,6 +177,82 @@ class Solver:
                                           len(a), body_slots, color.ctypes.data,
                                           slot.ctypes.data), "nph_gpu_graph_color")
         return color, slot
+
+
+class Batch:
+    """Many independent worlds stepped in one persistent launch (NphGpuBatch)."""
+
+    def __init__(self, device: int = 0, use_graph: bool = True):
+        L = lib()
+        d = abi.SolverDesc()
+        d.device = device
+        d.use_graph = 1 if use_graph else 0
+        h = _vp()
+        _check(L.nph_gpu_batch_create(ctypes.byref(d), ctypes.byref(h)), "nph_gpu_batch_create")
+        self._h = h
+        self.L = L
+        self._views = None
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.L.nph_gpu_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def stream(self) -> int:
+        return int(self.L.nph_gpu_batch_stream(self._h) or 0)
+
+    @staticmethod
+    def _c_views(views):
+        arr = (abi.WorldView * max(len(views), 1))()
+        for i, v in enumerate(views):
+            arr[i] = v.c_view()
+        return arr
+
+    def upload(self, views: list) -> None:
+        self._views = views
+        arr = self._c_views(views)
+        _check(self.L.nph_gpu_batch_upload(self._h, arr, len(views)), "nph_gpu_batch_upload")
+
+    def step_async(self, params: abi.WorldParams, dt: float, steps: int = 1) -> None:
+        _check(self.L.nph_gpu_batch_step_async(self._h, ctypes.byref(params), dt, steps),
+               "nph_gpu_batch_step_async")
+
+    def download(self, views: list) -> None:
+        arr = self._c_views(views)
+        _check(self.L.nph_gpu_batch_download(self._h, arr, len(views)), "nph_gpu_batch_download")
+
+    def phys_solve_worlds(self, views: list, params: abi.WorldParams, dt: float) -> None:
+        arr = self._c_views(views)
+        _check(self.L.nph_gpu_phys_solve_worlds(self._h, ctypes.byref(params), dt, arr,
+                                                len(views)), "nph_gpu_phys_solve_worlds")
+
+    def phys_solve_worlds_code(self, views: list, params: abi.WorldParams, dt: float) -> int:
+        arr = self._c_views(views)
+        return int(self.L.nph_gpu_phys_solve_worlds(self._h, ctypes.byref(params), dt, arr,
+                                                    len(views)))
+
+    def set_config(self, config: int, shared_velocities: bool) -> None:
+        _check(self.L.nph_gpu_batch_set_config(self._h, config, int(shared_velocities)),
+               "nph_gpu_batch_set_config")
+
+    def autotune(self, params: abi.WorldParams, dt: float, rounds: int = 1) -> dict:
+        t = abi.BatchTuning()
+        _check(self.L.nph_gpu_batch_autotune(self._h, ctypes.byref(params), dt, rounds,
+                                             ctypes.byref(t)), "nph_gpu_batch_autotune")
+        return {"config": t.config, "threads": t.threads,
+                "shared_velocities": t.shared_velocities, "ms_per_step": t.ms_per_step}
+
+    def info(self) -> dict:
+        i = abi.BatchInfo()
+        _check(self.L.nph_gpu_batch_info(self._h, ctypes.byref(i)), "nph_gpu_batch_info")
+        return {k: getattr(i, k) for k, _ in abi.BatchInfo._fields_ if k != "pad"}
 
 
 def version() -> str:

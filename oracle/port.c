@@ -27,6 +27,22 @@
 #undef ATAN2
 #undef ABS
 
+// FP32 with the correctly rounded arctangent (the double-precision atan2 rounded once to FP32),
+// the device solver's angle: the device must equal this instance bit for bit, and this
+// instance differs from the reference only through the host C library's atan2f rounding.
+static float atan2_cr(float y, float x) { return (float)atan2((double)y, (double)x); }
+#define REAL float
+#define SUF _f32cr
+#define SQRT sqrtf
+#define ATAN2 atan2_cr
+#define ABS fabsf
+#include "port_impl.h"
+#undef REAL
+#undef SUF
+#undef SQRT
+#undef ATAN2
+#undef ABS
+
 #define REAL double
 #define SUF _f64
 #define SQRT sqrt
@@ -84,6 +100,9 @@ static int joint_is_driven(const NphGpuJoint *j)
            j->u.hinge.motor_speed != 0.0F && j->u.hinge.max_motor_torque > 0.0F;
 }
 
+// The FP32 write-back of a step into the view (finalize, store, joints, driven sleep reset).
+static void write_back_f32(const Result_f32 *rp, float dt, NphGpuWorldView *v);
+
 // The FP32 solve, in place on the view, as the device library's nph_gpu_phys_solve.
 PORT_API int nph_port32_solve(const NphGpuWorldParams *wp, float dt, NphGpuWorldView *v)
 {
@@ -96,6 +115,32 @@ PORT_API int nph_port32_solve(const NphGpuWorldParams *wp, float dt, NphGpuWorld
     if (res != NPH_GPU_OK) {
         return res;
     }
+    write_back_f32(&r, dt, v);
+    return NPH_GPU_OK;
+}
+
+// The same with the correctly rounded arctangent in the joints' angle rows.
+PORT_API int nph_port32cr_solve(const NphGpuWorldParams *wp, float dt, NphGpuWorldView *v)
+{
+    const int bad = check_view(wp, v);
+    if (bad != NPH_GPU_OK) {
+        return bad;
+    }
+    Result_f32cr rc;
+    const int res = run_f32cr(wp, dt, v, &rc);
+    if (res != NPH_GPU_OK) {
+        return res;
+    }
+    // The two FP32 instances have the same layout: only their angle function differs.
+    Result_f32 r;
+    memcpy(&r, &rc, sizeof r);
+    write_back_f32(&r, dt, v);
+    return NPH_GPU_OK;
+}
+
+static void write_back_f32(const Result_f32 *rp, float dt, NphGpuWorldView *v)
+{
+    Result_f32 r = *rp;
     // finalize_body (solver.c:304-349). Recomputed from the FP32 prepare: q0 is the record's.
     for (unsigned i = 0U; i < r.n; ++i) {
         NphGpuBody *b = &v->bodies[i];
@@ -179,7 +224,6 @@ PORT_API int nph_port32_solve(const NphGpuWorldParams *wp, float dt, NphGpuWorld
     free(r.bodies);
     free(r.m);
     free(r.j);
-    return NPH_GPU_OK;
 }
 
 // What the FP64 step returns: the same results as the FP32 write-back, in double.

@@ -1,6 +1,7 @@
 """Golden vectors made by the reference itself (tests/golden/make_golden.py): one step of the
 reference's phys_solve per fixture, input and output views. The CPU restatement and the
-device solver must reproduce the outputs (the device's joint angle rows within 1e-5)."""
+device solver must reproduce the outputs; the device's joint angle rows (correctly rounded
+arctangent) equal the restatement with that angle, and the reference within its rounding."""
 from __future__ import annotations
 
 from pathlib import Path
@@ -33,7 +34,9 @@ def test_device_reproduces_reference_golden(path, solver):
     dev = vin.copy()
     solver.phys_solve(dev, params, dt)
     if path.stem in ANGLE_ROWS:
+        from oracle.refworld import port32cr
+        assert not helpers.mismatches(dev, port32cr(vin, params, dt))
         err = helpers.max_normwise_err(dev, vout)
-        assert max(err.values()) < 1e-5, err
+        assert max(err.values()) < 1e-3, err
     else:
         assert not helpers.mismatches(dev, vout)
