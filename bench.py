@@ -51,6 +51,10 @@ def parse():
                     help="lattice bodies per axis (128,128,64: 1,048,576 bodies)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=("lattice", "batched"), default="lattice",
+                    help="lattice: the 1M-body constraint graph (the headline); batched: "
+                         "--worlds independent worlds in one persistent launch")
+    ap.add_argument("--worlds", type=int, default=4096)
     return ap.parse_args()
 
 
@@ -241,6 +245,159 @@ def run_reference(args):
     return 0
 
 
+def step_bytes(n: int, m: int, points: int, nj: int, substeps: int) -> float:
+    """Algorithmic bytes of one solver step: each stage's records read and written once
+    (bodies n, manifolds m with `points` contact points, joints nj)."""
+    per_sub = (84.0 * n) * 2 + 120.0 * points + (224.0 * m + 148.0 * points) \
+        + (212.0 * m + 148.0 * points) + 3 * 330.0 * nj
+    return (368.0 * n + 330.0 * nj + 936.0 * m + substeps * per_sub + 40.0 * m + 160.0 * m
+            + 330.0 * nj + 200.0 * n)
+
+
+def reference_worlds_sample(scs, params, budget_s: float = 20.0) -> dict:
+    """The reference's phys_solve over worlds of the batch, one world per host thread (the
+    worlds are independent; each reference world runs without a job system), for about
+    budget_s seconds of wall time."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from oracle.refworld import scene_world
+    cores = os.cpu_count() or 1
+    worlds = [scene_world(sc, params) for sc in scs]
+    solves = [8.0 * len(sc.contacts) for sc in scs]
+
+    def run(i):
+        worlds[i].solve(DT)
+        return solves[i]
+
+    with ThreadPoolExecutor(max_workers=cores) as ex:
+        list(ex.map(run, range(len(worlds))))  # warm-up
+        done = 0.0
+        rounds = 0
+        t0 = time.perf_counter()
+        while time.perf_counter() - t0 < budget_s or rounds == 0:
+            done += sum(ex.map(run, range(len(worlds))))
+            rounds += 1
+        sec = time.perf_counter() - t0
+    for w in worlds:
+        w.close()
+    return {"value": done / sec, "threads": cores, "rounds": rounds,
+            "world_steps_per_s": rounds * len(worlds) / sec}
+
+
+def run_batched(args):
+    """--workload batched: independent worlds of the mixed kind, all stepped in one persistent
+    launch per step. With N ranks each rank steps the worlds i with i % N == rank."""
+    import torch
+
+    from nepheline_b200 import abi, scenes
+    from nepheline_b200.solver import Batch, Solver
+
+    rank, world, local, pg = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    params = abi.WorldParams.default()
+    clk = Clocks(local).__enter__()
+    t_build = time.perf_counter()
+    scs = scenes.batched_worlds(args.worlds, seed=0, shard=rank, shards=world)
+    solver = Solver(device=local)
+    views = scenes.color_scenes(solver, scs)
+    solver.close()
+    build_s = time.perf_counter() - t_build
+    n = sum(len(v.bodies) for v in views)
+    m = sum(len(v.contacts) for v in views)
+    nj = sum(len(v.joints) for v in views)
+    pts = int(sum(int(v.contacts["point_count"].sum()) for v in views))
+    solves_per_step = 2 * params.substeps * m
+
+    batch = Batch(device=local)
+    stream = torch.cuda.ExternalStream(batch.stream, device=local)
+    batch.upload(views)
+    tuned = batch.autotune(params, DT, rounds=1)
+    batch.upload(views)
+    batch.step_async(params, DT, args.warmup)
+    torch.cuda.synchronize()
+    barrier(pg)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    clk.lines.clear()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    batch.step_async(params, DT, args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = clk.summary()
+    clk.__exit__(None, None, None)
+    ms_rank = e0.elapsed_time(e1) / args.steps
+    barrier(pg)
+    ms = max_over_ranks(pg, ms_rank)
+    total = torch.tensor([float(solves_per_step), float(len(views))], dtype=torch.float64,
+                         device="cuda")
+    if pg is not None:
+        pg.all_reduce(total)
+    solves_all, worlds_all = float(total[0]), float(total[1])
+    value = solves_all / (ms * 1e-3)
+    info = batch.info()
+    nbytes = step_bytes(n, m, pts, nj, params.substeps)
+    achieved = nbytes / (ms_rank * 1e-3) / 1e9
+    pk = peaks()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                "frac": achieved / pk["hbm_gbs"], "traffic": None, "kernel": "k_worlds",
+                "peak_source": pk["source"], "launches_per_step": 1,
+                "ms_per_launch": ms_rank, "algorithmic_bytes_per_launch": nbytes}
+
+    # End to end: nph_gpu_phys_solve_worlds on pinned host records, every step.
+    pv = [pinned_copy(v) for v in views]
+    h2d = sum(v.bodies.nbytes + v.contacts.nbytes + v.joints.nbytes + v.fixed.nbytes for v in pv)
+    d2h = sum(v.bodies.nbytes + v.contacts.nbytes + v.joints.nbytes for v in pv)
+    batch.phys_solve_worlds(pv, params, DT)
+    torch.cuda.synchronize()
+    barrier(pg)
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        batch.phys_solve_worlds(pv, params, DT)
+    torch.cuda.synchronize()
+    e2e_ms = (time.perf_counter() - t0) / args.e2e_steps * 1e3
+    e2e_ms = max_over_ranks(pg, e2e_ms)
+    e2e_value = solves_all / (e2e_ms * 1e-3)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import refworld
+        if refworld.ref_available():
+            sample = scs[: max(1, len(scs) // 8)]
+            r = reference_worlds_sample(sample, params)
+            cpu = {"value": r["value"], "unit": UNIT, "cores": r["threads"], "kind": "reference",
+                   "sample": f"{len(sample)} of the batch's worlds, {r['rounds']} steps each of "
+                             f"the reference phys_solve, one world per host thread; "
+                             f"{cpu_model()}"}
+    if rank == 0:
+        out = {
+            "metric": "contact-solves/s (batched worlds)", "value": value, "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": f"batched worlds: {args.worlds} mixed worlds (box pyramids, "
+                                   f"box piles, capsule hinge chains on a ground), body counts "
+                                   f"log-uniform in 8-4096",
+                       "worlds": int(worlds_all), "bodies_rank0": n, "manifolds_rank0": m,
+                       "joints_rank0": nj, "substeps": params.substeps, "dt": DT,
+                       "parallelism": f"worlds sharded x{world}", "tuning": tuned,
+                       "batch_info": info, "scene_build_s": build_s,
+                       "l2": "inputs larger than L2"},
+            "world_steps_per_s": worlds_all / (ms * 1e-3),
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms},
+            "gpu_launches": args.steps,
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }
+        print(json.dumps(out))
+    batch.close()
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
 def workload_name(dims) -> str:
     n = dims[0] * dims[1] * dims[2]
     return f"synthetic constraint graph, {dims[0]}x{dims[1]}x{dims[2]} lattice, {n} bodies"
@@ -250,6 +407,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "batched":
+        return run_batched(args)
     import torch
 
     from nepheline_b200 import abi

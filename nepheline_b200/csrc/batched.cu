@@ -460,11 +460,10 @@ template <int T, int M> uint32_t resident(size_t smem)
     return (uint32_t)std::max(blocks, 1);
 }
 
-void enqueue_batch_step(NphGpuBatch *b, const StepConsts &K, uint32_t substeps)
+// The chosen kernel's shared-memory limit and residency (outside any stream capture).
+void configure_batch_kernel(NphGpuBatch *b)
 {
-    const BatchArgs A = batch_args(b);
     const size_t smem = shared_bytes(b);
-    cudaMemsetAsync(b->d_counters, 0, sizeof(uint32_t), b->stream);
     uint32_t per_sm = 1;
     switch (b->config) {
     case 0: configure_kernel<128, 4>(smem); per_sm = resident<128, 4>(smem); break;
@@ -474,7 +473,15 @@ void enqueue_batch_step(NphGpuBatch *b, const StepConsts &K, uint32_t substeps)
     default: configure_kernel<1024, 1>(smem); per_sm = resident<1024, 1>(smem); break;
     }
     b->blocks_per_sm = per_sm;
-    const uint32_t grid = std::max<uint32_t>(1, std::min<uint32_t>(b->world_count, per_sm * b->sms));
+}
+
+void enqueue_batch_step(NphGpuBatch *b, const StepConsts &K, uint32_t substeps)
+{
+    const BatchArgs A = batch_args(b);
+    const size_t smem = shared_bytes(b);
+    cudaMemsetAsync(b->d_counters, 0, sizeof(uint32_t), b->stream);
+    const uint32_t grid =
+        std::max<uint32_t>(1, std::min<uint32_t>(b->world_count, b->blocks_per_sm * (uint32_t)b->sms));
     switch (b->config) {
     case 0: k_worlds<128, 4><<<grid, 128, smem, b->stream>>>(A, K, substeps); break;
     case 1: k_worlds<256, 2><<<grid, 256, smem, b->stream>>>(A, K, substeps); break;
@@ -487,18 +494,13 @@ void enqueue_batch_step(NphGpuBatch *b, const StepConsts &K, uint32_t substeps)
 NphGpuResult launch_batch_step(NphGpuBatch *b, const StepConsts &K, uint32_t substeps)
 {
     if (!b->use_graph) {
+        configure_batch_kernel(b);
         enqueue_batch_step(b, K, substeps);
         return cuda_result(cudaGetLastError());
     }
     if (!b->graph_valid || b->graph_substeps != substeps || std::memcmp(&b->graph_consts, &K, sizeof K) != 0) {
         drop_batch_graph(b);
-        // The kernel's attributes are set outside the capture.
-        const size_t smem = shared_bytes(b);
-        configure_kernel<128, 4>(smem);
-        configure_kernel<256, 2>(smem);
-        configure_kernel<256, 1>(smem);
-        configure_kernel<512, 1>(smem);
-        configure_kernel<1024, 1>(smem);
+        configure_batch_kernel(b);
         cudaGraph_t g = nullptr;
         cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
         if (e != cudaSuccess) {

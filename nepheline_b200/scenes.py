@@ -473,9 +473,17 @@ def color_scenes(solver, scs: list) -> list:
     return views
 
 
-def batched_worlds(count: int = 4096, seed: int = 0, min_bodies: int = 8,
-                   max_bodies: int = 4096) -> list:
-    """`count` worlds with body counts log-uniform in [min_bodies, max_bodies]."""
+def batched_sizes(count: int = 4096, seed: int = 0, min_bodies: int = 8,
+                  max_bodies: int = 4096) -> np.ndarray:
+    """Body counts of the batch's worlds, log-uniform in [min_bodies, max_bodies]."""
     rng = np.random.default_rng(seed)
-    sizes = np.round(np.exp(rng.uniform(np.log(min_bodies), np.log(max_bodies), count))).astype(int)
-    return [mixed_world(int(n), seed * 1_000_003 + i) for i, n in enumerate(sizes)]
+    return np.round(np.exp(rng.uniform(np.log(min_bodies), np.log(max_bodies), count))).astype(int)
+
+
+def batched_worlds(count: int = 4096, seed: int = 0, min_bodies: int = 8,
+                   max_bodies: int = 4096, shard: int = 0, shards: int = 1) -> list:
+    """`count` worlds with body counts log-uniform in [min_bodies, max_bodies]; with `shards`
+    > 1 only the worlds i with i % shards == shard (each world is the same whichever shard
+    builds it)."""
+    sizes = batched_sizes(count, seed, min_bodies, max_bodies)
+    return [mixed_world(int(sizes[i]), seed * 1_000_003 + i) for i in range(shard, count, shards)]

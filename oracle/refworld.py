@@ -333,6 +333,21 @@ def port_graph_color(body_a, body_b, dynamic_bits, body_slots) -> tuple[np.ndarr
     return color, slot
 
 
+def scene_world(sc, params=None, workers: int = 0):
+    """A solver scene in the reference: its bodies (then its fixed bodies, as static bodies,
+    at the indices after them) created shapeless, joints made, manifolds injected in insertion
+    order (coloured by the reference's phys_graph_add)."""
+    w = RefWorld(params or abi.WorldParams.default(), enable_sleep=False, workers=workers)
+    bodies, mass = sc.bodies, sc.mass
+    if sc.fixed is not None and len(sc.fixed):
+        bodies = np.concatenate([bodies, sc.fixed])
+        mass = np.concatenate([mass, np.zeros(len(sc.fixed), np.float32)])
+    w.add_shapeless_bodies(bodies, mass)
+    w.add_joints(sc.joints)
+    w.inject_contacts(sc.contacts)
+    return w
+
+
 def lattice_world(dims, seed: int = 0, joint_fraction: float = 0.1, params=None, workers: int = 0):
     """The synthetic constraint graph in the reference: shapeless bodies created, joints made,
     manifolds injected in insertion order (coloured by the reference's phys_graph_add)."""

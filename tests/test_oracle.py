@@ -155,3 +155,23 @@ def test_port_rejects_malformed_views():
     if len(bad.joints):
         bad.joints["type"][0] = 3
         assert port32_result(bad, params, DT) == abi.UNSUPPORTED
+
+
+@pytest.mark.parametrize("bodies,seed", [(40, 1), (300, 2), (1200, 3)])
+def test_port_matches_reference_mixed_batch_world(ref_lib, bodies, seed):
+    """The batched workload's worlds (pyramids, piles and hinge chains on a fixed ground):
+    the reference colours them as the host colouring does and solves them as the port does."""
+    from oracle.refworld import port32, scene_world
+    params = abi.WorldParams.default()
+    sc = scenes.mixed_world(bodies, seed)
+    w = scene_world(sc, params)
+    c = w.constraints()
+    hc, hs = scenes.host_color(sc)
+    assert np.array_equal(hc, c["color"]) and np.array_equal(hs, c["slot"])
+    for s in range(5):
+        vin = w.export_view()
+        mine = port32(vin, params, DT)
+        w.solve(DT)
+        bad = helpers.mismatches(mine, w.export_view())
+        assert not bad, f"step {s}: {bad}"
+    w.close()
