@@ -55,6 +55,8 @@ def parse():
                     help="lattice: the 1M-body constraint graph (the headline); batched: "
                          "--worlds independent worlds in one persistent launch")
     ap.add_argument("--worlds", type=int, default=4096)
+    ap.add_argument("--pass-config", default=None,
+                    help="fixed pass configurations warm,solve,relax,restitution (no autotuner)")
     return ap.parse_args()
 
 
@@ -344,8 +346,16 @@ def run_batched(args):
                 "peak_source": pk["source"], "launches_per_step": 1,
                 "ms_per_launch": ms_rank, "algorithmic_bytes_per_launch": nbytes}
 
-    # End to end: nph_gpu_phys_solve_worlds on pinned host records, every step.
-    pv = [pinned_copy(v) for v in views]
+    # End to end: nph_gpu_phys_solve_worlds on the worlds' records packed in page-locked host
+    # arrays (one transfer per record kind each way), every step.
+    pins = []
+
+    def pinned(nbytes):
+        t = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+        pins.append(t)
+        return t.numpy()
+
+    pv = abi.pack_views(views, pinned)
     h2d = sum(v.bodies.nbytes + v.contacts.nbytes + v.joints.nbytes + v.fixed.nbytes for v in pv)
     d2h = sum(v.bodies.nbytes + v.contacts.nbytes + v.joints.nbytes for v in pv)
     batch.phys_solve_worlds(pv, params, DT)
@@ -428,7 +438,12 @@ def main():
 
     # Device-resident steps: the autotuner's timed steps, then the warm-up.
     solver.upload(view)
-    tuned = solver.autotune(params, DT, rounds=1)
+    if args.pass_config:
+        tuned = [int(x) for x in args.pass_config.split(",")]
+        for kind, cfg in enumerate(tuned):
+            solver.set_pass_config(kind, cfg)
+    else:
+        tuned = solver.autotune(params, DT, rounds=1)
     solver.step_async(params, DT, args.warmup)
     torch.cuda.synchronize()
     barrier(pg)
@@ -465,12 +480,11 @@ def main():
     per_launch_bytes = top[1]["bytes"] / top[1]["launches"]
     achieved = per_launch_bytes / (per_launch_ms * 1e-3) / 1e9
     traffic = None
-    tf = ROOT / "profiles" / "solve_traffic.json"
-    if tf.exists():
-        try:
-            traffic = json.loads(tf.read_text()).get("bytes_per_launch_at_full_size")
-        except Exception:
-            traffic = None
+    tf = ROOT / "profiles" / "solve_traffic_lattice.md"
+    if top[0] == "solve" and tf.exists():
+        import re
+        m = re.search(r"traffic bytes per launch at full size: (\d+)", tf.read_text())
+        traffic = int(m.group(1)) if m else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / pk["hbm_gbs"], "traffic": traffic, "kernel": top[0],
                 "peak_source": pk["source"], "launches_per_step": top[1]["launches"] // 3,
@@ -502,10 +516,14 @@ def main():
         from oracle import refworld
         if refworld.ref_available():
             r = reference_sample((128, 128, 16), steps=8, warmup=1, workers=-1)
+            r1 = reference_sample((128, 128, 8), steps=4, warmup=1, workers=0)
             cpu = {"value": r["value"], "unit": UNIT, "cores": r["threads"], "kind": "reference",
                    "sample": f"128x128x16 slab of the lattice ({r['bodies']} bodies, "
                              f"{r['manifolds']} manifolds), 8 steps of the reference phys_solve "
-                             f"on its job system; {cpu_model()}"}
+                             f"on its job system; {cpu_model()}",
+                   "single_thread": {"value": r1["value"], "unit": UNIT, "cores": 1,
+                                     "sample": f"128x128x8 slab ({r1['bodies']} bodies), 4 "
+                                               f"steps without a job system"}}
         else:
             from oracle.refworld import port32
             from nepheline_b200 import scenes

@@ -344,19 +344,27 @@ NPH_GPU_API NphGpuResult nph_gpu_solver_autotune(NphGpuSolver *solver,
  * Batched worlds: many independent worlds of uneven size in one persistent launch
  * ---------------------------------------------------------------------------------------
  * The reference steps one world per nph_physics_world_step; this steps a batch of worlds
- * with the same settings, each as phys_solve would, in one kernel launch per step: each
- * block takes a whole world at a time from a queue sorted by size and runs its stage list
- * with block barriers between stages and colours. A world solved in a batch gives the same
- * bits as the world solved alone by nph_gpu_phys_solve. */
+ * with the same settings, each as phys_solve would, in one kernel launch per step. Worlds are
+ * taken from queues sorted by size: a large world by a whole block (block barriers between
+ * stages and colours), a small one by a single warp (warp barriers), so one SM works on many
+ * small worlds at once. A world solved in a batch gives the same bits as the world solved
+ * alone by nph_gpu_phys_solve. */
 
 typedef struct NphGpuBatch NphGpuBatch;
 
-/* What the batch autotuner chose. */
+/* Shared-memory modes for a world's body velocities. */
+#define NPH_GPU_BATCH_SHARED_NONE 0u  /* in global memory */
+#define NPH_GPU_BATCH_SHARED_SMALL 1u /* up to 32 KiB per block */
+#define NPH_GPU_BATCH_SHARED_LARGE 2u /* up to 160 KiB per block (the largest world) */
+
+/* A batch launch configuration (results do not depend on it). */
 typedef struct NphGpuBatchTuning {
-    uint32_t config;            /* below nph_gpu_batch_config_count() */
-    uint32_t threads;           /* threads per block */
-    uint32_t shared_velocities; /* 1: a world's body velocities in shared memory */
-    float ms_per_step;
+    uint32_t config;            /* launch shape, below nph_gpu_batch_config_count() */
+    uint32_t threads;           /* threads per block of that shape (filled in) */
+    uint32_t shared_velocities; /* NPH_GPU_BATCH_SHARED_* */
+    uint32_t warp_color_max;    /* worlds whose largest colour holds at most this many
+                                   constraints run on one warp; 0: every world on a block */
+    float ms_per_step;          /* the autotuner's time for it (filled in) */
 } NphGpuBatchTuning;
 
 typedef struct NphGpuBatchInfo {
@@ -368,14 +376,17 @@ typedef struct NphGpuBatchInfo {
     uint32_t threads;
     uint32_t shared_velocities;
     uint32_t blocks_per_sm;
+    uint32_t warp_color_max;
+    uint32_t warp_worlds; /* worlds the current configuration runs on a warp */
     uint32_t pad;
 } NphGpuBatchInfo;
 
 NPH_GPU_API NphGpuResult nph_gpu_batch_create(const NphGpuSolverDesc *desc, NphGpuBatch **out);
 NPH_GPU_API void nph_gpu_batch_destroy(NphGpuBatch *batch);
 NPH_GPU_API void *nph_gpu_batch_stream(const NphGpuBatch *batch);
-/* Uploads `count` world views (device arrays sized to the batch). Refuses as
- * nph_gpu_phys_solve does. */
+/* Uploads `count` world views (device arrays grown to the batch when needed). Refuses as
+ * nph_gpu_phys_solve does. Worlds whose records lie back to back in host memory (consecutive
+ * slices of one array) are copied with one transfer per array. */
 NPH_GPU_API NphGpuResult nph_gpu_batch_upload(NphGpuBatch *batch, const NphGpuWorldView *worlds,
                                               uint32_t count);
 /* `steps` steps of every uploaded world, enqueued on the batch's stream (one CUDA graph launch
@@ -390,10 +401,9 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_download(NphGpuBatch *batch, NphGpuWorldV
 NPH_GPU_API NphGpuResult nph_gpu_phys_solve_worlds(NphGpuBatch *batch,
                                                    const NphGpuWorldParams *params, float dt,
                                                    NphGpuWorldView *worlds, uint32_t count);
-/* The launch configuration (threads per block) and whether velocities live in shared memory.
- * Results do not depend on either. */
-NPH_GPU_API NphGpuResult nph_gpu_batch_set_config(NphGpuBatch *batch, uint32_t config,
-                                                  uint32_t shared_velocities);
+/* Sets the launch configuration (tuning->ms_per_step and ->threads are ignored). */
+NPH_GPU_API NphGpuResult nph_gpu_batch_set_config(NphGpuBatch *batch,
+                                                  const NphGpuBatchTuning *tuning);
 NPH_GPU_API uint32_t nph_gpu_batch_config_count(void);
 /* The batch autotuner: times every configuration on the uploaded worlds (`rounds` timed steps
  * each after an untimed one; the worlds advance) and keeps the fastest. */

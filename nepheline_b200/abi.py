@@ -179,9 +179,13 @@ class KernelTime(ctypes.Structure):
     ]
 
 
+BATCH_SHARED_NONE, BATCH_SHARED_SMALL, BATCH_SHARED_LARGE = 0, 1, 2
+
+
 class BatchTuning(ctypes.Structure):
     _fields_ = [("config", ctypes.c_uint32), ("threads", ctypes.c_uint32),
-                ("shared_velocities", ctypes.c_uint32), ("ms_per_step", ctypes.c_float)]
+                ("shared_velocities", ctypes.c_uint32), ("warp_color_max", ctypes.c_uint32),
+                ("ms_per_step", ctypes.c_float)]
 
 
 class BatchInfo(ctypes.Structure):
@@ -189,6 +193,7 @@ class BatchInfo(ctypes.Structure):
                 ("bodies", ctypes.c_uint64), ("manifolds", ctypes.c_uint64),
                 ("joints", ctypes.c_uint64), ("threads", ctypes.c_uint32),
                 ("shared_velocities", ctypes.c_uint32), ("blocks_per_sm", ctypes.c_uint32),
+                ("warp_color_max", ctypes.c_uint32), ("warp_worlds", ctypes.c_uint32),
                 ("pad", ctypes.c_uint32)]
 
 
@@ -262,3 +267,35 @@ def layout_sizes() -> dict:
     return {"body": BODY_DTYPE.itemsize, "point": POINT_DTYPE.itemsize,
             "contact": CONTACT_DTYPE.itemsize, "joint": JOINT_DTYPE.itemsize,
             "params": ctypes.sizeof(WorldParams), "view": ctypes.sizeof(WorldView)}
+
+
+def pack_views(views: list, alloc=None) -> list:
+    """The same worlds with their records as consecutive slices of one array per record kind
+    (bodies, fixed bodies, manifolds, joints), so that a batch copies each kind with one
+    transfer. `alloc(nbytes)` gives the backing uint8 arrays (page-locked memory, say);
+    the default is plain numpy memory. The returned views keep the arrays alive."""
+    alloc = alloc or (lambda nbytes: np.empty(nbytes, np.uint8))
+
+    def packed(field, dtype):
+        total = sum(len(getattr(v, field)) for v in views)
+        raw = alloc(max(total, 1) * dtype.itemsize)
+        arr = raw[: total * dtype.itemsize].view(dtype)
+        out, first = [], 0
+        for v in views:
+            src = getattr(v, field)
+            arr[first:first + len(src)] = src
+            out.append(arr[first:first + len(src)])
+            first += len(src)
+        return out, raw
+
+    bodies, rb = packed("bodies", BODY_DTYPE)
+    fixed, rf = packed("fixed", BODY_DTYPE)
+    contacts, rc = packed("contacts", CONTACT_DTYPE)
+    joints, rj = packed("joints", JOINT_DTYPE)
+    out = []
+    for i, v in enumerate(views):
+        p = View(bodies[i], fixed[i], contacts[i], joints[i], v.contact_color_counts,
+                 v.joint_color_counts)
+        p._keep = (rb, rf, rc, rj)
+        out.append(p)
+    return out

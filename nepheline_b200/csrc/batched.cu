@@ -1,17 +1,21 @@
 // SPDX-License-Identifier: Apache-2.0
 //
-// Many independent worlds of uneven size solved in one persistent launch. Each block takes a
-// whole world at a time from a queue sorted by size (largest first, so the last worlds taken
-// are the smallest and the blocks finish together), and runs the world's entire solver stage
-// (the stage list of phys_solve, solver.c:1032-1067) inside the block: every stage and every
-// colour is a loop over the world's items by the block's threads, with a block barrier
-// between them. No block ever waits on another, so no device-wide barrier or spin exists.
+// Many independent worlds of uneven size solved in one persistent launch. Worlds are taken
+// whole from two queues sorted by size (largest first, so the last worlds taken are the
+// smallest and the blocks finish together): first the large worlds, each by a whole block,
+// then the small ones, each by a single warp. A team (the block or the warp) runs the
+// world's entire solver stage (the stage list of phys_solve, solver.c:1032-1067): every
+// stage and every colour is a loop over the world's items by the team's threads, with a team
+// barrier between them. No team ever waits on another, so no device-wide barrier or spin
+// exists. A warp team lets one SM overlap many small worlds, whose colours hold too few
+// constraints to occupy a block.
 //
 // Each world's arithmetic is the single-world solver's (the same device functions of
 // bodies.cuh, contacts.cuh and joints.cuh on the world's slice of the arrays), so a world in
-// a batch gives the same bits as the world solved alone. With `shared_velocities` the
-// world's body velocities (the only body rows the constraint passes write) live in shared
-// memory for the whole step.
+// a batch gives the same bits as the world solved alone. Each item of a stage is a separate
+// non-inlined function, so that the register allocation of one stage does not constrain
+// another. With shared velocities, a world's body velocities (the only body rows the
+// constraint passes write) live in the team's shared memory for the whole step when they fit.
 
 #include <cuda_runtime.h>
 
@@ -50,9 +54,10 @@ struct WorldSlice {
 
 struct BatchArgs {
     const WorldSlice *worlds;
-    const uint32_t *order; // world indices, largest first
+    const uint32_t *order; // world indices: the block worlds, then the warp worlds
     uint32_t count;
-    uint32_t *next;        // the queue's head
+    uint32_t block_worlds; // the first block_worlds of `order` run on a block
+    uint32_t *heads;       // [0] the block queue's head, [1] the warp queue's
     uint32_t *err;
     NphGpuBody *bodies;
     const NphGpuBody *fixed;
@@ -66,11 +71,23 @@ struct BatchArgs {
     uint32_t mcap;
     float4 *jw;
     uint32_t jcap;
-    uint32_t shared_velocities; // the world's velocities in shared memory
-    uint32_t max_slots;         // shared velocity rows available (bodies + dummy)
+    uint32_t block_slots; // velocity slots (two rows each) in a block's shared memory
+    uint32_t warp_slots;  // in a warp's share of it
 };
 
 enum Pass : int { kWarm = 0, kSolve = 1, kRelax = 2, kRestitution = 3 };
+
+struct BlockTeam {
+    __device__ static uint32_t rank() { return threadIdx.x; }
+    __device__ static uint32_t size() { return blockDim.x; }
+    __device__ static void sync() { __syncthreads(); }
+};
+
+struct WarpTeam {
+    __device__ static uint32_t rank() { return threadIdx.x & 31u; }
+    __device__ static uint32_t size() { return 32u; }
+    __device__ static void sync() { __syncwarp(); }
+};
 
 // The world's slice of the arrays: body indices in its rows are world-relative.
 __device__ DevSolver world_solver(const BatchArgs &A, const WorldSlice &W, float4 *vel)
@@ -92,61 +109,36 @@ __device__ DevSolver world_solver(const BatchArgs &A, const WorldSlice &W, float
     return S;
 }
 
-template <int P> __device__ void world_pass(const DevSolver &S, const WorldSlice &W, const StepConsts &K)
+// ---- the items of each stage, one non-inlined function each ----
+
+template <int P> __device__ __noinline__ void joint_item(const DevSolver &S, uint32_t j, const StepConsts &K)
 {
-    const uint32_t o = NPH_GPU_OVERFLOW;
-    // The overflow: one thread, its joints then its contacts in list order.
-    if ((W.ccount[o] > 0u || (P != kRestitution && W.jcount[o] > 0u))) {
-        if (threadIdx.x == 0) {
-            if (P != kRestitution) {
-                for (uint32_t j = 0; j < W.jcount[o]; ++j) {
-                    const uint32_t jj = W.jfirst[o] + j;
-                    if (P == kWarm) {
-                        warm_joint(S, jj);
-                    } else {
-                        solve_joint<P == kSolve>(S, jj, K);
-                    }
-                }
-            }
-            for (uint32_t g = 0; g < W.ccount[o]; ++g) {
-                const uint32_t gg = W.cfirst[o] + g;
-                if (P == kWarm) {
-                    warm_manifold(S, gg);
-                } else if (P == kRestitution) {
-                    restitution_manifold(S, gg, K);
-                } else {
-                    solve_manifold<P == kSolve>(S, gg, K);
-                }
-            }
-        }
-        __syncthreads();
+    if (P == kWarm) {
+        warm_joint(S, j);
+    } else {
+        solve_joint<P == kSolve>(S, j, K);
     }
-    for (uint32_t c = 0; c < NPH_GPU_COLORS; ++c) {
-        const uint32_t jc = P == kRestitution ? 0u : W.jcount[c];
-        const uint32_t cc = W.ccount[c];
-        if (jc + cc == 0u) {
-            continue;
-        }
-        for (uint32_t i = threadIdx.x; i < jc + cc; i += blockDim.x) {
-            if (i < jc) {
-                const uint32_t jj = W.jfirst[c] + i;
-                if (P == kWarm) {
-                    warm_joint(S, jj);
-                } else {
-                    solve_joint<P == kSolve>(S, jj, K);
-                }
-            } else {
-                const uint32_t gg = W.cfirst[c] + (i - jc);
-                if (P == kWarm) {
-                    warm_manifold(S, gg);
-                } else if (P == kRestitution) {
-                    restitution_manifold(S, gg, K);
-                } else {
-                    solve_manifold<P == kSolve>(S, gg, K);
-                }
-            }
-        }
-        __syncthreads();
+}
+
+template <int P>
+__device__ __noinline__ void manifold_item(const DevSolver &S, uint32_t g, const StepConsts &K)
+{
+    if (P == kWarm) {
+        warm_manifold(S, g);
+    } else if (P == kRestitution) {
+        restitution_manifold(S, g, K);
+    } else {
+        solve_manifold<P == kSolve>(S, g, K);
+    }
+}
+
+__device__ __noinline__ void body_prepare_item(const BodyArrays &B, uint32_t i, uint32_t n,
+                                               const NphGpuBody *bodies, const StepConsts &K)
+{
+    if (i < n) {
+        prepare_body(B, i, bodies[i], K);
+    } else {
+        prepare_dummy(B, n);
     }
 }
 
@@ -168,102 +160,160 @@ __device__ uint32_t world_group_points(const NphGpuContact *contacts, const Worl
     return gp;
 }
 
-__device__ void world_step(const BatchArgs &A, const WorldSlice &W, const StepConsts &K,
-                           uint32_t substeps, float4 *shared_vel)
+// phys_joint_prepare for joint i of the world, or the neutral rows of a malformed one.
+__device__ __noinline__ void joint_prepare_item(const DevSolver &S, const WorldSlice &W, uint32_t i,
+                                                const NphGpuJoint *joints, const NphGpuBody *bodies,
+                                                const NphGpuBody *fixed, float h, uint32_t *err)
 {
-    const bool in_shared = A.shared_velocities != 0u && W.n + 1u <= A.max_slots;
+    const uint32_t n = W.n, total = W.n + W.nf;
+    const NphGpuJoint &jr = joints[i];
+    if (jr.body_a >= total || jr.body_b >= total ||
+        (jr.type != NPH_GPU_JOINT_BALL && jr.type != NPH_GPU_JOINT_HINGE)) {
+        atomicOr(err, kErrBadJoint);
+        for (uint32_t r = 0; r < kJointRows; ++r) {
+            S.jw[r * S.jcap + i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        S.jw[kJrFrameA * S.jcap + i] = make_float4(0.f, 0.f, 0.f, 1.f);
+        S.jw[kJrFrameB * S.jcap + i] = make_float4(0.f, 0.f, 0.f, 1.f);
+        S.jw[kJrHead * S.jcap + i] = make_float4(__uint_as_float(n), __uint_as_float(n), 0.f, 0.f);
+        return;
+    }
+    const NphGpuBody &a = jr.body_a < n ? bodies[jr.body_a] : fixed[jr.body_a - n];
+    const NphGpuBody &b = jr.body_b < n ? bodies[jr.body_b] : fixed[jr.body_b - n];
+    prepare_joint(S, i, jr, a, b, jr.body_a < n ? jr.body_a : n, jr.body_b < n ? jr.body_b : n, h);
+}
+
+// prepare_group for manifold g of the world, or the neutral header of a malformed one.
+__device__ __noinline__ void manifold_prepare_item(const DevSolver &S, const WorldSlice &W, uint32_t g,
+                                                   const NphGpuContact *contacts, const NphGpuBody *bodies,
+                                                   const NphGpuBody *fixed, uint32_t *err)
+{
+    const uint32_t n = W.n, total = W.n + W.nf;
+    const NphGpuContact &c = contacts[g];
+    if (c.body_a >= total || c.body_b >= total) {
+        atomicOr(err, kErrBadIndex);
+        S.hdr[g] = make_uint4(n, n, 0u, 0u);
+        return;
+    }
+    if (c.point_count < 1u || c.point_count > NPH_GPU_MAX_POINTS) {
+        atomicOr(err, kErrBadPoints);
+        S.hdr[g] = make_uint4(n, n, 0u, 0u);
+        return;
+    }
+    const NphGpuBody &ra = c.body_a < n ? bodies[c.body_a] : fixed[c.body_a - n];
+    const NphGpuBody &rb = c.body_b < n ? bodies[c.body_b] : fixed[c.body_b - n];
+    const bool dyn_a = ra.type == NPH_GPU_BODY_DYNAMIC;
+    const bool dyn_b = rb.type == NPH_GPU_BODY_DYNAMIC;
+    S.nrm[g] = make_float4(c.normal[0], c.normal[1], c.normal[2], c.friction);
+    S.rest[g] = c.restitution;
+    prepare_manifold(S, g, c, c.body_a < n ? c.body_a : n, c.body_b < n ? c.body_b : n, dyn_a, dyn_b,
+                     dyn_a ? ra.inv_mass : 0.0f, dyn_b ? rb.inv_mass : 0.0f,
+                     world_group_points(contacts, W, g));
+}
+
+__device__ __noinline__ void finalize_item(const BodyArrays &B, uint32_t i, NphGpuBody *bodies, float dt)
+{
+    finalize_body(B, i, bodies[i], dt);
+}
+
+__device__ __noinline__ void store_manifold_item(const DevSolver &S, uint32_t g, NphGpuContact *contacts)
+{
+    store_manifold(S, g, contacts[g]);
+}
+
+__device__ __noinline__ void store_joint_item(const DevSolver &S, uint32_t j, NphGpuJoint *joints)
+{
+    store_joint(S, j, joints[j]);
+}
+
+template <int P, class Team> __device__ void world_pass(const DevSolver &S, const WorldSlice &W, const StepConsts &K)
+{
+    const uint32_t o = NPH_GPU_OVERFLOW;
+    // The overflow: one thread, its joints then its contacts in list order.
+    const uint32_t oj = P == kRestitution ? 0u : W.jcount[o];
+    if (W.ccount[o] > 0u || oj > 0u) {
+        if (Team::rank() == 0u) {
+            for (uint32_t j = 0; j < oj; ++j) {
+                joint_item<P>(S, W.jfirst[o] + j, K);
+            }
+            for (uint32_t g = 0; g < W.ccount[o]; ++g) {
+                manifold_item<P>(S, W.cfirst[o] + g, K);
+            }
+        }
+        Team::sync();
+    }
+    for (uint32_t c = 0; c < NPH_GPU_COLORS; ++c) {
+        const uint32_t jc = P == kRestitution ? 0u : W.jcount[c];
+        const uint32_t cc = W.ccount[c];
+        if (jc + cc == 0u) {
+            continue;
+        }
+        for (uint32_t i = Team::rank(); i < jc + cc; i += Team::size()) {
+            if (i < jc) {
+                joint_item<P>(S, W.jfirst[c] + i, K);
+            } else {
+                manifold_item<P>(S, W.cfirst[c] + (i - jc), K);
+            }
+        }
+        Team::sync();
+    }
+}
+
+template <class Team>
+__device__ void world_step(const BatchArgs &A, const WorldSlice &W, const StepConsts &K, uint32_t substeps,
+                           float4 *shared_vel, uint32_t shared_slots)
+{
+    const bool in_shared = W.n + 1u <= shared_slots;
     float4 *vel = in_shared ? shared_vel : A.vel + 2u * W.slot_first;
     const DevSolver S = world_solver(A, W, vel);
-    const BodyArrays B{vel, A.pos + 2u * W.slot_first, A.prm + 3u * W.slot_first,
-                       A.itg + 6u * W.slot_first};
+    const BodyArrays B{vel, A.pos + 2u * W.slot_first, A.prm + 3u * W.slot_first, A.itg + 6u * W.slot_first};
     NphGpuBody *bodies = A.bodies + W.body_first;
     const NphGpuBody *fixed = A.fixed + W.fixed_first;
     NphGpuContact *contacts = A.contacts + W.contact_first;
     NphGpuJoint *joints = A.joints + W.joint_first;
     const uint32_t n = W.n;
     // prepare_body (solver.c:131-168), the dummy last.
-    for (uint32_t i = threadIdx.x; i <= n; i += blockDim.x) {
-        if (i < n) {
-            prepare_body(B, i, bodies[i], K);
-        } else {
-            prepare_dummy(B, n);
-        }
+    for (uint32_t i = Team::rank(); i <= n; i += Team::size()) {
+        body_prepare_item(B, i, n, bodies, K);
     }
-    __syncthreads();
-    // The joints and the manifolds (prepare_group, phys_joint_prepare).
-    const uint32_t total = n + W.nf;
-    for (uint32_t i = threadIdx.x; i < W.nj + W.m; i += blockDim.x) {
+    Team::sync();
+    // The joints and the manifolds (phys_joint_prepare, prepare_group).
+    for (uint32_t i = Team::rank(); i < W.nj + W.m; i += Team::size()) {
         if (i < W.nj) {
-            const NphGpuJoint &jr = joints[i];
-            if (jr.body_a >= total || jr.body_b >= total ||
-                (jr.type != NPH_GPU_JOINT_BALL && jr.type != NPH_GPU_JOINT_HINGE)) {
-                atomicOr(A.err, kErrBadJoint);
-                for (uint32_t r = 0; r < kJointRows; ++r) {
-                    S.jw[r * S.jcap + i] = make_float4(0.f, 0.f, 0.f, 0.f);
-                }
-                S.jw[kJrFrameA * S.jcap + i] = make_float4(0.f, 0.f, 0.f, 1.f);
-                S.jw[kJrFrameB * S.jcap + i] = make_float4(0.f, 0.f, 0.f, 1.f);
-                S.jw[kJrHead * S.jcap + i] =
-                    make_float4(__uint_as_float(n), __uint_as_float(n), 0.f, 0.f);
-                continue;
-            }
-            const NphGpuBody &a = jr.body_a < n ? bodies[jr.body_a] : fixed[jr.body_a - n];
-            const NphGpuBody &b = jr.body_b < n ? bodies[jr.body_b] : fixed[jr.body_b - n];
-            prepare_joint(S, i, jr, a, b, jr.body_a < n ? jr.body_a : n, jr.body_b < n ? jr.body_b : n,
-                          K.h);
+            joint_prepare_item(S, W, i, joints, bodies, fixed, K.h, A.err);
         } else {
-            const uint32_t g = i - W.nj;
-            const NphGpuContact &c = contacts[g];
-            if (c.body_a >= total || c.body_b >= total) {
-                atomicOr(A.err, kErrBadIndex);
-                S.hdr[g] = make_uint4(n, n, 0u, 0u);
-                continue;
-            }
-            if (c.point_count < 1u || c.point_count > NPH_GPU_MAX_POINTS) {
-                atomicOr(A.err, kErrBadPoints);
-                S.hdr[g] = make_uint4(n, n, 0u, 0u);
-                continue;
-            }
-            const NphGpuBody &ra = c.body_a < n ? bodies[c.body_a] : fixed[c.body_a - n];
-            const NphGpuBody &rb = c.body_b < n ? bodies[c.body_b] : fixed[c.body_b - n];
-            const bool dyn_a = ra.type == NPH_GPU_BODY_DYNAMIC;
-            const bool dyn_b = rb.type == NPH_GPU_BODY_DYNAMIC;
-            S.nrm[g] = make_float4(c.normal[0], c.normal[1], c.normal[2], c.friction);
-            S.rest[g] = c.restitution;
-            prepare_manifold(S, g, c, c.body_a < n ? c.body_a : n, c.body_b < n ? c.body_b : n, dyn_a,
-                             dyn_b, dyn_a ? ra.inv_mass : 0.0f, dyn_b ? rb.inv_mass : 0.0f,
-                             world_group_points(contacts, W, g));
+            manifold_prepare_item(S, W, i - W.nj, contacts, bodies, fixed, A.err);
         }
     }
-    __syncthreads();
+    Team::sync();
     for (uint32_t sub = 0; sub < substeps; ++sub) {
-        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        for (uint32_t i = Team::rank(); i < n; i += Team::size()) {
             integrate_velocity(B, i, K.h);
         }
-        __syncthreads();
-        world_pass<kWarm>(S, W, K);
-        world_pass<kSolve>(S, W, K);
-        for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        Team::sync();
+        world_pass<kWarm, Team>(S, W, K);
+        world_pass<kSolve, Team>(S, W, K);
+        for (uint32_t i = Team::rank(); i < n; i += Team::size()) {
             integrate_position(B, i, K.h);
         }
-        __syncthreads();
-        world_pass<kRelax>(S, W, K);
+        Team::sync();
+        world_pass<kRelax, Team>(S, W, K);
     }
-    world_pass<kRestitution>(S, W, K);
+    world_pass<kRestitution, Team>(S, W, K);
     // store_group, the joints' impulses, finalize_body.
-    for (uint32_t g = threadIdx.x; g < W.m; g += blockDim.x) {
-        store_manifold(S, g, contacts[g]);
+    for (uint32_t g = Team::rank(); g < W.m; g += Team::size()) {
+        store_manifold_item(S, g, contacts);
     }
-    for (uint32_t j = threadIdx.x; j < W.nj; j += blockDim.x) {
-        store_joint(S, j, joints[j]);
+    for (uint32_t j = Team::rank(); j < W.nj; j += Team::size()) {
+        store_joint_item(S, j, joints);
     }
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-        finalize_body(B, i, bodies[i], K.dt);
+    for (uint32_t i = Team::rank(); i < n; i += Team::size()) {
+        finalize_item(B, i, bodies, K.dt);
     }
-    __syncthreads();
+    Team::sync();
     // post_finalize's driven joints (solver.c:851-857).
     if (W.driven > 0u) {
-        for (uint32_t j = threadIdx.x; j < W.nj; j += blockDim.x) {
+        for (uint32_t j = Team::rank(); j < W.nj; j += Team::size()) {
             uint32_t sa, sb, flags;
             joint_head(S, j, sa, sb, flags);
             if ((flags & kJDriven) != 0u) {
@@ -276,33 +326,49 @@ __device__ void world_step(const BatchArgs &A, const WorldSlice &W, const StepCo
             }
         }
     }
-    __syncthreads();
+    Team::sync();
 }
 
 template <int kThreads, int kMinBlocks>
-__global__ void __launch_bounds__(kThreads, kMinBlocks)
-k_worlds(BatchArgs A, StepConsts K, uint32_t substeps)
+__global__ void __launch_bounds__(kThreads, kMinBlocks) k_worlds(BatchArgs A, StepConsts K, uint32_t substeps)
 {
     extern __shared__ float4 shared_vel[];
     __shared__ uint32_t taken;
-    for (;;) {
-        if (threadIdx.x == 0) {
-            taken = atomicAdd(A.next, 1u);
+    // The large worlds, a block each.
+    if (A.block_worlds > 0u) {
+        for (;;) {
+            if (threadIdx.x == 0) {
+                taken = atomicAdd(&A.heads[0], 1u);
+            }
+            __syncthreads();
+            const uint32_t q = taken;
+            __syncthreads();
+            if (q >= A.block_worlds) {
+                break;
+            }
+            world_step<BlockTeam>(A, A.worlds[A.order[q]], K, substeps, shared_vel, A.block_slots);
         }
-        __syncthreads();
-        const uint32_t q = taken;
-        __syncthreads();
-        if (q >= A.count) {
+    }
+    // The small worlds, a warp each, in the warp's share of the shared memory.
+    const uint32_t warp = threadIdx.x >> 5;
+    float4 *mine = shared_vel + (size_t)warp * 2u * A.warp_slots;
+    for (;;) {
+        uint32_t q = 0;
+        if ((threadIdx.x & 31u) == 0u) {
+            q = atomicAdd(&A.heads[1], 1u);
+        }
+        q = __shfl_sync(0xFFFFFFFFu, q, 0);
+        if (q >= A.count - A.block_worlds) {
             return;
         }
-        world_step(A, A.worlds[A.order[q]], K, substeps, shared_vel);
+        world_step<WarpTeam>(A, A.worlds[A.order[A.block_worlds + q]], K, substeps, mine, A.warp_slots);
     }
 }
 
 struct BatchConfig {
     uint32_t threads, min_blocks;
 };
-constexpr BatchConfig kBatchConfigs[] = {{128, 4}, {256, 2}, {256, 1}, {512, 1}, {1024, 1}};
+constexpr BatchConfig kBatchConfigs[] = {{128, 4}, {256, 2}, {256, 1}, {512, 1}, {1024, 1}, {256, 4}, {512, 2}};
 constexpr uint32_t kBatchConfigCount = sizeof(kBatchConfigs) / sizeof(kBatchConfigs[0]);
 
 } // namespace
@@ -319,10 +385,12 @@ struct NphGpuBatch {
     bool own_stream = false;
     bool use_graph = true;
     uint32_t config = 1;
-    uint32_t shared_velocities = 1;
+    uint32_t shared_mode = NPH_GPU_BATCH_SHARED_SMALL;
+    uint32_t warp_color_max = 32;
     uint32_t blocks_per_sm = 0; // resident blocks of the chosen kernel (0: not yet known)
+    uint32_t block_worlds = 0;  // worlds of the current order that run on a block
     int sms = 148;
-    // Device arrays.
+    // Device arrays and their capacities (grown, never shrunk, by uploads).
     NphGpuBody *d_bodies = nullptr;
     NphGpuBody *d_fixed = nullptr;
     NphGpuContact *d_contacts = nullptr;
@@ -335,19 +403,20 @@ struct NphGpuBatch {
     float4 *jw = nullptr;
     WorldSlice *d_worlds = nullptr;
     uint32_t *d_order = nullptr;
-    uint32_t *d_counters = nullptr; // [0] queue head, [1] error bits
+    uint32_t *d_counters = nullptr; // [0] block queue head, [1] warp queue head, [2] error bits
     uint32_t *h_counters = nullptr;
-    // Sizes.
+    uint64_t cap_bodies = 0, cap_slots = 0, cap_fixed = 0, cap_contacts = 0, cap_joints = 0, cap_worlds = 0;
+    // Sizes of the uploaded batch.
     uint32_t world_count = 0;
     uint64_t bodies = 0, slots = 0, fixed = 0, contacts = 0, joints = 0;
     uint64_t max_world_slots = 0;
     std::vector<WorldSlice> worlds;
+    std::vector<uint32_t> order;
     // The step graph.
     cudaGraphExec_t graph = nullptr;
     bool graph_valid = false;
     StepConsts graph_consts{};
     uint32_t graph_substeps = 0;
-    size_t bytes_held = 0;
 };
 
 namespace {
@@ -396,6 +465,7 @@ void free_arrays(NphGpuBatch *b)
     bfree(b->jw);
     bfree(b->d_worlds);
     bfree(b->d_order);
+    b->cap_bodies = b->cap_slots = b->cap_fixed = b->cap_contacts = b->cap_joints = b->cap_worlds = 0;
     b->world_count = 0;
 }
 
@@ -407,14 +477,50 @@ NphGpuResult cuda_result(cudaError_t e)
     return e == cudaErrorMemoryAllocation ? NPH_GPU_OUT_OF_MEMORY : NPH_GPU_DEVICE_LOST;
 }
 
+// Dynamic shared memory of a block: two velocity rows per slot, for the largest world, within
+// the mode's limit.
 size_t shared_bytes(const NphGpuBatch *b)
 {
-    if (b->shared_velocities == 0u) {
+    if (b->shared_mode == NPH_GPU_BATCH_SHARED_NONE) {
         return 0;
     }
-    // Two velocity rows per slot, up to the largest world, within 160 KiB.
+    const uint64_t limit = b->shared_mode == NPH_GPU_BATCH_SHARED_SMALL ? (32ull << 10) : (160ull << 10);
     const uint64_t want = 2ull * b->max_world_slots * sizeof(float4);
-    return (size_t)std::min<uint64_t>(want, 160ull << 10);
+    return (size_t)std::min<uint64_t>(want, limit);
+}
+
+// The largest colour (constraints of one colour slot other than the overflow) of a world.
+uint32_t largest_color(const WorldSlice &s)
+{
+    uint32_t m = 0;
+    for (uint32_t c = 0; c < NPH_GPU_COLORS; ++c) {
+        m = std::max(m, s.ccount[c] + s.jcount[c]);
+    }
+    return m;
+}
+
+// The queue order for the configuration: the block worlds, then the warp worlds, each largest
+// first (a world's work grows with its manifolds, joints and bodies).
+void build_order(NphGpuBatch *b)
+{
+    const std::vector<WorldSlice> &w = b->worlds;
+    std::vector<uint32_t> order(w.size());
+    std::iota(order.begin(), order.end(), 0u);
+    auto on_warp = [&](uint32_t x) { return b->warp_color_max > 0u && largest_color(w[x]) <= b->warp_color_max; };
+    auto work = [&](uint32_t x) { return 4ull * w[x].m + 3ull * w[x].nj + w[x].n; };
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
+        const bool wx = on_warp(x), wy = on_warp(y);
+        if (wx != wy) {
+            return !wx;
+        }
+        return work(x) > work(y);
+    });
+    uint32_t blocks = 0;
+    while (blocks < order.size() && !on_warp(order[blocks])) {
+        ++blocks;
+    }
+    b->order = order;
+    b->block_worlds = blocks;
 }
 
 BatchArgs batch_args(const NphGpuBatch *b)
@@ -423,8 +529,9 @@ BatchArgs batch_args(const NphGpuBatch *b)
     A.worlds = b->d_worlds;
     A.order = b->d_order;
     A.count = b->world_count;
-    A.next = b->d_counters;
-    A.err = b->d_counters + 1;
+    A.block_worlds = b->block_worlds;
+    A.heads = b->d_counters;
+    A.err = b->d_counters + 2;
     A.bodies = b->d_bodies;
     A.fixed = b->d_fixed;
     A.contacts = b->d_contacts;
@@ -440,11 +547,13 @@ BatchArgs batch_args(const NphGpuBatch *b)
     A.pb = b->pb;
     A.pt = b->pt;
     A.pi = b->pi;
-    A.mcap = (uint32_t)std::max<uint64_t>(b->contacts, 1);
+    A.mcap = (uint32_t)std::max<uint64_t>(b->cap_contacts, 1);
     A.jw = b->jw;
-    A.jcap = (uint32_t)std::max<uint64_t>(b->joints, 1);
-    A.shared_velocities = shared_bytes(b) > 0 ? 1u : 0u;
-    A.max_slots = (uint32_t)(shared_bytes(b) / (2 * sizeof(float4)));
+    A.jcap = (uint32_t)std::max<uint64_t>(b->cap_joints, 1);
+    const size_t smem = shared_bytes(b);
+    const uint32_t warps = kBatchConfigs[b->config].threads / 32u;
+    A.block_slots = (uint32_t)(smem / (2 * sizeof(float4)));
+    A.warp_slots = (uint32_t)(smem / (2 * sizeof(float4)) / warps);
     return A;
 }
 
@@ -470,7 +579,9 @@ void configure_batch_kernel(NphGpuBatch *b)
     case 1: configure_kernel<256, 2>(smem); per_sm = resident<256, 2>(smem); break;
     case 2: configure_kernel<256, 1>(smem); per_sm = resident<256, 1>(smem); break;
     case 3: configure_kernel<512, 1>(smem); per_sm = resident<512, 1>(smem); break;
-    default: configure_kernel<1024, 1>(smem); per_sm = resident<1024, 1>(smem); break;
+    case 4: configure_kernel<1024, 1>(smem); per_sm = resident<1024, 1>(smem); break;
+    case 5: configure_kernel<256, 4>(smem); per_sm = resident<256, 4>(smem); break;
+    default: configure_kernel<512, 2>(smem); per_sm = resident<512, 2>(smem); break;
     }
     b->blocks_per_sm = per_sm;
 }
@@ -479,15 +590,19 @@ void enqueue_batch_step(NphGpuBatch *b, const StepConsts &K, uint32_t substeps)
 {
     const BatchArgs A = batch_args(b);
     const size_t smem = shared_bytes(b);
-    cudaMemsetAsync(b->d_counters, 0, sizeof(uint32_t), b->stream);
-    const uint32_t grid =
-        std::max<uint32_t>(1, std::min<uint32_t>(b->world_count, b->blocks_per_sm * (uint32_t)b->sms));
+    cudaMemsetAsync(b->d_counters, 0, 2 * sizeof(uint32_t), b->stream);
+    const uint32_t warps = kBatchConfigs[b->config].threads / 32u;
+    const uint64_t want = (uint64_t)b->block_worlds + (b->world_count - b->block_worlds + warps - 1u) / warps;
+    const uint32_t grid = (uint32_t)std::max<uint64_t>(
+        1, std::min<uint64_t>(want, (uint64_t)b->blocks_per_sm * (uint64_t)b->sms));
     switch (b->config) {
     case 0: k_worlds<128, 4><<<grid, 128, smem, b->stream>>>(A, K, substeps); break;
     case 1: k_worlds<256, 2><<<grid, 256, smem, b->stream>>>(A, K, substeps); break;
     case 2: k_worlds<256, 1><<<grid, 256, smem, b->stream>>>(A, K, substeps); break;
     case 3: k_worlds<512, 1><<<grid, 512, smem, b->stream>>>(A, K, substeps); break;
-    default: k_worlds<1024, 1><<<grid, 1024, smem, b->stream>>>(A, K, substeps); break;
+    case 4: k_worlds<1024, 1><<<grid, 1024, smem, b->stream>>>(A, K, substeps); break;
+    case 5: k_worlds<256, 4><<<grid, 256, smem, b->stream>>>(A, K, substeps); break;
+    default: k_worlds<512, 2><<<grid, 512, smem, b->stream>>>(A, K, substeps); break;
     }
 }
 
@@ -524,6 +639,19 @@ NphGpuResult launch_batch_step(NphGpuBatch *b, const StepConsts &K, uint32_t sub
     return cuda_result(cudaGraphLaunch(b->graph, b->stream));
 }
 
+// Uploads the queue order for the current configuration.
+NphGpuResult apply_order(NphGpuBatch *b)
+{
+    drop_batch_graph(b);
+    if (b->world_count == 0) {
+        return NPH_GPU_OK;
+    }
+    build_order(b);
+    cudaMemcpyAsync(b->d_order, b->order.data(), sizeof(uint32_t) * b->world_count, cudaMemcpyHostToDevice,
+                    b->stream);
+    return cuda_result(cudaStreamSynchronize(b->stream));
+}
+
 NphGpuResult check_world(const NphGpuWorldView &v)
 {
     uint64_t nc = 0, nj = 0;
@@ -544,6 +672,117 @@ NphGpuResult check_world(const NphGpuWorldView &v)
         }
     }
     return NPH_GPU_OK;
+}
+
+// Host<->device copies of many worlds' records, merged while both sides stay contiguous.
+class CopyRun {
+  public:
+    CopyRun(cudaStream_t st, cudaMemcpyKind kind) : st_(st), kind_(kind) {}
+    ~CopyRun() { flush(); }
+    void add(void *dst, const void *src, size_t bytes)
+    {
+        if (bytes == 0) {
+            return;
+        }
+        if (bytes_ > 0 && (char *)dst == dst_ + bytes_ && (const char *)src == src_ + bytes_) {
+            bytes_ += bytes;
+            return;
+        }
+        flush();
+        dst_ = (char *)dst;
+        src_ = (const char *)src;
+        bytes_ = bytes;
+    }
+    void flush()
+    {
+        if (bytes_ > 0) {
+            cudaMemcpyAsync(dst_, src_, bytes_, kind_, st_);
+            ++copies;
+        }
+        bytes_ = 0;
+    }
+    uint32_t copies = 0;
+
+  private:
+    cudaStream_t st_;
+    cudaMemcpyKind kind_;
+    char *dst_ = nullptr;
+    const char *src_ = nullptr;
+    size_t bytes_ = 0;
+};
+
+template <typename T> bool grow(T *&p, uint64_t &cap, uint64_t want)
+{
+    if (want <= cap && p != nullptr) {
+        return true;
+    }
+    const uint64_t c = std::max<uint64_t>(want, 1);
+    if (!balloc(p, c)) {
+        cap = 0;
+        return false;
+    }
+    cap = c;
+    return true;
+}
+
+// The body rows (velocities, positions, parameters, integration state) per solver slot.
+bool grow_slots(NphGpuBatch *b, uint64_t slots)
+{
+    if (slots <= b->cap_slots && b->vel != nullptr) {
+        return true;
+    }
+    const uint64_t c = std::max<uint64_t>(slots, 1);
+    b->cap_slots = 0;
+    if (!balloc(b->vel, 2 * c) || !balloc(b->pos, 2 * c) || !balloc(b->prm, 3 * c) || !balloc(b->itg, 6 * c)) {
+        return false;
+    }
+    b->cap_slots = c;
+    return true;
+}
+
+// The manifold records and rows; the point rows are strided by the capacity.
+bool grow_contacts(NphGpuBatch *b, uint64_t m)
+{
+    if (m <= b->cap_contacts && b->d_contacts != nullptr) {
+        return true;
+    }
+    const uint64_t c = std::max<uint64_t>(m, 1);
+    b->cap_contacts = 0;
+    if (!balloc(b->d_contacts, c) || !balloc(b->hdr, c) || !balloc(b->nrm, c) || !balloc(b->rest, c) ||
+        !balloc(b->pa, 4 * c) || !balloc(b->pb, 4 * c) || !balloc(b->pt, 4 * c) || !balloc(b->pi, 4 * c)) {
+        return false;
+    }
+    b->cap_contacts = c;
+    return true;
+}
+
+// The joint records and rows; the rows are strided by the capacity.
+bool grow_joints(NphGpuBatch *b, uint64_t nj)
+{
+    if (nj <= b->cap_joints && b->d_joints != nullptr) {
+        return true;
+    }
+    const uint64_t c = std::max<uint64_t>(nj, 1);
+    b->cap_joints = 0;
+    if (!balloc(b->d_joints, c) || !balloc(b->jw, (uint64_t)kJointRows * c)) {
+        return false;
+    }
+    b->cap_joints = c;
+    return true;
+}
+
+bool grow_worlds(NphGpuBatch *b, uint64_t count)
+{
+    if (count <= b->cap_worlds && b->d_worlds != nullptr) {
+        return true;
+    }
+    const uint64_t c = std::max<uint64_t>(count, 1);
+    b->cap_worlds = 0;
+    if (!balloc(b->d_worlds, c) || !balloc(b->d_order, c)) {
+        return false;
+    }
+    b->cap_worlds = c;
+    return true;
 }
 
 } // namespace
@@ -633,7 +872,7 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_upload(NphGpuBatch *b, const NphGpuWorldV
         }
     }
     cudaSetDevice(b->device);
-    // The slices, then the arrays sized to the batch.
+    // The slices, then the arrays grown to the batch.
     std::vector<WorldSlice> slices(count);
     uint64_t bodies = 0, slots = 0, fixed = 0, contacts = 0, joints = 0, max_slots = 0;
     for (uint32_t w = 0; w < count; ++w) {
@@ -672,20 +911,16 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_upload(NphGpuBatch *b, const NphGpuWorldV
         joints += v.joint_count;
         max_slots = std::max<uint64_t>(max_slots, v.body_count + 1u);
     }
-    if (slots >= 0xFFFFFFF0ull || contacts >= 0xFFFFFFF0ull || joints >= 0xFFFFFFF0ull) {
-        return NPH_GPU_INVALID_ARGUMENT;
+    if (slots >= 0xFFFFFFF0ull || contacts >= 0xFFFFFFF0ull || joints >= 0xFFFFFFF0ull ||
+        4ull * contacts >= 0xFFFFFFF0ull || (uint64_t)kJointRows * joints >= 0xFFFFFFF0ull) {
+        return NPH_GPU_TOO_LARGE;
     }
-    free_arrays(b);
-    bool ok = balloc(b->d_bodies, bodies) && balloc(b->d_fixed, fixed) &&
-              balloc(b->d_contacts, contacts) && balloc(b->d_joints, joints) &&
-              balloc(b->vel, 2 * slots) && balloc(b->pos, 2 * slots) && balloc(b->prm, 3 * slots) &&
-              balloc(b->itg, 6 * slots) && balloc(b->hdr, contacts) && balloc(b->nrm, contacts) &&
-              balloc(b->rest, contacts) && balloc(b->pa, 4 * std::max<uint64_t>(contacts, 1)) &&
-              balloc(b->pb, 4 * std::max<uint64_t>(contacts, 1)) &&
-              balloc(b->pt, 4 * std::max<uint64_t>(contacts, 1)) &&
-              balloc(b->pi, 4 * std::max<uint64_t>(contacts, 1)) &&
-              balloc(b->jw, (uint64_t)kJointRows * std::max<uint64_t>(joints, 1)) &&
-              balloc(b->d_worlds, count) && balloc(b->d_order, count);
+    drop_batch_graph(b);
+    // The point and joint rows are strided by their capacity: a capacity change reallocates
+    // them with the new stride.
+    const bool ok = grow(b->d_bodies, b->cap_bodies, bodies) && grow(b->d_fixed, b->cap_fixed, fixed) &&
+                    grow_slots(b, slots) && grow_contacts(b, contacts) && grow_joints(b, joints) &&
+                    grow_worlds(b, count);
     if (!ok) {
         free_arrays(b);
         cudaGetLastError();
@@ -699,34 +934,19 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_upload(NphGpuBatch *b, const NphGpuWorldV
     b->joints = joints;
     b->max_world_slots = max_slots;
     b->worlds = slices;
-    // Largest first: the work of a world grows with its manifolds, joints and bodies.
-    std::vector<uint32_t> order(count);
-    std::iota(order.begin(), order.end(), 0u);
-    std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
-        const uint64_t wx = 4ull * slices[x].m + 3ull * slices[x].nj + slices[x].n;
-        const uint64_t wy = 4ull * slices[y].m + 3ull * slices[y].nj + slices[y].n;
-        return wx > wy;
-    });
+    build_order(b);
     cudaMemcpyAsync(b->d_worlds, slices.data(), sizeof(WorldSlice) * count, cudaMemcpyHostToDevice, b->stream);
-    cudaMemcpyAsync(b->d_order, order.data(), sizeof(uint32_t) * count, cudaMemcpyHostToDevice, b->stream);
-    for (uint32_t w = 0; w < count; ++w) {
-        const NphGpuWorldView &v = worlds[w];
-        const WorldSlice &s = slices[w];
-        if (v.body_count > 0) {
-            cudaMemcpyAsync(b->d_bodies + s.body_first, v.bodies, sizeof(NphGpuBody) * v.body_count,
-                            cudaMemcpyHostToDevice, b->stream);
-        }
-        if (v.fixed_count > 0) {
-            cudaMemcpyAsync(b->d_fixed + s.fixed_first, v.fixed_bodies, sizeof(NphGpuBody) * v.fixed_count,
-                            cudaMemcpyHostToDevice, b->stream);
-        }
-        if (v.contact_count > 0) {
-            cudaMemcpyAsync(b->d_contacts + s.contact_first, v.contacts,
-                            sizeof(NphGpuContact) * v.contact_count, cudaMemcpyHostToDevice, b->stream);
-        }
-        if (v.joint_count > 0) {
-            cudaMemcpyAsync(b->d_joints + s.joint_first, v.joints, sizeof(NphGpuJoint) * v.joint_count,
-                            cudaMemcpyHostToDevice, b->stream);
+    cudaMemcpyAsync(b->d_order, b->order.data(), sizeof(uint32_t) * count, cudaMemcpyHostToDevice, b->stream);
+    {
+        CopyRun cb(b->stream, cudaMemcpyHostToDevice), cf(b->stream, cudaMemcpyHostToDevice),
+            cc(b->stream, cudaMemcpyHostToDevice), cj(b->stream, cudaMemcpyHostToDevice);
+        for (uint32_t w = 0; w < count; ++w) {
+            const NphGpuWorldView &v = worlds[w];
+            const WorldSlice &s = slices[w];
+            cb.add(b->d_bodies + s.body_first, v.bodies, sizeof(NphGpuBody) * v.body_count);
+            cf.add(b->d_fixed + s.fixed_first, v.fixed_bodies, sizeof(NphGpuBody) * v.fixed_count);
+            cc.add(b->d_contacts + s.contact_first, v.contacts, sizeof(NphGpuContact) * v.contact_count);
+            cj.add(b->d_joints + s.joint_first, v.joints, sizeof(NphGpuJoint) * v.joint_count);
         }
     }
     cudaMemsetAsync(b->d_counters, 0, 4 * sizeof(uint32_t), b->stream);
@@ -766,30 +986,27 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_download(NphGpuBatch *b, NphGpuWorldView 
     if (r != NPH_GPU_OK) {
         return r;
     }
-    if (b->h_counters[1] != 0u) {
+    if (b->h_counters[2] != 0u) {
         return NPH_GPU_INVALID_ARGUMENT; // a malformed record: nothing written back
     }
     for (uint32_t w = 0; w < count; ++w) {
-        NphGpuWorldView &v = worlds[w];
+        const NphGpuWorldView &v = worlds[w];
         const WorldSlice &s = b->worlds[w];
-        if (v.body_count != s.n || v.contact_count != s.m || v.joint_count != s.nj) {
+        if (v.body_count != s.n || v.contact_count != s.m || v.joint_count != s.nj ||
+            (s.n > 0 && v.bodies == nullptr) || (s.m > 0 && v.contacts == nullptr) ||
+            (s.nj > 0 && v.joints == nullptr)) {
             return NPH_GPU_INVALID_STATE;
         }
     }
-    for (uint32_t w = 0; w < count; ++w) {
-        NphGpuWorldView &v = worlds[w];
-        const WorldSlice &s = b->worlds[w];
-        if (s.n > 0) {
-            cudaMemcpyAsync(v.bodies, b->d_bodies + s.body_first, sizeof(NphGpuBody) * s.n,
-                            cudaMemcpyDeviceToHost, b->stream);
-        }
-        if (s.m > 0) {
-            cudaMemcpyAsync(v.contacts, b->d_contacts + s.contact_first, sizeof(NphGpuContact) * s.m,
-                            cudaMemcpyDeviceToHost, b->stream);
-        }
-        if (s.nj > 0) {
-            cudaMemcpyAsync(v.joints, b->d_joints + s.joint_first, sizeof(NphGpuJoint) * s.nj,
-                            cudaMemcpyDeviceToHost, b->stream);
+    {
+        CopyRun cb(b->stream, cudaMemcpyDeviceToHost), cc(b->stream, cudaMemcpyDeviceToHost),
+            cj(b->stream, cudaMemcpyDeviceToHost);
+        for (uint32_t w = 0; w < count; ++w) {
+            NphGpuWorldView &v = worlds[w];
+            const WorldSlice &s = b->worlds[w];
+            cb.add(v.bodies, b->d_bodies + s.body_first, sizeof(NphGpuBody) * s.n);
+            cc.add(v.contacts, b->d_contacts + s.contact_first, sizeof(NphGpuContact) * s.m);
+            cj.add(v.joints, b->d_joints + s.joint_first, sizeof(NphGpuJoint) * s.nj);
         }
     }
     return cuda_result(cudaStreamSynchronize(b->stream));
@@ -808,16 +1025,17 @@ NPH_GPU_API NphGpuResult nph_gpu_phys_solve_worlds(NphGpuBatch *b, const NphGpuW
     return r;
 }
 
-NPH_GPU_API NphGpuResult nph_gpu_batch_set_config(NphGpuBatch *b, uint32_t config,
-                                                  uint32_t shared_velocities)
+NPH_GPU_API NphGpuResult nph_gpu_batch_set_config(NphGpuBatch *b, const NphGpuBatchTuning *t)
 {
-    if (b == nullptr || config >= kBatchConfigCount) {
+    if (b == nullptr || t == nullptr || t->config >= kBatchConfigCount ||
+        t->shared_velocities > NPH_GPU_BATCH_SHARED_LARGE) {
         return NPH_GPU_INVALID_ARGUMENT;
     }
-    b->config = config;
-    b->shared_velocities = shared_velocities != 0u ? 1u : 0u;
-    drop_batch_graph(b);
-    return NPH_GPU_OK;
+    cudaSetDevice(b->device);
+    b->config = t->config;
+    b->shared_mode = t->shared_velocities;
+    b->warp_color_max = t->warp_color_max;
+    return apply_order(b);
 }
 
 NPH_GPU_API uint32_t nph_gpu_batch_config_count(void) { return kBatchConfigCount; }
@@ -825,7 +1043,7 @@ NPH_GPU_API uint32_t nph_gpu_batch_config_count(void) { return kBatchConfigCount
 NPH_GPU_API NphGpuResult nph_gpu_batch_autotune(NphGpuBatch *b, const NphGpuWorldParams *params,
                                                 float dt, uint32_t rounds, NphGpuBatchTuning *out)
 {
-    if (b == nullptr || params == nullptr) {
+    if (b == nullptr || params == nullptr || !(dt > 0.0f) || params->substeps == 0u || params->substeps > 64u) {
         return NPH_GPU_INVALID_ARGUMENT;
     }
     if (b->world_count == 0) {
@@ -836,45 +1054,51 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_autotune(NphGpuBatch *b, const NphGpuWorl
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
+    static const uint32_t kSplits[] = {0u, 16u, 32u, 64u, 128u, 0xFFFFFFFFu};
     float best = 1e30f;
-    uint32_t best_config = b->config, best_shared = b->shared_velocities;
+    NphGpuBatchTuning chosen{b->config, kBatchConfigs[b->config].threads, b->shared_mode, b->warp_color_max, 0.0f};
     rounds = rounds == 0u ? 1u : rounds;
     NphGpuResult r = NPH_GPU_OK;
-    for (uint32_t shared = 0; shared < 2u && r == NPH_GPU_OK; ++shared) {
+    for (uint32_t shared = 0; shared <= NPH_GPU_BATCH_SHARED_LARGE && r == NPH_GPU_OK; ++shared) {
         for (uint32_t c = 0; c < kBatchConfigCount && r == NPH_GPU_OK; ++c) {
-            b->config = c;
-            b->shared_velocities = shared;
-            drop_batch_graph(b);
-            r = launch_batch_step(b, K, params->substeps); // builds the graph, warms up
-            cudaEventRecord(e0, b->stream);
-            for (uint32_t i = 0; i < rounds && r == NPH_GPU_OK; ++i) {
-                r = launch_batch_step(b, K, params->substeps);
-            }
-            cudaEventRecord(e1, b->stream);
-            if (r == NPH_GPU_OK) {
-                r = cuda_result(cudaEventSynchronize(e1));
-            }
-            float ms = 0.0f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            if (r == NPH_GPU_OK && ms < best) {
-                best = ms;
-                best_config = c;
-                best_shared = shared;
+            for (uint32_t split : kSplits) {
+                if (r != NPH_GPU_OK) {
+                    break;
+                }
+                b->config = c;
+                b->shared_mode = shared;
+                b->warp_color_max = split;
+                r = apply_order(b);
+                if (r == NPH_GPU_OK) {
+                    r = launch_batch_step(b, K, params->substeps); // builds the graph, warms up
+                }
+                cudaEventRecord(e0, b->stream);
+                for (uint32_t i = 0; i < rounds && r == NPH_GPU_OK; ++i) {
+                    r = launch_batch_step(b, K, params->substeps);
+                }
+                cudaEventRecord(e1, b->stream);
+                if (r == NPH_GPU_OK) {
+                    r = cuda_result(cudaEventSynchronize(e1));
+                }
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (r == NPH_GPU_OK && ms < best) {
+                    best = ms;
+                    chosen = NphGpuBatchTuning{c, kBatchConfigs[c].threads, shared, split, ms / (float)rounds};
+                }
             }
         }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    b->config = best_config;
-    b->shared_velocities = best_shared;
-    drop_batch_graph(b);
+    b->config = chosen.config;
+    b->shared_mode = chosen.shared_velocities;
+    b->warp_color_max = chosen.warp_color_max;
+    const NphGpuResult ro = apply_order(b);
     if (out != nullptr) {
-        out->config = best_config;
-        out->threads = kBatchConfigs[best_config].threads;
-        out->shared_velocities = best_shared;
-        out->ms_per_step = best / (float)rounds;
+        *out = chosen;
     }
-    return r;
+    return r != NPH_GPU_OK ? r : ro;
 }
 
 NPH_GPU_API NphGpuResult nph_gpu_batch_info(const NphGpuBatch *b, NphGpuBatchInfo *out)
@@ -889,8 +1113,10 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_info(const NphGpuBatch *b, NphGpuBatchInf
     out->joints = b->joints;
     out->config = b->config;
     out->threads = kBatchConfigs[b->config].threads;
-    out->shared_velocities = b->shared_velocities;
+    out->shared_velocities = b->shared_mode;
     out->blocks_per_sm = b->blocks_per_sm;
+    out->warp_color_max = b->warp_color_max;
+    out->warp_worlds = b->world_count - b->block_worlds;
     return NPH_GPU_OK;
 }
 

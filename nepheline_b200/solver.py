@@ -60,7 +60,7 @@ def lib() -> ctypes.CDLL:
         "nph_gpu_batch_download": (ctypes.c_int32, [_vp, P(abi.WorldView), _u32]),
         "nph_gpu_phys_solve_worlds": (ctypes.c_int32, [_vp, P(abi.WorldParams), ctypes.c_float,
                                                        P(abi.WorldView), _u32]),
-        "nph_gpu_batch_set_config": (ctypes.c_int32, [_vp, _u32, _u32]),
+        "nph_gpu_batch_set_config": (ctypes.c_int32, [_vp, P(abi.BatchTuning)]),
         "nph_gpu_batch_config_count": (_u32, []),
         "nph_gpu_batch_autotune": (ctypes.c_int32, [_vp, P(abi.WorldParams), ctypes.c_float,
                                                     _u32, P(abi.BatchTuning)]),
@@ -238,16 +238,27 @@ class Batch:
         return int(self.L.nph_gpu_phys_solve_worlds(self._h, ctypes.byref(params), dt, arr,
                                                     len(views)))
 
-    def set_config(self, config: int, shared_velocities: bool) -> None:
-        _check(self.L.nph_gpu_batch_set_config(self._h, config, int(shared_velocities)),
+    def set_config(self, config: int, shared_velocities: int = abi.BATCH_SHARED_SMALL,
+                   warp_color_max: int = 32) -> None:
+        """Launch shape, shared-memory mode for velocities (abi.BATCH_SHARED_*) and the
+        largest colour a world may have to run on one warp (0: every world on a block)."""
+        t = abi.BatchTuning()
+        t.config = config
+        t.shared_velocities = int(shared_velocities)
+        t.warp_color_max = warp_color_max
+        _check(self.L.nph_gpu_batch_set_config(self._h, ctypes.byref(t)),
                "nph_gpu_batch_set_config")
+
+    def config_count(self) -> int:
+        return int(self.L.nph_gpu_batch_config_count())
 
     def autotune(self, params: abi.WorldParams, dt: float, rounds: int = 1) -> dict:
         t = abi.BatchTuning()
         _check(self.L.nph_gpu_batch_autotune(self._h, ctypes.byref(params), dt, rounds,
                                              ctypes.byref(t)), "nph_gpu_batch_autotune")
         return {"config": t.config, "threads": t.threads,
-                "shared_velocities": t.shared_velocities, "ms_per_step": t.ms_per_step}
+                "shared_velocities": t.shared_velocities, "warp_color_max": t.warp_color_max,
+                "ms_per_step": t.ms_per_step}
 
     def info(self) -> dict:
         i = abi.BatchInfo()

@@ -30,11 +30,12 @@ def test_record_layouts_match_the_header(tmp_path):
     src = tmp_path / "sizes.c"
     src.write_text(
         '#include <stdio.h>\n#include <stddef.h>\n#include "nepheline_b200.h"\n'
-        'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\\n",'
+        'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\\n",'
         'sizeof(NphGpuBody),sizeof(NphGpuContactPoint),sizeof(NphGpuContact),'
         'sizeof(NphGpuJoint),sizeof(NphGpuWorldParams),sizeof(NphGpuWorldView),'
         'offsetof(NphGpuJoint,linear_impulse),offsetof(NphGpuContact,points),'
-        'sizeof(NphGpuKernelTime));return 0;}\n')
+        'sizeof(NphGpuKernelTime),sizeof(NphGpuBatchTuning),sizeof(NphGpuBatchInfo),'
+        'sizeof(NphGpuStepStats),sizeof(NphGpuSolverDesc));return 0;}\n')
     exe = tmp_path / "sizes"
     subprocess.run(["gcc", f"-I{HEADER.parent}", str(src), "-o", str(exe)], check=True)
     got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True,
@@ -43,7 +44,9 @@ def test_record_layouts_match_the_header(tmp_path):
     import ctypes
     assert got == [sz["body"], sz["point"], sz["contact"], sz["joint"], sz["params"], sz["view"],
                    abi.JOINT_DTYPE.fields["linear_impulse"][1],
-                   abi.CONTACT_DTYPE.fields["points"][1], ctypes.sizeof(abi.KernelTime)]
+                   abi.CONTACT_DTYPE.fields["points"][1], ctypes.sizeof(abi.KernelTime),
+                   ctypes.sizeof(abi.BatchTuning), ctypes.sizeof(abi.BatchInfo),
+                   ctypes.sizeof(abi.StepStats), ctypes.sizeof(abi.SolverDesc)]
 
 
 def test_library_exports_every_declared_entry_point():

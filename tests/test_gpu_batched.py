@@ -12,8 +12,37 @@ pytestmark = pytest.mark.gpu
 DT = 1.0 / 60.0
 
 
+def hub_view(spokes=30):
+    """A hub body touching `spokes` dynamic bodies: colours 0..19 fill, the rest overflow."""
+    nb = spokes + 1
+    bodies = scenes.body_records(nb)
+    mass = np.full(nb, 2.0, np.float32)
+    inertia = np.zeros((nb, 9), np.float32)
+    inertia[:, [0, 4, 8]] = 2.0 / 6.0
+    scenes.set_mass(bodies, mass, inertia)
+    ang = np.linspace(0, 2 * np.pi, spokes, endpoint=False)
+    bodies["center"][1:, 0] = np.cos(ang)
+    bodies["center"][1:, 2] = np.sin(ang)
+    bodies["linear_velocity"][1:, 0] = -0.5 * np.cos(ang)
+    contacts = np.zeros(spokes, abi.CONTACT_DTYPE)
+    contacts["body_a"] = 0
+    contacts["body_b"] = np.arange(1, nb)
+    contacts["point_count"] = 1
+    contacts["friction"] = 0.5
+    n = np.stack([np.cos(ang), np.zeros_like(ang), np.sin(ang)], 1).astype(np.float32)
+    contacts["normal"] = n
+    pts = contacts["points"]
+    pts["anchor_a"][:, 0] = n * 0.5
+    pts["anchor_b"][:, 0] = -n * 0.5
+    pts["separation"][:, 0] = -0.01
+    sc = scenes.SolverScene(bodies, mass, np.zeros(0, abi.JOINT_DTYPE), contacts)
+    color, slot = scenes.host_color(sc)
+    return sc.to_view(color, slot)
+
+
 def reference_views(steps_warm=30):
-    """Solver inputs cut from reference scenes of different kinds and sizes."""
+    """Solver inputs cut from reference scenes of different kinds and sizes, lattices, mixed
+    batch worlds, a world with overflow constraints and a world without constraints."""
     views = []
     for w in (ref_scenes.pyramid(rows=8), ref_scenes.sphere_pour(count=125),
               ref_scenes.box_pile(count=30), ref_scenes.hinge_chain(links=6, limits=False,
@@ -23,17 +52,24 @@ def reference_views(steps_warm=30):
             w.step(DT)
         w.collide()
         views.append(w.export_view())
-    for edge, seed in ((3, 1), (5, 2), (9, 3)):
+    for edge, seed in ((3, 1), (5, 2), (9, 3), (14, 4)):
         sc = scenes.lattice_graph(edge, seed=seed, joint_fraction=0.2)
         color, slot = scenes.host_color(sc)
         views.append(sc.to_view(color, slot))
+    for bodies, seed in ((12, 1), (90, 2), (700, 3)):
+        sc = scenes.mixed_world(bodies, seed)
+        color, slot = scenes.host_color(sc)
+        views.append(sc.to_view(color, slot))
+    views.append(hub_view())
+    sc = scenes.lattice_graph(2, seed=9, joint_fraction=0.0)
+    sc.contacts = sc.contacts[:0]
+    color, slot = scenes.host_color(sc)
+    views.append(sc.to_view(color, slot))
     return views
 
 
-@pytest.mark.parametrize("config", [0, 1, 2, 3, 4])
-@pytest.mark.parametrize("shared", [False, True])
-def test_batch_equals_worlds_solved_alone(solver, ref_lib, config, shared):
-    from nepheline_b200.solver import Batch
+@pytest.fixture(scope="module")
+def solved_alone(solver):
     params = abi.WorldParams.default()
     views = reference_views()
     alone = []
@@ -41,14 +77,53 @@ def test_batch_equals_worlds_solved_alone(solver, ref_lib, config, shared):
         out = v.copy()
         solver.phys_solve(out, params, DT)
         alone.append(out)
+    return views, alone
+
+
+@pytest.mark.parametrize("shared", [abi.BATCH_SHARED_NONE, abi.BATCH_SHARED_SMALL,
+                                    abi.BATCH_SHARED_LARGE])
+def test_batch_equals_worlds_solved_alone(solved_alone, ref_lib, shared):
+    """Every launch shape, with every world on a block, on a warp, or split by size."""
+    from nepheline_b200.solver import Batch
+    params = abi.WorldParams.default()
+    views, alone = solved_alone
     batch = Batch()
-    batch.set_config(config, shared)
-    together = [v.copy() for v in views]
-    batch.phys_solve_worlds(together, params, DT)
-    for i, (a, b) in enumerate(zip(together, alone)):
+    for config in range(batch.config_count()):
+        for split in (0, 24, 0xFFFFFFFF):
+            batch.set_config(config, shared, split)
+            together = [v.copy() for v in views]
+            batch.phys_solve_worlds(together, params, DT)
+            info = batch.info()
+            if split == 0:
+                assert info["warp_worlds"] == 0
+            if split == 0xFFFFFFFF:
+                assert info["warp_worlds"] == len(views)
+            for i, (a, b) in enumerate(zip(together, alone)):
+                where = f"world {i}, config {config}, shared {shared}, split {split}"
+                assert a.bodies.tobytes() == b.bodies.tobytes(), where
+                assert a.contacts.tobytes() == b.contacts.tobytes(), where
+                assert a.joints.tobytes() == b.joints.tobytes(), where
+    batch.close()
+
+
+def test_packed_worlds_copy_back_to_their_slices(solved_alone):
+    """Worlds whose records are consecutive slices of shared host arrays (the coalesced copy
+    path) get the same results as separately allocated worlds."""
+    from nepheline_b200.solver import Batch
+    params = abi.WorldParams.default()
+    views, alone = solved_alone
+    packed = abi.pack_views([v.copy() for v in views])
+    batch = Batch()
+    batch.phys_solve_worlds(packed, params, DT)
+    for i, (a, b) in enumerate(zip(packed, alone)):
         assert a.bodies.tobytes() == b.bodies.tobytes(), f"world {i}"
         assert a.contacts.tobytes() == b.contacts.tobytes(), f"world {i}"
         assert a.joints.tobytes() == b.joints.tobytes(), f"world {i}"
+    # A smaller batch after a larger one reuses the device arrays.
+    few = abi.pack_views([v.copy() for v in views[:3]])
+    batch.phys_solve_worlds(few, params, DT)
+    for i in range(3):
+        assert few[i].bodies.tobytes() == alone[i].bodies.tobytes()
     batch.close()
 
 
@@ -85,6 +160,7 @@ def test_batch_autotuner_keeps_results(solver):
     batch.upload(views)
     tuned = batch.autotune(params, DT, rounds=1)
     assert tuned["threads"] in (128, 256, 512, 1024)
+    assert tuned["shared_velocities"] in (0, 1, 2)
     batch.upload(views)
     batch.step_async(params, DT, 1)
     got = [v.copy() for v in views]
