@@ -453,6 +453,106 @@ NPH_GPU_API NphGpuResult nph_gpu_graph_color_static(void *stream, const uint32_t
                                                     uint32_t *out_slot);
 
 /* ------------------------------------------------------------------------------------
+ * The learned warm start: no counterpart in the reference, whose contact points that are new
+ * this step start at zero impulse (contact.c:547-565) and whose persisted points start at
+ * their matched impulses. A small network predicts a new point's normal and two friction
+ * impulses from features of its contact; the plain warm start stays for every other point.
+ * ---------------------------------------------------------------------------------- */
+
+/* The network: NPH_GPU_MLP_INPUTS -> 3 x NPH_GPU_MLP_HIDDEN (ReLU) -> NPH_GPU_MLP_OUTPUTS,
+ * BF16 weights and activations on the tensor cores with FP32 accumulation, FP32 master
+ * weights trained with Adam. Parameters, in order: W1 [64][16], b1 [64], W2 [64][64], b2,
+ * W3 [64][64], b3, W4 [3][64], b4 [3] (weights row-major by output unit). */
+#define NPH_GPU_MLP_INPUTS 16
+#define NPH_GPU_MLP_HIDDEN 64
+#define NPH_GPU_MLP_OUTPUTS 3
+#define NPH_GPU_MLP_PARAMS 9603
+
+typedef struct NphGpuMlp NphGpuMlp;
+
+/* A network on `device` with seeded initial weights (uniform, scale sqrt(6 / fan_in); the
+ * output layer's a tenth of that; zero biases). */
+NPH_GPU_API NphGpuResult nph_gpu_mlp_create(int32_t device, uint64_t seed, NphGpuMlp **out);
+NPH_GPU_API void nph_gpu_mlp_destroy(NphGpuMlp *mlp);
+/* NPH_GPU_MLP_PARAMS floats in the order above; setting resets the optimiser. */
+NPH_GPU_API NphGpuResult nph_gpu_mlp_set_weights(NphGpuMlp *mlp, const float *params);
+NPH_GPU_API NphGpuResult nph_gpu_mlp_get_weights(const NphGpuMlp *mlp, float *params);
+/* Outputs (count x 3) of `count` feature rows (count x 16), host arrays. */
+NPH_GPU_API NphGpuResult nph_gpu_mlp_predict(NphGpuMlp *mlp, const float *features, uint64_t count,
+                                             float *out);
+/* The gradient (NPH_GPU_MLP_PARAMS floats) and value of the mean over the samples of the
+ * squared error summed over the three outputs. */
+NPH_GPU_API NphGpuResult nph_gpu_mlp_gradients(NphGpuMlp *mlp, const float *features,
+                                               const float *targets, uint64_t count, float *grad,
+                                               float *loss);
+/* `epochs` passes of Adam (beta 0.9, 0.999, eps 1e-8, step `lr`) over mini-batches of
+ * `batch` samples in a seeded shuffled order; writes the final loss over all samples. */
+NPH_GPU_API NphGpuResult nph_gpu_mlp_train(NphGpuMlp *mlp, const float *features,
+                                           const float *targets, uint64_t count, uint32_t epochs,
+                                           uint32_t batch, float lr, uint64_t shuffle_seed,
+                                           float *final_loss);
+
+/* Point slots: manifold g's point k is slot 4 g + k (g in the uploaded colour order). */
+#define NPH_GPU_POINT_NONE 0u /* k >= the manifold's point count */
+#define NPH_GPU_POINT_WARM 1u /* starts at a persisted (non-zero) impulse */
+#define NPH_GPU_POINT_COLD 2u /* starts at zero impulse: new this step */
+
+/* The features of every point slot of the uploaded world at the step's start (host arrays of
+ * 4 x manifolds entries; features 16 per slot): in the contact frame (n, t1 =
+ * perpendicular(n), t2 = n x t1) with g = |gravity| (1 m/s^2 without gravity) and
+ * h = dt / substeps,
+ *   0-2  the relative velocity at the point along n, t1, t2, over g h
+ *   3-5  n
+ *   6    the separation over 0.02 m
+ *   7-10 inverse masses of A and B and the angular terms (rA x n).IA^-1(rA x n), same for B,
+ *        each over their sum kn (the inverse normal mass)
+ *   11   point count / 4
+ *   12   friction
+ *   13   -n . gravity / |gravity|
+ *   14   1 when one side is not dynamic
+ *   15   the tangent effective-mass inverse's first entry times kn
+ * `scale` is g h / kn, the impulse a network output of 1 stands for; `kind` a
+ * NPH_GPU_POINT_* value. */
+NPH_GPU_API NphGpuResult nph_gpu_world_features(NphGpuSolver *solver,
+                                                const NphGpuWorldParams *params, float dt,
+                                                float *features, float *scale, uint32_t *kind,
+                                                uint64_t slots);
+
+/* Attaches a network to the solver (NULL detaches it): every following step then starts
+ * each cold point at the network's prediction (normal impulse max(out0, 0) x scale, friction
+ * out1 and out2 x scale along t1 and t2, scaled back onto the friction cone) instead of
+ * zero. */
+NPH_GPU_API NphGpuResult nph_gpu_solver_set_warm_start_model(NphGpuSolver *solver, NphGpuMlp *mlp);
+
+/* The residual-driven mode that judges a warm start. On the uploaded world: prepare, the
+ * first substep's velocity integration and warm start (plain, or learned when `learned` and a
+ * network is attached), then rigid passes (the relax pass: no softness, speculative rows for
+ * separated points) over every colour until the velocity-constraint residual falls to
+ * `tolerance` x the reference residual, or `max_passes`. The residual is the L2 norm over
+ * points of r_n = |vn + b| where the normal impulse is positive, max(-(vn + b), 0) where not
+ * (b = separation / h for a separated point, else 0), plus the slip |vt| of points whose
+ * friction impulse is inside the cone. `reference_residual` <= 0 uses this run's own
+ * initial residual. `residuals` (optional, max_passes + 1 floats) gets the residual after
+ * the warm start and after each pass; `impulses` (optional, 12 per manifold) the final
+ * normal, t1 and t2 impulses of every point slot. The uploaded records are not changed. */
+typedef struct NphGpuConvergeStats {
+    uint32_t passes;           /* passes run */
+    uint32_t converged;        /* 1 when the residual reached the tolerance */
+    uint32_t cold_points;      /* points that started cold */
+    uint32_t predicted_points; /* cold points the network started */
+    float initial_residual;    /* after the warm start */
+    float final_residual;
+    float reference_residual;  /* the denominator */
+    float ms;                  /* device time from prepare to the last pass */
+} NphGpuConvergeStats;
+NPH_GPU_API NphGpuResult nph_gpu_world_converge(NphGpuSolver *solver,
+                                                const NphGpuWorldParams *params, float dt,
+                                                uint32_t learned, float tolerance,
+                                                uint32_t max_passes, float reference_residual,
+                                                float *residuals, float *impulses,
+                                                NphGpuConvergeStats *out);
+
+/* ------------------------------------------------------------------------------------
  * Version
  * ---------------------------------------------------------------------------------- */
 

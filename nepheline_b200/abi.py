@@ -181,6 +181,19 @@ class KernelTime(ctypes.Structure):
 
 BATCH_SHARED_NONE, BATCH_SHARED_SMALL, BATCH_SHARED_LARGE = 0, 1, 2
 
+# The learned warm start's network and point slots (nepheline_b200.h).
+MLP_INPUTS, MLP_HIDDEN, MLP_OUTPUTS = 16, 64, 3
+MLP_PARAMS = (MLP_HIDDEN * MLP_INPUTS + MLP_HIDDEN + 2 * (MLP_HIDDEN * MLP_HIDDEN + MLP_HIDDEN)
+              + MLP_OUTPUTS * MLP_HIDDEN + MLP_OUTPUTS)
+POINT_NONE, POINT_WARM, POINT_COLD = 0, 1, 2
+
+
+class ConvergeStats(ctypes.Structure):
+    _fields_ = [("passes", ctypes.c_uint32), ("converged", ctypes.c_uint32),
+                ("cold_points", ctypes.c_uint32), ("predicted_points", ctypes.c_uint32),
+                ("initial_residual", ctypes.c_float), ("final_residual", ctypes.c_float),
+                ("reference_residual", ctypes.c_float), ("ms", ctypes.c_float)]
+
 
 class BatchTuning(ctypes.Structure):
     _fields_ = [("config", ctypes.c_uint32), ("threads", ctypes.c_uint32),

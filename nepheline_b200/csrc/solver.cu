@@ -27,6 +27,14 @@
 #include "contacts.cuh"
 #include "contacts_staged.cuh"
 #include "joints.cuh"
+#include "learned.cuh"
+
+// The network's inference (mlp.cu): `count` rows, or the first *count_dev of at most
+// max_count rows.
+void nph_mlp_forward_device(const NphGpuMlp *n, const float *x, uint32_t count, float *y, cudaStream_t st);
+void nph_mlp_forward_device_count(const NphGpuMlp *n, const float *x, const uint32_t *count_dev,
+                                  uint32_t max_count, float *y, cudaStream_t st);
+int nph_mlp_device(const NphGpuMlp *n);
 
 namespace nph {
 
@@ -516,6 +524,16 @@ struct NphGpuSolver {
     cudaEvent_t ev[6] = {};
     NphGpuStepStats stats{};
     uint32_t launches = 0;
+    // The learned warm start: the attached network and its cold-point buffers.
+    NphGpuMlp *mlp = nullptr;
+    uint32_t lcap = 0;            // cold points the buffers hold
+    float *l_feat = nullptr, *l_pred = nullptr, *l_scale = nullptr;
+    uint32_t *l_slot = nullptr;
+    uint32_t *l_counts = nullptr; // [0] cold points, [1] features written
+    // The residual-driven mode's buffers.
+    uint32_t rcap = 0;            // residual slots (passes + 1)
+    float *r_sq = nullptr, *r_val = nullptr, *r_ref = nullptr;
+    uint32_t *r_state = nullptr;  // [0] done, [1] passes, [2] cold points, [3] predicted
 };
 
 namespace {
@@ -719,13 +737,12 @@ template <int P> void enqueue_pass(NphGpuSolver *s, const StepConsts &K)
     }
 }
 
-// One step's launches on the solver's stream (the stage list, solver.c:1032-1067).
-void enqueue_step(NphGpuSolver *s, const StepConsts &K, uint32_t substeps)
+// The step's prepare stage: bodies, then joints and contacts (solver.c:1032-1041).
+void enqueue_prepare(NphGpuSolver *s, const StepConsts &K)
 {
     const DevSolver S = dev_solver(s);
     const BodyArrays B = body_arrays(s);
     const double n = s->n;
-    s->launches = 0;
     mark_begin(s, kKPrepareBodies, s->n, 368.0 * n);
     k_prepare_bodies<<<stage_blocks(s->n + 1u), kStage, 0, s->stream>>>(B, s->d_bodies, s->n, K);
     mark_end(s);
@@ -748,6 +765,49 @@ void enqueue_step(NphGpuSolver *s, const StepConsts &K, uint32_t substeps)
         mark_end(s);
         s->launches++;
     }
+}
+
+// The feature scales: g = |gravity| (1 m/s^2 without gravity) and h.
+FeatureConsts feature_consts(const StepConsts &K)
+{
+    const double gx = K.gravity[0], gy = K.gravity[1], gz = K.gravity[2];
+    const double gl = std::sqrt(gx * gx + gy * gy + gz * gz);
+    const double g = gl > 0.0 ? gl : 1.0;
+    FeatureConsts F;
+    F.gh = (float)(g * K.h);
+    F.inv_gh = (float)(1.0 / (g * K.h));
+    F.gdir[0] = gl > 0.0 ? (float)(gx / gl) : 0.0f;
+    F.gdir[1] = gl > 0.0 ? (float)(gy / gl) : 0.0f;
+    F.gdir[2] = gl > 0.0 ? (float)(gz / gl) : 0.0f;
+    return F;
+}
+
+// The learned warm start of the cold points (after prepare): their features, the network's
+// predictions, and the predictions written as their warm-start impulses.
+void enqueue_learned_init(NphGpuSolver *s, const StepConsts &K)
+{
+    if (s->mlp == nullptr || s->m == 0u || s->lcap == 0u) {
+        return;
+    }
+    const DevSolver S = dev_solver(s);
+    cudaMemsetAsync(s->l_counts, 0, 2 * sizeof(uint32_t), s->stream);
+    k_cold_features<<<blocks_for(s->m), 256, 0, s->stream>>>(S, s->m, feature_consts(K), s->l_feat, s->l_scale,
+                                                             s->l_slot, s->l_counts, s->lcap, 1u);
+    nph_mlp_forward_device_count(s->mlp, s->l_feat, s->l_counts + 1, s->lcap, s->l_pred, s->stream);
+    k_apply_predictions<<<blocks_for(s->lcap), 256, 0, s->stream>>>(S, s->l_pred, s->l_scale, s->l_slot,
+                                                                    s->l_counts, s->lcap);
+    s->launches += 3;
+}
+
+// One step's launches on the solver's stream (the stage list, solver.c:1032-1067).
+void enqueue_step(NphGpuSolver *s, const StepConsts &K, uint32_t substeps)
+{
+    const DevSolver S = dev_solver(s);
+    const BodyArrays B = body_arrays(s);
+    const double n = s->n;
+    s->launches = 0;
+    enqueue_prepare(s, K);
+    enqueue_learned_init(s, K);
     for (uint32_t sub = 0; sub < substeps; ++sub) {
         mark_begin(s, kKIntegrateVelocity, s->n, 84.0 * n);
         k_integrate_velocity<<<blocks_for(s->n), kBlock, 0, s->stream>>>(B, s->n, K.h);
@@ -797,8 +857,14 @@ NphGpuResult check_cuda(cudaError_t e)
 }
 
 // Replays (capturing first if needed) one step as a graph, or launches it directly.
+NphGpuResult ensure_learned(NphGpuSolver *s);
+
 NphGpuResult launch_step(NphGpuSolver *s, const StepConsts &K, uint32_t substeps)
 {
+    const NphGpuResult lr = ensure_learned(s);
+    if (lr != NPH_GPU_OK) {
+        return lr;
+    }
     if (!s->use_graph) {
         enqueue_step(s, K, substeps);
         return check_cuda(cudaGetLastError());
@@ -965,6 +1031,67 @@ void fill_stats(NphGpuSolver *s)
     s->stats.launches = s->launches;
 }
 
+// The cold-point buffers of the learned warm start, for every point slot of the world.
+NphGpuResult ensure_learned(NphGpuSolver *s)
+{
+    const uint64_t want = 4ull * s->m;
+    if (s->mlp == nullptr || want <= s->lcap) {
+        return NPH_GPU_OK;
+    }
+    if (want > 0x7FFFFFFFull) {
+        return NPH_GPU_TOO_LARGE;
+    }
+    const uint32_t cap = (uint32_t)(want + want / 8u + 64u);
+    drop_graph(s);
+    const bool ok = dalloc(s->l_feat, (size_t)cap * NPH_GPU_MLP_INPUTS) && dalloc(s->l_pred, (size_t)cap * 3u) &&
+                    dalloc(s->l_scale, cap) && dalloc(s->l_slot, cap) && dalloc(s->l_counts, 2);
+    if (!ok) {
+        s->lcap = 0;
+        cudaGetLastError();
+        return NPH_GPU_OUT_OF_MEMORY;
+    }
+    s->lcap = cap;
+    return NPH_GPU_OK;
+}
+
+NphGpuResult ensure_residuals(NphGpuSolver *s, uint32_t slots)
+{
+    if (slots <= s->rcap && s->r_state != nullptr) {
+        return NPH_GPU_OK;
+    }
+    const bool ok = dalloc(s->r_sq, slots) && dalloc(s->r_val, slots) && dalloc(s->r_ref, 1) &&
+                    dalloc(s->r_state, 4);
+    if (!ok) {
+        s->rcap = 0;
+        cudaGetLastError();
+        return NPH_GPU_OUT_OF_MEMORY;
+    }
+    s->rcap = slots;
+    return NPH_GPU_OK;
+}
+
+// One rigid pass of the residual-driven mode: the overflow, then every colour's joints and
+// contacts (a colour's joints and contacts share no dynamic body).
+void enqueue_converge_pass(NphGpuSolver *s, const StepConsts &K, const uint32_t *done)
+{
+    const DevSolver S = dev_solver(s);
+    const uint32_t o = NPH_GPU_OVERFLOW;
+    if (s->ccount[o] > 0u || s->jcount[o] > 0u) {
+        k_converge_overflow<<<1, 32, 0, s->stream>>>(S, s->cfirst[o], s->ccount[o], s->jfirst[o], s->jcount[o], K,
+                                                     done);
+    }
+    for (uint32_t c = 0; c < NPH_GPU_COLORS; ++c) {
+        if (s->jcount[c] > 0u) {
+            k_converge_joint_pass<<<blocks_for(s->jcount[c]), 256, 0, s->stream>>>(S, s->jfirst[c], s->jcount[c], K,
+                                                                                   done);
+        }
+        if (s->ccount[c] > 0u) {
+            k_converge_pass<128><<<(s->ccount[c] + 127u) / 128u, 128, 0, s->stream>>>(S, s->cfirst[c], s->ccount[c],
+                                                                                      K, done);
+        }
+    }
+}
+
 } // namespace
 
 // ------------------------------------------------------------------------------------
@@ -1059,6 +1186,15 @@ NPH_GPU_API void nph_gpu_solver_destroy(NphGpuSolver *s)
     dfree(s->pt);
     dfree(s->pi);
     dfree(s->jw);
+    dfree(s->l_feat);
+    dfree(s->l_pred);
+    dfree(s->l_scale);
+    dfree(s->l_slot);
+    dfree(s->l_counts);
+    dfree(s->r_sq);
+    dfree(s->r_val);
+    dfree(s->r_ref);
+    dfree(s->r_state);
     dfree(s->d_err);
     if (s->h_err != nullptr) {
         cudaFreeHost(s->h_err);
@@ -1342,6 +1478,187 @@ NPH_GPU_API NphGpuResult nph_gpu_solver_stats(const NphGpuSolver *s, NphGpuStepS
 NPH_GPU_API void *nph_gpu_solver_stream(const NphGpuSolver *s)
 {
     return s != nullptr ? (void *)s->stream : nullptr;
+}
+
+NPH_GPU_API NphGpuResult nph_gpu_solver_set_warm_start_model(NphGpuSolver *s, NphGpuMlp *mlp)
+{
+    if (s == nullptr || (mlp != nullptr && nph_mlp_device(mlp) != s->device)) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    cudaSetDevice(s->device);
+    cudaStreamSynchronize(s->stream);
+    s->mlp = mlp;
+    drop_graph(s);
+    return ensure_learned(s);
+}
+
+NPH_GPU_API NphGpuResult nph_gpu_world_features(NphGpuSolver *s, const NphGpuWorldParams *params, float dt,
+                                                float *features, float *scale, uint32_t *kind, uint64_t slots)
+{
+    if (s == nullptr) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    NphGpuResult r = validate_params(params, dt);
+    if (r != NPH_GPU_OK) {
+        return r;
+    }
+    if (!s->uploaded) {
+        return NPH_GPU_INVALID_STATE;
+    }
+    const uint64_t need = 4ull * s->m;
+    if (slots < need || (need > 0 && (features == nullptr || scale == nullptr || kind == nullptr))) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    if (need == 0) {
+        return NPH_GPU_OK;
+    }
+    cudaSetDevice(s->device);
+    const StepConsts K = make_step_consts(*params, dt);
+    float *d_feat = nullptr, *d_scale = nullptr;
+    uint32_t *d_kind = nullptr;
+    if (!dalloc(d_feat, need * NPH_GPU_MLP_INPUTS) || !dalloc(d_scale, need) || !dalloc(d_kind, need)) {
+        dfree(d_feat);
+        dfree(d_scale);
+        dfree(d_kind);
+        cudaGetLastError();
+        return NPH_GPU_OUT_OF_MEMORY;
+    }
+    s->marks = nullptr;
+    enqueue_prepare(s, K);
+    k_all_features<<<blocks_for(s->m), 256, 0, s->stream>>>(dev_solver(s), s->m, feature_consts(K), d_feat,
+                                                            d_scale, d_kind);
+    cudaMemcpyAsync(features, d_feat, need * NPH_GPU_MLP_INPUTS * sizeof(float), cudaMemcpyDeviceToHost,
+                    s->stream);
+    cudaMemcpyAsync(scale, d_scale, need * sizeof(float), cudaMemcpyDeviceToHost, s->stream);
+    cudaMemcpyAsync(kind, d_kind, need * sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream);
+    r = check_cuda(cudaStreamSynchronize(s->stream));
+    dfree(d_feat);
+    dfree(d_scale);
+    dfree(d_kind);
+    if (r == NPH_GPU_OK) {
+        r = read_error(s);
+    }
+    return r;
+}
+
+NPH_GPU_API NphGpuResult nph_gpu_world_converge(NphGpuSolver *s, const NphGpuWorldParams *params, float dt,
+                                                uint32_t learned, float tolerance, uint32_t max_passes,
+                                                float reference_residual, float *residuals, float *impulses,
+                                                NphGpuConvergeStats *out)
+{
+    if (s == nullptr || out == nullptr || !(tolerance > 0.0f) || max_passes > 1000000u) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    NphGpuResult r = validate_params(params, dt);
+    if (r != NPH_GPU_OK) {
+        return r;
+    }
+    if (!s->uploaded || (learned != 0u && s->mlp == nullptr)) {
+        return NPH_GPU_INVALID_STATE;
+    }
+    std::memset(out, 0, sizeof *out);
+    cudaSetDevice(s->device);
+    const StepConsts K = make_step_consts(*params, dt);
+    r = ensure_residuals(s, max_passes + 1u);
+    if (r == NPH_GPU_OK) {
+        r = ensure_learned(s);
+    }
+    if (r != NPH_GPU_OK) {
+        return r;
+    }
+    const DevSolver S = dev_solver(s);
+    const BodyArrays B = body_arrays(s);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaMemsetAsync(s->r_sq, 0, (max_passes + 1u) * sizeof(float), s->stream);
+    cudaMemsetAsync(s->r_val, 0, (max_passes + 1u) * sizeof(float), s->stream);
+    cudaMemsetAsync(s->r_state, 0, 4 * sizeof(uint32_t), s->stream);
+    s->marks = nullptr;
+    const uint32_t *done = s->r_state;
+    const uint32_t res_blocks = std::max<uint32_t>(1u, std::min<uint32_t>(blocks_for(s->m), 148u * 8u));
+    cudaEventRecord(e0, s->stream);
+    enqueue_prepare(s, K);
+    // Cold points: counted (plain), or counted and started by the network (learned).
+    const bool use = learned != 0u && s->lcap > 0u;
+    if (s->m > 0u) {
+        k_cold_features<<<blocks_for(s->m), 256, 0, s->stream>>>(S, s->m, feature_consts(K), s->l_feat, s->l_scale,
+                                                                 s->l_slot, s->r_state + 2, use ? s->lcap : 0u,
+                                                                 use ? 1u : 0u);
+        if (use) {
+            nph_mlp_forward_device_count(s->mlp, s->l_feat, s->r_state + 3, s->lcap, s->l_pred, s->stream);
+            k_apply_predictions<<<blocks_for(s->lcap), 256, 0, s->stream>>>(S, s->l_pred, s->l_scale, s->l_slot,
+                                                                            s->r_state + 2, s->lcap);
+        }
+    }
+    k_integrate_velocity<<<blocks_for(s->n), kBlock, 0, s->stream>>>(B, s->n, K.h);
+    enqueue_pass<kWarm>(s, K);
+    k_residual<<<res_blocks, 256, 0, s->stream>>>(S, s->m, K.inv_h, s->r_sq, done);
+    k_residual_check<<<1, 1, 0, s->stream>>>(s->r_sq, s->r_val, s->r_ref, 0u, tolerance, reference_residual,
+                                             s->r_state);
+    // Passes in chunks of eight; the host stops issuing once the residual reached the tolerance.
+    uint32_t state[4] = {0u, 0u, 0u, 0u};
+    uint32_t issued = 0;
+    while (issued < max_passes) {
+        cudaMemcpyAsync(state, s->r_state, sizeof state, cudaMemcpyDeviceToHost, s->stream);
+        r = check_cuda(cudaStreamSynchronize(s->stream));
+        if (r != NPH_GPU_OK || state[0] != 0u) {
+            break;
+        }
+        const uint32_t chunk = std::min<uint32_t>(8u, max_passes - issued);
+        for (uint32_t q = 0; q < chunk; ++q) {
+            const uint32_t p = ++issued;
+            enqueue_converge_pass(s, K, done);
+            k_residual<<<res_blocks, 256, 0, s->stream>>>(S, s->m, K.inv_h, s->r_sq + p, done);
+            k_residual_check<<<1, 1, 0, s->stream>>>(s->r_sq, s->r_val, s->r_ref, p, tolerance, reference_residual,
+                                                     s->r_state);
+        }
+    }
+    cudaEventRecord(e1, s->stream);
+    float ref = 0.0f;
+    cudaMemcpyAsync(state, s->r_state, sizeof state, cudaMemcpyDeviceToHost, s->stream);
+    cudaMemcpyAsync(&ref, s->r_ref, sizeof ref, cudaMemcpyDeviceToHost, s->stream);
+    std::vector<float> vals(max_passes + 1u, 0.0f);
+    cudaMemcpyAsync(vals.data(), s->r_val, vals.size() * sizeof(float), cudaMemcpyDeviceToHost, s->stream);
+    if (r == NPH_GPU_OK) {
+        r = check_cuda(cudaStreamSynchronize(s->stream));
+    }
+    float ms = 0.0f;
+    if (r == NPH_GPU_OK) {
+        cudaEventElapsedTime(&ms, e0, e1);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (r == NPH_GPU_OK && impulses != nullptr && s->m > 0u) {
+        float *d_imp = nullptr;
+        if (!dalloc(d_imp, 12ull * s->m)) {
+            cudaGetLastError();
+            return NPH_GPU_OUT_OF_MEMORY;
+        }
+        k_slot_impulses<<<blocks_for(s->m), 256, 0, s->stream>>>(S, s->m, d_imp);
+        cudaMemcpyAsync(impulses, d_imp, 12ull * s->m * sizeof(float), cudaMemcpyDeviceToHost, s->stream);
+        r = check_cuda(cudaStreamSynchronize(s->stream));
+        dfree(d_imp);
+    }
+    if (r == NPH_GPU_OK) {
+        r = read_error(s);
+    }
+    if (r != NPH_GPU_OK) {
+        return r;
+    }
+    const uint32_t passes = state[1];
+    if (residuals != nullptr) {
+        std::memcpy(residuals, vals.data(), (passes + 1u) * sizeof(float));
+    }
+    out->passes = passes;
+    out->converged = state[0];
+    out->cold_points = state[2];
+    out->predicted_points = use ? std::min(state[3], s->lcap) : 0u;
+    out->initial_residual = vals[0];
+    out->final_residual = vals[passes];
+    out->reference_residual = ref;
+    out->ms = ms;
+    return NPH_GPU_OK;
 }
 
 NPH_GPU_API const char *nph_gpu_version(void)

@@ -51,6 +51,22 @@ def lib() -> ctypes.CDLL:
         "nph_gpu_world_profile_step": (ctypes.c_int32, [_vp, P(abi.WorldParams), ctypes.c_float,
                                                         P(abi.KernelTime), _u32, P(_u32)]),
         "nph_gpu_solver_set_pass_config": (ctypes.c_int32, [_vp, _u32, _u32]),
+        "nph_gpu_mlp_create": (ctypes.c_int32, [ctypes.c_int32, ctypes.c_uint64, P(_vp)]),
+        "nph_gpu_mlp_destroy": (None, [_vp]),
+        "nph_gpu_mlp_set_weights": (ctypes.c_int32, [_vp, _vp]),
+        "nph_gpu_mlp_get_weights": (ctypes.c_int32, [_vp, _vp]),
+        "nph_gpu_mlp_predict": (ctypes.c_int32, [_vp, _vp, ctypes.c_uint64, _vp]),
+        "nph_gpu_mlp_gradients": (ctypes.c_int32, [_vp, _vp, _vp, ctypes.c_uint64, _vp,
+                                                   P(ctypes.c_float)]),
+        "nph_gpu_mlp_train": (ctypes.c_int32, [_vp, _vp, _vp, ctypes.c_uint64, _u32, _u32,
+                                               ctypes.c_float, ctypes.c_uint64,
+                                               P(ctypes.c_float)]),
+        "nph_gpu_world_features": (ctypes.c_int32, [_vp, P(abi.WorldParams), ctypes.c_float, _vp,
+                                                    _vp, _vp, ctypes.c_uint64]),
+        "nph_gpu_solver_set_warm_start_model": (ctypes.c_int32, [_vp, _vp]),
+        "nph_gpu_world_converge": (ctypes.c_int32, [_vp, P(abi.WorldParams), ctypes.c_float,
+                                                    _u32, ctypes.c_float, _u32, ctypes.c_float,
+                                                    _vp, _vp, P(abi.ConvergeStats)]),
         "nph_gpu_batch_create": (ctypes.c_int32, [P(abi.SolverDesc), P(_vp)]),
         "nph_gpu_batch_destroy": (None, [_vp]),
         "nph_gpu_batch_stream": (_vp, [_vp]),
@@ -128,6 +144,7 @@ class Solver:
     def upload(self, view: abi.View) -> None:
         cv = view.c_view()
         _check(self.L.nph_gpu_world_upload(self._h, ctypes.byref(cv)), "nph_gpu_world_upload")
+        self._m = len(view.contacts)
 
     def step_async(self, params: abi.WorldParams, dt: float, steps: int = 1) -> None:
         _check(self.L.nph_gpu_world_step_async(self._h, ctypes.byref(params), dt, steps),
@@ -159,6 +176,41 @@ class Solver:
         _check(self.L.nph_gpu_solver_set_pass_config(self._h, pass_kind, config),
                "nph_gpu_solver_set_pass_config")
 
+    def features(self, params: abi.WorldParams, dt: float):
+        """Features (4m x 16), impulse scales and kinds of every point slot of the uploaded
+        world at the step's start."""
+        slots = 4 * int(self._m)
+        f = np.zeros((slots, abi.MLP_INPUTS), np.float32)
+        sc = np.zeros(slots, np.float32)
+        kind = np.zeros(slots, np.uint32)
+        _check(self.L.nph_gpu_world_features(self._h, ctypes.byref(params), dt, f.ctypes.data,
+                                             sc.ctypes.data, kind.ctypes.data, slots),
+               "nph_gpu_world_features")
+        return f, sc, kind
+
+    def set_warm_start_model(self, mlp) -> None:
+        _check(self.L.nph_gpu_solver_set_warm_start_model(self._h, None if mlp is None
+                                                          else mlp.handle),
+               "nph_gpu_solver_set_warm_start_model")
+
+    def converge(self, params: abi.WorldParams, dt: float, learned: bool = False,
+                 tolerance: float = 1e-4, max_passes: int = 2000,
+                 reference_residual: float = 0.0, impulses: bool = False) -> dict:
+        """The residual-driven mode on the uploaded world (nph_gpu_world_converge)."""
+        res = np.zeros(max_passes + 1, np.float32)
+        imp = np.zeros(12 * int(self._m), np.float32) if impulses else None
+        st = abi.ConvergeStats()
+        _check(self.L.nph_gpu_world_converge(self._h, ctypes.byref(params), dt, int(learned),
+                                             tolerance, max_passes, reference_residual,
+                                             res.ctypes.data,
+                                             None if imp is None else imp.ctypes.data,
+                                             ctypes.byref(st)), "nph_gpu_world_converge")
+        out = {k: getattr(st, k) for k, _ in abi.ConvergeStats._fields_}
+        out["residuals"] = res[: st.passes + 1].copy()
+        if imp is not None:
+            out["impulses"] = imp.reshape(-1, 4, 3)
+        return out
+
     def autotune(self, params: abi.WorldParams, dt: float, rounds: int = 1) -> list[int]:
         """Picks the fastest launch configuration per pass kind on the uploaded world."""
         chosen = (_u32 * 4)()
@@ -177,6 +229,69 @@ class Solver:
                                           len(a), body_slots, color.ctypes.data,
                                           slot.ctypes.data), "nph_gpu_graph_color")
         return color, slot
+
+
+class Mlp:
+    """The learned warm start's network (NphGpuMlp): BF16 weights on the tensor cores, FP32
+    master weights trained with Adam by the library's own kernels."""
+
+    def __init__(self, device: int = 0, seed: int = 0):
+        L = lib()
+        h = _vp()
+        _check(L.nph_gpu_mlp_create(device, seed, ctypes.byref(h)), "nph_gpu_mlp_create")
+        self._h = h
+        self.L = L
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.L.nph_gpu_mlp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def get_weights(self) -> np.ndarray:
+        w = np.zeros(abi.MLP_PARAMS, np.float32)
+        _check(self.L.nph_gpu_mlp_get_weights(self._h, w.ctypes.data), "nph_gpu_mlp_get_weights")
+        return w
+
+    def set_weights(self, w: np.ndarray) -> None:
+        w = np.ascontiguousarray(w, np.float32)
+        assert w.shape == (abi.MLP_PARAMS,)
+        _check(self.L.nph_gpu_mlp_set_weights(self._h, w.ctypes.data), "nph_gpu_mlp_set_weights")
+
+    def predict(self, x: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, abi.MLP_INPUTS)
+        y = np.zeros((len(x), abi.MLP_OUTPUTS), np.float32)
+        _check(self.L.nph_gpu_mlp_predict(self._h, x.ctypes.data, len(x), y.ctypes.data),
+               "nph_gpu_mlp_predict")
+        return y
+
+    def gradients(self, x: np.ndarray, t: np.ndarray) -> tuple[np.ndarray, float]:
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, abi.MLP_INPUTS)
+        t = np.ascontiguousarray(t, np.float32).reshape(-1, abi.MLP_OUTPUTS)
+        g = np.zeros(abi.MLP_PARAMS, np.float32)
+        loss = ctypes.c_float()
+        _check(self.L.nph_gpu_mlp_gradients(self._h, x.ctypes.data, t.ctypes.data, len(x),
+                                            g.ctypes.data, ctypes.byref(loss)),
+               "nph_gpu_mlp_gradients")
+        return g, float(loss.value)
+
+    def train(self, x: np.ndarray, t: np.ndarray, epochs: int, batch: int, lr: float,
+              seed: int = 0) -> float:
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, abi.MLP_INPUTS)
+        t = np.ascontiguousarray(t, np.float32).reshape(-1, abi.MLP_OUTPUTS)
+        loss = ctypes.c_float()
+        _check(self.L.nph_gpu_mlp_train(self._h, x.ctypes.data, t.ctypes.data, len(x), epochs,
+                                        batch, lr, seed, ctypes.byref(loss)), "nph_gpu_mlp_train")
+        return float(loss.value)
 
 
 class Batch:

@@ -119,6 +119,19 @@ PORT_API int nph_port32_solve(const NphGpuWorldParams *wp, float dt, NphGpuWorld
     return NPH_GPU_OK;
 }
 
+// The residual-driven mode (nph_gpu_world_converge) in FP32 with the correctly rounded
+// arctangent, the residual in double: residuals[0..passes], 1 + max_passes doubles.
+PORT_API int nph_port32_converge(const NphGpuWorldParams *wp, float dt, const NphGpuWorldView *v,
+                                 const float *init, double tol, unsigned max_passes, double ref,
+                                 double *residuals, unsigned *passes, unsigned *cold, float *impulses)
+{
+    const int bad = check_view(wp, v);
+    if (bad != NPH_GPU_OK) {
+        return bad;
+    }
+    return converge_f32cr(wp, dt, v, init, tol, max_passes, ref, residuals, passes, cold, impulses);
+}
+
 // The same with the correctly rounded arctangent in the joints' angle rows.
 PORT_API int nph_port32cr_solve(const NphGpuWorldParams *wp, float dt, NphGpuWorldView *v)
 {

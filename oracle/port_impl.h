@@ -1165,8 +1165,8 @@ typedef struct FN(Result) {
     unsigned n;
 } FN(Result);
 
-// The whole stage: returns the working state for the caller to read back (and free).
-static int FN(run)(const NphGpuWorldParams *wp, float dt, const NphGpuWorldView *v, FN(Result) *out)
+// The step's constants and the prepare stage (solver.c:985-1041): allocates the working state.
+static int FN(setup)(FN(Step) *sp, const NphGpuWorldParams *wp, float dt, const NphGpuWorldView *v)
 {
     const unsigned n = v->body_count;
     FN(Step) s;
@@ -1227,6 +1227,19 @@ static int FN(run)(const NphGpuWorldParams *wp, float dt, const NphGpuWorldView 
                                  v->fixed_bodies, &s.m[s.color_first[c] + i], group_points);
         }
     }
+    *sp = s;
+    return NPH_GPU_OK;
+}
+
+// The whole stage: returns the working state for the caller to read back (and free).
+static int FN(run)(const NphGpuWorldParams *wp, float dt, const NphGpuWorldView *v, FN(Result) *out)
+{
+    const unsigned n = v->body_count;
+    FN(Step) s;
+    const int rc = FN(setup)(&s, wp, dt, v);
+    if (rc != NPH_GPU_OK) {
+        return rc;
+    }
     for (unsigned sub = 0U; sub < wp->substeps; ++sub) {
         for (unsigned i = 0U; i < n; ++i) {
             FN(integrate_velocity)(&s, i);
@@ -1244,6 +1257,107 @@ static int FN(run)(const NphGpuWorldParams *wp, float dt, const NphGpuWorldView 
     out->m = s.m;
     out->j = s.j;
     out->n = n;
+    return NPH_GPU_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// The residual-driven mode that judges a warm start (no counterpart in the reference; the
+// device's nph_gpu_world_converge): prepare, the first substep's velocity integration and
+// warm start, then rigid passes (the relax pass) until the velocity-constraint residual
+// falls to `tol` x the reference residual.
+// ---------------------------------------------------------------------------------------
+
+// The residual, in double: over points, r_n = |vn + b| where the normal impulse is positive,
+// else max(-(vn + b), 0) (b = separation / h for a separated point), plus the slip |vt|
+// where the friction impulse is inside the cone (|tau| < 0.999 mu lambda).
+static double FN(residual)(const FN(Step) *s, unsigned count)
+{
+    double sum = 0.0;
+    for (unsigned g = 0U; g < count; ++g) {
+        const FN(Manifold) *m = &s->m[g];
+        const FN(Body) *a = &s->bodies[m->ia];
+        const FN(Body) *b = &s->bodies[m->ib];
+        for (unsigned k = 0U; k < m->point_count; ++k) {
+            const FN(Point) *p = &m->p[k];
+            const REAL sep = FN(separation)(a, b, p, m->n);
+            const V3 dv = FN(sub)(FN(add)(b->v, FN(cross)(b->w, p->rb)), FN(add)(a->v, FN(cross)(a->w, p->ra)));
+            const double vn = (double)FN(dot)(dv, m->n) + (sep > R(0) ? (double)sep * (double)s->inv_h : 0.0);
+            const double lambda = (double)p->normal_impulse;
+            const double rn = lambda > 0.0 ? fabs(vn) : (vn < 0.0 ? -vn : 0.0);
+            double rt = 0.0;
+            const double t1 = (double)p->tangent_impulse[0], t2 = (double)p->tangent_impulse[1];
+            if (sqrt(t1 * t1 + t2 * t2) < (double)m->friction * lambda * 0.999) {
+                const double v1 = (double)FN(dot)(dv, m->t1), v2 = (double)FN(dot)(dv, m->t2);
+                rt = v1 * v1 + v2 * v2;
+            }
+            sum += rn * rn + rt;
+        }
+    }
+    return sqrt(sum);
+}
+
+// `init` (12 floats per manifold, or NULL): the starting normal, t1 and t2 impulses of cold
+// points (those whose warm start is zero), per point slot 4 g + k. Writes the residual after
+// the warm start and after each pass to residuals[0..passes], the passes run, the cold points
+// and (when `impulses` is given) every slot's final impulses.
+static int FN(converge)(const NphGpuWorldParams *wp, float dt, const NphGpuWorldView *v, const float *init,
+                        double tol, unsigned max_passes, double ref, double *residuals, unsigned *passes_out,
+                        unsigned *cold_out, float *impulses)
+{
+    const unsigned n = v->body_count;
+    const unsigned count = v->contact_count;
+    FN(Step) s;
+    const int rc = FN(setup)(&s, wp, dt, v);
+    if (rc != NPH_GPU_OK) {
+        return rc;
+    }
+    unsigned cold = 0U;
+    for (unsigned g = 0U; g < count; ++g) {
+        FN(Manifold) *m = &s.m[g];
+        for (unsigned k = 0U; k < m->point_count; ++k) {
+            FN(Point) *p = &m->p[k];
+            if (p->normal_impulse == R(0) && p->tangent_impulse[0] == R(0) && p->tangent_impulse[1] == R(0)) {
+                ++cold;
+                if (init != NULL) {
+                    const float *q = &init[12U * g + 3U * k];
+                    p->normal_impulse = R(q[0]);
+                    p->tangent_impulse[0] = R(q[1]);
+                    p->tangent_impulse[1] = R(q[2]);
+                }
+            }
+        }
+    }
+    for (unsigned i = 0U; i < n; ++i) {
+        FN(integrate_velocity)(&s, i);
+    }
+    FN(contact_pass)(&s, v, FN(PASS_WARM));
+    double r = FN(residual)(&s, count);
+    residuals[0] = r;
+    const double reference = ref > 0.0 ? ref : r;
+    unsigned passes = 0U;
+    while (r > tol * reference && passes < max_passes) {
+        FN(contact_pass)(&s, v, FN(PASS_RELAX));
+        ++passes;
+        r = FN(residual)(&s, count);
+        residuals[passes] = r;
+    }
+    *passes_out = passes;
+    *cold_out = cold;
+    if (impulses != NULL) {
+        for (unsigned g = 0U; g < count; ++g) {
+            for (unsigned k = 0U; k < 4U; ++k) {
+                const FN(Point) *p = &s.m[g].p[k];
+                const int live = k < s.m[g].point_count;
+                impulses[12U * g + 3U * k] = live ? (float)p->normal_impulse : 0.0F;
+                impulses[12U * g + 3U * k + 1U] = live ? (float)p->tangent_impulse[0] : 0.0F;
+                impulses[12U * g + 3U * k + 2U] = live ? (float)p->tangent_impulse[1] : 0.0F;
+            }
+        }
+    }
+    free(s.params);
+    free(s.bodies);
+    free(s.m);
+    free(s.j);
     return NPH_GPU_OK;
 }
 

@@ -90,6 +90,10 @@ def _port_lib():
         lib.nph_port64_solve.restype = ctypes.c_int
         lib.nph_port64_solve.argtypes = [ctypes.POINTER(abi.WorldParams), _f32,
                                          ctypes.POINTER(abi.WorldView), _vp]
+        lib.nph_port32_converge.restype = ctypes.c_int
+        lib.nph_port32_converge.argtypes = [ctypes.POINTER(abi.WorldParams), _f32,
+                                            ctypes.POINTER(abi.WorldView), _vp, ctypes.c_double,
+                                            ctypes.c_uint, ctypes.c_double, _vp, _vp, _vp, _vp]
         lib.nph_port_graph_color.restype = ctypes.c_int
         lib.nph_port_graph_color.argtypes = [_vp, _vp, _vp, _u32, _u32, _vp, _vp]
         _port = lib
@@ -358,3 +362,25 @@ def lattice_world(dims, seed: int = 0, joint_fraction: float = 0.1, params=None,
     w.add_joints(sc.joints)
     w.inject_contacts(sc.contacts)
     return w, sc
+
+
+def port32_converge(view, params, dt: float, init=None, tol: float = 1e-4,
+                    max_passes: int = 2000, ref: float = 0.0) -> dict:
+    """The residual-driven mode restated on the CPU (FP32 solver, residual in double): the
+    checker of nph_gpu_world_converge. `init`: 12 floats per manifold, the starting impulses
+    of cold point slots."""
+    lib = _port_lib()
+    cv = view.c_view()
+    res = np.zeros(max_passes + 1, np.float64)
+    passes = ctypes.c_uint()
+    cold = ctypes.c_uint()
+    imp = np.zeros(12 * max(len(view.contacts), 1), np.float32)
+    ini = None if init is None else np.ascontiguousarray(init, np.float32).reshape(-1)
+    rc = lib.nph_port32_converge(ctypes.byref(params), dt, ctypes.byref(cv),
+                                 None if ini is None else _p(ini), tol, max_passes, ref,
+                                 _p(res), ctypes.byref(passes), ctypes.byref(cold), _p(imp))
+    if rc != abi.OK:
+        raise RuntimeError(f"port converge failed: {rc}")
+    return {"passes": passes.value, "cold_points": cold.value,
+            "residuals": res[: passes.value + 1].copy(),
+            "impulses": imp[: 12 * len(view.contacts)].reshape(-1, 4, 3)}
