@@ -487,3 +487,230 @@ def batched_worlds(count: int = 4096, seed: int = 0, min_bodies: int = 8,
     builds it)."""
     sizes = batched_sizes(count, seed, min_bodies, max_bodies)
     return [mixed_world(int(sizes[i]), seed * 1_000_003 + i) for i in range(shard, count, shards)]
+
+
+# ---- collapsing box piles (the learned warm start's workload) ---------------------------
+
+def _rect_corners(c: np.ndarray, half: np.ndarray, yaw: np.ndarray) -> np.ndarray:
+    """Corners (n, 4, 2) in the ground plane (x, z) of rectangles centred at c (n, 2) with
+    half extents (n, 2) turned by yaw about the vertical axis, counter-clockwise."""
+    s = np.array([[-1, -1], [1, -1], [1, 1], [-1, 1]], np.float64)
+    local = s[None, :, :] * half[:, None, :]
+    cy, sy = np.cos(yaw)[:, None], np.sin(yaw)[:, None]
+    # A turn by yaw about +y maps (x, z) to (x cos + z sin, -x sin + z cos).
+    x = local[:, :, 0] * cy + local[:, :, 1] * sy
+    z = -local[:, :, 0] * sy + local[:, :, 1] * cy
+    return np.stack([x, z], axis=2) + c[:, None, :]
+
+
+def _inside(p: np.ndarray, rect: np.ndarray) -> np.ndarray:
+    """Whether points p (n, k, 2) lie in the convex quads rect (n, 4, 2)."""
+    ok = np.ones(p.shape[:2], bool)
+    for e in range(4):
+        a = rect[:, e][:, None, :]
+        b = rect[:, (e + 1) % 4][:, None, :]
+        cr = (b[..., 0] - a[..., 0]) * (p[..., 1] - a[..., 1]) - (b[..., 1] - a[..., 1]) * (p[..., 0] - a[..., 0])
+        ok &= cr >= -1e-9
+    return ok
+
+
+def _overlap_points(ra: np.ndarray, rb: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """Up to four points spanning the overlap of quads ra and rb (n, 4, 2): the overlap's
+    vertices (corners of each inside the other, edge crossings), reduced as a manifold is: the
+    vertex furthest along a fixed direction, the one furthest from it, then the furthest on
+    each side of the line through both. Returns points (n, 4, 2) and their count (n,)."""
+    n = len(ra)
+    cand = [rb, ra]
+    ok = [_inside(rb, ra), _inside(ra, rb)]
+    for i in range(4):
+        p0, p1 = ra[:, i], ra[:, (i + 1) % 4]
+        for j in range(4):
+            q0, q1 = rb[:, j], rb[:, (j + 1) % 4]
+            d1, d2 = p1 - p0, q1 - q0
+            den = d1[:, 0] * d2[:, 1] - d1[:, 1] * d2[:, 0]
+            w = q0 - p0
+            safe = np.where(np.abs(den) > 1e-12, den, 1.0)
+            t = (w[:, 0] * d2[:, 1] - w[:, 1] * d2[:, 0]) / safe
+            u = (w[:, 0] * d1[:, 1] - w[:, 1] * d1[:, 0]) / safe
+            hit = (np.abs(den) > 1e-12) & (t >= 0) & (t <= 1) & (u >= 0) & (u <= 1)
+            cand.append((p0 + t[:, None] * d1)[:, None, :])
+            ok.append(hit[:, None])
+    pts = np.concatenate(cand, axis=1)
+    valid = np.concatenate(ok, axis=1)
+    big = 1e30
+    rows = np.arange(n)
+    # 1: furthest along a fixed direction; 2: furthest from it.
+    d = np.array([0.8, 0.6])
+    i0 = np.argmax(np.where(valid, pts @ d, -big), axis=1)
+    p0 = pts[rows, i0]
+    dist = np.where(valid, np.sum((pts - p0[:, None, :]) ** 2, axis=2), -big)
+    i1 = np.argmax(dist, axis=1)
+    p1 = pts[rows, i1]
+    e = p1 - p0
+    area = e[:, None, 0] * (pts[..., 1] - p0[:, None, 1]) - e[:, None, 1] * (pts[..., 0] - p0[:, None, 0])
+    i2 = np.argmax(np.where(valid, area, -big), axis=1)
+    i3 = np.argmin(np.where(valid, area, big), axis=1)
+    a2 = area[rows, i2]
+    a3 = area[rows, i3]
+    out = np.stack([p0, p1, pts[rows, i2], pts[rows, i3]], axis=1)
+    tol = 1e-6
+    has1 = dist[rows, i1] > tol
+    has2 = a2 > tol
+    has3 = a3 < -tol
+    count = 1 + has1.astype(int) + (has1 & has2).astype(int) + (has1 & has3).astype(int)
+    # Pack the points present to the front.
+    order = np.stack([np.zeros(n, bool) | True, has1, has1 & has2, has1 & has3], axis=1)
+    packed = np.zeros_like(out)
+    for r in range(n):
+        packed[r, : count[r]] = out[r][order[r]]
+    return packed, count
+
+
+def box_pile_world(boxes: int, seed: int, dt: float = 1.0 / 60.0, substeps: int = 4,
+                   gravity: float = 9.81, max_height: int = 8,
+                   new_share: float | None = None) -> SolverScene:
+    """A collapsing box pile: `boxes` boxes (half extents uniform in 0.2-1.0 m, density
+    1000 kg/m^3, friction 0.6, each turned by a seeded angle about the vertical) stacked in
+    columns of 1-8 on a fixed ground, every box resting on the one below through the
+    overlap of their faces (up to 4 points, penetration uniform in 0-1 cm). The pile is
+    collapsing: every box moves a little, the columns' top boxes have just been dropped onto
+    them (approach speed uniform in 0.5-3 m/s), and a seeded share of the other contacts has
+    just formed. Contacts that persisted carry the impulses of the column's resting load
+    (the weight above times g h, shared by the points); the new ones start at zero.
+    `max_height` caps the columns (1: every box on the ground); `new_share` fixes the share of
+    new contacts (default: seeded, uniform in 0.1-0.5, plus every dropped box's)."""
+    rng = np.random.default_rng(seed)
+    h = dt / substeps
+    heights = []
+    left = boxes
+    while left > 0:
+        k = int(min(left, rng.integers(1, max_height + 1)))
+        heights.append(k)
+        left -= k
+    cols = len(heights)
+    side = int(np.ceil(np.sqrt(cols)))
+    half = rng.uniform(0.2, 1.0, (boxes, 3))
+    yaw = rng.uniform(0.0, 2.0 * np.pi, boxes)
+    pen = rng.uniform(0.0, 0.01, boxes)
+    share = rng.uniform(0.1, 0.5) if new_share is None else new_share
+    center = np.zeros((boxes, 3))
+    below = np.full(boxes, -1, np.int64)  # the box each rests on (-1: the ground)
+    top = np.zeros(boxes, bool)
+    level = np.zeros(boxes, np.int64)
+    i = 0
+    for c, k in enumerate(heights):
+        base = np.array([(c % side) * 3.4, (c // side) * 3.4])
+        y = 0.0
+        for lev in range(k):
+            if lev == 0:
+                xz = base
+                y_bottom = 0.0 - pen[i]
+            else:
+                j = i - 1
+                reach = 0.5 * min(half[j, 0], half[j, 2], half[i, 0], half[i, 2])
+                xz = center[j, [0, 2]] + rng.uniform(-reach, reach, 2)
+                y_bottom = y - pen[i]
+                below[i] = j
+            center[i] = (xz[0], y_bottom + half[i, 1], xz[1])
+            y = center[i, 1] + half[i, 1]
+            level[i] = lev
+            i += 1
+        top[i - 1] = k > 1
+    mass = (_DENSITY * 8.0 * half[:, 0] * half[:, 1] * half[:, 2]).astype(F32)
+    inertia = np.zeros((boxes, 9), F32)
+    inertia[:, 0] = mass / 3.0 * (half[:, 1] ** 2 + half[:, 2] ** 2)
+    inertia[:, 4] = mass / 3.0 * (half[:, 0] ** 2 + half[:, 2] ** 2)
+    inertia[:, 8] = mass / 3.0 * (half[:, 0] ** 2 + half[:, 1] ** 2)
+    bodies = body_records(boxes)
+    set_mass(bodies, mass, inertia)
+    bodies["center"] = center
+    bodies["origin"] = center
+    bodies["rotation"][:, 1] = np.sin(0.5 * yaw)
+    bodies["rotation"][:, 3] = np.cos(0.5 * yaw)
+    bodies["max_extent"] = np.linalg.norm(half, axis=1)
+    v = rng.normal(0.0, 0.05, (boxes, 3))
+    w = rng.normal(0.0, 0.1, (boxes, 3))
+    v[top, 1] = -rng.uniform(0.5, 3.0, int(top.sum()))
+    v[top, 0] += rng.normal(0.0, 0.3, int(top.sum()))
+    v[top, 2] += rng.normal(0.0, 0.3, int(top.sum()))
+    w[top] += rng.normal(0.0, 0.5, (int(top.sum()), 3))
+    bodies["linear_velocity"] = v.astype(F32)
+    bodies["angular_velocity"] = w.astype(F32)
+    # Contacts: one per box with what is below it (A below, B the box), normal +y.
+    fixed = _ground()
+    ground = boxes  # the fixed body's index
+    on_box = below >= 0
+    lower = np.where(on_box, below, 0)
+    rect_b = _rect_corners(center[:, [0, 2]], half[:, [0, 2]], yaw)
+    rect_a = np.where(on_box[:, None, None],
+                      _rect_corners(center[lower][:, [0, 2]], half[lower][:, [0, 2]], yaw[lower]),
+                      _rect_corners(center[:, [0, 2]], half[:, [0, 2]] * 3.0, yaw))
+    pts, count = _overlap_points(rect_a, rect_b)
+    contacts = np.zeros(boxes, abi.CONTACT_DTYPE)
+    contacts["body_a"] = np.where(on_box, below, ground)
+    contacts["body_b"] = np.arange(boxes)
+    contacts["point_count"] = count
+    contacts["friction"] = 0.6
+    contacts["normal"] = (0.0, 1.0, 0.0)
+    a_center = np.where(on_box[:, None], center[lower], np.array([0.0, -1.0, 0.0]))
+    y_plane = center[:, 1] - half[:, 1] + pen  # the top face of what is below
+    # The load each contact carries at rest: the box and every box above it in its column.
+    load = mass.astype(np.float64).copy()
+    for b in range(boxes - 1, -1, -1):
+        if below[b] >= 0:
+            load[below[b]] += load[b]
+    new = (top & (new_share is None)) | (rng.random(boxes) < share)
+    for k in range(4):
+        live = k < count
+        p = np.stack([pts[:, k, 0], y_plane, pts[:, k, 1]], axis=1)
+        cp = contacts["points"][:, k]
+        cp["anchor_a"] = np.where(live[:, None], p - a_center, 0.0).astype(F32)
+        cp["anchor_b"] = np.where(live[:, None], p - center, 0.0).astype(F32)
+        cp["separation"] = np.where(live, -pen, 0.0).astype(F32)
+        cp["id"] = k
+        rest = load * gravity * h / np.maximum(count, 1)
+        cp["normal_impulse"] = np.where(live & ~new, rest, 0.0).astype(F32)
+    return SolverScene(bodies=bodies, mass=mass, joints=np.zeros(0, abi.JOINT_DTYPE),
+                       contacts=contacts, fixed=fixed)
+
+
+def merge_scenes(scs: list) -> SolverScene:
+    """Disjoint worlds as one: bodies and contacts concatenated in order, each world's fixed
+    bodies after all bodies (a body index below the total body count is an awake body, the
+    fixed body k of world w is index total + w's first fixed + k)."""
+    nb = [len(s.bodies) for s in scs]
+    nf = [0 if s.fixed is None else len(s.fixed) for s in scs]
+    total = int(sum(nb))
+    boff = np.concatenate([[0], np.cumsum(nb)[:-1]]).astype(np.int64)
+    foff = np.concatenate([[0], np.cumsum(nf)[:-1]]).astype(np.int64)
+
+    def remap(idx, w):
+        idx = idx.astype(np.int64)
+        own = idx < nb[w]
+        return np.where(own, idx + boff[w], idx - nb[w] + total + foff[w]).astype(np.uint32)
+
+    cs, js = [], []
+    for w, s in enumerate(scs):
+        c = s.contacts.copy()
+        c["body_a"] = remap(c["body_a"], w)
+        c["body_b"] = remap(c["body_b"], w)
+        cs.append(c)
+        j = s.joints.copy()
+        if len(j):
+            j["body_a"] = remap(j["body_a"], w)
+            j["body_b"] = remap(j["body_b"], w)
+        js.append(j)
+    fixed = [s.fixed for s in scs if s.fixed is not None and len(s.fixed)]
+    return SolverScene(bodies=np.concatenate([s.bodies for s in scs]),
+                       mass=np.concatenate([s.mass for s in scs]),
+                       joints=np.concatenate(js) if js else np.zeros(0, abi.JOINT_DTYPE),
+                       contacts=np.concatenate(cs),
+                       fixed=np.concatenate(fixed) if fixed else None)
+
+
+def box_pile_batch(worlds: int = 256, seed: int = 0, min_boxes: int = 500,
+                   max_boxes: int = 5000) -> list:
+    """`worlds` collapsing box piles with box counts uniform in [min_boxes, max_boxes]."""
+    rng = np.random.default_rng(seed)
+    sizes = rng.integers(min_boxes, max_boxes + 1, worlds)
+    return [box_pile_world(int(n), seed * 1_000_003 + i) for i, n in enumerate(sizes)]
