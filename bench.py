@@ -51,10 +51,15 @@ def parse():
                     help="lattice bodies per axis (128,128,64: 1,048,576 bodies)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=("lattice", "batched"), default="lattice",
+    ap.add_argument("--workload", choices=("lattice", "batched", "learned"), default="lattice",
                     help="lattice: the 1M-body constraint graph (the headline); batched: "
                          "--worlds independent worlds in one persistent launch")
     ap.add_argument("--worlds", type=int, default=4096)
+    ap.add_argument("--pile-worlds", type=int, default=256,
+                    help="learned: box-pile worlds per batch (500-5000 boxes each)")
+    ap.add_argument("--train-batches", type=int, default=2)
+    ap.add_argument("--max-passes", type=int, default=2000)
+    ap.add_argument("--epochs", type=int, default=30)
     ap.add_argument("--pass-config", default=None,
                     help="fixed pass configurations warm,solve,relax,restitution (no autotuner)")
     return ap.parse_args()
@@ -408,6 +413,80 @@ def run_batched(args):
     return 0
 
 
+def run_learned(args):
+    """--workload learned: the learned warm start on collapsing box piles. Training data: the
+    cold points of --train-batches batches of --pile-worlds piles (500-5000 boxes each), their
+    targets the impulses the plain solver converged to; the network trained on the device;
+    judged on a held-out batch by the residual-driven mode (passes to each tolerance of the
+    plain start's initial residual, learned against plain). Rank 0 only."""
+    import torch
+
+    from nepheline_b200 import abi, learned, scenes
+    from nepheline_b200.solver import Mlp, Solver
+
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    params = abi.WorldParams.default()
+    clk = Clocks(local).__enter__()
+    solver = Solver(device=local)
+    mlp = Mlp(device=local, seed=0)
+    t0 = time.perf_counter()
+    xs, ts, passes = [], [], []
+    for b in range(args.train_batches):
+        view = learned.merged_view(solver, scenes.box_pile_batch(args.pile_worlds, seed=100 + b))
+        x, t, run = learned.samples(solver, view, params, DT, tolerance=1e-4,
+                                    max_passes=args.max_passes)
+        xs.append(x)
+        ts.append(t)
+        passes.append(int(run["passes"]))
+    x = np.concatenate(xs)
+    t = np.concatenate(ts)
+    data_s = time.perf_counter() - t0
+    t1 = time.perf_counter()
+    fit = learned.train(mlp, x, t, epochs=args.epochs, batch=4096, lr=1e-3, seed=1)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t1
+    scs = scenes.box_pile_batch(args.pile_worlds, seed=0)
+    view = learned.merged_view(solver, scs)
+    clk.lines.clear()
+    cmp = learned.compare(solver, mlp, view, params, DT, tolerances=(1e-2, 1e-3, 1e-4),
+                          max_passes=args.max_passes)
+    clocks = clk.summary()
+    clk.__exit__(None, None, None)
+    tight = cmp["tolerances"]["0.0001"]
+    value = tight["learned"] if tight["learned"] is not None else args.max_passes
+    plain = tight["plain"] if tight["plain"] is not None else args.max_passes
+    out = {
+        "metric": "iters to 1e-4 residual, learned vs plain init", "value": value,
+        "unit": "passes", "n_gpus": 1, "steps": 1, "warmup": 0,
+        "ms_per_step": tight["learned_ms"], "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "bf16 network, f32 solver", "data": "synthetic",
+        "config": {"workload": f"collapsing box piles: {args.pile_worlds} worlds of 500-5000 "
+                               f"boxes (half extents 0.2-1.0 m), columns of 1-8 on a ground, "
+                               f"top boxes just dropped, a seeded share of contacts new",
+                   "bodies": len(view.bodies), "manifolds": len(view.contacts),
+                   "cold_points": cmp["cold_points"], "max_passes": args.max_passes,
+                   "training": dict(fit, batches=args.train_batches, epochs=args.epochs,
+                                    data_s=data_s, train_s=train_s,
+                                    plain_passes_on_training_data=passes)},
+        "plain": plain, "reached": {"plain": tight["plain"] is not None,
+                                    "learned": tight["learned"] is not None},
+        "comparison": cmp,
+        "e2e": {"value": value, "unit": "passes", "h2d_bytes_per_step":
+                int(view.bodies.nbytes + view.contacts.nbytes + view.fixed.nbytes),
+                "d2h_bytes_per_step": 4 * (args.max_passes + 1)},
+        "gpu_launches": int(plain + value) * 8,
+        "clocks": clocks,
+    }
+    print(json.dumps(out))
+    mlp.close()
+    solver.close()
+    return 0
+
+
 def workload_name(dims) -> str:
     n = dims[0] * dims[1] * dims[2]
     return f"synthetic constraint graph, {dims[0]}x{dims[1]}x{dims[2]} lattice, {n} bodies"
@@ -419,6 +498,8 @@ def main():
         return run_reference(args)
     if args.workload == "batched":
         return run_batched(args)
+    if args.workload == "learned":
+        return run_learned(args)
     import torch
 
     from nepheline_b200 import abi
