@@ -55,6 +55,8 @@ def parse():
                     help="lattice: the 1M-body constraint graph (the headline); batched: "
                          "--worlds independent worlds in one persistent launch")
     ap.add_argument("--worlds", type=int, default=4096)
+    ap.add_argument("--batch-config", default=None,
+                    help="batched: fixed launch shape,shared mode,warp split (no autotuner)")
     ap.add_argument("--pile-worlds", type=int, default=256,
                     help="learned: box-pile worlds per batch (500-5000 boxes each)")
     ap.add_argument("--train-batches", type=int, default=2)
@@ -318,7 +320,12 @@ def run_batched(args):
     batch = Batch(device=local)
     stream = torch.cuda.ExternalStream(batch.stream, device=local)
     batch.upload(views)
-    tuned = batch.autotune(params, DT, rounds=1)
+    if args.batch_config:
+        c, sh, split = (int(x) for x in args.batch_config.split(","))
+        batch.set_config(c, sh, split)
+        tuned = {"config": c, "shared_velocities": sh, "warp_color_max": split}
+    else:
+        tuned = batch.autotune(params, DT, rounds=1)
     batch.upload(views)
     batch.step_async(params, DT, args.warmup)
     torch.cuda.synchronize()
