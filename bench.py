@@ -56,7 +56,7 @@ def parse():
                          "--worlds independent worlds in one persistent launch")
     ap.add_argument("--worlds", type=int, default=4096)
     ap.add_argument("--batch-config", default=None,
-                    help="batched: fixed launch shape,shared mode,warp split (no autotuner)")
+                    help="batched: fixed launch shape,shared mode,items per thread (no autotuner)")
     ap.add_argument("--pile-worlds", type=int, default=256,
                     help="learned: box-pile worlds per batch (500-5000 boxes each)")
     ap.add_argument("--train-batches", type=int, default=2)
@@ -323,7 +323,7 @@ def run_batched(args):
     if args.batch_config:
         c, sh, split = (int(x) for x in args.batch_config.split(","))
         batch.set_config(c, sh, split)
-        tuned = {"config": c, "shared_velocities": sh, "warp_color_max": split}
+        tuned = {"config": c, "shared_velocities": sh, "items_per_thread": split}
     else:
         tuned = batch.autotune(params, DT, rounds=1)
     batch.upload(views)

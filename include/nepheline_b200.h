@@ -345,10 +345,10 @@ NPH_GPU_API NphGpuResult nph_gpu_solver_autotune(NphGpuSolver *solver,
  * ---------------------------------------------------------------------------------------
  * The reference steps one world per nph_physics_world_step; this steps a batch of worlds
  * with the same settings, each as phys_solve would, in one kernel launch per step. Worlds are
- * taken from queues sorted by size: a large world by a whole block (block barriers between
- * stages and colours), a small one by a single warp (warp barriers), so one SM works on many
- * small worlds at once. A world solved in a batch gives the same bits as the world solved
- * alone by nph_gpu_phys_solve. */
+ * taken whole from queues sorted by size, one queue per team size: a team of a whole block,
+ * half a block, ... down to one warp runs a world, with barriers of its own between stages
+ * and colours, so one SM works on several worlds at once. A world solved in a batch gives the
+ * same bits as the world solved alone by nph_gpu_phys_solve. */
 
 typedef struct NphGpuBatch NphGpuBatch;
 
@@ -362,8 +362,9 @@ typedef struct NphGpuBatchTuning {
     uint32_t config;            /* launch shape, below nph_gpu_batch_config_count() */
     uint32_t threads;           /* threads per block of that shape (filled in) */
     uint32_t shared_velocities; /* NPH_GPU_BATCH_SHARED_* */
-    uint32_t warp_color_max;    /* worlds whose largest colour holds at most this many
-                                   constraints run on one warp; 0: every world on a block */
+    uint32_t items_per_thread;  /* a world runs on the smallest team (1, 2, 4, ... warps, up
+                                   to the block) whose threads cover its largest colour at
+                                   this many constraints a thread; 0: every world on a block */
     float ms_per_step;          /* the autotuner's time for it (filled in) */
 } NphGpuBatchTuning;
 
@@ -376,9 +377,9 @@ typedef struct NphGpuBatchInfo {
     uint32_t threads;
     uint32_t shared_velocities;
     uint32_t blocks_per_sm;
-    uint32_t warp_color_max;
-    uint32_t warp_worlds; /* worlds the current configuration runs on a warp */
-    uint32_t pad;
+    uint32_t items_per_thread;
+    uint32_t warp_worlds;  /* worlds the current configuration runs on one warp */
+    uint32_t block_worlds; /* worlds it runs on a whole block */
 } NphGpuBatchInfo;
 
 NPH_GPU_API NphGpuResult nph_gpu_batch_create(const NphGpuSolverDesc *desc, NphGpuBatch **out);

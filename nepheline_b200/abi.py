@@ -197,7 +197,7 @@ class ConvergeStats(ctypes.Structure):
 
 class BatchTuning(ctypes.Structure):
     _fields_ = [("config", ctypes.c_uint32), ("threads", ctypes.c_uint32),
-                ("shared_velocities", ctypes.c_uint32), ("warp_color_max", ctypes.c_uint32),
+                ("shared_velocities", ctypes.c_uint32), ("items_per_thread", ctypes.c_uint32),
                 ("ms_per_step", ctypes.c_float)]
 
 
@@ -206,8 +206,8 @@ class BatchInfo(ctypes.Structure):
                 ("bodies", ctypes.c_uint64), ("manifolds", ctypes.c_uint64),
                 ("joints", ctypes.c_uint64), ("threads", ctypes.c_uint32),
                 ("shared_velocities", ctypes.c_uint32), ("blocks_per_sm", ctypes.c_uint32),
-                ("warp_color_max", ctypes.c_uint32), ("warp_worlds", ctypes.c_uint32),
-                ("pad", ctypes.c_uint32)]
+                ("items_per_thread", ctypes.c_uint32), ("warp_worlds", ctypes.c_uint32),
+                ("block_worlds", ctypes.c_uint32)]
 
 
 class SolverDesc(ctypes.Structure):

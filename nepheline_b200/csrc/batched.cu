@@ -52,12 +52,18 @@ struct WorldSlice {
     uint32_t jcount[NPH_GPU_COLOR_SLOTS];
 };
 
+// Team sizes: a block of B warps runs its worlds in teams of B, B/2, ..., 1 warps (size
+// class c: B >> c warps), each team on its own named barrier.
+constexpr uint32_t kMaxClasses = 5; // 16, 8, 4, 2, 1 warps
+
 struct BatchArgs {
     const WorldSlice *worlds;
-    const uint32_t *order; // world indices: the block worlds, then the warp worlds
+    const uint32_t *order; // world indices: the worlds of size class 0, then class 1, ...
     uint32_t count;
-    uint32_t block_worlds; // the first block_worlds of `order` run on a block
-    uint32_t *heads;       // [0] the block queue's head, [1] the warp queue's
+    uint32_t class_first[kMaxClasses]; // where each class's worlds start in `order`
+    uint32_t class_count[kMaxClasses];
+    uint32_t classes;
+    uint32_t *heads;       // one queue head per class
     uint32_t *err;
     NphGpuBody *bodies;
     const NphGpuBody *fixed;
@@ -72,21 +78,25 @@ struct BatchArgs {
     float4 *jw;
     uint32_t jcap;
     uint32_t block_slots; // velocity slots (two rows each) in a block's shared memory
-    uint32_t warp_slots;  // in a warp's share of it
 };
 
 enum Pass : int { kWarm = 0, kSolve = 1, kRelax = 2, kRestitution = 3 };
 
-struct BlockTeam {
-    __device__ static uint32_t rank() { return threadIdx.x; }
-    __device__ static uint32_t size() { return blockDim.x; }
-    __device__ static void sync() { __syncthreads(); }
-};
+// A team of threads that runs one world: a warp (synchronised by __syncwarp) or several
+// warps on a named barrier of their own (barrier.sync id, threads), so teams of one block work
+// on different worlds without waiting for each other.
+struct Team {
+    uint32_t rank, size, barrier; // barrier 0: the team is one warp
 
-struct WarpTeam {
-    __device__ static uint32_t rank() { return threadIdx.x & 31u; }
-    __device__ static uint32_t size() { return 32u; }
-    __device__ static void sync() { __syncwarp(); }
+    __device__ void sync() const
+    {
+        if (barrier == 0u) {
+            __syncwarp();
+        } else {
+            // The non-aligned form: a warp's threads may arrive after divergent item loops.
+            asm volatile("barrier.sync %0, %1;" ::"r"(barrier), "r"(size) : "memory");
+        }
+    }
 };
 
 // The world's slice of the arrays: body indices in its rows are world-relative.
@@ -226,13 +236,13 @@ __device__ __noinline__ void store_joint_item(const DevSolver &S, uint32_t j, Np
     store_joint(S, j, joints[j]);
 }
 
-template <int P, class Team> __device__ void world_pass(const DevSolver &S, const WorldSlice &W, const StepConsts &K)
+template <int P> __device__ void world_pass(const Team &T, const DevSolver &S, const WorldSlice &W, const StepConsts &K)
 {
     const uint32_t o = NPH_GPU_OVERFLOW;
     // The overflow: one thread, its joints then its contacts in list order.
     const uint32_t oj = P == kRestitution ? 0u : W.jcount[o];
     if (W.ccount[o] > 0u || oj > 0u) {
-        if (Team::rank() == 0u) {
+        if (T.rank == 0u) {
             for (uint32_t j = 0; j < oj; ++j) {
                 joint_item<P>(S, W.jfirst[o] + j, K);
             }
@@ -240,7 +250,7 @@ template <int P, class Team> __device__ void world_pass(const DevSolver &S, cons
                 manifold_item<P>(S, W.cfirst[o] + g, K);
             }
         }
-        Team::sync();
+        T.sync();
     }
     for (uint32_t c = 0; c < NPH_GPU_COLORS; ++c) {
         const uint32_t jc = P == kRestitution ? 0u : W.jcount[c];
@@ -248,20 +258,19 @@ template <int P, class Team> __device__ void world_pass(const DevSolver &S, cons
         if (jc + cc == 0u) {
             continue;
         }
-        for (uint32_t i = Team::rank(); i < jc + cc; i += Team::size()) {
+        for (uint32_t i = T.rank; i < jc + cc; i += T.size) {
             if (i < jc) {
                 joint_item<P>(S, W.jfirst[c] + i, K);
             } else {
                 manifold_item<P>(S, W.cfirst[c] + (i - jc), K);
             }
         }
-        Team::sync();
+        T.sync();
     }
 }
 
-template <class Team>
-__device__ void world_step(const BatchArgs &A, const WorldSlice &W, const StepConsts &K, uint32_t substeps,
-                           float4 *shared_vel, uint32_t shared_slots)
+__device__ void world_step(const Team &T, const BatchArgs &A, const WorldSlice &W, const StepConsts &K,
+                           uint32_t substeps, float4 *shared_vel, uint32_t shared_slots)
 {
     const bool in_shared = W.n + 1u <= shared_slots;
     float4 *vel = in_shared ? shared_vel : A.vel + 2u * W.slot_first;
@@ -273,47 +282,47 @@ __device__ void world_step(const BatchArgs &A, const WorldSlice &W, const StepCo
     NphGpuJoint *joints = A.joints + W.joint_first;
     const uint32_t n = W.n;
     // prepare_body (solver.c:131-168), the dummy last.
-    for (uint32_t i = Team::rank(); i <= n; i += Team::size()) {
+    for (uint32_t i = T.rank; i <= n; i += T.size) {
         body_prepare_item(B, i, n, bodies, K);
     }
-    Team::sync();
+    T.sync();
     // The joints and the manifolds (phys_joint_prepare, prepare_group).
-    for (uint32_t i = Team::rank(); i < W.nj + W.m; i += Team::size()) {
+    for (uint32_t i = T.rank; i < W.nj + W.m; i += T.size) {
         if (i < W.nj) {
             joint_prepare_item(S, W, i, joints, bodies, fixed, K.h, A.err);
         } else {
             manifold_prepare_item(S, W, i - W.nj, contacts, bodies, fixed, A.err);
         }
     }
-    Team::sync();
+    T.sync();
     for (uint32_t sub = 0; sub < substeps; ++sub) {
-        for (uint32_t i = Team::rank(); i < n; i += Team::size()) {
+        for (uint32_t i = T.rank; i < n; i += T.size) {
             integrate_velocity(B, i, K.h);
         }
-        Team::sync();
-        world_pass<kWarm, Team>(S, W, K);
-        world_pass<kSolve, Team>(S, W, K);
-        for (uint32_t i = Team::rank(); i < n; i += Team::size()) {
+        T.sync();
+        world_pass<kWarm>(T, S, W, K);
+        world_pass<kSolve>(T, S, W, K);
+        for (uint32_t i = T.rank; i < n; i += T.size) {
             integrate_position(B, i, K.h);
         }
-        Team::sync();
-        world_pass<kRelax, Team>(S, W, K);
+        T.sync();
+        world_pass<kRelax>(T, S, W, K);
     }
-    world_pass<kRestitution, Team>(S, W, K);
+    world_pass<kRestitution>(T, S, W, K);
     // store_group, the joints' impulses, finalize_body.
-    for (uint32_t g = Team::rank(); g < W.m; g += Team::size()) {
+    for (uint32_t g = T.rank; g < W.m; g += T.size) {
         store_manifold_item(S, g, contacts);
     }
-    for (uint32_t j = Team::rank(); j < W.nj; j += Team::size()) {
+    for (uint32_t j = T.rank; j < W.nj; j += T.size) {
         store_joint_item(S, j, joints);
     }
-    for (uint32_t i = Team::rank(); i < n; i += Team::size()) {
+    for (uint32_t i = T.rank; i < n; i += T.size) {
         finalize_item(B, i, bodies, K.dt);
     }
-    Team::sync();
+    T.sync();
     // post_finalize's driven joints (solver.c:851-857).
     if (W.driven > 0u) {
-        for (uint32_t j = Team::rank(); j < W.nj; j += Team::size()) {
+        for (uint32_t j = T.rank; j < W.nj; j += T.size) {
             uint32_t sa, sb, flags;
             joint_head(S, j, sa, sb, flags);
             if ((flags & kJDriven) != 0u) {
@@ -326,49 +335,54 @@ __device__ void world_step(const BatchArgs &A, const WorldSlice &W, const StepCo
             }
         }
     }
-    Team::sync();
+    T.sync();
 }
 
 template <int kThreads, int kMinBlocks>
 __global__ void __launch_bounds__(kThreads, kMinBlocks) k_worlds(BatchArgs A, StepConsts K, uint32_t substeps)
 {
     extern __shared__ float4 shared_vel[];
-    __shared__ uint32_t taken;
-    // The large worlds, a block each.
-    if (A.block_worlds > 0u) {
+    __shared__ uint32_t taken[16];
+    const uint32_t warps = kThreads / 32u;
+    const uint32_t warp = threadIdx.x >> 5;
+    // Size class by size class, largest teams first: a team takes worlds from its class's queue
+    // until it is empty, then splits into the next class's teams. Barrier ids are unique over
+    // every (class, team): class c's teams use ids warps / tw .. 2 warps / tw - 1.
+    for (uint32_t c = 0; c < A.classes; ++c) {
+        const uint32_t tw = warps >> c; // warps per team
+        const uint32_t team = warp / tw;
+        const Team T{threadIdx.x - team * tw * 32u, tw * 32u, tw == 1u ? 0u : warps / tw + team};
+        const uint32_t slots = A.block_slots / (warps / tw);
+        float4 *mine = shared_vel + (size_t)team * 2u * slots;
         for (;;) {
-            if (threadIdx.x == 0) {
-                taken = atomicAdd(&A.heads[0], 1u);
+            uint32_t q = 0;
+            if (T.rank == 0u) {
+                q = atomicAdd(&A.heads[c], 1u);
             }
-            __syncthreads();
-            const uint32_t q = taken;
-            __syncthreads();
-            if (q >= A.block_worlds) {
+            if (tw == 1u) {
+                q = __shfl_sync(0xFFFFFFFFu, q, 0);
+            } else {
+                if (T.rank == 0u) {
+                    taken[T.barrier] = q;
+                }
+                T.sync();
+                q = taken[T.barrier];
+                T.sync();
+            }
+            if (q >= A.class_count[c]) {
                 break;
             }
-            world_step<BlockTeam>(A, A.worlds[A.order[q]], K, substeps, shared_vel, A.block_slots);
+            world_step(T, A, A.worlds[A.order[A.class_first[c] + q]], K, substeps, mine, slots);
         }
-    }
-    // The small worlds, a warp each, in the warp's share of the shared memory.
-    const uint32_t warp = threadIdx.x >> 5;
-    float4 *mine = shared_vel + (size_t)warp * 2u * A.warp_slots;
-    for (;;) {
-        uint32_t q = 0;
-        if ((threadIdx.x & 31u) == 0u) {
-            q = atomicAdd(&A.heads[1], 1u);
-        }
-        q = __shfl_sync(0xFFFFFFFFu, q, 0);
-        if (q >= A.count - A.block_worlds) {
-            return;
-        }
-        world_step<WarpTeam>(A, A.worlds[A.order[A.block_worlds + q]], K, substeps, mine, A.warp_slots);
     }
 }
 
 struct BatchConfig {
     uint32_t threads, min_blocks;
 };
-constexpr BatchConfig kBatchConfigs[] = {{128, 4}, {256, 2}, {256, 1}, {512, 1}, {1024, 1}, {256, 4}, {512, 2}};
+// Up to 16 warps a block: a block's named barriers (ids 1-15) cover every team of every
+// size class.
+constexpr BatchConfig kBatchConfigs[] = {{128, 4}, {256, 2}, {256, 1}, {512, 1}, {256, 4}, {512, 2}};
 constexpr uint32_t kBatchConfigCount = sizeof(kBatchConfigs) / sizeof(kBatchConfigs[0]);
 
 } // namespace
@@ -386,9 +400,11 @@ struct NphGpuBatch {
     bool use_graph = true;
     uint32_t config = 1;
     uint32_t shared_mode = NPH_GPU_BATCH_SHARED_SMALL;
-    uint32_t warp_color_max = 32;
+    uint32_t items_per_thread = 2; // a world's team: the smallest whose threads cover its
+                                   // largest colour at this many items a thread (0: a block)
     uint32_t blocks_per_sm = 0; // resident blocks of the chosen kernel (0: not yet known)
-    uint32_t block_worlds = 0;  // worlds of the current order that run on a block
+    uint32_t class_first[kMaxClasses] = {}, class_count[kMaxClasses] = {};
+    uint32_t classes = 1;
     int sms = 148;
     // Device arrays and their capacities (grown, never shrunk, by uploads).
     NphGpuBody *d_bodies = nullptr;
@@ -403,7 +419,7 @@ struct NphGpuBatch {
     float4 *jw = nullptr;
     WorldSlice *d_worlds = nullptr;
     uint32_t *d_order = nullptr;
-    uint32_t *d_counters = nullptr; // [0] block queue head, [1] warp queue head, [2] error bits
+    uint32_t *d_counters = nullptr; // [0..4] the size classes' queue heads, [6] error bits
     uint32_t *h_counters = nullptr;
     uint64_t cap_bodies = 0, cap_slots = 0, cap_fixed = 0, cap_contacts = 0, cap_joints = 0, cap_worlds = 0;
     // Sizes of the uploaded batch.
@@ -499,28 +515,62 @@ uint32_t largest_color(const WorldSlice &s)
     return m;
 }
 
-// The queue order for the configuration: the block worlds, then the warp worlds, each largest
-// first (a world's work grows with its manifolds, joints and bodies).
+// The size classes of the configuration's block: teams of B, B/2, ..., 1 warps.
+uint32_t class_count_of(uint32_t threads)
+{
+    uint32_t warps = threads / 32u, classes = 1;
+    while (warps > 1u) {
+        warps >>= 1;
+        ++classes;
+    }
+    return classes;
+}
+
+// The queue order for the configuration: each world's size class (the smallest team whose
+// threads cover its largest colour at items_per_thread items a thread; a whole block when
+// items_per_thread is 0), the classes in order, each largest first (a world's work grows with
+// its manifolds, joints and bodies).
 void build_order(NphGpuBatch *b)
 {
     const std::vector<WorldSlice> &w = b->worlds;
+    const uint32_t warps = kBatchConfigs[b->config].threads / 32u;
+    b->classes = class_count_of(kBatchConfigs[b->config].threads);
+    std::vector<uint32_t> cls(w.size(), 0u);
+    if (b->items_per_thread > 0u) {
+        for (size_t i = 0; i < w.size(); ++i) {
+            const uint64_t need = (largest_color(w[i]) + (uint64_t)b->items_per_thread - 1u) / b->items_per_thread;
+            uint32_t tw = 1u;
+            while (tw < warps && 32ull * tw < need) {
+                tw <<= 1;
+            }
+            uint32_t c = 0;
+            while ((warps >> c) > tw) {
+                ++c;
+            }
+            cls[i] = c;
+        }
+    }
     std::vector<uint32_t> order(w.size());
     std::iota(order.begin(), order.end(), 0u);
-    auto on_warp = [&](uint32_t x) { return b->warp_color_max > 0u && largest_color(w[x]) <= b->warp_color_max; };
     auto work = [&](uint32_t x) { return 4ull * w[x].m + 3ull * w[x].nj + w[x].n; };
     std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
-        const bool wx = on_warp(x), wy = on_warp(y);
-        if (wx != wy) {
-            return !wx;
+        if (cls[x] != cls[y]) {
+            return cls[x] < cls[y];
         }
         return work(x) > work(y);
     });
-    uint32_t blocks = 0;
-    while (blocks < order.size() && !on_warp(order[blocks])) {
-        ++blocks;
+    for (uint32_t c = 0; c < kMaxClasses; ++c) {
+        b->class_first[c] = 0;
+        b->class_count[c] = 0;
+    }
+    for (size_t i = 0; i < order.size(); ++i) {
+        const uint32_t c = cls[order[i]];
+        if (b->class_count[c] == 0u) {
+            b->class_first[c] = (uint32_t)i;
+        }
+        b->class_count[c]++;
     }
     b->order = order;
-    b->block_worlds = blocks;
 }
 
 BatchArgs batch_args(const NphGpuBatch *b)
@@ -529,9 +579,13 @@ BatchArgs batch_args(const NphGpuBatch *b)
     A.worlds = b->d_worlds;
     A.order = b->d_order;
     A.count = b->world_count;
-    A.block_worlds = b->block_worlds;
+    for (uint32_t c = 0; c < kMaxClasses; ++c) {
+        A.class_first[c] = b->class_first[c];
+        A.class_count[c] = b->class_count[c];
+    }
+    A.classes = b->classes;
     A.heads = b->d_counters;
-    A.err = b->d_counters + 2;
+    A.err = b->d_counters + 6;
     A.bodies = b->d_bodies;
     A.fixed = b->d_fixed;
     A.contacts = b->d_contacts;
@@ -550,10 +604,7 @@ BatchArgs batch_args(const NphGpuBatch *b)
     A.mcap = (uint32_t)std::max<uint64_t>(b->cap_contacts, 1);
     A.jw = b->jw;
     A.jcap = (uint32_t)std::max<uint64_t>(b->cap_joints, 1);
-    const size_t smem = shared_bytes(b);
-    const uint32_t warps = kBatchConfigs[b->config].threads / 32u;
-    A.block_slots = (uint32_t)(smem / (2 * sizeof(float4)));
-    A.warp_slots = (uint32_t)(smem / (2 * sizeof(float4)) / warps);
+    A.block_slots = (uint32_t)(shared_bytes(b) / (2 * sizeof(float4)));
     return A;
 }
 
@@ -579,8 +630,7 @@ void configure_batch_kernel(NphGpuBatch *b)
     case 1: configure_kernel<256, 2>(smem); per_sm = resident<256, 2>(smem); break;
     case 2: configure_kernel<256, 1>(smem); per_sm = resident<256, 1>(smem); break;
     case 3: configure_kernel<512, 1>(smem); per_sm = resident<512, 1>(smem); break;
-    case 4: configure_kernel<1024, 1>(smem); per_sm = resident<1024, 1>(smem); break;
-    case 5: configure_kernel<256, 4>(smem); per_sm = resident<256, 4>(smem); break;
+    case 4: configure_kernel<256, 4>(smem); per_sm = resident<256, 4>(smem); break;
     default: configure_kernel<512, 2>(smem); per_sm = resident<512, 2>(smem); break;
     }
     b->blocks_per_sm = per_sm;
@@ -590,18 +640,15 @@ void enqueue_batch_step(NphGpuBatch *b, const StepConsts &K, uint32_t substeps)
 {
     const BatchArgs A = batch_args(b);
     const size_t smem = shared_bytes(b);
-    cudaMemsetAsync(b->d_counters, 0, 2 * sizeof(uint32_t), b->stream);
-    const uint32_t warps = kBatchConfigs[b->config].threads / 32u;
-    const uint64_t want = (uint64_t)b->block_worlds + (b->world_count - b->block_worlds + warps - 1u) / warps;
+    cudaMemsetAsync(b->d_counters, 0, kMaxClasses * sizeof(uint32_t), b->stream);
     const uint32_t grid = (uint32_t)std::max<uint64_t>(
-        1, std::min<uint64_t>(want, (uint64_t)b->blocks_per_sm * (uint64_t)b->sms));
+        1, std::min<uint64_t>(b->world_count, (uint64_t)b->blocks_per_sm * (uint64_t)b->sms));
     switch (b->config) {
     case 0: k_worlds<128, 4><<<grid, 128, smem, b->stream>>>(A, K, substeps); break;
     case 1: k_worlds<256, 2><<<grid, 256, smem, b->stream>>>(A, K, substeps); break;
     case 2: k_worlds<256, 1><<<grid, 256, smem, b->stream>>>(A, K, substeps); break;
     case 3: k_worlds<512, 1><<<grid, 512, smem, b->stream>>>(A, K, substeps); break;
-    case 4: k_worlds<1024, 1><<<grid, 1024, smem, b->stream>>>(A, K, substeps); break;
-    case 5: k_worlds<256, 4><<<grid, 256, smem, b->stream>>>(A, K, substeps); break;
+    case 4: k_worlds<256, 4><<<grid, 256, smem, b->stream>>>(A, K, substeps); break;
     default: k_worlds<512, 2><<<grid, 512, smem, b->stream>>>(A, K, substeps); break;
     }
 }
@@ -825,8 +872,8 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_create(const NphGpuSolverDesc *desc, NphG
         delete b;
         return NPH_GPU_DEVICE_LOST;
     }
-    if (!balloc(b->d_counters, 4) ||
-        cudaMallocHost((void **)&b->h_counters, 4 * sizeof(uint32_t)) != cudaSuccess) {
+    if (!balloc(b->d_counters, 8) ||
+        cudaMallocHost((void **)&b->h_counters, 8 * sizeof(uint32_t)) != cudaSuccess) {
         nph_gpu_batch_destroy(b);
         return NPH_GPU_OUT_OF_MEMORY;
     }
@@ -949,7 +996,7 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_upload(NphGpuBatch *b, const NphGpuWorldV
             cj.add(b->d_joints + s.joint_first, v.joints, sizeof(NphGpuJoint) * v.joint_count);
         }
     }
-    cudaMemsetAsync(b->d_counters, 0, 4 * sizeof(uint32_t), b->stream);
+    cudaMemsetAsync(b->d_counters, 0, 8 * sizeof(uint32_t), b->stream);
     return cuda_result(cudaStreamSynchronize(b->stream));
 }
 
@@ -981,12 +1028,12 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_download(NphGpuBatch *b, NphGpuWorldView 
         return NPH_GPU_INVALID_ARGUMENT;
     }
     cudaSetDevice(b->device);
-    cudaMemcpyAsync(b->h_counters, b->d_counters, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, b->stream);
+    cudaMemcpyAsync(b->h_counters, b->d_counters, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost, b->stream);
     NphGpuResult r = cuda_result(cudaStreamSynchronize(b->stream));
     if (r != NPH_GPU_OK) {
         return r;
     }
-    if (b->h_counters[2] != 0u) {
+    if (b->h_counters[6] != 0u) {
         return NPH_GPU_INVALID_ARGUMENT; // a malformed record: nothing written back
     }
     for (uint32_t w = 0; w < count; ++w) {
@@ -1034,7 +1081,7 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_set_config(NphGpuBatch *b, const NphGpuBa
     cudaSetDevice(b->device);
     b->config = t->config;
     b->shared_mode = t->shared_velocities;
-    b->warp_color_max = t->warp_color_max;
+    b->items_per_thread = t->items_per_thread;
     return apply_order(b);
 }
 
@@ -1054,9 +1101,9 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_autotune(NphGpuBatch *b, const NphGpuWorl
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    static const uint32_t kSplits[] = {0u, 16u, 32u, 64u, 128u, 0xFFFFFFFFu};
+    static const uint32_t kSplits[] = {0u, 1u, 2u, 4u, 8u};
     float best = 1e30f;
-    NphGpuBatchTuning chosen{b->config, kBatchConfigs[b->config].threads, b->shared_mode, b->warp_color_max, 0.0f};
+    NphGpuBatchTuning chosen{b->config, kBatchConfigs[b->config].threads, b->shared_mode, b->items_per_thread, 0.0f};
     rounds = rounds == 0u ? 1u : rounds;
     NphGpuResult r = NPH_GPU_OK;
     for (uint32_t shared = 0; shared <= NPH_GPU_BATCH_SHARED_LARGE && r == NPH_GPU_OK; ++shared) {
@@ -1067,7 +1114,7 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_autotune(NphGpuBatch *b, const NphGpuWorl
                 }
                 b->config = c;
                 b->shared_mode = shared;
-                b->warp_color_max = split;
+                b->items_per_thread = split;
                 r = apply_order(b);
                 if (r == NPH_GPU_OK) {
                     r = launch_batch_step(b, K, params->substeps); // builds the graph, warms up
@@ -1093,7 +1140,7 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_autotune(NphGpuBatch *b, const NphGpuWorl
     cudaEventDestroy(e1);
     b->config = chosen.config;
     b->shared_mode = chosen.shared_velocities;
-    b->warp_color_max = chosen.warp_color_max;
+    b->items_per_thread = chosen.items_per_thread;
     const NphGpuResult ro = apply_order(b);
     if (out != nullptr) {
         *out = chosen;
@@ -1115,8 +1162,9 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_info(const NphGpuBatch *b, NphGpuBatchInf
     out->threads = kBatchConfigs[b->config].threads;
     out->shared_velocities = b->shared_mode;
     out->blocks_per_sm = b->blocks_per_sm;
-    out->warp_color_max = b->warp_color_max;
-    out->warp_worlds = b->world_count - b->block_worlds;
+    out->items_per_thread = b->items_per_thread;
+    out->warp_worlds = b->class_count[b->classes - 1u];
+    out->block_worlds = b->class_count[0];
     return NPH_GPU_OK;
 }
 

@@ -354,13 +354,14 @@ class Batch:
                                                     len(views)))
 
     def set_config(self, config: int, shared_velocities: int = abi.BATCH_SHARED_SMALL,
-                   warp_color_max: int = 32) -> None:
+                   items_per_thread: int = 2) -> None:
         """Launch shape, shared-memory mode for velocities (abi.BATCH_SHARED_*) and the
-        largest colour a world may have to run on one warp (0: every world on a block)."""
+        constraints a thread takes per colour when sizing a world's team (0: every world on a
+        whole block)."""
         t = abi.BatchTuning()
         t.config = config
         t.shared_velocities = int(shared_velocities)
-        t.warp_color_max = warp_color_max
+        t.items_per_thread = items_per_thread
         _check(self.L.nph_gpu_batch_set_config(self._h, ctypes.byref(t)),
                "nph_gpu_batch_set_config")
 
@@ -372,13 +373,13 @@ class Batch:
         _check(self.L.nph_gpu_batch_autotune(self._h, ctypes.byref(params), dt, rounds,
                                              ctypes.byref(t)), "nph_gpu_batch_autotune")
         return {"config": t.config, "threads": t.threads,
-                "shared_velocities": t.shared_velocities, "warp_color_max": t.warp_color_max,
+                "shared_velocities": t.shared_velocities, "items_per_thread": t.items_per_thread,
                 "ms_per_step": t.ms_per_step}
 
     def info(self) -> dict:
         i = abi.BatchInfo()
         _check(self.L.nph_gpu_batch_info(self._h, ctypes.byref(i)), "nph_gpu_batch_info")
-        return {k: getattr(i, k) for k, _ in abi.BatchInfo._fields_ if k != "pad"}
+        return {k: getattr(i, k) for k, _ in abi.BatchInfo._fields_}
 
 
 def version() -> str:

@@ -83,23 +83,23 @@ def solved_alone(solver):
 @pytest.mark.parametrize("shared", [abi.BATCH_SHARED_NONE, abi.BATCH_SHARED_SMALL,
                                     abi.BATCH_SHARED_LARGE])
 def test_batch_equals_worlds_solved_alone(solved_alone, ref_lib, shared):
-    """Every launch shape, with every world on a block, on a warp, or split by size."""
+    """Every launch shape, with every world on a block, on a warp, or on teams sized to it."""
     from nepheline_b200.solver import Batch
     params = abi.WorldParams.default()
     views, alone = solved_alone
     batch = Batch()
     for config in range(batch.config_count()):
-        for split in (0, 24, 0xFFFFFFFF):
-            batch.set_config(config, shared, split)
+        for per_thread in (0, 1, 1 << 20):
+            batch.set_config(config, shared, per_thread)
             together = [v.copy() for v in views]
             batch.phys_solve_worlds(together, params, DT)
             info = batch.info()
-            if split == 0:
-                assert info["warp_worlds"] == 0
-            if split == 0xFFFFFFFF:
+            if per_thread == 0:
+                assert info["block_worlds"] == len(views)
+            if per_thread == 1 << 20:
                 assert info["warp_worlds"] == len(views)
             for i, (a, b) in enumerate(zip(together, alone)):
-                where = f"world {i}, config {config}, shared {shared}, split {split}"
+                where = f"world {i}, config {config}, shared {shared}, per thread {per_thread}"
                 assert a.bodies.tobytes() == b.bodies.tobytes(), where
                 assert a.contacts.tobytes() == b.contacts.tobytes(), where
                 assert a.joints.tobytes() == b.joints.tobytes(), where
