@@ -352,6 +352,13 @@ NPH_GPU_API NphGpuResult nph_gpu_solver_autotune(NphGpuSolver *solver,
 
 typedef struct NphGpuBatch NphGpuBatch;
 
+/* Packings of a batch. */
+#define NPH_GPU_BATCH_PERSISTENT 0u /* one persistent launch a step: teams take whole worlds */
+#define NPH_GPU_BATCH_MERGED 1u     /* the batch as one world: a launch per stage and colour over
+                                       every world at once (each world's colour lists padded to
+                                       whole eight-lane groups, so each world's results stay
+                                       the same bits), replayed as a CUDA graph */
+
 /* Shared-memory modes for a world's body velocities. */
 #define NPH_GPU_BATCH_SHARED_NONE 0u  /* in global memory */
 #define NPH_GPU_BATCH_SHARED_SMALL 1u /* up to 32 KiB per block */
@@ -365,6 +372,8 @@ typedef struct NphGpuBatchTuning {
     uint32_t items_per_thread;  /* a world runs on the smallest team (1, 2, 4, ... warps, up
                                    to the block) whose threads cover its largest colour at
                                    this many constraints a thread; 0: every world on a block */
+    uint32_t packing;           /* NPH_GPU_BATCH_PERSISTENT or NPH_GPU_BATCH_MERGED; the fields
+                                   above apply to the persistent packing */
     float ms_per_step;          /* the autotuner's time for it (filled in) */
 } NphGpuBatchTuning;
 
@@ -380,6 +389,8 @@ typedef struct NphGpuBatchInfo {
     uint32_t items_per_thread;
     uint32_t warp_worlds;  /* worlds the current configuration runs on one warp */
     uint32_t block_worlds; /* worlds it runs on a whole block */
+    uint32_t packing;
+    uint32_t pad;
 } NphGpuBatchInfo;
 
 NPH_GPU_API NphGpuResult nph_gpu_batch_create(const NphGpuSolverDesc *desc, NphGpuBatch **out);

@@ -180,6 +180,7 @@ class KernelTime(ctypes.Structure):
 
 
 BATCH_SHARED_NONE, BATCH_SHARED_SMALL, BATCH_SHARED_LARGE = 0, 1, 2
+BATCH_PERSISTENT, BATCH_MERGED = 0, 1
 
 # The learned warm start's network and point slots (nepheline_b200.h).
 MLP_INPUTS, MLP_HIDDEN, MLP_OUTPUTS = 16, 64, 3
@@ -198,7 +199,7 @@ class ConvergeStats(ctypes.Structure):
 class BatchTuning(ctypes.Structure):
     _fields_ = [("config", ctypes.c_uint32), ("threads", ctypes.c_uint32),
                 ("shared_velocities", ctypes.c_uint32), ("items_per_thread", ctypes.c_uint32),
-                ("ms_per_step", ctypes.c_float)]
+                ("packing", ctypes.c_uint32), ("ms_per_step", ctypes.c_float)]
 
 
 class BatchInfo(ctypes.Structure):
@@ -207,7 +208,8 @@ class BatchInfo(ctypes.Structure):
                 ("joints", ctypes.c_uint64), ("threads", ctypes.c_uint32),
                 ("shared_velocities", ctypes.c_uint32), ("blocks_per_sm", ctypes.c_uint32),
                 ("items_per_thread", ctypes.c_uint32), ("warp_worlds", ctypes.c_uint32),
-                ("block_worlds", ctypes.c_uint32)]
+                ("block_worlds", ctypes.c_uint32), ("packing", ctypes.c_uint32),
+                ("pad", ctypes.c_uint32)]
 
 
 class SolverDesc(ctypes.Structure):

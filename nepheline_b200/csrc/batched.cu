@@ -26,6 +26,7 @@
 #include <vector>
 
 #include "nepheline_b200.h"
+#include "solver_link.h"
 
 #include "bodies.cuh"
 #include "contacts.cuh"
@@ -377,6 +378,97 @@ __global__ void __launch_bounds__(kThreads, kMinBlocks) k_worlds(BatchArgs A, St
     }
 }
 
+// ---- the merged packing: the batch as one world --------------------------------------
+
+// A world-local body index in the merged world: its awake bodies after the worlds before it,
+// its fixed bodies after every awake body and the fixed bodies of the worlds before it. An
+// index outside the world maps outside every world, where prepare marks the record inert and
+// reports it.
+__device__ __forceinline__ uint32_t merged_body(uint32_t x, const WorldSlice &w, uint32_t n_total)
+{
+    if (x < w.n) {
+        return w.body_first + x;
+    }
+    if (x - w.n < w.nf) {
+        return n_total + w.fixed_first + (x - w.n);
+    }
+    return 0xFFFFFFF0u;
+}
+
+// The merged contact list: each world's colour lists in turn, each padded to whole groups of
+// eight with an inert manifold (its two sides the pad body, which is not dynamic: one point,
+// apart, nothing written), so the eight-lane group decisions are each world's own.
+__global__ void __launch_bounds__(256) k_merge_contacts(const NphGpuContact *packed, const uint32_t *map,
+                                                        const uint32_t *mworld, const WorldSlice *worlds,
+                                                        uint32_t n_total, uint32_t pad_body, NphGpuContact *out,
+                                                        uint32_t count)
+{
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= count) {
+        return;
+    }
+    const uint32_t src = map[p];
+    NphGpuContact c;
+    if (src == NPH_GPU_NULL) {
+        memset(&c, 0, sizeof c);
+        c.body_a = pad_body;
+        c.body_b = pad_body;
+        c.point_count = 1u;
+        c.normal[1] = 1.0f;
+        c.points[0].separation = 1.0f;
+    } else {
+        c = packed[src];
+        const WorldSlice &w = worlds[mworld[p]];
+        c.body_a = merged_body(c.body_a, w, n_total);
+        c.body_b = merged_body(c.body_b, w, n_total);
+    }
+    out[p] = c;
+}
+
+// Back into each world's slice: the results, with the world's own body indices.
+__global__ void __launch_bounds__(256) k_unmerge_contacts(const NphGpuContact *merged, const uint32_t *map,
+                                                          NphGpuContact *packed, uint32_t count)
+{
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= count || map[p] == NPH_GPU_NULL) {
+        return;
+    }
+    NphGpuContact c = merged[p];
+    NphGpuContact &dst = packed[map[p]];
+    c.body_a = dst.body_a;
+    c.body_b = dst.body_b;
+    dst = c;
+}
+
+__global__ void __launch_bounds__(256) k_merge_joints(const NphGpuJoint *packed, const uint32_t *map,
+                                                      const uint32_t *mworld, const WorldSlice *worlds,
+                                                      uint32_t n_total, NphGpuJoint *out, uint32_t count)
+{
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= count) {
+        return;
+    }
+    NphGpuJoint j = packed[map[p]];
+    const WorldSlice &w = worlds[mworld[p]];
+    j.body_a = merged_body(j.body_a, w, n_total);
+    j.body_b = merged_body(j.body_b, w, n_total);
+    out[p] = j;
+}
+
+__global__ void __launch_bounds__(256) k_unmerge_joints(const NphGpuJoint *merged, const uint32_t *map,
+                                                        NphGpuJoint *packed, uint32_t count)
+{
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= count) {
+        return;
+    }
+    NphGpuJoint j = merged[p];
+    NphGpuJoint &dst = packed[map[p]];
+    j.body_a = dst.body_a;
+    j.body_b = dst.body_b;
+    dst = j;
+}
+
 struct BatchConfig {
     uint32_t threads, min_blocks;
 };
@@ -405,6 +497,17 @@ struct NphGpuBatch {
     uint32_t blocks_per_sm = 0; // resident blocks of the chosen kernel (0: not yet known)
     uint32_t class_first[kMaxClasses] = {}, class_count[kMaxClasses] = {};
     uint32_t classes = 1;
+    // The merged packing: a single-world solver on the batch's stream, the merged lists'
+    // sources (packed index, or NPH_GPU_NULL for a pad) and worlds, and whether the current
+    // state lives in the solver (true after a merged step, until the next upload).
+    uint32_t packing = NPH_GPU_BATCH_PERSISTENT;
+    NphGpuSolver *merged = nullptr;
+    uint32_t *d_cmap = nullptr, *d_cworld = nullptr, *d_jmap = nullptr, *d_jworld = nullptr;
+    uint64_t cap_cmap = 0, cap_jmap = 0;
+    bool maps_valid = false;
+    bool live_in_merged = false;
+    NphGpuWorldView merged_shape{};
+    uint32_t merged_driven = 0;
     int sms = 148;
     // Device arrays and their capacities (grown, never shrunk, by uploads).
     NphGpuBody *d_bodies = nullptr;
@@ -481,6 +584,13 @@ void free_arrays(NphGpuBatch *b)
     bfree(b->jw);
     bfree(b->d_worlds);
     bfree(b->d_order);
+    bfree(b->d_cmap);
+    bfree(b->d_cworld);
+    bfree(b->d_jmap);
+    bfree(b->d_jworld);
+    b->cap_cmap = b->cap_jmap = 0;
+    b->maps_valid = false;
+    b->live_in_merged = false;
     b->cap_bodies = b->cap_slots = b->cap_fixed = b->cap_contacts = b->cap_joints = b->cap_worlds = 0;
     b->world_count = 0;
 }
@@ -699,6 +809,165 @@ NphGpuResult apply_order(NphGpuBatch *b)
     return cuda_result(cudaStreamSynchronize(b->stream));
 }
 
+// The merged lists of the uploaded batch (built on the host, once per upload): colour by
+// colour, each world's list in turn, contact lists padded to whole groups of eight.
+NphGpuResult build_merge_maps(NphGpuBatch *b)
+{
+    if (b->maps_valid) {
+        return NPH_GPU_OK;
+    }
+    std::vector<uint32_t> cmap, cworld, jmap, jworld;
+    cmap.reserve(b->contacts + 8ull * b->world_count);
+    cworld.reserve(b->contacts + 8ull * b->world_count);
+    jmap.reserve(b->joints);
+    jworld.reserve(b->joints);
+    NphGpuWorldView &shape = b->merged_shape;
+    std::memset(&shape, 0, sizeof shape);
+    uint32_t driven = 0;
+    for (uint32_t c = 0; c < NPH_GPU_COLOR_SLOTS; ++c) {
+        for (uint32_t w = 0; w < b->world_count; ++w) {
+            const WorldSlice &ws = b->worlds[w];
+            for (uint32_t i = 0; i < ws.ccount[c]; ++i) {
+                cmap.push_back(ws.contact_first + ws.cfirst[c] + i);
+                cworld.push_back(w);
+            }
+            const uint32_t pad = c < NPH_GPU_COLORS ? (8u - ws.ccount[c] % 8u) % 8u : 0u;
+            for (uint32_t i = 0; i < pad; ++i) {
+                cmap.push_back(NPH_GPU_NULL);
+                cworld.push_back(w);
+            }
+            shape.contact_color_counts[c] += ws.ccount[c] + pad;
+            for (uint32_t i = 0; i < ws.jcount[c]; ++i) {
+                jmap.push_back(ws.joint_first + ws.jfirst[c] + i);
+                jworld.push_back(w);
+            }
+            shape.joint_color_counts[c] += ws.jcount[c];
+        }
+    }
+    for (uint32_t w = 0; w < b->world_count; ++w) {
+        driven += b->worlds[w].driven;
+    }
+    if (cmap.size() >= 0xFFFFFFF0ull || b->bodies + b->fixed + 1u >= 0xFFFFFFF0ull) {
+        return NPH_GPU_TOO_LARGE;
+    }
+    if (cmap.size() > b->cap_cmap || b->d_cmap == nullptr) {
+        const uint64_t cap = std::max<uint64_t>(cmap.size(), 1);
+        b->cap_cmap = 0;
+        if (!balloc(b->d_cmap, cap) || !balloc(b->d_cworld, cap)) {
+            return NPH_GPU_OUT_OF_MEMORY;
+        }
+        b->cap_cmap = cap;
+    }
+    if (jmap.size() > b->cap_jmap || b->d_jmap == nullptr) {
+        const uint64_t cap = std::max<uint64_t>(jmap.size(), 1);
+        b->cap_jmap = 0;
+        if (!balloc(b->d_jmap, cap) || !balloc(b->d_jworld, cap)) {
+            return NPH_GPU_OUT_OF_MEMORY;
+        }
+        b->cap_jmap = cap;
+    }
+    cudaMemcpyAsync(b->d_cmap, cmap.data(), cmap.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, b->stream);
+    cudaMemcpyAsync(b->d_cworld, cworld.data(), cworld.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                    b->stream);
+    if (!jmap.empty()) {
+        cudaMemcpyAsync(b->d_jmap, jmap.data(), jmap.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, b->stream);
+        cudaMemcpyAsync(b->d_jworld, jworld.data(), jworld.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                        b->stream);
+    }
+    shape.body_count = (uint32_t)b->bodies;
+    shape.fixed_count = (uint32_t)b->fixed + 1u; // and the pad body
+    shape.contact_count = (uint32_t)cmap.size();
+    shape.joint_count = (uint32_t)jmap.size();
+    b->merged_driven = driven;
+    const NphGpuResult r = cuda_result(cudaStreamSynchronize(b->stream));
+    b->maps_valid = r == NPH_GPU_OK;
+    return r;
+}
+
+// Packed -> the merged solver (the state then lives there).
+NphGpuResult merged_setup(NphGpuBatch *b)
+{
+    if (b->live_in_merged) {
+        return NPH_GPU_OK;
+    }
+    NphGpuResult r = build_merge_maps(b);
+    if (r != NPH_GPU_OK) {
+        return r;
+    }
+    if (b->merged == nullptr) {
+        NphGpuSolverDesc d{};
+        d.device = b->device;
+        d.stream = b->stream;
+        d.use_graph = b->use_graph ? 1u : 0u;
+        r = nph_gpu_solver_create(&d, &b->merged);
+        if (r != NPH_GPU_OK) {
+            b->merged = nullptr;
+            return r;
+        }
+    }
+    NphSolverRecords R;
+    r = nph_solver_bind_device(b->merged, &b->merged_shape, b->merged_driven, &R);
+    if (r != NPH_GPU_OK) {
+        return r;
+    }
+    const uint32_t n_total = (uint32_t)b->bodies;
+    if (b->bodies > 0) {
+        cudaMemcpyAsync(R.bodies, b->d_bodies, sizeof(NphGpuBody) * b->bodies, cudaMemcpyDeviceToDevice, b->stream);
+    }
+    if (b->fixed > 0) {
+        cudaMemcpyAsync(R.fixed, b->d_fixed, sizeof(NphGpuBody) * b->fixed, cudaMemcpyDeviceToDevice, b->stream);
+    }
+    NphGpuBody pad;
+    std::memset(&pad, 0, sizeof pad);
+    pad.rotation[3] = 1.0f;
+    pad.type = NPH_GPU_BODY_STATIC;
+    cudaMemcpyAsync(R.fixed + b->fixed, &pad, sizeof pad, cudaMemcpyHostToDevice, b->stream);
+    const uint32_t mc = b->merged_shape.contact_count, mj = b->merged_shape.joint_count;
+    if (mc > 0) {
+        k_merge_contacts<<<(mc + 255u) / 256u, 256, 0, b->stream>>>(b->d_contacts, b->d_cmap, b->d_cworld, b->d_worlds,
+                                                                  n_total, n_total + (uint32_t)b->fixed, R.contacts, mc);
+    }
+    if (mj > 0) {
+        k_merge_joints<<<(mj + 255u) / 256u, 256, 0, b->stream>>>(b->d_joints, b->d_jmap, b->d_jworld, b->d_worlds,
+                                                                n_total, R.joints, mj);
+    }
+    r = cuda_result(cudaStreamSynchronize(b->stream));
+    b->live_in_merged = r == NPH_GPU_OK;
+    return r;
+}
+
+// The merged solver's state -> packed (both then hold it).
+NphGpuResult merged_to_packed(NphGpuBatch *b)
+{
+    if (!b->live_in_merged) {
+        return NPH_GPU_OK;
+    }
+    NphSolverRecords R;
+    NphGpuResult r = nph_solver_records(b->merged, &R);
+    if (r != NPH_GPU_OK) {
+        return r;
+    }
+    if (b->bodies > 0) {
+        cudaMemcpyAsync(b->d_bodies, R.bodies, sizeof(NphGpuBody) * b->bodies, cudaMemcpyDeviceToDevice, b->stream);
+    }
+    const uint32_t mc = b->merged_shape.contact_count, mj = b->merged_shape.joint_count;
+    if (mc > 0) {
+        k_unmerge_contacts<<<(mc + 255u) / 256u, 256, 0, b->stream>>>(R.contacts, b->d_cmap, b->d_contacts, mc);
+    }
+    if (mj > 0) {
+        k_unmerge_joints<<<(mj + 255u) / 256u, 256, 0, b->stream>>>(R.joints, b->d_jmap, b->d_joints, mj);
+    }
+    return cuda_result(cudaStreamSynchronize(b->stream));
+}
+
+// Makes the packed arrays the live state (for the persistent packing).
+NphGpuResult leave_merged(NphGpuBatch *b)
+{
+    const NphGpuResult r = merged_to_packed(b);
+    b->live_in_merged = false;
+    return r;
+}
+
 NphGpuResult check_world(const NphGpuWorldView &v)
 {
     uint64_t nc = 0, nj = 0;
@@ -891,6 +1160,10 @@ NPH_GPU_API void nph_gpu_batch_destroy(NphGpuBatch *b)
         cudaStreamSynchronize(b->stream);
     }
     free_arrays(b);
+    if (b->merged != nullptr) {
+        nph_gpu_solver_destroy(b->merged);
+        b->merged = nullptr;
+    }
     bfree(b->d_counters);
     if (b->h_counters != nullptr) {
         cudaFreeHost(b->h_counters);
@@ -981,6 +1254,8 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_upload(NphGpuBatch *b, const NphGpuWorldV
     b->joints = joints;
     b->max_world_slots = max_slots;
     b->worlds = slices;
+    b->maps_valid = false;
+    b->live_in_merged = false;
     build_order(b);
     cudaMemcpyAsync(b->d_worlds, slices.data(), sizeof(WorldSlice) * count, cudaMemcpyHostToDevice, b->stream);
     cudaMemcpyAsync(b->d_order, b->order.data(), sizeof(uint32_t) * count, cudaMemcpyHostToDevice, b->stream);
@@ -1014,8 +1289,12 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_step_async(NphGpuBatch *b, const NphGpuWo
         return NPH_GPU_OK;
     }
     cudaSetDevice(b->device);
+    if (b->packing == NPH_GPU_BATCH_MERGED) {
+        const NphGpuResult r = merged_setup(b);
+        return r != NPH_GPU_OK ? r : nph_gpu_world_step_async(b->merged, params, dt, steps);
+    }
+    NphGpuResult r = leave_merged(b);
     const StepConsts K = make_step_consts(*params, dt);
-    NphGpuResult r = NPH_GPU_OK;
     for (uint32_t i = 0; i < steps && r == NPH_GPU_OK; ++i) {
         r = launch_batch_step(b, K, params->substeps);
     }
@@ -1028,8 +1307,18 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_download(NphGpuBatch *b, NphGpuWorldView 
         return NPH_GPU_INVALID_ARGUMENT;
     }
     cudaSetDevice(b->device);
+    NphGpuResult r = NPH_GPU_OK;
+    if (b->live_in_merged) {
+        r = nph_solver_check(b->merged);
+        if (r == NPH_GPU_OK) {
+            r = merged_to_packed(b);
+        }
+        if (r != NPH_GPU_OK) {
+            return r;
+        }
+    }
     cudaMemcpyAsync(b->h_counters, b->d_counters, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost, b->stream);
-    NphGpuResult r = cuda_result(cudaStreamSynchronize(b->stream));
+    r = cuda_result(cudaStreamSynchronize(b->stream));
     if (r != NPH_GPU_OK) {
         return r;
     }
@@ -1075,10 +1364,17 @@ NPH_GPU_API NphGpuResult nph_gpu_phys_solve_worlds(NphGpuBatch *b, const NphGpuW
 NPH_GPU_API NphGpuResult nph_gpu_batch_set_config(NphGpuBatch *b, const NphGpuBatchTuning *t)
 {
     if (b == nullptr || t == nullptr || t->config >= kBatchConfigCount ||
-        t->shared_velocities > NPH_GPU_BATCH_SHARED_LARGE) {
+        t->shared_velocities > NPH_GPU_BATCH_SHARED_LARGE || t->packing > NPH_GPU_BATCH_MERGED) {
         return NPH_GPU_INVALID_ARGUMENT;
     }
     cudaSetDevice(b->device);
+    if (t->packing != b->packing) {
+        const NphGpuResult r = leave_merged(b);
+        if (r != NPH_GPU_OK) {
+            return r;
+        }
+    }
+    b->packing = t->packing;
     b->config = t->config;
     b->shared_mode = t->shared_velocities;
     b->items_per_thread = t->items_per_thread;
@@ -1103,15 +1399,34 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_autotune(NphGpuBatch *b, const NphGpuWorl
     cudaEventCreate(&e1);
     static const uint32_t kSplits[] = {0u, 1u, 2u, 4u, 8u};
     float best = 1e30f;
-    NphGpuBatchTuning chosen{b->config, kBatchConfigs[b->config].threads, b->shared_mode, b->items_per_thread, 0.0f};
+    NphGpuBatchTuning chosen{b->config, kBatchConfigs[b->config].threads, b->shared_mode, b->items_per_thread,
+                             b->packing, 0.0f};
     rounds = rounds == 0u ? 1u : rounds;
-    NphGpuResult r = NPH_GPU_OK;
+    auto timed = [&](auto &&step) -> float {
+        cudaEventRecord(e0, b->stream);
+        NphGpuResult q = NPH_GPU_OK;
+        for (uint32_t i = 0; i < rounds && q == NPH_GPU_OK; ++i) {
+            q = step();
+        }
+        cudaEventRecord(e1, b->stream);
+        if (q == NPH_GPU_OK) {
+            q = cuda_result(cudaEventSynchronize(e1));
+        }
+        float ms = 1e30f;
+        if (q == NPH_GPU_OK) {
+            cudaEventElapsedTime(&ms, e0, e1);
+        }
+        return ms;
+    };
+    // The persistent packing: every launch shape, shared-memory mode and team sizing.
+    NphGpuResult r = leave_merged(b);
     for (uint32_t shared = 0; shared <= NPH_GPU_BATCH_SHARED_LARGE && r == NPH_GPU_OK; ++shared) {
         for (uint32_t c = 0; c < kBatchConfigCount && r == NPH_GPU_OK; ++c) {
             for (uint32_t split : kSplits) {
                 if (r != NPH_GPU_OK) {
                     break;
                 }
+                b->packing = NPH_GPU_BATCH_PERSISTENT;
                 b->config = c;
                 b->shared_mode = shared;
                 b->items_per_thread = split;
@@ -1119,29 +1434,51 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_autotune(NphGpuBatch *b, const NphGpuWorl
                 if (r == NPH_GPU_OK) {
                     r = launch_batch_step(b, K, params->substeps); // builds the graph, warms up
                 }
-                cudaEventRecord(e0, b->stream);
-                for (uint32_t i = 0; i < rounds && r == NPH_GPU_OK; ++i) {
-                    r = launch_batch_step(b, K, params->substeps);
+                if (r != NPH_GPU_OK) {
+                    break;
                 }
-                cudaEventRecord(e1, b->stream);
-                if (r == NPH_GPU_OK) {
-                    r = cuda_result(cudaEventSynchronize(e1));
-                }
-                float ms = 0.0f;
-                cudaEventElapsedTime(&ms, e0, e1);
-                if (r == NPH_GPU_OK && ms < best) {
+                const float ms = timed([&] { return launch_batch_step(b, K, params->substeps); });
+                if (ms < best) {
                     best = ms;
-                    chosen = NphGpuBatchTuning{c, kBatchConfigs[c].threads, shared, split, ms / (float)rounds};
+                    chosen = NphGpuBatchTuning{c, kBatchConfigs[c].threads, shared, split, NPH_GPU_BATCH_PERSISTENT,
+                                               ms / (float)rounds};
                 }
+            }
+        }
+    }
+    // The merged packing, its passes tuned by the single-world autotuner.
+    if (r == NPH_GPU_OK) {
+        b->packing = NPH_GPU_BATCH_MERGED;
+        r = merged_setup(b);
+        uint32_t pass[4];
+        if (r == NPH_GPU_OK) {
+            r = nph_gpu_solver_autotune(b->merged, params, dt, rounds, pass);
+        }
+        if (r == NPH_GPU_OK) {
+            r = nph_gpu_world_step_async(b->merged, params, dt, 1); // builds the graph, warms up
+        }
+        if (r == NPH_GPU_OK) {
+            const float ms = timed([&] { return nph_gpu_world_step_async(b->merged, params, dt, 1); });
+            if (ms < best) {
+                best = ms;
+                chosen = NphGpuBatchTuning{b->config, kBatchConfigs[b->config].threads, b->shared_mode,
+                                           b->items_per_thread, NPH_GPU_BATCH_MERGED, ms / (float)rounds};
             }
         }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    NphGpuResult ro = NPH_GPU_OK;
+    if (chosen.packing == NPH_GPU_BATCH_PERSISTENT) {
+        ro = leave_merged(b);
+    }
+    b->packing = chosen.packing;
     b->config = chosen.config;
     b->shared_mode = chosen.shared_velocities;
     b->items_per_thread = chosen.items_per_thread;
-    const NphGpuResult ro = apply_order(b);
+    if (ro == NPH_GPU_OK) {
+        ro = apply_order(b);
+    }
     if (out != nullptr) {
         *out = chosen;
     }
@@ -1163,6 +1500,7 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_info(const NphGpuBatch *b, NphGpuBatchInf
     out->shared_velocities = b->shared_mode;
     out->blocks_per_sm = b->blocks_per_sm;
     out->items_per_thread = b->items_per_thread;
+    out->packing = b->packing;
     out->warp_worlds = b->class_count[b->classes - 1u];
     out->block_worlds = b->class_count[0];
     return NPH_GPU_OK;

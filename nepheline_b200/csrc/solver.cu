@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "nepheline_b200.h"
+#include "solver_link.h"
 
 #include "bodies.cuh"
 #include "contacts.cuh"
@@ -1093,6 +1094,77 @@ void enqueue_converge_pass(NphGpuSolver *s, const StepConsts &K, const uint32_t 
 }
 
 } // namespace
+
+// ------------------------------------------------------------------------------------
+// Internal links (solver_link.h)
+// ------------------------------------------------------------------------------------
+
+NphGpuResult nph_solver_bind_device(NphGpuSolver *s, const NphGpuWorldView *v, uint32_t driven,
+                                    NphSolverRecords *out)
+{
+    if (s == nullptr || v == nullptr || out == nullptr) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    uint64_t nc = 0, nj = 0;
+    for (uint32_t c = 0; c < NPH_GPU_COLOR_SLOTS; ++c) {
+        nc += v->contact_color_counts[c];
+        nj += v->joint_color_counts[c];
+    }
+    if (nc != v->contact_count || nj != v->joint_count ||
+        (uint64_t)v->body_count + v->fixed_count >= 0xFFFFFFF0ull) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    cudaSetDevice(s->device);
+    NphGpuResult r = ensure_capacity(s, v->body_count, v->fixed_count, v->contact_count, v->joint_count);
+    if (r != NPH_GPU_OK) {
+        return r;
+    }
+    const bool same_shape = s->uploaded && s->n == v->body_count && s->nf == v->fixed_count &&
+                            s->m == v->contact_count && s->nj == v->joint_count &&
+                            std::memcmp(s->ccount, v->contact_color_counts, sizeof s->ccount) == 0 &&
+                            std::memcmp(s->jcount, v->joint_color_counts, sizeof s->jcount) == 0;
+    s->n = v->body_count;
+    s->nf = v->fixed_count;
+    s->m = v->contact_count;
+    s->nj = v->joint_count;
+    uint32_t cf = 0, jf = 0;
+    for (uint32_t c = 0; c < NPH_GPU_COLOR_SLOTS; ++c) {
+        s->ccount[c] = v->contact_color_counts[c];
+        s->jcount[c] = v->joint_color_counts[c];
+        s->cfirst[c] = cf;
+        s->jfirst[c] = jf;
+        cf += s->ccount[c];
+        jf += s->jcount[c];
+    }
+    if (!same_shape || driven != s->driven) {
+        drop_graph(s);
+    }
+    s->driven = driven;
+    cudaMemsetAsync(s->d_err, 0, 32 * sizeof(uint32_t), s->stream);
+    s->uploaded = true;
+    return nph_solver_records(s, out);
+}
+
+NphGpuResult nph_solver_records(NphGpuSolver *s, NphSolverRecords *out)
+{
+    if (s == nullptr || out == nullptr || !s->uploaded) {
+        return NPH_GPU_INVALID_STATE;
+    }
+    out->bodies = s->d_bodies;
+    out->fixed = s->d_fixed;
+    out->contacts = s->d_contacts;
+    out->joints = s->d_joints;
+    return NPH_GPU_OK;
+}
+
+NphGpuResult nph_solver_check(NphGpuSolver *s)
+{
+    if (s == nullptr) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    cudaSetDevice(s->device);
+    return read_error(s);
+}
 
 // ------------------------------------------------------------------------------------
 // The C ABI

@@ -353,15 +353,17 @@ class Batch:
         return int(self.L.nph_gpu_phys_solve_worlds(self._h, ctypes.byref(params), dt, arr,
                                                     len(views)))
 
-    def set_config(self, config: int, shared_velocities: int = abi.BATCH_SHARED_SMALL,
-                   items_per_thread: int = 2) -> None:
-        """Launch shape, shared-memory mode for velocities (abi.BATCH_SHARED_*) and the
+    def set_config(self, config: int = 3, shared_velocities: int = abi.BATCH_SHARED_SMALL,
+                   items_per_thread: int = 2, packing: int = abi.BATCH_PERSISTENT) -> None:
+        """Packing (abi.BATCH_PERSISTENT or abi.BATCH_MERGED); for the persistent packing the
+        launch shape, shared-memory mode for velocities (abi.BATCH_SHARED_*) and the
         constraints a thread takes per colour when sizing a world's team (0: every world on a
         whole block)."""
         t = abi.BatchTuning()
         t.config = config
         t.shared_velocities = int(shared_velocities)
         t.items_per_thread = items_per_thread
+        t.packing = packing
         _check(self.L.nph_gpu_batch_set_config(self._h, ctypes.byref(t)),
                "nph_gpu_batch_set_config")
 
@@ -374,12 +376,13 @@ class Batch:
                                              ctypes.byref(t)), "nph_gpu_batch_autotune")
         return {"config": t.config, "threads": t.threads,
                 "shared_velocities": t.shared_velocities, "items_per_thread": t.items_per_thread,
+                "packing": t.packing,
                 "ms_per_step": t.ms_per_step}
 
     def info(self) -> dict:
         i = abi.BatchInfo()
         _check(self.L.nph_gpu_batch_info(self._h, ctypes.byref(i)), "nph_gpu_batch_info")
-        return {k: getattr(i, k) for k, _ in abi.BatchInfo._fields_}
+        return {k: getattr(i, k) for k, _ in abi.BatchInfo._fields_ if k != "pad"}
 
 
 def version() -> str:

@@ -159,8 +159,9 @@ def test_batch_autotuner_keeps_results(solver):
     batch = Batch()
     batch.upload(views)
     tuned = batch.autotune(params, DT, rounds=1)
-    assert tuned["threads"] in (128, 256, 512, 1024)
+    assert tuned["threads"] in (128, 256, 512)
     assert tuned["shared_velocities"] in (0, 1, 2)
+    assert tuned["packing"] in (abi.BATCH_PERSISTENT, abi.BATCH_MERGED)
     batch.upload(views)
     batch.step_async(params, DT, 1)
     got = [v.copy() for v in views]
@@ -181,6 +182,66 @@ def test_batch_refuses_malformed_worlds(solver):
     bad = good.copy()
     bad.contacts["body_a"][0] = 10_000
     batch = Batch()
+    before = bad.copy()
+    assert batch.phys_solve_worlds_code([good.copy(), bad], params, DT) == abi.INVALID_ARGUMENT
+    assert bad.bodies.tobytes() == before.bodies.tobytes()
+    batch.close()
+
+
+def test_merged_packing_equals_worlds_solved_alone(solved_alone):
+    """The batch as one world (colour lists padded to whole groups of eight per world) gives
+    each world the bits it has alone; so do switches between the packings."""
+    from nepheline_b200.solver import Batch
+    params = abi.WorldParams.default()
+    views, alone = solved_alone
+    batch = Batch()
+    for packing in (abi.BATCH_MERGED, abi.BATCH_PERSISTENT, abi.BATCH_MERGED):
+        batch.set_config(packing=packing)
+        together = [v.copy() for v in views]
+        batch.phys_solve_worlds(together, params, DT)
+        assert batch.info()["packing"] == packing
+        for i, (a, b) in enumerate(zip(together, alone)):
+            assert a.bodies.tobytes() == b.bodies.tobytes(), f"world {i}, packing {packing}"
+            assert a.contacts.tobytes() == b.contacts.tobytes(), f"world {i}, packing {packing}"
+            assert a.joints.tobytes() == b.joints.tobytes(), f"world {i}, packing {packing}"
+    batch.close()
+
+
+def test_merged_resident_steps_and_packing_switches(solver):
+    """Resident steps alternating between the packings equal repeated solves of each world."""
+    from nepheline_b200.solver import Batch
+    params = abi.WorldParams.default()
+    views = []
+    for edge, seed in ((4, 5), (7, 6), (6, 7), (2, 8)):
+        sc = scenes.lattice_graph(edge, seed=seed, joint_fraction=0.1)
+        c, s = scenes.host_color(sc)
+        views.append(sc.to_view(c, s))
+    views.append(hub_view(27))
+    batch = Batch()
+    batch.upload(views)
+    for packing in (abi.BATCH_MERGED, abi.BATCH_MERGED, abi.BATCH_PERSISTENT, abi.BATCH_MERGED):
+        batch.set_config(packing=packing)
+        batch.step_async(params, DT, 1)
+    got = [v.copy() for v in views]
+    batch.download(got)
+    for v, g in zip(views, got):
+        want = v.copy()
+        for _ in range(4):
+            solver.phys_solve(want, params, DT)
+        assert not helpers.mismatches(g, want)
+    batch.close()
+
+
+def test_merged_packing_refuses_malformed_worlds(solver):
+    from nepheline_b200.solver import Batch
+    params = abi.WorldParams.default()
+    sc = scenes.lattice_graph(3, seed=1)
+    c, s = scenes.host_color(sc)
+    good = sc.to_view(c, s)
+    bad = good.copy()
+    bad.contacts["body_a"][0] = 10_000
+    batch = Batch()
+    batch.set_config(packing=abi.BATCH_MERGED)
     before = bad.copy()
     assert batch.phys_solve_worlds_code([good.copy(), bad], params, DT) == abi.INVALID_ARGUMENT
     assert bad.bodies.tobytes() == before.bodies.tobytes()
