@@ -353,10 +353,14 @@ def run_batched(args):
     nbytes = step_bytes(n, m, pts, nj, params.substeps)
     achieved = nbytes / (ms_rank * 1e-3) / 1e9
     pk = peaks()
+    merged = info.get("packing") == abi.BATCH_MERGED
+    launches = int(info.get("launches_per_step", 1))
     roofline = {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
-                "frac": achieved / pk["hbm_gbs"], "traffic": None, "kernel": "k_worlds",
-                "peak_source": pk["source"], "launches_per_step": 1,
-                "ms_per_launch": ms_rank, "algorithmic_bytes_per_launch": nbytes}
+                "frac": achieved / pk["hbm_gbs"], "traffic": None,
+                "kernel": "whole step, merged packing (a launch per stage and colour)" if merged
+                else "k_worlds (one persistent launch a step)",
+                "peak_source": pk["source"], "launches_per_step": launches,
+                "ms_per_step": ms_rank, "algorithmic_bytes_per_step": nbytes}
 
     # End to end: nph_gpu_phys_solve_worlds on the worlds' records packed in page-locked host
     # arrays (one transfer per record kind each way), every step.
@@ -408,7 +412,7 @@ def run_batched(args):
             "world_steps_per_s": worlds_all / (ms * 1e-3),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms},
-            "gpu_launches": args.steps,
+            "gpu_launches": args.steps * launches,
             "roofline": roofline,
             "cpu_baseline": cpu,
             "clocks": clocks,

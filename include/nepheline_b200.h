@@ -390,7 +390,7 @@ typedef struct NphGpuBatchInfo {
     uint32_t warp_worlds;  /* worlds the current configuration runs on one warp */
     uint32_t block_worlds; /* worlds it runs on a whole block */
     uint32_t packing;
-    uint32_t pad;
+    uint32_t launches_per_step; /* kernel launches a step makes (1 for the persistent packing) */
 } NphGpuBatchInfo;
 
 NPH_GPU_API NphGpuResult nph_gpu_batch_create(const NphGpuSolverDesc *desc, NphGpuBatch **out);

@@ -209,7 +209,7 @@ class BatchInfo(ctypes.Structure):
                 ("shared_velocities", ctypes.c_uint32), ("blocks_per_sm", ctypes.c_uint32),
                 ("items_per_thread", ctypes.c_uint32), ("warp_worlds", ctypes.c_uint32),
                 ("block_worlds", ctypes.c_uint32), ("packing", ctypes.c_uint32),
-                ("pad", ctypes.c_uint32)]
+                ("launches_per_step", ctypes.c_uint32)]
 
 
 class SolverDesc(ctypes.Structure):

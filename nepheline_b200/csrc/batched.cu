@@ -1501,6 +1501,13 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_info(const NphGpuBatch *b, NphGpuBatchInf
     out->blocks_per_sm = b->blocks_per_sm;
     out->items_per_thread = b->items_per_thread;
     out->packing = b->packing;
+    out->launches_per_step = 1u;
+    if (b->packing == NPH_GPU_BATCH_MERGED && b->merged != nullptr) {
+        NphGpuStepStats st;
+        if (nph_gpu_solver_stats(b->merged, &st) == NPH_GPU_OK) {
+            out->launches_per_step = st.launches;
+        }
+    }
     out->warp_worlds = b->class_count[b->classes - 1u];
     out->block_worlds = b->class_count[0];
     return NPH_GPU_OK;

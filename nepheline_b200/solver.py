@@ -382,7 +382,7 @@ class Batch:
     def info(self) -> dict:
         i = abi.BatchInfo()
         _check(self.L.nph_gpu_batch_info(self._h, ctypes.byref(i)), "nph_gpu_batch_info")
-        return {k: getattr(i, k) for k, _ in abi.BatchInfo._fields_ if k != "pad"}
+        return {k: getattr(i, k) for k, _ in abi.BatchInfo._fields_}
 
 
 def version() -> str:
