@@ -33,9 +33,9 @@ NPH_D void copy16(float4 *dst, const float4 *src) { __pipeline_memcpy_async(dst,
 
 // Issues the manifold's loads into the lane's column: the rows of its own points (pt only
 // when `tangents`), the velocities of both bodies, their displacements and rotations when
-// `poses`, and the inertia of the sides that take results.
+// `poses`, and the inertia of the sides that take results. The copies are not committed.
 template <uint32_t kLanes>
-NPH_D void stage_manifold(const DevSolver &S, uint32_t g, uint4 hdr, const Tile<kLanes> &T,
+NPH_D void issue_manifold(const DevSolver &S, uint32_t g, uint4 hdr, const Tile<kLanes> &T,
                           bool tangents, bool poses)
 {
     const uint32_t bits = hdr.z;
@@ -72,6 +72,14 @@ NPH_D void stage_manifold(const DevSolver &S, uint32_t g, uint4 hdr, const Tile<
         copy16(T.at(kSlotIb + 1u), &S.prm[3u * hdr.y + 1u]);
         copy16(T.at(kSlotIb + 2u), &S.prm[3u * hdr.y + 2u]);
     }
+}
+
+// The same, committed and waited for.
+template <uint32_t kLanes>
+NPH_D void stage_manifold(const DevSolver &S, uint32_t g, uint4 hdr, const Tile<kLanes> &T,
+                          bool tangents, bool poses)
+{
+    issue_manifold(S, g, hdr, T, tangents, poses);
     __pipeline_commit();
     __pipeline_wait_prior(0);
 }
@@ -99,7 +107,9 @@ template <uint32_t kLanes> NPH_D Sides staged_sides(const Tile<kLanes> &T, uint3
 }
 
 // warm_manifold (solver_impl.h:181-258) on the staged loads.
-template <uint32_t kLanes>
+// kIssued: the lane's column already holds the manifold's loads (a pipelined pass issued and
+// waited for them).
+template <uint32_t kLanes, bool kIssued = false>
 NPH_D void warm_manifold_staged(const DevSolver &S, uint32_t g, const Tile<kLanes> &T)
 {
     uint4 hdr = S.hdr[g];
@@ -109,7 +119,9 @@ NPH_D void warm_manifold_staged(const DevSolver &S, uint32_t g, const Tile<kLane
     if (pc == 0u) {
         return;
     }
-    stage_manifold(S, g, hdr, T, false, false);
+    if (!kIssued) {
+        stage_manifold(S, g, hdr, T, false, false);
+    }
     const Sides sd = staged_sides(T, bits);
     BodyState a = BodyState{v3(T.get(kSlotVa)), v3(T.get(kSlotWa))};
     BodyState b = BodyState{v3(T.get(kSlotVb)), v3(T.get(kSlotWb))};
@@ -164,7 +176,7 @@ NPH_D void warm_manifold_staged(const DevSolver &S, uint32_t g, const Tile<kLane
 }
 
 // solve_manifold (solver_impl.h:484-602) on the staged loads.
-template <bool kUseBias, uint32_t kLanes>
+template <bool kUseBias, uint32_t kLanes, bool kIssued = false>
 NPH_D void solve_manifold_staged(const DevSolver &S, uint32_t g, const StepConsts &K,
                                  const Tile<kLanes> &T)
 {
@@ -175,7 +187,9 @@ NPH_D void solve_manifold_staged(const DevSolver &S, uint32_t g, const StepConst
     if (pc == 0u) {
         return;
     }
-    stage_manifold(S, g, hdr, T, true, true);
+    if (!kIssued) {
+        stage_manifold(S, g, hdr, T, true, true);
+    }
     const Sides sd = staged_sides(T, bits);
     BodyState a = BodyState{v3(T.get(kSlotVa)), v3(T.get(kSlotWa))};
     BodyState b = BodyState{v3(T.get(kSlotVb)), v3(T.get(kSlotWb))};

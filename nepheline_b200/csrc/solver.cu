@@ -286,6 +286,51 @@ k_pass_staged(DevSolver S, uint32_t cfirst, uint32_t ccount, StepConsts K)
     }
 }
 
+// The staged pass, pipelined: a persistent grid whose blocks walk the colour's manifolds in
+// chunks of one per lane, issuing the next chunk's loads into a second tile before computing
+// the current one, so a warp's loads overlap its arithmetic. A colour's manifolds share no
+// dynamic body, so loads issued ahead read what no other manifold of the colour writes, and
+// each lane reads and writes only its own column of the tiles.
+template <int P, uint32_t kLanes, int kMinBlocks>
+__global__ void __launch_bounds__(kLanes, kMinBlocks)
+k_pass_pipelined(DevSolver S, uint32_t cfirst, uint32_t ccount, StepConsts K)
+{
+    extern __shared__ float4 tiles[];
+    const uint32_t lane = threadIdx.x;
+    const uint32_t chunks = (ccount + kLanes - 1u) / kLanes;
+    const Tile<kLanes> T[2] = {Tile<kLanes>{tiles, lane}, Tile<kLanes>{tiles + kSlots * kLanes, lane}};
+    const bool tangents = P != kWarm;
+    const bool poses = P != kWarm;
+    auto header = [&](uint32_t chunk) -> uint4 {
+        const uint32_t g = chunk * kLanes + lane;
+        return chunk < chunks && g < ccount ? S.hdr[cfirst + g] : make_uint4(0u, 0u, 0u, 0u);
+    };
+    auto issue = [&](uint32_t chunk, uint4 hdr, uint32_t t) {
+        if ((hdr.z & kHdrPointsMask) != 0u) {
+            issue_manifold(S, cfirst + chunk * kLanes + lane, hdr, T[t], tangents, poses);
+        }
+        __pipeline_commit();
+    };
+    uint32_t c = blockIdx.x;
+    issue(c, header(c), 0u);
+    uint4 hdr_next = header(c + gridDim.x);
+    for (uint32_t i = 0; c < chunks; ++i, c += gridDim.x) {
+        const uint32_t next = c + gridDim.x;
+        issue(next, hdr_next, (i + 1u) & 1u);
+        hdr_next = header(next + gridDim.x);
+        __pipeline_wait_prior(1); // this chunk's copies are in
+        const uint32_t g = c * kLanes + lane;
+        if (g < ccount) {
+            if (P == kWarm) {
+                warm_manifold_staged<kLanes, true>(S, cfirst + g, T[i & 1u]);
+            } else {
+                solve_manifold_staged<P == kSolve, kLanes, true>(S, cfirst + g, K, T[i & 1u]);
+            }
+        }
+    }
+    __pipeline_wait_prior(0);
+}
+
 // The pass configurations: threads per block and the blocks per SM the register budget
 // allows (65,536 registers / (threads x blocks)); the last two stage the loads through
 // shared memory (kSlots x threads x 16 bytes per block).
@@ -293,7 +338,8 @@ struct PassConfig {
     uint32_t threads, min_blocks, staged;
 };
 constexpr PassConfig kPassConfigs[] = {{256, 1, 0}, {256, 2, 0}, {128, 4, 0}, {256, 3, 0},
-                                       {64, 6, 1},  {64, 7, 1},  {128, 3, 1}, {32, 14, 1}};
+                                       {64, 6, 1},  {64, 7, 1},  {128, 3, 1}, {32, 14, 1},
+                                       {32, 7, 2},  {64, 3, 2}};
 constexpr uint32_t kPassConfigCount = sizeof(kPassConfigs) / sizeof(kPassConfigs[0]);
 
 template <int P>
@@ -303,6 +349,26 @@ void launch_pass(uint32_t config, uint32_t cc, cudaStream_t st, const DevSolver 
     const uint32_t t = kPassConfigs[config].threads;
     const uint32_t grid = (cc + t - 1) / t;
     const size_t tile = kPassConfigs[config].staged ? (size_t)kSlots * t * sizeof(float4) : 0;
+    if (kPassConfigs[config].staged == 2u) {
+        if (P == kRestitution) { // no loads worth pipelining: the plain kernel
+            k_pass<P, 128, 4><<<(cc + 127u) / 128u, 128, 0, st>>>(S, cfirst, cc, K);
+            return;
+        }
+        // A persistent grid: the SMs times the blocks each holds.
+        static const uint32_t sms = [] {
+            int dev = 0, n = 148;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+            return (uint32_t)n;
+        }();
+        const uint32_t blocks = std::max<uint32_t>(1u, std::min<uint32_t>(grid, sms * kPassConfigs[config].min_blocks));
+        if (config == 8) {
+            k_pass_pipelined<P, 32, 7><<<blocks, 32, 2 * tile, st>>>(S, cfirst, cc, K);
+        } else {
+            k_pass_pipelined<P, 64, 3><<<blocks, 64, 2 * tile, st>>>(S, cfirst, cc, K);
+        }
+        return;
+    }
     switch (config) {
     case 0: k_pass<P, 256, 1><<<grid, 256, 0, st>>>(S, cfirst, cc, K); break;
     case 1: k_pass<P, 256, 2><<<grid, 256, 0, st>>>(S, cfirst, cc, K); break;
@@ -320,6 +386,10 @@ template <int P> void allow_tiles()
 {
     cudaFuncSetAttribute(k_pass_staged<P, 128, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)(kSlots * 128 * sizeof(float4)));
+    if (P != kRestitution) {
+        cudaFuncSetAttribute(k_pass_pipelined<P, 64, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(2 * kSlots * 64 * sizeof(float4)));
+    }
 }
 
 // The overflow: its joints, then its contacts, one at a time in list order (they may share

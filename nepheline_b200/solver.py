@@ -172,6 +172,9 @@ class Solver:
                  "units": arr[i].units, "total_ms": arr[i].total_ms,
                  "algorithmic_bytes": arr[i].algorithmic_bytes} for i in range(n.value)]
 
+    def pass_config_count(self) -> int:
+        return int(self.L.nph_gpu_pass_config_count())
+
     def set_pass_config(self, pass_kind: int, config: int) -> None:
         _check(self.L.nph_gpu_solver_set_pass_config(self._h, pass_kind, config),
                "nph_gpu_solver_set_pass_config")

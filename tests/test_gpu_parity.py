@@ -240,3 +240,29 @@ def test_empty_world_is_a_no_op(solver):
     empty = abi.View(np.zeros(0, abi.BODY_DTYPE), None, np.zeros(0, abi.CONTACT_DTYPE), None,
                      np.zeros(25, np.uint32), np.zeros(25, np.uint32))
     solver.phys_solve(empty, abi.WorldParams.default(), DT)
+
+
+def test_every_pass_configuration_gives_the_same_bits(ref_lib):
+    """Every launch configuration the autotuner chooses from (plain, staged and pipelined
+    kernels) for every pass kind: the same bits as the restatement, on a jointed lattice large
+    enough for the pipelined passes' blocks to walk several chunks, and on a batch world."""
+    from nepheline_b200.solver import Solver
+    from oracle.refworld import port32cr
+    params = abi.WorldParams.default()
+    views = []
+    sc = scenes.lattice_graph((80, 80, 24), seed=3, joint_fraction=0.1)
+    c, s_ = scenes.host_color(sc)
+    views.append(sc.to_view(c, s_))
+    sc = scenes.mixed_world(800, 5)
+    c, s_ = scenes.host_color(sc)
+    views.append(sc.to_view(c, s_))
+    want = [port32cr(v, params, DT) for v in views]
+    solver = Solver(device=0)
+    for config in range(solver.pass_config_count()):
+        for kind in range(4):
+            solver.set_pass_config(kind, config)
+        for v, w in zip(views, want):
+            got = v.copy()
+            solver.phys_solve(got, params, DT)
+            assert not helpers.mismatches(got, w), f"configuration {config}"
+    solver.close()
