@@ -465,6 +465,23 @@ NPH_GPU_API NphGpuResult nph_gpu_graph_color_static(void *stream, const uint32_t
                                                     uint32_t *out_slot);
 
 /* ------------------------------------------------------------------------------------
+ * The contact update on the device
+ * ---------------------------------------------------------------------------------- */
+
+/* The next step's contacts, warm-started on the device from the records the last step
+ * stored, as the reference's contact update does for pairs of convex shapes
+ * (phys_contact_update, contact.c:516-565: by feature id, then by place within twice the
+ * linear slop on both anchors; warm_by_id and warm_by_place, contact.c:332-380). `fresh`
+ * holds this step's manifolds from the narrow phase for the uploaded contacts, in the same
+ * order (normal, surface, points with anchors, separations and ids; impulses zero); each
+ * takes its pair and flags from the uploaded record and, point by point, the impulses last
+ * step's points carry over. Bodies and joints stay on the device: a step that keeps its
+ * contact set needs this and nph_gpu_world_step_async, not a re-upload. Refuses a count
+ * that differs from the uploaded one (NPH_GPU_INVALID_STATE) and point counts outside 1..4. */
+NPH_GPU_API NphGpuResult nph_gpu_world_update_contacts(NphGpuSolver *solver,
+                                                       const NphGpuContact *fresh, uint32_t count);
+
+/* ------------------------------------------------------------------------------------
  * The learned warm start: no counterpart in the reference, whose contact points that are new
  * this step start at zero impulse (contact.c:547-565) and whose persisted points start at
  * their matched impulses. A small network predicts a new point's normal and two friction

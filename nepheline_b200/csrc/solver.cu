@@ -29,6 +29,7 @@
 #include "contacts_staged.cuh"
 #include "joints.cuh"
 #include "learned.cuh"
+#include "warm_match.h"
 
 // The network's inference (mlp.cu): `count` rows, or the first *count_dev of at most
 // max_count rows.
@@ -284,6 +285,21 @@ k_pass_staged(DevSolver S, uint32_t cfirst, uint32_t ccount, StepConsts K)
     } else {
         restitution_manifold(S, cfirst + g, K);
     }
+}
+
+// The contact update for the next step (contact.c:516-565): each contact's record becomes the
+// narrow phase's manifold with its pair, flags and warm-started impulses from the record the
+// last step stored.
+__global__ void __launch_bounds__(128) k_warm_update(NphGpuContact *contacts, const NphGpuContact *fresh,
+                                                     uint32_t m)
+{
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= m) {
+        return;
+    }
+    NphGpuContact out;
+    nph_warm_update(&contacts[g], &fresh[g], &out);
+    contacts[g] = out;
 }
 
 // The staged pass, pipelined: a persistent grid whose blocks walk the colour's manifolds in
@@ -595,6 +611,9 @@ struct NphGpuSolver {
     cudaEvent_t ev[6] = {};
     NphGpuStepStats stats{};
     uint32_t launches = 0;
+    // The contact update's staging of the narrow phase's manifolds (capacity mcap).
+    NphGpuContact *d_fresh = nullptr;
+    uint32_t fresh_cap = 0;
     // The learned warm start: the attached network and its cold-point buffers.
     NphGpuMlp *mlp = nullptr;
     uint32_t lcap = 0;            // cold points the buffers hold
@@ -1328,6 +1347,7 @@ NPH_GPU_API void nph_gpu_solver_destroy(NphGpuSolver *s)
     dfree(s->pt);
     dfree(s->pi);
     dfree(s->jw);
+    dfree(s->d_fresh);
     dfree(s->l_feat);
     dfree(s->l_pred);
     dfree(s->l_scale);
@@ -1620,6 +1640,37 @@ NPH_GPU_API NphGpuResult nph_gpu_solver_stats(const NphGpuSolver *s, NphGpuStepS
 NPH_GPU_API void *nph_gpu_solver_stream(const NphGpuSolver *s)
 {
     return s != nullptr ? (void *)s->stream : nullptr;
+}
+
+NPH_GPU_API NphGpuResult nph_gpu_world_update_contacts(NphGpuSolver *s, const NphGpuContact *fresh,
+                                                       uint32_t count)
+{
+    if (s == nullptr || (count > 0 && fresh == nullptr)) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    if (!s->uploaded || count != s->m) {
+        return NPH_GPU_INVALID_STATE;
+    }
+    if (count == 0) {
+        return NPH_GPU_OK;
+    }
+    for (uint32_t g = 0; g < count; ++g) {
+        if (fresh[g].point_count < 1u || fresh[g].point_count > NPH_GPU_MAX_POINTS) {
+            return NPH_GPU_INVALID_ARGUMENT;
+        }
+    }
+    cudaSetDevice(s->device);
+    if (s->fresh_cap < count) {
+        if (!dalloc(s->d_fresh, s->mcap)) {
+            s->fresh_cap = 0;
+            cudaGetLastError();
+            return NPH_GPU_OUT_OF_MEMORY;
+        }
+        s->fresh_cap = s->mcap;
+    }
+    cudaMemcpyAsync(s->d_fresh, fresh, sizeof(NphGpuContact) * count, cudaMemcpyHostToDevice, s->stream);
+    k_warm_update<<<(count + 127u) / 128u, 128, 0, s->stream>>>(s->d_contacts, s->d_fresh, count);
+    return check_cuda(cudaStreamSynchronize(s->stream));
 }
 
 NPH_GPU_API NphGpuResult nph_gpu_solver_set_warm_start_model(NphGpuSolver *s, NphGpuMlp *mlp)

@@ -64,6 +64,7 @@ def lib() -> ctypes.CDLL:
         "nph_gpu_world_features": (ctypes.c_int32, [_vp, P(abi.WorldParams), ctypes.c_float, _vp,
                                                     _vp, _vp, ctypes.c_uint64]),
         "nph_gpu_solver_set_warm_start_model": (ctypes.c_int32, [_vp, _vp]),
+        "nph_gpu_world_update_contacts": (ctypes.c_int32, [_vp, _vp, _u32]),
         "nph_gpu_world_converge": (ctypes.c_int32, [_vp, P(abi.WorldParams), ctypes.c_float,
                                                     _u32, ctypes.c_float, _u32, ctypes.c_float,
                                                     _vp, _vp, P(abi.ConvergeStats)]),
@@ -178,6 +179,13 @@ class Solver:
     def set_pass_config(self, pass_kind: int, config: int) -> None:
         _check(self.L.nph_gpu_solver_set_pass_config(self._h, pass_kind, config),
                "nph_gpu_solver_set_pass_config")
+
+    def update_contacts(self, fresh: np.ndarray) -> None:
+        """This step's manifolds (one per uploaded contact, same order, impulses zero),
+        warm-started on the device from the records the last step stored."""
+        fresh = np.ascontiguousarray(fresh, abi.CONTACT_DTYPE)
+        _check(self.L.nph_gpu_world_update_contacts(self._h, fresh.ctypes.data, len(fresh)),
+               "nph_gpu_world_update_contacts")
 
     def features(self, params: abi.WorldParams, dt: float):
         """Features (4m x 16), impulse scales and kinds of every point slot of the uploaded

@@ -132,6 +132,82 @@ PORT_API int nph_port32_converge(const NphGpuWorldParams *wp, float dt, const Np
     return converge_f32cr(wp, dt, v, init, tol, max_passes, ref, residuals, passes, cold, impulses);
 }
 
+// The contact update's warm start for pairs of convex shapes (contact.c:332-380, 516-565),
+// contact by contact: `old` last step's record of the pair (point_count 0 for a pair that
+// starts touching), `fresh` the narrow phase's manifold (impulses zero); `out` the manifold
+// with the pair and flags of the old record and the impulses its points carry over: by
+// feature id first (the first old point with the id, claimed or not), then, when a point found
+// no id and an old point is left, the nearest unclaimed old point in point order, its anchors
+// within 2 x the linear slop on both bodies (the larger of the two squared distances).
+PORT_API int nph_port_warm_update(const NphGpuContact *old, const NphGpuContact *fresh, unsigned count,
+                                  NphGpuContact *out)
+{
+    const float reach = 2.0F * 0.005F;
+    for (unsigned g = 0U; g < count; ++g) {
+        const NphGpuContact *o = &old[g];
+        NphGpuContact c = fresh[g];
+        const unsigned oc = o->point_count, nc = c.point_count;
+        if (oc > NPH_GPU_MAX_POINTS || nc > NPH_GPU_MAX_POINTS) {
+            return NPH_GPU_INVALID_ARGUMENT;
+        }
+        c.body_a = o->body_a;
+        c.body_b = o->body_b;
+        c.flags = o->flags;
+        unsigned taken = 0U, open = 0U;
+        for (unsigned i = 0U; i < nc; ++i) {
+            unsigned k = oc;
+            for (unsigned q = 0U; q < oc && k == oc; ++q) {
+                k = o->points[q].id == c.points[i].id ? q : oc;
+            }
+            if (k == oc) {
+                open |= 1U << i;
+                continue;
+            }
+            c.points[i].normal_impulse = o->points[k].normal_impulse;
+            memcpy(c.points[i].tangent_impulse, o->points[k].tangent_impulse, sizeof(float) * 3U);
+            taken |= 1U << k;
+        }
+        const unsigned all = (1U << oc) - 1U;
+        for (unsigned i = 0U; i < nc && open != 0U && taken != all; ++i) {
+            if ((open & (1U << i)) == 0U) {
+                continue;
+            }
+            unsigned pick = NPH_GPU_NULL;
+            float nearest = reach * reach;
+            for (unsigned q = 0U; q < oc; ++q) {
+                if ((taken >> q) & 1U) {
+                    continue;
+                }
+                float da = 0.0F, db = 0.0F;
+                {
+                    const float x = o->points[q].anchor_a[0] - c.points[i].anchor_a[0];
+                    const float y = o->points[q].anchor_a[1] - c.points[i].anchor_a[1];
+                    const float z = o->points[q].anchor_a[2] - c.points[i].anchor_a[2];
+                    da = x * x + y * y + z * z;
+                }
+                {
+                    const float x = o->points[q].anchor_b[0] - c.points[i].anchor_b[0];
+                    const float y = o->points[q].anchor_b[1] - c.points[i].anchor_b[1];
+                    const float z = o->points[q].anchor_b[2] - c.points[i].anchor_b[2];
+                    db = x * x + y * y + z * z;
+                }
+                const float d = da > db ? da : db;
+                if (d < nearest) {
+                    nearest = d;
+                    pick = q;
+                }
+            }
+            if (pick != NPH_GPU_NULL) {
+                c.points[i].normal_impulse = o->points[pick].normal_impulse;
+                memcpy(c.points[i].tangent_impulse, o->points[pick].tangent_impulse, sizeof(float) * 3U);
+                taken |= 1U << pick;
+            }
+        }
+        out[g] = c;
+    }
+    return NPH_GPU_OK;
+}
+
 // The same with the correctly rounded arctangent in the joints' angle rows.
 PORT_API int nph_port32cr_solve(const NphGpuWorldParams *wp, float dt, NphGpuWorldView *v)
 {

@@ -94,6 +94,8 @@ def _port_lib():
         lib.nph_port32_converge.argtypes = [ctypes.POINTER(abi.WorldParams), _f32,
                                             ctypes.POINTER(abi.WorldView), _vp, ctypes.c_double,
                                             ctypes.c_uint, ctypes.c_double, _vp, _vp, _vp, _vp]
+        lib.nph_port_warm_update.restype = ctypes.c_int
+        lib.nph_port_warm_update.argtypes = [_vp, _vp, ctypes.c_uint, _vp]
         lib.nph_port_graph_color.restype = ctypes.c_int
         lib.nph_port_graph_color.argtypes = [_vp, _vp, _vp, _u32, _u32, _vp, _vp]
         _port = lib
@@ -384,3 +386,15 @@ def port32_converge(view, params, dt: float, init=None, tol: float = 1e-4,
     return {"passes": passes.value, "cold_points": cold.value,
             "residuals": res[: passes.value + 1].copy(),
             "impulses": imp[: 12 * len(view.contacts)].reshape(-1, 4, 3)}
+
+
+def port_warm_update(old_contacts: np.ndarray, fresh_contacts: np.ndarray) -> np.ndarray:
+    """The contact update's warm start restated on the CPU, contact by contact."""
+    old_contacts = np.ascontiguousarray(old_contacts, abi.CONTACT_DTYPE)
+    fresh_contacts = np.ascontiguousarray(fresh_contacts, abi.CONTACT_DTYPE)
+    assert len(old_contacts) == len(fresh_contacts)
+    out = np.zeros_like(fresh_contacts)
+    rc = _port_lib().nph_port_warm_update(_p(old_contacts), _p(fresh_contacts), len(out), _p(out))
+    if rc != abi.OK:
+        raise RuntimeError(f"port warm update failed: {rc}")
+    return out

@@ -175,3 +175,47 @@ def test_port_matches_reference_mixed_batch_world(ref_lib, bodies, seed):
         bad = helpers.mismatches(mine, w.export_view())
         assert not bad, f"step {s}: {bad}"
     w.close()
+
+
+def aligned_old(old: abi.View, new: abi.View) -> np.ndarray:
+    """Last step's record of each of this step's contacts, found by its pair (a zero record,
+    no points, for a pair that starts touching)."""
+    by_pair = {(int(c["body_a"]), int(c["body_b"])): c for c in old.contacts}
+    out = np.zeros(len(new.contacts), abi.CONTACT_DTYPE)
+    for i, c in enumerate(new.contacts):
+        rec = by_pair.get((int(c["body_a"]), int(c["body_b"])))
+        if rec is not None:
+            out[i] = rec
+        else:
+            out[i]["body_a"] = c["body_a"]
+            out[i]["body_b"] = c["body_b"]
+    return out
+
+
+def raw_manifolds(view: abi.View) -> np.ndarray:
+    """The narrow phase's manifolds of an updated view: its points without their impulses."""
+    raw = view.contacts.copy()
+    raw["points"]["normal_impulse"] = 0.0
+    raw["points"]["tangent_impulse"] = 0.0
+    return raw
+
+
+def test_port_warm_update_matches_the_reference_contact_update(ref_lib):
+    """contact.c:516-565 on a box pile settling: every contact's warm start, by id and by
+    place, equals the reference's, step after step."""
+    from oracle.refworld import port_warm_update
+    w = ref_scenes.box_pile(count=40, seed=4)
+    old = None
+    carried = 0
+    for s in range(150):
+        w.collide()
+        new = w.export_view()
+        if old is not None and len(new.contacts):
+            got = port_warm_update(aligned_old(old, new), raw_manifolds(new))
+            assert got.tobytes() == new.contacts.tobytes(), f"step {s}"
+            carried += int(np.count_nonzero(new.contacts["points"]["normal_impulse"]))
+        w.solve(DT)
+        w.finish()
+        old = w.export_view()
+    assert carried > 0
+    w.close()
