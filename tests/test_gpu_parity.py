@@ -34,16 +34,22 @@ def gpu_solve(solver, view, params, dt=DT):
     return out
 
 
-def cut_and_compare(solver, w, steps, params, dt=DT, every=1, exact=True):
+def cut_and_compare(solver, w, steps, params, dt=DT, every=1, exact=True, stats=None):
+    """The world steps with the reference's solver; every `every` steps the device solves the
+    same input and its results are compared with the reference's."""
     worst_bits = 1.0
     for s in range(steps):
         w.collide()
+        if s % every:
+            w.solve(dt)
+            w.finish()
+            continue
         vin = w.export_view()
         dev = gpu_solve(solver, vin, params, dt)
+        if stats is not None:
+            stats.append((s, len(vin.bodies), len(vin.contacts), vin.colors_used))
         w.solve(dt)
         w.finish()
-        if s % every:
-            continue
         ref = w.export_view()
         if exact:
             bad = helpers.mismatches(dev, ref)
@@ -266,3 +272,27 @@ def test_every_pass_configuration_gives_the_same_bits(ref_lib):
             solver.phys_solve(got, params, DT)
             assert not helpers.mismatches(got, w), f"configuration {config}"
     solver.close()
+
+
+def test_pyramid_configuration_600_steps_every_step(solver, ref_lib):
+    """The pyramid configuration at its size: 20 rows (210 boxes, +-1 mm jitter) on a ground,
+    600 steps, the device's solve compared with the reference's at every step."""
+    params = abi.WorldParams.default()
+    w = ref_scenes.pyramid(rows=20, jitter=1e-3)
+    bits = cut_and_compare(solver, w, 600, params, every=1)
+    assert bits > 0.999
+    w.close()
+
+
+def test_sphere_pour_configuration_65536_spheres(solver, ref_lib):
+    """The pour configuration at its size: 65,536 spheres (radius 0.5 m, density, friction and
+    restitution seeded per sphere) dropped from a 43 m lattice onto the ground, 300 steps of
+    the reference's collision, the device's solve compared with the reference's every 30 steps
+    (each with tens of thousands of contacts once the pour lands)."""
+    params = abi.WorldParams.default()
+    w = ref_scenes.sphere_pour(count=65536, extent=40.0, workers=-1)
+    stats = []
+    cut_and_compare(solver, w, 300, params, every=30, stats=stats)
+    assert max(c for _, _, c, _ in stats) > 10000
+    assert all(colours <= abi.COLORS for _, _, _, colours in stats)
+    w.close()
