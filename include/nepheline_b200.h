@@ -465,6 +465,49 @@ NPH_GPU_API NphGpuResult nph_gpu_graph_color_static(void *stream, const uint32_t
                                                     uint32_t *out_slot);
 
 /* ------------------------------------------------------------------------------------
+ * The narrow phase's closed-form pairs on the device
+ * ---------------------------------------------------------------------------------- */
+
+/* Convex shapes (NphPhysicsShapeType, geometry.h:38-44, in its order). */
+#define NPH_GPU_SHAPE_SPHERE 0u  /* dims[0]: radius */
+#define NPH_GPU_SHAPE_CAPSULE 1u /* dims[0]: half the core's length (along y), dims[1]: radius */
+#define NPH_GPU_SHAPE_BOX 2u     /* dims: half extents */
+
+typedef struct NphGpuShape {
+    uint32_t type;
+    float dims[3];
+} NphGpuShape;
+
+/* A shape's pose (NphPhysicsPose, types.h:65-68). */
+typedef struct NphGpuPose {
+    float position[3];
+    float rotation[4]; /* x, y, z, w */
+} NphGpuPose;
+
+/* NphPhysicsManifold (collide.h:66-79). */
+typedef struct NphGpuManifoldPoint {
+    float point[3];   /* midway between the surfaces */
+    float separation; /* along the normal; negative when overlapping */
+    uint32_t id;      /* the features that made the point */
+} NphGpuManifoldPoint;
+
+typedef struct NphGpuManifold {
+    float normal[3]; /* from shape A towards shape B */
+    uint32_t point_count;
+    NphGpuManifoldPoint points[NPH_GPU_MAX_POINTS];
+} NphGpuManifold;
+
+/* nph_physics_collide (collide.c:524-535) for `count` pairs (host arrays), on the device, for the
+ * pairs with a closed form: sphere-sphere, capsule-sphere, capsule-capsule and box-sphere, in
+ * either order (collide.c:281-458); each manifold is the same bits as the reference's. Two
+ * boxes, hulls and meshes are the reference's separating-axis and clipping code and are refused
+ * (NPH_GPU_UNSUPPORTED), as is an unknown type. Runs on the current device. */
+NPH_GPU_API NphGpuResult nph_gpu_collide(const NphGpuShape *a, const NphGpuPose *pose_a,
+                                         const NphGpuShape *b, const NphGpuPose *pose_b,
+                                         const float *speculative, uint32_t count,
+                                         NphGpuManifold *out);
+
+/* ------------------------------------------------------------------------------------
  * The contact update on the device
  * ---------------------------------------------------------------------------------- */
 

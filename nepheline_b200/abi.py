@@ -314,3 +314,13 @@ def pack_views(views: list, alloc=None) -> list:
         p._keep = (rb, rf, rc, rj)
         out.append(p)
     return out
+
+
+# The narrow phase's records (nepheline_b200.h).
+SHAPE_SPHERE, SHAPE_CAPSULE, SHAPE_BOX = 0, 1, 2
+SHAPE_DTYPE = np.dtype([("type", "<u4"), ("dims", "<f4", 3)], align=True)
+POSE_DTYPE = np.dtype([("position", "<f4", 3), ("rotation", "<f4", 4)], align=True)
+MANIFOLD_POINT_DTYPE = np.dtype([("point", "<f4", 3), ("separation", "<f4"), ("id", "<u4")],
+                                align=True)
+MANIFOLD_DTYPE = np.dtype([("normal", "<f4", 3), ("point_count", "<u4"),
+                           ("points", MANIFOLD_POINT_DTYPE, MAX_POINTS)], align=True)

@@ -68,6 +68,7 @@ def lib() -> ctypes.CDLL:
         "nph_gpu_world_converge": (ctypes.c_int32, [_vp, P(abi.WorldParams), ctypes.c_float,
                                                     _u32, ctypes.c_float, _u32, ctypes.c_float,
                                                     _vp, _vp, P(abi.ConvergeStats)]),
+        "nph_gpu_collide": (ctypes.c_int32, [_vp, _vp, _vp, _vp, _vp, _u32, _vp]),
         "nph_gpu_batch_create": (ctypes.c_int32, [P(abi.SolverDesc), P(_vp)]),
         "nph_gpu_batch_destroy": (None, [_vp]),
         "nph_gpu_batch_stream": (_vp, [_vp]),
@@ -394,6 +395,22 @@ class Batch:
         i = abi.BatchInfo()
         _check(self.L.nph_gpu_batch_info(self._h, ctypes.byref(i)), "nph_gpu_batch_info")
         return {k: getattr(i, k) for k, _ in abi.BatchInfo._fields_}
+
+
+def collide(a: np.ndarray, pose_a: np.ndarray, b: np.ndarray, pose_b: np.ndarray,
+            speculative: np.ndarray) -> np.ndarray:
+    """The narrow phase's closed-form pairs on the device (nph_gpu_collide)."""
+    a = np.ascontiguousarray(a, abi.SHAPE_DTYPE)
+    b = np.ascontiguousarray(b, abi.SHAPE_DTYPE)
+    pa = np.ascontiguousarray(pose_a, abi.POSE_DTYPE)
+    pb = np.ascontiguousarray(pose_b, abi.POSE_DTYPE)
+    sp = np.ascontiguousarray(speculative, np.float32)
+    n = len(a)
+    assert len(b) == len(pa) == len(pb) == len(sp) == n
+    out = np.zeros(n, abi.MANIFOLD_DTYPE)
+    _check(lib().nph_gpu_collide(a.ctypes.data, pa.ctypes.data, b.ctypes.data, pb.ctypes.data,
+                                 sp.ctypes.data, n, out.ctypes.data), "nph_gpu_collide")
+    return out
 
 
 def version() -> str:

@@ -777,3 +777,46 @@ REF_API void nphref_set_velocity(RefWorld *r, u32 body, const f32 v[3], const f3
     nph_physics_body_set_linear_velocity(r->w, r->bodies[body], nph_vec3(v[0], v[1], v[2]));
     nph_physics_body_set_angular_velocity(r->w, r->bodies[body], nph_vec3(w[0], w[1], w[2]));
 }
+
+/* The reference's narrow phase for `count` pairs of convex shapes (nph_physics_collide,
+ * collide.c:524-535), in the device library's records. */
+REF_API void nphref_collide_pairs(const NphGpuShape *a, const NphGpuPose *pa, const NphGpuShape *b,
+                                  const NphGpuPose *pb, const float *spec, uint32_t count,
+                                  NphGpuManifold *out)
+{
+    for (uint32_t i = 0U; i < count; ++i) {
+        NphPhysicsGeometry g[2];
+        const NphGpuShape *sh[2] = {&a[i], &b[i]};
+        for (uint32_t k = 0U; k < 2U; ++k) {
+            const NphGpuShape *s = sh[k];
+            if (s->type == NPH_GPU_SHAPE_SPHERE) {
+                g[k] = nph_physics_geometry_sphere(s->dims[0]);
+            } else if (s->type == NPH_GPU_SHAPE_CAPSULE) {
+                g[k] = nph_physics_geometry_capsule(s->dims[0], s->dims[1]);
+            } else {
+                g[k] = nph_physics_geometry_box(nph_vec3(s->dims[0], s->dims[1], s->dims[2]));
+            }
+        }
+        const NphPhysicsPose p0 = nph_physics_pose(
+            nph_vec3(pa[i].position[0], pa[i].position[1], pa[i].position[2]),
+            nph_quat(pa[i].rotation[0], pa[i].rotation[1], pa[i].rotation[2], pa[i].rotation[3]));
+        const NphPhysicsPose p1 = nph_physics_pose(
+            nph_vec3(pb[i].position[0], pb[i].position[1], pb[i].position[2]),
+            nph_quat(pb[i].rotation[0], pb[i].rotation[1], pb[i].rotation[2], pb[i].rotation[3]));
+        NphPhysicsManifold m;
+        memset(&m, 0, sizeof m);
+        nph_physics_collide(&g[0], p0, &g[1], p1, spec[i], NULL, &m);
+        memset(&out[i], 0, sizeof out[i]);
+        out[i].normal[0] = m.normal.x;
+        out[i].normal[1] = m.normal.y;
+        out[i].normal[2] = m.normal.z;
+        out[i].point_count = m.point_count;
+        for (uint32_t k = 0U; k < m.point_count; ++k) {
+            out[i].points[k].point[0] = m.points[k].point.x;
+            out[i].points[k].point[1] = m.points[k].point.y;
+            out[i].points[k].point[2] = m.points[k].point.z;
+            out[i].points[k].separation = m.points[k].separation;
+            out[i].points[k].id = m.points[k].id;
+        }
+    }
+}

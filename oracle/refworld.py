@@ -68,6 +68,7 @@ def _ref_lib():
             "nphref_import": (ctypes.c_int, [_vp, ctypes.POINTER(abi.WorldView), _f32]),
             "nphref_stats": (None, [_vp, _vp, _vp, _vp, _vp, _vp]),
             "nphref_set_velocity": (None, [_vp, _u32, _vp, _vp]),
+            "nphref_collide_pairs": (None, [_vp, _vp, _vp, _vp, _vp, _u32, _vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -397,4 +398,16 @@ def port_warm_update(old_contacts: np.ndarray, fresh_contacts: np.ndarray) -> np
     rc = _port_lib().nph_port_warm_update(_p(old_contacts), _p(fresh_contacts), len(out), _p(out))
     if rc != abi.OK:
         raise RuntimeError(f"port warm update failed: {rc}")
+    return out
+
+
+def ref_collide(a, pose_a, b, pose_b, speculative) -> np.ndarray:
+    """The reference's nph_physics_collide for each pair (oracle/_ref)."""
+    a = np.ascontiguousarray(a, abi.SHAPE_DTYPE)
+    b = np.ascontiguousarray(b, abi.SHAPE_DTYPE)
+    pa = np.ascontiguousarray(pose_a, abi.POSE_DTYPE)
+    pb = np.ascontiguousarray(pose_b, abi.POSE_DTYPE)
+    sp = np.ascontiguousarray(speculative, np.float32)
+    out = np.zeros(len(a), abi.MANIFOLD_DTYPE)
+    _ref_lib().nphref_collide_pairs(_p(a), _p(pa), _p(b), _p(pb), _p(sp), len(a), _p(out))
     return out
