@@ -141,3 +141,44 @@ def lattice(edge: int = 6, seed: int = 3, joint_fraction: float = 0.1, params=No
     from oracle.refworld import lattice_world
     return lattice_world(edge, seed=seed, joint_fraction=joint_fraction, params=params,
                          workers=workers)
+
+
+def featured_lattice(edge: int = 8, seed: int = 7, params=None):
+    """The jointed lattice with every body feature the solver stage reads: a tenth of the bodies
+    kinematic and moving, a tenth with lock bits, every body damped (linear and angular, 0-2)
+    and gravity-scaled (-1 to 2), a fifth pushed by forces and torques, a fifth with unequal
+    principal inertias and spin (the gyroscopic step), and some past the angular and linear
+    speed caps."""
+    from oracle.refworld import RefWorld
+    rng = np.random.default_rng(seed)
+    sc = scenes.lattice_graph(edge, seed=seed, joint_fraction=0.15)
+    b = sc.bodies
+    n = len(b)
+    kin = rng.random(n) < 0.1
+    b["type"][kin] = abi.BODY_KINEMATIC
+    b["linear_velocity"][kin] = rng.normal(0.0, 1.0, (int(kin.sum()), 3))
+    b["angular_velocity"][kin] = rng.normal(0.0, 1.0, (int(kin.sum()), 3))
+    locked = (rng.random(n) < 0.1) & ~kin
+    b["locks"][locked] = rng.integers(1, 64, int(locked.sum()))
+    b["linear_damping"] = rng.uniform(0.0, 2.0, n)
+    b["angular_damping"] = rng.uniform(0.0, 2.0, n)
+    b["gravity_scale"] = rng.uniform(-1.0, 2.0, n)
+    pushed = rng.random(n) < 0.2
+    b["force"][pushed] = rng.normal(0.0, 50.0, (int(pushed.sum()), 3))
+    b["torque"][pushed] = rng.normal(0.0, 20.0, (int(pushed.sum()), 3))
+    odd = (rng.random(n) < 0.2) & ~kin
+    inertia = np.zeros((n, 9), np.float32)
+    diag = np.repeat((sc.mass / 6.0)[:, None], 3, axis=1)
+    diag[odd] *= rng.uniform(0.3, 3.0, (int(odd.sum()), 3))
+    inertia[:, 0], inertia[:, 4], inertia[:, 8] = diag[:, 0], diag[:, 1], diag[:, 2]
+    scenes.set_mass(b, sc.mass, inertia)
+    b["angular_velocity"][odd] = rng.normal(0.0, 5.0, (int(odd.sum()), 3))
+    spin = (rng.random(n) < 0.05) & ~kin
+    b["angular_velocity"][spin] = rng.normal(0.0, 300.0, (int(spin.sum()), 3))
+    fast = (rng.random(n) < 0.05) & ~kin
+    b["linear_velocity"][fast] = rng.normal(0.0, 500.0, (int(fast.sum()), 3))
+    w = RefWorld(params or abi.WorldParams.default(), enable_sleep=False)
+    w.add_shapeless_bodies(b, sc.mass)
+    w.add_joints(sc.joints)
+    w.inject_contacts(sc.contacts)
+    return w

@@ -296,3 +296,24 @@ def test_sphere_pour_configuration_65536_spheres(solver, ref_lib):
     assert max(c for _, _, c, _ in stats) > 10000
     assert all(colours <= abi.COLORS for _, _, _, colours in stats)
     w.close()
+
+
+def test_every_body_feature_matches(solver, ref_lib):
+    """Kinematic bodies, locks, damping, gravity scale, forces and torques, unequal inertias
+    (the gyroscopic step) and both speed caps: the device equals the restatement with the
+    correctly rounded angle value for value, and the reference on bodies and contacts (its
+    joint rows differ only by its atan2f rounding)."""
+    from oracle.refworld import port32cr
+    params = abi.WorldParams.default()
+    w = ref_scenes.featured_lattice(edge=9, seed=11)
+    for s in range(12):
+        vin = w.export_view()
+        dev = gpu_solve(solver, vin, params)
+        assert not helpers.mismatches(dev, port32cr(vin, params, DT)), f"step {s}"
+        w.solve(DT)
+        ref = w.export_view()
+        bad = {k: v for k, v in helpers.mismatches(dev, ref).items() if not k.startswith("joint.")}
+        assert not bad, f"step {s}: {bad}"
+        err = helpers.max_normwise_err(dev, ref)
+        assert max(err.values()) < ANGLE_ROUNDING_TOL, f"step {s}: {err}"
+    w.close()

@@ -219,3 +219,23 @@ def test_port_warm_update_matches_the_reference_contact_update(ref_lib):
         old = w.export_view()
     assert carried > 0
     w.close()
+
+
+def test_port_matches_reference_with_every_body_feature(ref_lib):
+    """Kinematic bodies, locks, damping, gravity scale, forces and torques, the gyroscopic step
+    and both speed caps."""
+    from oracle.refworld import port32cr
+    params = abi.WorldParams.default()
+    w = ref_scenes.featured_lattice(edge=7, seed=7)
+    v0 = w.export_view()
+    assert (v0.bodies["type"] == abi.BODY_KINEMATIC).any() and v0.bodies["locks"].any()
+    for s in range(12):
+        vin = w.export_view()
+        mine = port32cr(vin, params, DT)
+        w.solve(DT)
+        err = helpers.max_normwise_err(mine, w.export_view())
+        assert max(err.values()) < 1e-3, f"step {s}: {err}"
+        bad = {k: v for k, v in helpers.mismatches(mine, w.export_view()).items()
+               if not k.startswith("joint.")}
+        assert not bad, f"step {s}: {bad}"
+    w.close()
