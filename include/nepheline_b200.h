@@ -102,8 +102,11 @@ typedef int32_t NphGpuResult;
 #define NPH_GPU_JOINT_BALL 0u
 #define NPH_GPU_JOINT_HINGE 1u
 
-/* Solvers (NphPhysicsSolver, world.h). The device solver runs the soft step. */
+/* Solvers (NphPhysicsSolver, world.h:86-101). The device solver runs the soft step and TGS;
+ * XPBD is refused with NPH_GPU_UNSUPPORTED. The learned warm start is the soft step's: a
+ * TGS step does not apply it, and its feature and convergence calls refuse TGS. */
 #define NPH_GPU_SOLVER_SOFT_STEP 0u
+#define NPH_GPU_SOLVER_TGS 1u
 
 /* ------------------------------------------------------------------------------------
  * Records
@@ -113,7 +116,7 @@ typedef int32_t NphGpuResult;
  * defaults at world.c:85-104. */
 typedef struct NphGpuWorldParams {
     float gravity[3];
-    uint32_t solver; /* NPH_GPU_SOLVER_SOFT_STEP */
+    uint32_t solver; /* NPH_GPU_SOLVER_SOFT_STEP or NPH_GPU_SOLVER_TGS */
     uint32_t substeps;
     float contact_hertz; /* 0: an eighth of the substep rate (solver.c:996-997) */
     float contact_damping_ratio;

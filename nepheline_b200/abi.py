@@ -43,6 +43,7 @@ CONSTRAINT_JOINT = 4
 JOINT_BALL = 0
 JOINT_HINGE = 1
 SOLVER_SOFT_STEP = 0
+SOLVER_TGS = 1
 
 BODY_DTYPE = np.dtype([
     ("center", "<f8", 3), ("origin", "<f8", 3), ("rotation", "<f4", 4),

@@ -307,6 +307,11 @@ __device__ void world_step(const Team &T, const BatchArgs &A, const WorldSlice &
             integrate_position(B, i, K.h);
         }
         T.sync();
+        if (K.solver == NPH_GPU_SOLVER_SOFT_STEP) {
+            world_pass<kRelax>(T, S, W, K);
+        }
+    }
+    if (K.solver == NPH_GPU_SOLVER_TGS) {
         world_pass<kRelax>(T, S, W, K);
     }
     world_pass<kRestitution>(T, S, W, K);
@@ -1282,7 +1287,8 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_step_async(NphGpuBatch *b, const NphGpuWo
         params->substeps > 64u) {
         return NPH_GPU_INVALID_ARGUMENT;
     }
-    if (params->solver != NPH_GPU_SOLVER_SOFT_STEP || params->enable_continuous != 0u) {
+    if ((params->solver != NPH_GPU_SOLVER_SOFT_STEP && params->solver != NPH_GPU_SOLVER_TGS) ||
+        params->enable_continuous != 0u) {
         return NPH_GPU_UNSUPPORTED;
     }
     if (b->world_count == 0) {

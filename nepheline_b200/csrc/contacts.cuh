@@ -261,12 +261,12 @@ NPH_D float separation(const BodyPose &a, const BodyPose &b, V3 ra, V3 rb, float
     return dot(d, n) + adjusted;
 }
 
-// solver_impl.h:471-482 (the soft step's slop is zero).
-NPH_D void normal_row(float s, float inv_h, float soft_bias, float min_bias, float soft_mass,
+// solver_impl.h:471-482 (`slop`: TGS's; the soft step's is zero).
+NPH_D void normal_row(float s, float inv_h, float slop, float soft_bias, float min_bias, float soft_mass,
                       float soft_impulse, float &bias, float &mass_scale, float &impulse_scale)
 {
     const bool apart = s > 0.0f;
-    const float overlap = fmin_ref(s + 0.0f, 0.0f);
+    const float overlap = fmin_ref(s + slop, 0.0f);
     bias = apart ? s * inv_h : fmax_ref(soft_bias * overlap, min_bias);
     mass_scale = apart ? 1.0f : soft_mass;
     impulse_scale = apart ? 0.0f : soft_impulse;
@@ -343,8 +343,8 @@ NPH_D void solve_manifold(const DevSolver &S, uint32_t g, const StepConsts &K)
     for (uint32_t k = 0; k < 4u; ++k) {
         if (k < pc) {
             float bias, mass_scale, impulse_scale;
-            normal_row(separation(pa_, pb_, ra[k], rb[k], adj[k], n), K.inv_h, soft_bias, min_bias,
-                       soft_mass, soft_impulse, bias, mass_scale, impulse_scale);
+            normal_row(separation(pa_, pb_, ra[k], rb[k], adj[k], n), K.inv_h, K.slop, soft_bias,
+                       min_bias, soft_mass, soft_impulse, bias, mass_scale, impulse_scale);
             const float vn = dot(rel_vel(a, b, ra[k], rb[k]), n);
             const float row = nm[k] * mass_scale;
             const float acc = im[k].x;
@@ -356,6 +356,10 @@ NPH_D void solve_manifold(const DevSolver &S, uint32_t g, const StepConsts &K)
             apply2(sd, a, b, delta, n, ra[k], rb[k]);
         }
     }
+    // Under TGS a hit scales the next warm start (solver_impl.h:528-532).
+    if (K.scale_hits != 0u && (bits & kHdrImpact) != 0u) {
+        S.hdr[g].z = bits | kHdrImpacted;
+    }
     const uint32_t gp = (bits >> kHdrGroupShift) & kHdrPointsMask;
     if (gp > 1u && (bits & kHdrImpact) != 0u) {
         // The rows as the pass made them (the bodies have not moved), swept seven more times
@@ -365,7 +369,7 @@ NPH_D void solve_manifold(const DevSolver &S, uint32_t g, const StepConsts &K)
         for (uint32_t k = 0; k < 4u; ++k) {
             if (k < pc) {
                 float mass_scale;
-                normal_row(separation(pa_, pb_, ra[k], rb[k], adj[k], n), K.inv_h, soft_bias,
+                normal_row(separation(pa_, pb_, ra[k], rb[k], adj[k], n), K.inv_h, K.slop, soft_bias,
                            min_bias, soft_mass, soft_impulse, row_bias[k], mass_scale, row_soft[k]);
                 row_mass[k] = nm[k] * mass_scale;
             }
@@ -447,6 +451,11 @@ NPH_D void restitution_manifold(const DevSolver &S, uint32_t g, const StepConsts
     }
     if (!bounced) {
         return;
+    }
+    // Under TGS a bounce is the step's alone, not the next step's warm start
+    // (solver_impl.h:662-665).
+    if (K.scale_hits != 0u) {
+        S.hdr[g].z = bits | kHdrImpacted;
     }
     const Sides sd = load_sides(S.prm, hdr.x, hdr.y, bits);
     BodyState a = load_state(S.vel, hdr.x);

@@ -207,8 +207,8 @@ NPH_D void solve_manifold_staged(const DevSolver &S, uint32_t g, const StepConst
         float4 im = T.get(4u * k + 2u);
         const V3 ra = v3(A), rb = v3(B);
         float bias, mass_scale, impulse_scale;
-        normal_row(separation(pa_, pb_, ra, rb, A.w, n), K.inv_h, soft_bias, min_bias, soft_mass,
-                   soft_impulse, bias, mass_scale, impulse_scale);
+        normal_row(separation(pa_, pb_, ra, rb, A.w, n), K.inv_h, K.slop, soft_bias, min_bias,
+                   soft_mass, soft_impulse, bias, mass_scale, impulse_scale);
         const float vn = dot(rel_vel(a, b, ra, rb), n);
         const float row = B.w * mass_scale;
         const float acc = im.x;
@@ -220,6 +220,9 @@ NPH_D void solve_manifold_staged(const DevSolver &S, uint32_t g, const StepConst
         *T.at(4u * k + 2u) = im;
         apply2(sd, a, b, delta, n, ra, rb);
     }
+    if (K.scale_hits != 0u && (bits & kHdrImpact) != 0u) {
+        S.hdr[g].z = bits | kHdrImpacted;
+    }
     const uint32_t gp = (bits >> kHdrGroupShift) & kHdrPointsMask;
     if (gp > 1u && (bits & kHdrImpact) != 0u) {
         float row_bias[4], row_mass[4], row_soft[4];
@@ -228,8 +231,8 @@ NPH_D void solve_manifold_staged(const DevSolver &S, uint32_t g, const StepConst
             if (k < pc) {
                 const float4 A = T.get(4u * k), B = T.get(4u * k + 1u);
                 float mass_scale;
-                normal_row(separation(pa_, pb_, v3(A), v3(B), A.w, n), K.inv_h, soft_bias, min_bias,
-                           soft_mass, soft_impulse, row_bias[k], mass_scale, row_soft[k]);
+                normal_row(separation(pa_, pb_, v3(A), v3(B), A.w, n), K.inv_h, K.slop, soft_bias,
+                           min_bias, soft_mass, soft_impulse, row_bias[k], mass_scale, row_soft[k]);
                 row_mass[k] = B.w * mass_scale;
             }
         }

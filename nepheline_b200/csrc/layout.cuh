@@ -84,6 +84,9 @@ struct StepConsts {
     Soft contact_soft, static_soft, joint_soft;
     float max_angular_speed_sq, max_linear_speed_sq;
     float gravity[3];
+    float slop;          // TGS: the overlap its Baumgarte bias leaves alone (0: the soft step)
+    uint32_t scale_hits; // TGS: a hit scales the next warm start (solver.c:411-416)
+    uint32_t solver;     // NPH_GPU_SOLVER_*: the stage list (solver.c:1036-1060)
 };
 
 // The body side of a constraint: what the passes read and write of one body.

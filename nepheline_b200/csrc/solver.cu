@@ -532,7 +532,8 @@ static Soft host_make_soft(float hertz, float zeta, float h)
 
 static float minf_ref(float a, float b) { return a < b ? a : b; }
 
-// phys_solve's step constants, solver.c:985-1006 (soft step).
+// phys_solve's step constants, solver.c:985-1017: the soft step's springs, or TGS's rigid
+// rows with a fifth of the error taken back a substep and a linear slop left alone.
 StepConsts make_step_consts(const NphGpuWorldParams &p, float dt)
 {
     StepConsts K;
@@ -554,6 +555,15 @@ StepConsts make_step_consts(const NphGpuWorldParams &p, float dt)
     K.gravity[0] = p.gravity[0];
     K.gravity[1] = p.gravity[1];
     K.gravity[2] = p.gravity[2];
+    K.solver = p.solver;
+    if (p.solver == NPH_GPU_SOLVER_TGS) {
+        const Soft hard = Soft{0.2f * K.inv_h, 1.0f, 0.0f};
+        K.contact_soft = hard;
+        K.static_soft = hard;
+        K.joint_soft = hard;
+        K.slop = 0.005f; // NPH_PHYSICS_LINEAR_SLOP, types.h:38
+        K.scale_hits = 1u;
+    }
     return K;
 }
 
@@ -876,8 +886,8 @@ FeatureConsts feature_consts(const StepConsts &K)
 // predictions, and the predictions written as their warm-start impulses.
 void enqueue_learned_init(NphGpuSolver *s, const StepConsts &K)
 {
-    if (s->mlp == nullptr || s->m == 0u || s->lcap == 0u) {
-        return;
+    if (s->mlp == nullptr || s->m == 0u || s->lcap == 0u || K.solver != NPH_GPU_SOLVER_SOFT_STEP) {
+        return; // the model is the soft step's; TGS warm-starts as the reference does
     }
     const DevSolver S = dev_solver(s);
     cudaMemsetAsync(s->l_counts, 0, 2 * sizeof(uint32_t), s->stream);
@@ -907,8 +917,13 @@ void enqueue_step(NphGpuSolver *s, const StepConsts &K, uint32_t substeps)
         mark_begin(s, kKIntegratePosition, s->n, 84.0 * n);
         k_integrate_position<<<blocks_for(s->n), kBlock, 0, s->stream>>>(B, s->n, K.h);
         mark_end(s);
-        enqueue_pass<kRelax>(s, K);
+        if (K.solver == NPH_GPU_SOLVER_SOFT_STEP) {
+            enqueue_pass<kRelax>(s, K);
+        }
         s->launches += 2;
+    }
+    if (K.solver == NPH_GPU_SOLVER_TGS) {
+        enqueue_pass<kRelax>(s, K); // TGS's velocity iteration: the bias velocity taken back once
     }
     enqueue_pass<kRestitution>(s, K);
     if (s->m > 0u) {
@@ -990,10 +1005,18 @@ NphGpuResult validate_params(const NphGpuWorldParams *p, float dt)
     if (p == nullptr || !(dt > 0.0f) || p->substeps == 0u || p->substeps > 64u) {
         return NPH_GPU_INVALID_ARGUMENT;
     }
-    if (p->solver != NPH_GPU_SOLVER_SOFT_STEP || p->enable_continuous != 0u) {
+    if ((p->solver != NPH_GPU_SOLVER_SOFT_STEP && p->solver != NPH_GPU_SOLVER_TGS) ||
+        p->enable_continuous != 0u) {
         return NPH_GPU_UNSUPPORTED;
     }
     return NPH_GPU_OK;
+}
+
+// The learned warm start and its convergence runs are the soft step's.
+static NphGpuResult validate_soft_params(const NphGpuWorldParams *p, float dt)
+{
+    const NphGpuResult r = validate_params(p, dt);
+    return r == NPH_GPU_OK && p->solver != NPH_GPU_SOLVER_SOFT_STEP ? NPH_GPU_UNSUPPORTED : r;
 }
 
 NphGpuResult validate_view(const NphGpuWorldView *v)
@@ -1691,7 +1714,7 @@ NPH_GPU_API NphGpuResult nph_gpu_world_features(NphGpuSolver *s, const NphGpuWor
     if (s == nullptr) {
         return NPH_GPU_INVALID_ARGUMENT;
     }
-    NphGpuResult r = validate_params(params, dt);
+    NphGpuResult r = validate_soft_params(params, dt);
     if (r != NPH_GPU_OK) {
         return r;
     }
@@ -1742,7 +1765,7 @@ NPH_GPU_API NphGpuResult nph_gpu_world_converge(NphGpuSolver *s, const NphGpuWor
     if (s == nullptr || out == nullptr || !(tolerance > 0.0f) || max_passes > 1000000u) {
         return NPH_GPU_INVALID_ARGUMENT;
     }
-    NphGpuResult r = validate_params(params, dt);
+    NphGpuResult r = validate_soft_params(params, dt);
     if (r != NPH_GPU_OK) {
         return r;
     }

@@ -59,7 +59,8 @@ static float atan2_cr(float y, float x) { return (float)atan2((double)y, (double
 // counts that add up, supported joint types and settings.
 static int check_view(const NphGpuWorldParams *wp, const NphGpuWorldView *v)
 {
-    if (wp == NULL || v == NULL || wp->substeps == 0U || wp->solver != NPH_GPU_SOLVER_SOFT_STEP) {
+    if (wp == NULL || v == NULL || wp->substeps == 0U ||
+        (wp->solver != NPH_GPU_SOLVER_SOFT_STEP && wp->solver != NPH_GPU_SOLVER_TGS)) {
         return NPH_GPU_INVALID_ARGUMENT;
     }
     const unsigned total = v->body_count + v->fixed_count;
@@ -128,6 +129,9 @@ PORT_API int nph_port32_converge(const NphGpuWorldParams *wp, float dt, const Np
     const int bad = check_view(wp, v);
     if (bad != NPH_GPU_OK) {
         return bad;
+    }
+    if (wp->solver != NPH_GPU_SOLVER_SOFT_STEP) {
+        return NPH_GPU_UNSUPPORTED; // the residual-driven mode is the soft step's
     }
     return converge_f32cr(wp, dt, v, init, tol, max_passes, ref, residuals, passes, cold, impulses);
 }

@@ -257,6 +257,9 @@ typedef struct FN(Joint) { // the step data of PhysJoint, world_internal.h:317-3
 typedef struct FN(Step) { // StepContext, solver.c:67-85
     REAL dt, h, inv_h, push_max, restitution_threshold;
     FN(Soft) contact_soft, static_soft, joint_soft;
+    REAL slop;           // TGS's linear slop (solver.c:1016); 0 for the soft step
+    unsigned scale_hits; // TGS: a hit scales the next warm start (solver.c:411-416)
+    unsigned solver;     // the stage list (solver.c:1036-1060)
     unsigned dummy;
     FN(Body) *bodies;
     FN(Param) *params;
@@ -603,11 +606,12 @@ static REAL FN(separation)(const FN(Body) *a, const FN(Body) *b, const FN(Point)
 }
 
 // solver_impl.h:471-482 (the soft step's slop is zero).
-static void FN(normal_row)(REAL sep, REAL inv_h, REAL soft_bias, REAL min_bias, REAL soft_mass,
-                           REAL soft_impulse, REAL *bias, REAL *mass_scale, REAL *impulse_scale)
+static void FN(normal_row)(REAL sep, REAL inv_h, REAL slop, REAL soft_bias, REAL min_bias,
+                           REAL soft_mass, REAL soft_impulse, REAL *bias, REAL *mass_scale,
+                           REAL *impulse_scale)
 {
     const int apart = sep > R(0);
-    const REAL overlap = FN(min)(sep + R(0), R(0));
+    const REAL overlap = FN(min)(sep + slop, R(0));
     *bias = apart ? sep * inv_h : FN(max)(soft_bias * overlap, min_bias);
     *mass_scale = apart ? R(1) : soft_mass;
     *impulse_scale = apart ? R(0) : soft_impulse;
@@ -627,8 +631,8 @@ static void FN(solve)(FN(Step) *s, FN(Manifold) *m, int use_bias)
         REAL bias;
         REAL mass_scale;
         REAL impulse_scale;
-        FN(normal_row)(FN(separation)(&a, &b, p, m->n), s->inv_h, soft_bias, min_bias, soft_mass,
-                       soft_impulse, &bias, &mass_scale, &impulse_scale);
+        FN(normal_row)(FN(separation)(&a, &b, p, m->n), s->inv_h, s->slop, soft_bias, min_bias,
+                       soft_mass, soft_impulse, &bias, &mass_scale, &impulse_scale);
         const REAL vn = FN(dot)(FN(relative_velocity)(&a, &b, p->ra, p->rb), m->n);
         const REAL row = p->normal_mass * mass_scale;
         const REAL acc = p->normal_impulse;
@@ -639,14 +643,18 @@ static void FN(solve)(FN(Step) *s, FN(Manifold) *m, int use_bias)
         p->max_normal_impulse = FN(max)(p->max_normal_impulse, total);
         FN(apply)(&a, &b, m->ma, m->mb, delta, m->n, p->ang_a[0], p->ang_b[0]);
     }
+    if (s->scale_hits != 0U && m->impact) {
+        m->impacted = 1U; // solver_impl.h:528-532
+    }
     if (m->group_points > 1U && m->impact) {
         REAL row_bias[4];
         REAL row_mass[4];
         REAL row_soft[4];
         for (unsigned k = 0U; k < m->point_count; ++k) {
             REAL mass_scale;
-            FN(normal_row)(FN(separation)(&a, &b, &m->p[k], m->n), s->inv_h, soft_bias, min_bias,
-                           soft_mass, soft_impulse, &row_bias[k], &mass_scale, &row_soft[k]);
+            FN(normal_row)(FN(separation)(&a, &b, &m->p[k], m->n), s->inv_h, s->slop, soft_bias,
+                           min_bias, soft_mass, soft_impulse, &row_bias[k], &mass_scale,
+                           &row_soft[k]);
             row_mass[k] = m->p[k].normal_mass * mass_scale;
         }
         for (unsigned sweep = 0U; sweep < 7U; ++sweep) { // PHYS_IMPACT_SWEEPS
@@ -700,6 +708,9 @@ static void FN(restitution)(FN(Step) *s, FN(Manifold) *m)
     }
     if (!bounced) {
         return;
+    }
+    if (s->scale_hits != 0U) {
+        m->impacted = 1U; // solver_impl.h:662-665
     }
     FN(Body) a = s->bodies[m->ia];
     FN(Body) b = s->bodies[m->ib];
@@ -1183,6 +1194,15 @@ static int FN(setup)(FN(Step) *sp, const NphGpuWorldParams *wp, float dt, const 
     s.contact_soft = FN(make_soft)(hertz, R(wp->contact_damping_ratio), s.h);
     s.static_soft = FN(make_soft)(R(2.0F) * hertz, R(wp->contact_damping_ratio), s.h);
     s.joint_soft = FN(make_soft)(FN(min)(joint_hertz, R(0.25F) * s.inv_h), R(wp->joint_damping_ratio), s.h);
+    s.solver = wp->solver;
+    if (wp->solver == NPH_GPU_SOLVER_TGS) { // solver.c:1007-1017
+        const FN(Soft) hard = {R(0.2F) * s.inv_h, R(1), R(0)};
+        s.contact_soft = hard;
+        s.static_soft = hard;
+        s.joint_soft = hard;
+        s.slop = R(0.005F); // NPH_PHYSICS_LINEAR_SLOP
+        s.scale_hits = 1U;
+    }
     s.bodies = (FN(Body) *)calloc((size_t)n + 1U, sizeof(FN(Body)));
     s.params = (FN(Param) *)calloc((size_t)n + 1U, sizeof(FN(Param)));
     s.m = (FN(Manifold) *)calloc((size_t)v->contact_count + 1U, sizeof(FN(Manifold)));
@@ -1249,7 +1269,12 @@ static int FN(run)(const NphGpuWorldParams *wp, float dt, const NphGpuWorldView 
         for (unsigned i = 0U; i < n; ++i) {
             FN(integrate_position)(&s, i);
         }
-        FN(contact_pass)(&s, v, FN(PASS_RELAX));
+        if (s.solver == NPH_GPU_SOLVER_SOFT_STEP) {
+            FN(contact_pass)(&s, v, FN(PASS_RELAX));
+        }
+    }
+    if (s.solver == NPH_GPU_SOLVER_TGS) {
+        FN(contact_pass)(&s, v, FN(PASS_RELAX)); // TGS's one velocity pass without bias
     }
     FN(contact_pass)(&s, v, FN(PASS_RESTITUTION));
     free(s.params);

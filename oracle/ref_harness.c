@@ -75,7 +75,7 @@ REF_API RefWorld *nphref_world_create(const NphGpuWorldParams *p, u32 enable_sle
     NphPhysicsWorldDesc d = nph_physics_world_desc_default();
     d.alloc = nph_allocator_system();
     d.gravity = nph_vec3(p->gravity[0], p->gravity[1], p->gravity[2]);
-    d.solver = NPH_PHYSICS_SOLVER_SOFT_STEP;
+    d.solver = (NphPhysicsSolver)p->solver;
     d.substeps = p->substeps;
     d.contact_hertz = p->contact_hertz;
     d.contact_damping_ratio = p->contact_damping_ratio;
