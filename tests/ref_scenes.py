@@ -155,6 +155,9 @@ def featured_lattice(edge: int = 8, seed: int = 7, params=None):
     b = sc.bodies
     n = len(b)
     kin = rng.random(n) < 0.1
+    # The reference creates no joint between two bodies that are not dynamic.
+    both = kin[sc.joints["body_a"]] & kin[sc.joints["body_b"]]
+    kin[sc.joints["body_b"][both]] = False
     b["type"][kin] = abi.BODY_KINEMATIC
     b["linear_velocity"][kin] = rng.normal(0.0, 1.0, (int(kin.sum()), 3))
     b["angular_velocity"][kin] = rng.normal(0.0, 1.0, (int(kin.sum()), 3))
