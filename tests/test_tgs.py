@@ -135,7 +135,8 @@ def test_device_matches_reference_under_tgs(solver, ref_lib, kind):
 
 
 @pytest.mark.gpu
-def test_device_matches_the_restatement_under_tgs_every_pass_configuration(solver, ref_lib):
+def test_device_matches_the_restatement_under_tgs_every_pass_configuration(ref_lib):
+    from nepheline_b200.solver import Solver
     from oracle.refworld import port32cr
     w = ref_scenes.box_pile(count=40, params=tgs())
     for _ in range(30):
@@ -143,12 +144,14 @@ def test_device_matches_the_restatement_under_tgs_every_pass_configuration(solve
     w.collide()
     vin = w.export_view()
     want = port32cr(vin, tgs(), DT)
-    for c in range(solver.pass_config_count()):
-        solver.set_pass_config(c)
+    solver = Solver(device=0)
+    for config in range(solver.pass_config_count()):
+        for kind in range(4):
+            solver.set_pass_config(kind, config)
         v = vin.copy()
         solver.phys_solve(v, tgs(), DT)
-        assert not helpers.mismatches(v, want), f"pass config {c}"
-    solver.set_pass_config(0)
+        assert not helpers.mismatches(v, want), f"pass config {config}"
+    solver.close()
     w.close()
 
 
