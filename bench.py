@@ -62,9 +62,26 @@ def parse():
     ap.add_argument("--train-batches", type=int, default=2)
     ap.add_argument("--max-passes", type=int, default=2000)
     ap.add_argument("--epochs", type=int, default=30)
+    ap.add_argument("--solver", choices=("soft_step", "tgs"), default="soft_step",
+                    help="the world's solver (lattice and batched workloads; learned: soft step)")
     ap.add_argument("--pass-config", default=None,
                     help="fixed pass configurations warm,solve,relax,restitution (no autotuner)")
     return ap.parse_args()
+
+
+def world_params(args):
+    from nepheline_b200 import abi
+    return abi.WorldParams.default(
+        solver=abi.SOLVER_TGS if getattr(args, "solver", "soft_step") == "tgs" else abi.SOLVER_SOFT_STEP)
+
+
+def passes_per_step(params) -> int:
+    """Contact passes that count as solves: solve and relax per substep for the soft step;
+    solve per substep and one relax after them for TGS (solver.c:1036-1060)."""
+    from nepheline_b200 import abi
+    if params.solver == abi.SOLVER_TGS:
+        return params.substeps + 1
+    return 2 * params.substeps
 
 
 def peaks() -> dict:
@@ -187,11 +204,9 @@ def pinned_copy(view):
     return v
 
 
-def reference_sample(dims, steps: int, warmup: int, workers: int) -> dict:
+def reference_sample(dims, steps: int, warmup: int, workers: int, params) -> dict:
     """The reference's phys_solve on its job system over a dims lattice (the same scene)."""
-    from nepheline_b200 import abi
     from oracle.refworld import lattice_world
-    params = abi.WorldParams.default()
     w, sc = lattice_world(dims, seed=0, joint_fraction=0.1, params=params, workers=workers)
     for _ in range(warmup):
         w.solve(DT)
@@ -202,7 +217,8 @@ def reference_sample(dims, steps: int, warmup: int, workers: int) -> dict:
     threads = w.workers + 1 if w.workers > 0 else 1
     manifolds = len(sc.contacts)
     w.close()
-    return {"value": 8.0 * manifolds / sec, "ms_per_step": 1e3 * sec, "threads": threads,
+    return {"value": passes_per_step(params) * manifolds / sec, "ms_per_step": 1e3 * sec,
+            "threads": threads,
             "manifolds": manifolds, "bodies": len(sc.bodies), "dims": tuple(dims)}
 
 
@@ -234,7 +250,7 @@ def run_reference(args):
     sample = list(dims)
     while sample[2] > 4 and est(sample) * (args.steps + args.warmup) > 150.0:
         sample[2] = max(4, int(sample[2] * 0.75))
-    r = reference_sample(sample, args.steps, args.warmup, workers=-1)
+    r = reference_sample(sample, args.steps, args.warmup, workers=-1, params=world_params(args))
     sample_txt = (f"{sample[0]}x{sample[1]}x{sample[2]} lattice ({r['bodies']} bodies, "
                   f"{r['manifolds']} manifolds), {args.steps} timed steps after {args.warmup}; "
                   f"{cpu_model()}")
@@ -244,7 +260,7 @@ def run_reference(args):
         "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": workload_name(dims), "dims": dims, "sample_dims": sample,
-                   "substeps": 4, "dt": DT},
+                   "substeps": 4, "dt": DT, "solver": args.solver},
         "cpu_baseline": {"value": r["value"], "unit": UNIT, "cores": r["threads"],
                          "kind": "reference", "sample": sample_txt},
         "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
@@ -254,13 +270,13 @@ def run_reference(args):
     return 0
 
 
-def step_bytes(n: int, m: int, points: int, nj: int, substeps: int) -> float:
+def step_bytes(n: int, m: int, points: int, nj: int, substeps: int, relax_passes: int) -> float:
     """Algorithmic bytes of one solver step: each stage's records read and written once
     (bodies n, manifolds m with `points` contact points, joints nj)."""
-    per_sub = (84.0 * n) * 2 + 120.0 * points + (224.0 * m + 148.0 * points) \
-        + (212.0 * m + 148.0 * points) + 3 * 330.0 * nj
-    return (368.0 * n + 330.0 * nj + 936.0 * m + substeps * per_sub + 40.0 * m + 160.0 * m
-            + 330.0 * nj + 200.0 * n)
+    per_sub = (84.0 * n) * 2 + 120.0 * points + (224.0 * m + 148.0 * points) + 2 * 330.0 * nj
+    relax = 212.0 * m + 148.0 * points + 330.0 * nj
+    return (368.0 * n + 330.0 * nj + 936.0 * m + substeps * per_sub + relax_passes * relax
+            + 40.0 * m + 160.0 * m + 330.0 * nj + 200.0 * n)
 
 
 def reference_worlds_sample(scs, params, budget_s: float = 20.0) -> dict:
@@ -272,7 +288,7 @@ def reference_worlds_sample(scs, params, budget_s: float = 20.0) -> dict:
     from oracle.refworld import scene_world
     cores = os.cpu_count() or 1
     worlds = [scene_world(sc, params) for sc in scs]
-    solves = [8.0 * len(sc.contacts) for sc in scs]
+    solves = [passes_per_step(params) * len(sc.contacts) for sc in scs]
 
     def run(i):
         worlds[i].solve(DT)
@@ -303,7 +319,7 @@ def run_batched(args):
 
     rank, world, local, pg = dist_setup(args.gpus)
     torch.cuda.set_device(local)
-    params = abi.WorldParams.default()
+    params = world_params(args)
     clk = Clocks(local).__enter__()
     t_build = time.perf_counter()
     scs = scenes.batched_worlds(args.worlds, seed=0, shard=rank, shards=world)
@@ -315,7 +331,7 @@ def run_batched(args):
     m = sum(len(v.contacts) for v in views)
     nj = sum(len(v.joints) for v in views)
     pts = int(sum(int(v.contacts["point_count"].sum()) for v in views))
-    solves_per_step = 2 * params.substeps * m
+    solves_per_step = passes_per_step(params) * m
 
     batch = Batch(device=local)
     stream = torch.cuda.ExternalStream(batch.stream, device=local)
@@ -350,7 +366,8 @@ def run_batched(args):
     solves_all, worlds_all = float(total[0]), float(total[1])
     value = solves_all / (ms * 1e-3)
     info = batch.info()
-    nbytes = step_bytes(n, m, pts, nj, params.substeps)
+    nbytes = step_bytes(n, m, pts, nj, params.substeps,
+                        passes_per_step(params) - params.substeps)
     achieved = nbytes / (ms_rank * 1e-3) / 1e9
     pk = peaks()
     merged = info.get("packing") == abi.BATCH_MERGED
@@ -405,7 +422,7 @@ def run_batched(args):
                                    f"box piles, capsule hinge chains on a ground), body counts "
                                    f"log-uniform in 8-4096",
                        "worlds": int(worlds_all), "bodies_rank0": n, "manifolds_rank0": m,
-                       "joints_rank0": nj, "substeps": params.substeps, "dt": DT,
+                       "joints_rank0": nj, "substeps": params.substeps, "dt": DT, "solver": args.solver,
                        "parallelism": f"worlds sharded x{world}", "tuning": tuned,
                        "batch_info": info, "scene_build_s": build_s,
                        "l2": "inputs larger than L2"},
@@ -522,11 +539,11 @@ def main():
     solver = Solver(device=local)
     # The solver launches on its own stream: the events are recorded on that stream.
     stream = torch.cuda.ExternalStream(solver.stream, device=local)
-    params = abi.WorldParams.default()
+    params = world_params(args)
     clk = Clocks(local).__enter__()
     sc, view = build_view(dims, seed=rank, solver=solver)
     manifolds = len(view.contacts)
-    solves_per_step = 2 * params.substeps * manifolds
+    solves_per_step = passes_per_step(params) * manifolds
 
     # Device-resident steps: the autotuner's timed steps, then the warm-up.
     solver.upload(view)
@@ -607,8 +624,8 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import refworld
         if refworld.ref_available():
-            r = reference_sample((128, 128, 16), steps=8, warmup=1, workers=-1)
-            r1 = reference_sample((128, 128, 8), steps=4, warmup=1, workers=0)
+            r = reference_sample((128, 128, 16), steps=8, warmup=1, workers=-1, params=params)
+            r1 = reference_sample((128, 128, 8), steps=4, warmup=1, workers=0, params=params)
             cpu = {"value": r["value"], "unit": UNIT, "cores": r["threads"], "kind": "reference",
                    "sample": f"128x128x16 slab of the lattice ({r['bodies']} bodies, "
                              f"{r['manifolds']} manifolds), 8 steps of the reference phys_solve "
@@ -626,7 +643,8 @@ def main():
             for _ in range(3):
                 v = port32(v, params, DT)
             sec = (time.perf_counter() - t0) / 3
-            cpu = {"value": 8.0 * len(small.contacts) / sec, "unit": UNIT, "cores": 1,
+            cpu = {"value": passes_per_step(params) * len(small.contacts) / sec, "unit": UNIT,
+                   "cores": 1,
                    "kind": "port", "sample": "32^3 lattice, 3 steps of the FP32 restatement"}
 
     if rank == 0:
@@ -638,6 +656,7 @@ def main():
             "config": {"workload": workload_name(dims),
                        "bodies": len(view.bodies), "manifolds": manifolds,
                        "joints": len(view.joints), "colors": view.colors_used, "substeps": 4,
+                       "solver": args.solver,
                        "dt": DT, "parallelism": f"replicas x{world}",
                        "pass_configs": tuned,
                        "l2": "inputs larger than L2 (about 2 GB of manifold rows per step)"},
