@@ -183,6 +183,7 @@ def test_learned_calls_refuse_tgs(solver):
     from nepheline_b200.solver import SolverError
     sc = scenes.lattice_graph(3, seed=1)
     v = sc.to_view(*scenes.host_color(sc))
-    solver.phys_solve(v.copy(), tgs(), DT)
+    solver.upload(v)
     with pytest.raises(SolverError):
         solver.features(tgs(), DT)
+    solver.features(abi.WorldParams.default(), DT)
