@@ -97,10 +97,34 @@ typedef int32_t NphGpuResult;
 #define NPH_GPU_CONSTRAINT_B_DYNAMIC 2u
 #define NPH_GPU_CONSTRAINT_JOINT 4u
 
-/* Joint types (NphPhysicsJointType, joint.h). The device solver runs ball and hinge
- * joints; the world's other types are refused with NPH_GPU_UNSUPPORTED. */
+/* Joint types (NphPhysicsJointType, joint.h:60-68): the device solver runs all six. */
 #define NPH_GPU_JOINT_BALL 0u
 #define NPH_GPU_JOINT_HINGE 1u
+#define NPH_GPU_JOINT_FIXED 2u
+#define NPH_GPU_JOINT_SLIDER 3u
+#define NPH_GPU_JOINT_DISTANCE 4u
+#define NPH_GPU_JOINT_D6 5u
+
+/* How a 6-DOF joint's axis moves (NphPhysicsAxisMotion, joint.h:144-148), and its axes in A's
+ * frame: translation along X, Y, Z, then twist about X and swing about Y and Z. */
+#define NPH_GPU_AXIS_LOCKED 0u
+#define NPH_GPU_AXIS_LIMITED 1u
+#define NPH_GPU_AXIS_FREE 2u
+#define NPH_GPU_D6_AXES 6u
+
+/* A slider's, 6-DOF joint's or distance joint's rows per axis (PHYS_ROW_*,
+ * world_internal.h:273-278): the lock or lower limit, the upper limit, the motor, the spring. */
+#define NPH_GPU_ROW_LOCK 0u
+#define NPH_GPU_ROW_UPPER 1u
+#define NPH_GPU_ROW_MOTOR 2u
+#define NPH_GPU_ROW_SPRING 3u
+
+/* Joint flags, in and out: the blocks a slider or 6-DOF joint solved its rows as last step
+ * (PHYS_JOINT_BLOCK_*, joint_solver.c:103-112). A change of block zeroes the block's
+ * accumulated impulse, whose meaning changes with it. */
+#define NPH_GPU_JOINT_BLOCK_ROTATION (1u << 11)
+#define NPH_GPU_JOINT_BLOCK_SWING (1u << 12)
+#define NPH_GPU_JOINT_BLOCK_POINT (1u << 13)
 
 /* Solvers (NphPhysicsSolver, world.h:86-101). The device solver runs the soft step and TGS;
  * XPBD is refused with NPH_GPU_UNSUPPORTED. The learned warm start is the soft step's: a
@@ -207,13 +231,55 @@ typedef struct NphGpuHingeJoint {
     float spring_target;
 } NphGpuHingeJoint;
 
+/* Slider joint settings (NphPhysicsSliderJoint, joint.h:107-121): along A's X axis. */
+typedef struct NphGpuSliderJoint {
+    uint32_t enable_limit;
+    float lower;
+    float upper;
+    uint32_t enable_motor;
+    float motor_speed;
+    float max_motor_force;
+    uint32_t enable_spring;
+    float spring_hertz;
+    float spring_damping_ratio;
+    float spring_target;
+} NphGpuSliderJoint;
+
+/* Distance joint settings (NphPhysicsDistanceJoint, joint.h:128-140). */
+typedef struct NphGpuDistanceJoint {
+    float length;
+    uint32_t enable_limit;
+    float min_length;
+    float max_length;
+    uint32_t enable_spring;
+    float spring_hertz;
+    float spring_damping_ratio;
+    uint32_t enable_motor;
+    float motor_speed;
+    float max_motor_force;
+} NphGpuDistanceJoint;
+
+/* One axis of a 6-DOF joint (NphPhysicsD6Axis, joint.h:152-163). */
+typedef struct NphGpuD6Axis {
+    uint32_t motion; /* NPH_GPU_AXIS_* */
+    float lower;
+    float upper;
+    uint32_t enable_motor;
+    float motor_speed;
+    float max_motor_force;
+    uint32_t enable_spring;
+    float spring_hertz;
+    float spring_damping_ratio;
+    float spring_target;
+} NphGpuD6Axis;
+
 /* A joint of the constraint graph, as PhysJoint (world_internal.h:280-330): its frames
  * in the bodies' frames, its settings, and its accumulated impulses (in and out). */
 typedef struct NphGpuJoint {
-    uint32_t type;              /* NPH_GPU_JOINT_BALL or NPH_GPU_JOINT_HINGE */
+    uint32_t type;              /* NPH_GPU_JOINT_* */
     uint32_t body_a;            /* as NphGpuContact */
     uint32_t body_b;
-    uint32_t pad0;
+    uint32_t flags;             /* NPH_GPU_JOINT_BLOCK_*: in and out */
     float frame_a_position[3];  /* in body A's frame (its origin) */
     float frame_a_rotation[4];
     float frame_b_position[3];
@@ -221,15 +287,19 @@ typedef struct NphGpuJoint {
     union {
         NphGpuBallJoint ball;
         NphGpuHingeJoint hinge;
+        NphGpuSliderJoint slider;
+        NphGpuDistanceJoint distance;
+        NphGpuD6Axis d6[NPH_GPU_D6_AXES];
     } u;
-    float linear_impulse[3];
-    float angular_impulse[3];
+    float linear_impulse[3];    /* the anchors as one block, world */
+    float angular_impulse[3];   /* the hinge's or swing block's two rows, or a world vector */
     float friction_impulse[3];
     float lower_impulse;
     float upper_impulse;
     float swing_impulse;
     float motor_impulse;
     float spring_impulse;
+    float axis_impulse[NPH_GPU_D6_AXES][4]; /* NPH_GPU_ROW_* per axis (distance: axis 0) */
 } NphGpuJoint;
 
 /* The solver stage's part of a world. The arrays are the caller's; a solve updates
@@ -285,9 +355,9 @@ NPH_GPU_API void nph_gpu_solver_destroy(NphGpuSolver *solver);
  * start, solve, integrate positions, relax, each constraint pass colour by colour with the
  * overflow first; then restitution, store, finalize) and writes the results back into the
  * view's arrays. Returns NPH_GPU_INVALID_ARGUMENT for a malformed view (an index out of
- * range, a point count outside 1..4, colour counts that do not add up), NPH_GPU_UNSUPPORTED
- * for a setting the device solver does not run (another solver, continuous collision, a
- * joint type other than ball and hinge), NPH_GPU_OUT_OF_MEMORY when the device buffers
+ * range, a point count outside 1..4, colour counts that do not add up, an axis motion other
+ * than NPH_GPU_AXIS_*), NPH_GPU_UNSUPPORTED for a setting the device solver does not run
+ * (XPBD, continuous collision, an unknown joint type), NPH_GPU_OUT_OF_MEMORY when the device buffers
  * cannot grow (the view is then untouched: the step did not happen), and
  * NPH_GPU_DEVICE_LOST when a device wait gave up or the device reported an error. */
 NPH_GPU_API NphGpuResult nph_gpu_phys_solve(NphGpuSolver *solver, const NphGpuWorldParams *params,

@@ -42,6 +42,16 @@ CONSTRAINT_B_DYNAMIC = 2
 CONSTRAINT_JOINT = 4
 JOINT_BALL = 0
 JOINT_HINGE = 1
+JOINT_FIXED = 2
+JOINT_SLIDER = 3
+JOINT_DISTANCE = 4
+JOINT_D6 = 5
+AXIS_LOCKED, AXIS_LIMITED, AXIS_FREE = 0, 1, 2
+D6_AXES = 6
+ROW_LOCK, ROW_UPPER, ROW_MOTOR, ROW_SPRING = 0, 1, 2, 3
+JOINT_BLOCK_ROTATION = 1 << 11
+JOINT_BLOCK_SWING = 1 << 12
+JOINT_BLOCK_POINT = 1 << 13
 SOLVER_SOFT_STEP = 0
 SOLVER_TGS = 1
 
@@ -66,7 +76,7 @@ CONTACT_DTYPE = np.dtype([
     ("points", POINT_DTYPE, MAX_POINTS),
 ], align=True)
 
-# The settings union: ball and hinge fields overlay the same 40 bytes.
+# The settings union: ball, hinge, slider, distance and 6-DOF fields overlay the same 240 bytes.
 _BALL = [("enable_swing_limit", "<u4", 0), ("swing_y", "<f4", 4), ("swing_z", "<f4", 8),
          ("enable_twist_limit", "<u4", 12), ("twist_lower", "<f4", 16),
          ("twist_upper", "<f4", 20), ("friction_torque", "<f4", 24)]
@@ -75,7 +85,22 @@ _HINGE = [("enable_limit", "<u4", 0), ("lower", "<f4", 4), ("upper", "<f4", 8),
           ("max_motor_torque", "<f4", 20), ("enable_spring", "<u4", 24),
           ("spring_hertz", "<f4", 28), ("spring_damping_ratio", "<f4", 32),
           ("spring_target", "<f4", 36)]
+_SLIDER = [("enable_limit", "<u4", 0), ("lower", "<f4", 4), ("upper", "<f4", 8),
+           ("enable_motor", "<u4", 12), ("motor_speed", "<f4", 16),
+           ("max_motor_force", "<f4", 20), ("enable_spring", "<u4", 24),
+           ("spring_hertz", "<f4", 28), ("spring_damping_ratio", "<f4", 32),
+           ("spring_target", "<f4", 36)]
+_DISTANCE = [("length", "<f4", 0), ("enable_limit", "<u4", 4), ("min_length", "<f4", 8),
+             ("max_length", "<f4", 12), ("enable_spring", "<u4", 16), ("spring_hertz", "<f4", 20),
+             ("spring_damping_ratio", "<f4", 24), ("enable_motor", "<u4", 28),
+             ("motor_speed", "<f4", 32), ("max_motor_force", "<f4", 36)]
+D6_AXIS_DTYPE = np.dtype([
+    ("motion", "<u4"), ("lower", "<f4"), ("upper", "<f4"), ("enable_motor", "<u4"),
+    ("motor_speed", "<f4"), ("max_motor_force", "<f4"), ("enable_spring", "<u4"),
+    ("spring_hertz", "<f4"), ("spring_damping_ratio", "<f4"), ("spring_target", "<f4"),
+])
 _SETTINGS_BASE = 72
+_IMPULSES = 312
 
 
 def _joint_dtype() -> np.dtype:
@@ -89,25 +114,27 @@ def _joint_dtype() -> np.dtype:
     add("type", "<u4", 0)
     add("body_a", "<u4", 4)
     add("body_b", "<u4", 8)
-    add("pad0", "<u4", 12)
+    add("flags", "<u4", 12)
     add("frame_a_position", ("<f4", 3), 16)
     add("frame_a_rotation", ("<f4", 4), 28)
     add("frame_b_position", ("<f4", 3), 44)
     add("frame_b_rotation", ("<f4", 4), 56)
-    add("settings", ("<u4", 10), _SETTINGS_BASE)
-    for name, fmt, off in _BALL:
-        add("ball_" + name, fmt, _SETTINGS_BASE + off)
-    for name, fmt, off in _HINGE:
-        add("hinge_" + name, fmt, _SETTINGS_BASE + off)
-    add("linear_impulse", ("<f4", 3), 112)
-    add("angular_impulse", ("<f4", 3), 124)
-    add("friction_impulse", ("<f4", 3), 136)
-    add("lower_impulse", "<f4", 148)
-    add("upper_impulse", "<f4", 152)
-    add("swing_impulse", "<f4", 156)
-    add("motor_impulse", "<f4", 160)
-    add("spring_impulse", "<f4", 164)
-    return np.dtype({"names": names, "formats": formats, "offsets": offsets, "itemsize": 168})
+    add("settings", ("<u4", 60), _SETTINGS_BASE)
+    for prefix, fields in (("ball_", _BALL), ("hinge_", _HINGE), ("slider_", _SLIDER),
+                           ("distance_", _DISTANCE)):
+        for name, fmt, off in fields:
+            add(prefix + name, fmt, _SETTINGS_BASE + off)
+    add("d6_axes", (D6_AXIS_DTYPE, D6_AXES), _SETTINGS_BASE)
+    add("linear_impulse", ("<f4", 3), _IMPULSES)
+    add("angular_impulse", ("<f4", 3), _IMPULSES + 12)
+    add("friction_impulse", ("<f4", 3), _IMPULSES + 24)
+    add("lower_impulse", "<f4", _IMPULSES + 36)
+    add("upper_impulse", "<f4", _IMPULSES + 40)
+    add("swing_impulse", "<f4", _IMPULSES + 44)
+    add("motor_impulse", "<f4", _IMPULSES + 48)
+    add("spring_impulse", "<f4", _IMPULSES + 52)
+    add("axis_impulse", ("<f4", (D6_AXES, 4)), _IMPULSES + 56)
+    return np.dtype({"names": names, "formats": formats, "offsets": offsets, "itemsize": 464})
 
 
 JOINT_DTYPE = _joint_dtype()

@@ -178,8 +178,7 @@ __device__ __noinline__ void joint_prepare_item(const DevSolver &S, const WorldS
 {
     const uint32_t n = W.n, total = W.n + W.nf;
     const NphGpuJoint &jr = joints[i];
-    if (jr.body_a >= total || jr.body_b >= total ||
-        (jr.type != NPH_GPU_JOINT_BALL && jr.type != NPH_GPU_JOINT_HINGE)) {
+    if (jr.body_a >= total || jr.body_b >= total || nph_joint_check(&jr) != NPH_GPU_OK) {
         atomicOr(err, kErrBadJoint);
         for (uint32_t r = 0; r < kJointRows; ++r) {
             S.jw[r * S.jcap + i] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -988,8 +987,9 @@ NphGpuResult check_world(const NphGpuWorldView &v)
         return NPH_GPU_INVALID_ARGUMENT;
     }
     for (uint32_t j = 0; j < v.joint_count; ++j) {
-        if (v.joints[j].type != NPH_GPU_JOINT_BALL && v.joints[j].type != NPH_GPU_JOINT_HINGE) {
-            return NPH_GPU_UNSUPPORTED;
+        const int bad = nph_joint_check(&v.joints[j]);
+        if (bad != NPH_GPU_OK) {
+            return (NphGpuResult)bad;
         }
     }
     return NPH_GPU_OK;
@@ -1224,10 +1224,7 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_upload(NphGpuBatch *b, const NphGpuWorldV
         }
         for (uint32_t j = 0; j < v.joint_count; ++j) {
             const NphGpuJoint &jr = v.joints[j];
-            s.driven += (jr.type == NPH_GPU_JOINT_HINGE && jr.u.hinge.enable_motor != 0u &&
-                         jr.u.hinge.motor_speed != 0.0f && jr.u.hinge.max_motor_torque > 0.0f)
-                            ? 1u
-                            : 0u;
+            s.driven += nph_joint_is_driven(&jr) ? 1u : 0u;
         }
         bodies += v.body_count;
         slots += v.body_count + 1u;

@@ -51,7 +51,20 @@ constexpr uint32_t kJSpring = 1u << 5;     // hinge spring
 constexpr uint32_t kJSwing = 1u << 6;      // ball cone
 constexpr uint32_t kJTwist = 1u << 7;      // ball twist limits
 constexpr uint32_t kJFriction = 1u << 8;   // ball friction (torque > 0)
-constexpr uint32_t kJDriven = 1u << 9;     // a hinge motor driving to a non-zero speed
+constexpr uint32_t kJDriven = 1u << 9;     // a motor driving to a non-zero speed (any type)
+// The blocks of a slider or 6-DOF joint: the bits of NPH_GPU_JOINT_BLOCK_*.
+constexpr uint32_t kJBlockRotation = 1u << 11;
+constexpr uint32_t kJBlockSwing = 1u << 12;
+constexpr uint32_t kJBlockPoint = 1u << 13;
+constexpr uint32_t kJBlocks = kJBlockRotation | kJBlockSwing | kJBlockPoint;
+constexpr uint32_t kJTypeShift = 16u;      // NPH_GPU_JOINT_* in bits 16..18
+constexpr uint32_t kJTypeMask = 7u;
+// Per axis of a slider, 6-DOF or distance joint, four bits of row 0 .w: the motion (2 bits,
+// NPH_GPU_AXIS_*), the motor, the spring. A distance joint's axis 0 is its line: limited when
+// its limits are on, else locked unless its spring is on.
+constexpr uint32_t kJAxisBits = 4u;
+constexpr uint32_t kJAxisMotor = 1u << 2;
+constexpr uint32_t kJAxisSpring = 1u << 3;
 
 // Joint rows.
 enum : uint32_t {
@@ -69,7 +82,12 @@ enum : uint32_t {
     kJrAngular = 10, // angular_impulse.xyz, upper_impulse
     kJrFric = 11,    // friction_impulse.xyz, swing_impulse
     kJrMotor = 12,   // motor_impulse, spring_impulse
-    kJointRows = 13,
+    // Slider, 6-DOF and distance joints only, per axis i (distance: axis 0):
+    kJrAxisSet = 13,     // row 13 + 2i: lower, upper, motor_speed, h x max motor force
+                         // row 14 + 2i: spring target, the spring's softness
+                         // (distance: min and max length; length)
+    kJrAxisImpulse = 25, // row 25 + i: the lock or lower, upper, motor and spring impulses
+    kJointRows = 31,
 };
 
 // Device error bits.

@@ -56,6 +56,7 @@ enum Pass : int { kWarm = 0, kSolve = 1, kRelax = 2, kRestitution = 3 };
 // Record staging: a block copies its records between global and shared memory with 16- or
 // 8-byte accesses covering whole cache lines, and the threads work on the shared copies.
 constexpr uint32_t kStage = 128;
+constexpr uint32_t kJointStage = 64; // joint records are 464 bytes: 29 KB of shared memory
 
 template <typename V, typename Rec>
 __device__ __forceinline__ void stage_in(const Rec *src, uint32_t count, Rec *dst)
@@ -182,13 +183,13 @@ k_prepare_contacts(DevSolver S, const NphGpuContact *contacts, const NphGpuBody 
     }
 }
 
-__global__ void __launch_bounds__(kStage)
+__global__ void __launch_bounds__(kJointStage)
 k_prepare_joints(DevSolver S, const NphGpuJoint *joints, const NphGpuBody *bodies,
                  const NphGpuBody *fixed, uint32_t n, uint32_t nf, uint32_t nj, float h, uint32_t *err)
 {
-    __shared__ NphGpuJoint rec[kStage];
-    const uint32_t first = blockIdx.x * kStage;
-    const uint32_t count = min(kStage, nj - first);
+    __shared__ NphGpuJoint rec[kJointStage];
+    const uint32_t first = blockIdx.x * kJointStage;
+    const uint32_t count = min(kJointStage, nj - first);
     stage_in<uint2>(joints + first, count, rec);
     __syncthreads();
     if (threadIdx.x >= count) {
@@ -197,8 +198,7 @@ k_prepare_joints(DevSolver S, const NphGpuJoint *joints, const NphGpuBody *bodie
     const uint32_t j = first + threadIdx.x;
     const uint32_t total = n + nf;
     const NphGpuJoint &jr = rec[threadIdx.x];
-    if (jr.body_a >= total || jr.body_b >= total ||
-        (jr.type != NPH_GPU_JOINT_BALL && jr.type != NPH_GPU_JOINT_HINGE)) {
+    if (jr.body_a >= total || jr.body_b >= total || nph_joint_check(&jr) != NPH_GPU_OK) {
         atomicOr(err, kErrBadJoint);
         // Inert: both ends the dummy, no impulse, nothing written.
         for (uint32_t r = 0; r < kJointRows; ++r) {
@@ -460,11 +460,11 @@ __global__ void __launch_bounds__(kStage) k_store_contacts(DevSolver S, NphGpuCo
 }
 
 // The joints' accumulated impulses back into their records.
-__global__ void __launch_bounds__(kStage) k_store_joints(DevSolver S, NphGpuJoint *joints, uint32_t nj)
+__global__ void __launch_bounds__(kJointStage) k_store_joints(DevSolver S, NphGpuJoint *joints, uint32_t nj)
 {
-    __shared__ NphGpuJoint rec[kStage];
-    const uint32_t first = blockIdx.x * kStage;
-    const uint32_t count = min(kStage, nj - first);
+    __shared__ NphGpuJoint rec[kJointStage];
+    const uint32_t first = blockIdx.x * kJointStage;
+    const uint32_t count = min(kJointStage, nj - first);
     stage_in<uint2>(joints + first, count, rec);
     __syncthreads();
     if (threadIdx.x < count) {
@@ -516,6 +516,10 @@ __global__ void __launch_bounds__(kBlock) k_driven(DevSolver S, NphGpuBody *bodi
 
 static uint32_t blocks_for(uint64_t count) { return (uint32_t)((count + kBlock - 1) / kBlock); }
 static uint32_t stage_blocks(uint64_t count) { return (uint32_t)((count + kStage - 1) / kStage); }
+static uint32_t joint_stage_blocks(uint64_t count)
+{
+    return (uint32_t)((count + kJointStage - 1) / kJointStage);
+}
 
 // solver.c:48-65 on the host, in FP32 as the reference.
 static Soft host_make_soft(float hertz, float zeta, float h)
@@ -853,7 +857,7 @@ void enqueue_prepare(NphGpuSolver *s, const StepConsts &K)
     cudaMemsetAsync(s->d_err + 1, 0, NPH_GPU_COLOR_SLOTS * sizeof(uint32_t), s->stream);
     if (s->nj > 0u) {
         mark_begin(s, kKPrepareConstraints, s->nj, 330.0 * s->nj);
-        k_prepare_joints<<<stage_blocks(s->nj), kStage, 0, s->stream>>>(
+        k_prepare_joints<<<joint_stage_blocks(s->nj), kJointStage, 0, s->stream>>>(
             S, s->d_joints, s->d_bodies, s->d_fixed, s->n, s->nf, s->nj, K.h, s->d_err);
         mark_end(s);
         s->launches++;
@@ -934,7 +938,7 @@ void enqueue_step(NphGpuSolver *s, const StepConsts &K, uint32_t substeps)
     }
     if (s->nj > 0u) {
         mark_begin(s, kKStoreFinalize, s->nj, 330.0 * s->nj);
-        k_store_joints<<<stage_blocks(s->nj), kStage, 0, s->stream>>>(S, s->d_joints, s->nj);
+        k_store_joints<<<joint_stage_blocks(s->nj), kJointStage, 0, s->stream>>>(S, s->d_joints, s->nj);
         mark_end(s);
         s->launches++;
     }
@@ -1048,17 +1052,15 @@ NphGpuResult upload(NphGpuSolver *s, const NphGpuWorldView *v)
     if (r != NPH_GPU_OK) {
         return r;
     }
-    // The joint types first: a refused view leaves the solver as it was.
+    // The joint records first: a refused view leaves the solver as it was.
     uint32_t driven = 0;
     for (uint32_t j = 0; j < v->joint_count; ++j) {
         const NphGpuJoint &jr = v->joints[j];
-        if (jr.type != NPH_GPU_JOINT_BALL && jr.type != NPH_GPU_JOINT_HINGE) {
-            return NPH_GPU_UNSUPPORTED;
+        const int bad = nph_joint_check(&jr);
+        if (bad != NPH_GPU_OK) {
+            return (NphGpuResult)bad;
         }
-        driven += (jr.type == NPH_GPU_JOINT_HINGE && jr.u.hinge.enable_motor != 0u &&
-                   jr.u.hinge.motor_speed != 0.0f && jr.u.hinge.max_motor_torque > 0.0f)
-                      ? 1u
-                      : 0u;
+        driven += nph_joint_is_driven(&jr) ? 1u : 0u;
     }
     r = ensure_capacity(s, v->body_count, v->fixed_count, v->contact_count, v->joint_count);
     if (r != NPH_GPU_OK) {

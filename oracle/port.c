@@ -15,6 +15,39 @@
 
 #define PORT_API __attribute__((visibility("default")))
 
+// d6_config (joint_solver.c:399-421): a 6-DOF joint's axes, or a slider's (translation X
+// free or limited with the slider's drives, the rest locked).
+static void port_axes(const NphGpuJoint *j, NphGpuD6Axis out[NPH_GPU_D6_AXES])
+{
+    if (j->type == NPH_GPU_JOINT_D6) {
+        memcpy(out, j->u.d6, sizeof j->u.d6);
+        return;
+    }
+    memset(out, 0, sizeof(NphGpuD6Axis) * NPH_GPU_D6_AXES);
+    const NphGpuSliderJoint *sl = &j->u.slider;
+    out[0].motion = sl->enable_limit != 0U ? NPH_GPU_AXIS_LIMITED : NPH_GPU_AXIS_FREE;
+    out[0].lower = sl->lower;
+    out[0].upper = sl->upper;
+    out[0].enable_motor = sl->enable_motor;
+    out[0].motor_speed = sl->motor_speed;
+    out[0].max_motor_force = sl->max_motor_force;
+    out[0].enable_spring = sl->enable_spring;
+    out[0].spring_hertz = sl->spring_hertz;
+    out[0].spring_damping_ratio = sl->spring_damping_ratio;
+    out[0].spring_target = sl->spring_target;
+}
+
+// all_locked (joint_solver.c:423-431).
+static int port_all_locked(const NphGpuD6Axis *ax, unsigned first, unsigned count)
+{
+    for (unsigned i = first; i < first + count; ++i) {
+        if (ax[i].motion != NPH_GPU_AXIS_LOCKED) {
+            return 0;
+        }
+    }
+    return 1;
+}
+
 #define REAL float
 #define SUF _f32
 #define SQRT sqrtf
@@ -85,8 +118,15 @@ static int check_view(const NphGpuWorldParams *wp, const NphGpuWorldView *v)
         if (j->body_a >= total || j->body_b >= total) {
             return NPH_GPU_INVALID_ARGUMENT;
         }
-        if (j->type != NPH_GPU_JOINT_BALL && j->type != NPH_GPU_JOINT_HINGE) {
+        if (j->type > NPH_GPU_JOINT_D6) {
             return NPH_GPU_UNSUPPORTED;
+        }
+        if (j->type == NPH_GPU_JOINT_D6) {
+            for (unsigned a = 0U; a < NPH_GPU_D6_AXES; ++a) {
+                if (j->u.d6[a].motion > NPH_GPU_AXIS_FREE) {
+                    return NPH_GPU_INVALID_ARGUMENT;
+                }
+            }
         }
     }
     if (wp->enable_continuous != 0U) {
@@ -95,10 +135,28 @@ static int check_view(const NphGpuWorldParams *wp, const NphGpuWorldView *v)
     return NPH_GPU_OK;
 }
 
+// phys_joint_is_driven (joint_solver.c:1410-1434).
 static int joint_is_driven(const NphGpuJoint *j)
 {
-    return j->type == NPH_GPU_JOINT_HINGE && j->u.hinge.enable_motor != 0U &&
-           j->u.hinge.motor_speed != 0.0F && j->u.hinge.max_motor_torque > 0.0F;
+    if (j->type == NPH_GPU_JOINT_HINGE) {
+        return j->u.hinge.enable_motor != 0U && j->u.hinge.motor_speed != 0.0F &&
+               j->u.hinge.max_motor_torque > 0.0F;
+    }
+    if (j->type == NPH_GPU_JOINT_DISTANCE) {
+        return j->u.distance.enable_motor != 0U && j->u.distance.motor_speed != 0.0F &&
+               j->u.distance.max_motor_force > 0.0F;
+    }
+    if (j->type == NPH_GPU_JOINT_SLIDER || j->type == NPH_GPU_JOINT_D6) {
+        NphGpuD6Axis ax[NPH_GPU_D6_AXES];
+        port_axes(j, ax);
+        for (unsigned i = 0U; i < NPH_GPU_D6_AXES; ++i) {
+            if (ax[i].motion != NPH_GPU_AXIS_LOCKED && ax[i].enable_motor != 0U &&
+                ax[i].motor_speed != 0.0F && ax[i].max_motor_force > 0.0F) {
+                return 1;
+            }
+        }
+    }
+    return 0;
 }
 
 // The FP32 write-back of a step into the view (finalize, store, joints, driven sleep reset).
@@ -301,6 +359,12 @@ static void write_back_f32(const Result_f32 *rp, float dt, NphGpuWorldView *v)
         jr->swing_impulse = j->swing_impulse;
         jr->motor_impulse = j->motor_impulse;
         jr->spring_impulse = j->spring_impulse;
+        for (unsigned a = 0U; a < NPH_GPU_D6_AXES; ++a) {
+            for (unsigned k = 0U; k < 4U; ++k) {
+                jr->axis_impulse[a][k] = j->axis_impulse[a][k];
+            }
+        }
+        jr->flags = j->flags;
     }
     // post_finalize (solver.c:851-857): a driven joint keeps its bodies awake.
     for (unsigned i = 0U; i < v->joint_count; ++i) {

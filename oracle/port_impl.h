@@ -251,6 +251,9 @@ typedef struct FN(Joint) { // the step data of PhysJoint, world_internal.h:317-3
     FN(Soft) spring_soft;
     V3 linear_impulse, angular_impulse, friction_impulse;
     REAL lower_impulse, upper_impulse, swing_impulse, motor_impulse, spring_impulse;
+    REAL axis_impulse[NPH_GPU_D6_AXES][4]; // PHYS_ROW_* per axis (distance: axis 0)
+    unsigned flags;                        // the record's flags with this step's blocks
+    NphGpuD6Axis ax[NPH_GPU_D6_AXES];      // a slider's or 6-DOF joint's axes (d6_config)
     const NphGpuJoint *rec;
 } FN(Joint);
 
@@ -1028,7 +1031,336 @@ static void FN(solve_ball)(FN(Step) *s, FN(Joint) *j, FN(JState) *st, int use_bi
     }
 }
 
-// joint_solver.c:726-771 (ball and hinge).
+// ---------------------------------------------------------------------------------------
+// Joints: fixed, slider, 6-DOF and distance (joint_solver.c:232-262, 395-720)
+// ---------------------------------------------------------------------------------------
+
+// joint_solver.c:232-262.
+static void FN(solve_rotation_lock)(FN(Step) *s, FN(Joint) *j, FN(JState) *st, int use_bias)
+{
+    const V3 cdot = FN(relative_angular)(st);
+    V3 bias = FN(v3)(R(0), R(0), R(0));
+    REAL mass_scale = R(1);
+    REAL impulse_scale = R(0);
+    if (use_bias) {
+        Q4 e = FN(q_mul)(st->qb, FN(q_conj)(st->qa));
+        if (e.w < R(0)) {
+            e.x = -e.x;
+            e.y = -e.y;
+            e.z = -e.z;
+            e.w = -e.w;
+        }
+        bias = FN(scale)(FN(v3)(e.x, e.y, e.z), R(2) * s->joint_soft.bias_rate);
+        mass_scale = s->joint_soft.mass_scale;
+        impulse_scale = s->joint_soft.impulse_scale;
+    }
+    V3 k[3];
+    FN(angular_mass)(j, k);
+    const V3 x = FN(solve3)(k, FN(add)(cdot, bias));
+    const V3 impulse = FN(sub)(FN(scale)(x, -mass_scale), FN(scale)(j->angular_impulse, impulse_scale));
+    j->angular_impulse = FN(add)(j->angular_impulse, impulse);
+    FN(apply_angular)(j, st, impulse);
+}
+
+// joint_solver.c:480-509.
+typedef struct FN(Row) {
+    V3 u, ca, cb;
+    REAL mass;
+} FN(Row);
+
+static FN(Row) FN(row_make)(const FN(Joint) *j, V3 u, V3 ca, V3 cb)
+{
+    FN(Row) r;
+    r.u = u;
+    r.ca = ca;
+    r.cb = cb;
+    const REAL k = (j->ma + j->mb) * FN(dot)(u, u) + FN(dot)(ca, FN(m_mul_v)(j->ia, ca)) +
+                   FN(dot)(cb, FN(m_mul_v)(j->ib, cb));
+    r.mass = k > R(0) ? R(1) / k : R(0);
+    return r;
+}
+
+static FN(Row) FN(linear_row)(const FN(Joint) *j, const FN(JState) *st, V3 d, V3 u)
+{
+    return FN(row_make)(j, u, FN(cross)(FN(add)(st->ra, d), u), FN(cross)(st->rb, u));
+}
+
+static FN(Row) FN(angular_row)(const FN(Joint) *j, V3 axis)
+{
+    return FN(row_make)(j, FN(v3)(R(0), R(0), R(0)), axis, axis);
+}
+
+// joint_solver.c:511-530.
+static REAL FN(row_speed)(const FN(JState) *st, const FN(Row) *r)
+{
+    return FN(dot)(FN(sub)(st->b->v, st->a->v), r->u) + FN(dot)(st->b->w, r->cb) -
+           FN(dot)(st->a->w, r->ca);
+}
+
+static void FN(row_apply)(const FN(Joint) *j, FN(JState) *st, const FN(Row) *r, REAL lambda)
+{
+    if (j->write_a) {
+        st->a->v = FN(mul_add)(st->a->v, r->u, -j->ma * lambda);
+        st->a->w = FN(sub)(st->a->w, FN(m_mul_v)(j->ia, FN(scale)(r->ca, lambda)));
+    }
+    if (j->write_b) {
+        st->b->v = FN(mul_add)(st->b->v, r->u, j->mb * lambda);
+        st->b->w = FN(add)(st->b->w, FN(m_mul_v)(j->ib, FN(scale)(r->cb, lambda)));
+    }
+}
+
+// joint_solver.c:531-549.
+static void FN(row_lock)(FN(Step) *s, const FN(Joint) *j, FN(JState) *st, const FN(Row) *r, REAL c,
+                         REAL *accumulated, int use_bias)
+{
+    REAL bias = R(0);
+    REAL mass_scale = R(1);
+    REAL impulse_scale = R(0);
+    if (use_bias) {
+        bias = s->joint_soft.bias_rate * c;
+        mass_scale = s->joint_soft.mass_scale;
+        impulse_scale = s->joint_soft.impulse_scale;
+    }
+    const REAL impulse =
+        -r->mass * mass_scale * (FN(row_speed)(st, r) + bias) - impulse_scale * *accumulated;
+    *accumulated += impulse;
+    FN(row_apply)(j, st, r, impulse);
+}
+
+// joint_solver.c:550-562 with limit_soft (178-190).
+static void FN(row_limit)(FN(Step) *s, const FN(Joint) *j, FN(JState) *st, const FN(Row) *r, REAL c,
+                          REAL sign, REAL *accumulated, int use_bias)
+{
+    REAL bias = R(0);
+    REAL mass_scale = R(1);
+    REAL impulse_scale = R(0);
+    if (c > R(0)) {
+        bias = c * s->inv_h;
+    } else if (use_bias) {
+        bias = s->joint_soft.bias_rate * c;
+        mass_scale = s->joint_soft.mass_scale;
+        impulse_scale = s->joint_soft.impulse_scale;
+    }
+    const REAL impulse = -r->mass * mass_scale * (sign * FN(row_speed)(st, r) + bias) -
+                         impulse_scale * *accumulated;
+    const REAL total = FN(max)(*accumulated + impulse, R(0));
+    const REAL delta = total - *accumulated;
+    *accumulated = total;
+    FN(row_apply)(j, st, r, sign * delta);
+}
+
+// joint_solver.c:564-571.
+static void FN(row_motor)(const FN(Joint) *j, FN(JState) *st, const FN(Row) *r, REAL speed,
+                          REAL max_impulse, REAL *accumulated)
+{
+    const REAL old = *accumulated;
+    const REAL v = old - r->mass * (FN(row_speed)(st, r) - speed);
+    *accumulated = v < -max_impulse ? -max_impulse : (v > max_impulse ? max_impulse : v);
+    FN(row_apply)(j, st, r, *accumulated - old);
+}
+
+// joint_solver.c:573-585.
+static void FN(row_spring)(FN(Step) *s, const FN(Joint) *j, FN(JState) *st, const FN(Row) *r, REAL c,
+                           float hertz, float zeta, REAL *accumulated)
+{
+    const FN(Soft) soft = FN(make_soft)(R(hertz), R(zeta), s->h);
+    const REAL impulse = -soft.mass_scale * r->mass * (FN(row_speed)(st, r) + soft.bias_rate * c) -
+                         soft.impulse_scale * *accumulated;
+    *accumulated += impulse;
+    FN(row_apply)(j, st, r, impulse);
+}
+
+// vec.h:337-350.
+static V3 FN(normalize_or)(V3 v, V3 fallback)
+{
+    const REAL len_sq = FN(dot)(v, v);
+    if (len_sq > R(0) && len_sq <= R(3.40282347e38F)) {
+        return FN(scale)(v, R(1) / SQRT(len_sq));
+    }
+    if (!(len_sq > R(3.40282347e38F)) || !isfinite(v.x) || !isfinite(v.y) || !isfinite(v.z)) {
+        return fallback;
+    }
+    const REAL m = FN(max)(ABS(v.x), FN(max)(ABS(v.y), ABS(v.z)));
+    const V3 u = FN(scale)(v, R(1) / m);
+    return FN(scale)(u, R(1) / SQRT(FN(dot)(u, u)));
+}
+
+// joint_solver.c:432-470.
+typedef struct FN(AxesNow) {
+    V3 d;
+    V3 axis[NPH_GPU_D6_AXES];
+    REAL value[NPH_GPU_D6_AXES];
+} FN(AxesNow);
+
+static FN(AxesNow) FN(axes_of)(Q4 qa, Q4 qb, V3 d)
+{
+    FN(AxesNow) n;
+    n.d = d;
+    n.axis[0] = FN(axis_x)(qa);
+    n.axis[1] = FN(axis_y)(qa);
+    n.axis[2] = FN(axis_z)(qa);
+    for (unsigned i = 0U; i < 3U; ++i) {
+        n.value[i] = FN(dot)(d, n.axis[i]);
+    }
+    Q4 r = FN(q_mul)(FN(q_conj)(qa), qb);
+    if (r.w < R(0)) {
+        r.x = -r.x;
+        r.y = -r.y;
+        r.z = -r.z;
+        r.w = -r.w;
+    }
+    n.value[3] = R(2) * ATAN2(r.x, r.w);
+    const REAL tl = SQRT(r.x * r.x + r.w * r.w);
+    Q4 twist = FN(q_identity)();
+    if (tl > R(1e-9F)) {
+        twist.x = r.x / tl;
+        twist.y = R(0);
+        twist.z = R(0);
+        twist.w = r.w / tl;
+    }
+    const Q4 swing = FN(q_mul)(r, FN(q_conj)(twist));
+    n.value[4] = R(2) * ATAN2(swing.y, swing.w);
+    n.value[5] = R(2) * ATAN2(swing.z, swing.w);
+    n.axis[3] = FN(normalize_or)(FN(add)(n.axis[0], FN(axis_x)(qb)), n.axis[0]);
+    n.axis[4] = n.axis[1];
+    n.axis[5] = n.axis[2];
+    return n;
+}
+
+// joint_solver.c:471-476.
+static V3 FN(anchor_offset)(const FN(Joint) *j, const FN(JState) *st)
+{
+    return FN(add)(FN(add)(FN(sub)(st->b->dp, st->a->dp), FN(sub)(st->rb, st->ra)), j->delta_center);
+}
+
+static FN(Row) FN(axis_row)(const FN(Joint) *j, const FN(JState) *st, const FN(AxesNow) *n, unsigned i)
+{
+    return i < 3U ? FN(linear_row)(j, st, n->d, n->axis[i]) : FN(angular_row)(j, n->axis[i]);
+}
+
+// joint_solver.c:597-652.
+static void FN(solve_axes)(FN(Step) *s, FN(Joint) *j, FN(JState) *st, int use_bias)
+{
+    const NphGpuD6Axis *ax = j->ax;
+    const FN(AxesNow) n = FN(axes_of)(st->qa, st->qb, FN(anchor_offset)(j, st));
+    for (unsigned i = 0U; i < NPH_GPU_D6_AXES; ++i) {
+        const NphGpuD6Axis *a = &ax[i];
+        if (a->motion == NPH_GPU_AXIS_LOCKED) {
+            continue;
+        }
+        REAL *imp = j->axis_impulse[i];
+        const FN(Row) r = FN(axis_row)(j, st, &n, i);
+        if (a->enable_spring != 0U && use_bias) {
+            const REAL e = n.value[i] - R(a->spring_target);
+            FN(row_spring)(s, j, st, &r, i >= 3U ? FN(unwind)(e) : e, a->spring_hertz,
+                           a->spring_damping_ratio, &imp[NPH_GPU_ROW_SPRING]);
+        }
+        if (a->enable_motor != 0U) {
+            FN(row_motor)(j, st, &r, R(a->motor_speed), s->h * R(a->max_motor_force),
+                          &imp[NPH_GPU_ROW_MOTOR]);
+        }
+        if (a->motion == NPH_GPU_AXIS_LIMITED) {
+            FN(row_limit)(s, j, st, &r, n.value[i] - R(a->lower), R(1), &imp[NPH_GPU_ROW_LOCK], use_bias);
+            FN(row_limit)(s, j, st, &r, R(a->upper) - n.value[i], R(-1), &imp[NPH_GPU_ROW_UPPER],
+                          use_bias);
+        }
+    }
+    if (port_all_locked(ax, 3U, 3U)) {
+        FN(solve_rotation_lock)(s, j, st, use_bias);
+    } else {
+        const int swings = port_all_locked(ax, 4U, 2U);
+        if (swings) {
+            FN(solve_axis_lock)(s, j, st, use_bias);
+        }
+        for (unsigned i = 3U; i < NPH_GPU_D6_AXES; ++i) {
+            if (ax[i].motion == NPH_GPU_AXIS_LOCKED && (i == 3U || !swings)) {
+                const FN(Row) r = FN(angular_row)(j, n.axis[i]);
+                FN(row_lock)(s, j, st, &r, n.value[i], &j->axis_impulse[i][NPH_GPU_ROW_LOCK], use_bias);
+            }
+        }
+    }
+    if (port_all_locked(ax, 0U, 3U)) {
+        FN(solve_point)(s, j, st, use_bias);
+    } else {
+        for (unsigned i = 0U; i < 3U; ++i) {
+            if (ax[i].motion == NPH_GPU_AXIS_LOCKED) {
+                const FN(Row) r = FN(linear_row)(j, st, n.d, n.axis[i]);
+                FN(row_lock)(s, j, st, &r, n.value[i], &j->axis_impulse[i][NPH_GPU_ROW_LOCK], use_bias);
+            }
+        }
+    }
+}
+
+// joint_solver.c:654-682.
+static void FN(warm_axes)(FN(Joint) *j, FN(JState) *st)
+{
+    const NphGpuD6Axis *ax = j->ax;
+    const FN(AxesNow) n = FN(axes_of)(st->qa, st->qb, FN(anchor_offset)(j, st));
+    const int rotation_block = port_all_locked(ax, 3U, 3U);
+    const int swing_block = !rotation_block && port_all_locked(ax, 4U, 2U);
+    const int point_block = port_all_locked(ax, 0U, 3U);
+    for (unsigned i = 0U; i < NPH_GPU_D6_AXES; ++i) {
+        const REAL *imp = j->axis_impulse[i];
+        const REAL total = imp[NPH_GPU_ROW_LOCK] - imp[NPH_GPU_ROW_UPPER] + imp[NPH_GPU_ROW_MOTOR] +
+                           imp[NPH_GPU_ROW_SPRING];
+        if (total != R(0)) {
+            const FN(Row) r = FN(axis_row)(j, st, &n, i);
+            FN(row_apply)(j, st, &r, total);
+        }
+    }
+    if (rotation_block) {
+        FN(apply_angular)(j, st, j->angular_impulse);
+    } else if (swing_block) {
+        FN(apply_angular)(j, st, FN(add)(FN(scale)(FN(axis_y)(st->qa), j->angular_impulse.x),
+                                         FN(scale)(FN(axis_z)(st->qa), j->angular_impulse.y)));
+    }
+    if (point_block) {
+        FN(apply_linear)(j, st, j->linear_impulse);
+    }
+}
+
+// joint_solver.c:683-707.
+static void FN(solve_distance)(FN(Step) *s, FN(Joint) *j, FN(JState) *st, int use_bias)
+{
+    const NphGpuDistanceJoint *dj = &j->rec->u.distance;
+    const V3 d = FN(anchor_offset)(j, st);
+    const REAL len = FN(length)(d);
+    if (!(len > R(1e-6F))) {
+        return;
+    }
+    const FN(Row) r = FN(linear_row)(j, st, d, FN(scale)(d, R(1) / len));
+    REAL *imp = j->axis_impulse[0];
+    if (dj->enable_spring != 0U && use_bias) {
+        FN(row_spring)(s, j, st, &r, len - R(dj->length), dj->spring_hertz, dj->spring_damping_ratio,
+                       &imp[NPH_GPU_ROW_SPRING]);
+    }
+    if (dj->enable_motor != 0U) {
+        FN(row_motor)(j, st, &r, R(dj->motor_speed), s->h * R(dj->max_motor_force),
+                      &imp[NPH_GPU_ROW_MOTOR]);
+    }
+    if (dj->enable_limit != 0U) {
+        FN(row_limit)(s, j, st, &r, len - R(dj->min_length), R(1), &imp[NPH_GPU_ROW_LOCK], use_bias);
+        FN(row_limit)(s, j, st, &r, R(dj->max_length) - len, R(-1), &imp[NPH_GPU_ROW_UPPER], use_bias);
+    } else if (dj->enable_spring == 0U) {
+        FN(row_lock)(s, j, st, &r, len - R(dj->length), &imp[NPH_GPU_ROW_LOCK], use_bias);
+    }
+}
+
+// joint_solver.c:709-720.
+static void FN(warm_distance)(FN(Joint) *j, FN(JState) *st)
+{
+    const V3 d = FN(anchor_offset)(j, st);
+    const REAL len = FN(length)(d);
+    const REAL *imp = j->axis_impulse[0];
+    const REAL total = imp[NPH_GPU_ROW_LOCK] - imp[NPH_GPU_ROW_UPPER] + imp[NPH_GPU_ROW_MOTOR] +
+                       imp[NPH_GPU_ROW_SPRING];
+    if (len > R(1e-6F) && total != R(0)) {
+        const FN(Row) r = FN(linear_row)(j, st, d, FN(scale)(d, R(1) / len));
+        FN(row_apply)(j, st, &r, total);
+    }
+}
+
+// joint_solver.c:726-824, every type.
 static void FN(prepare_joint)(FN(Step) *s, const NphGpuJoint *jr, unsigned body_count,
                               const NphGpuBody *bodies, const NphGpuBody *fixed, FN(Joint) *j)
 {
@@ -1064,6 +1396,12 @@ static void FN(prepare_joint)(FN(Step) *s, const NphGpuJoint *jr, unsigned body_
     j->swing_impulse = R(jr->swing_impulse);
     j->motor_impulse = R(jr->motor_impulse);
     j->spring_impulse = R(jr->spring_impulse);
+    for (unsigned a = 0U; a < NPH_GPU_D6_AXES; ++a) {
+        for (unsigned k = 0U; k < 4U; ++k) {
+            j->axis_impulse[a][k] = R(jr->axis_impulse[a][k]);
+        }
+    }
+    j->flags = jr->flags;
     if (jr->type == NPH_GPU_JOINT_HINGE) {
         const NphGpuHingeJoint *h = &jr->u.hinge;
         if (h->enable_limit == 0U) {
@@ -1078,7 +1416,55 @@ static void FN(prepare_joint)(FN(Step) *s, const NphGpuJoint *jr, unsigned body_
         }
         j->spring_soft = FN(make_soft)(h->enable_spring != 0U ? R(h->spring_hertz) : R(0),
                                        R(h->spring_damping_ratio), s->h);
-    } else {
+    } else if (jr->type == NPH_GPU_JOINT_DISTANCE) {
+        const NphGpuDistanceJoint *dj = &jr->u.distance;
+        REAL *imp = j->axis_impulse[0];
+        if (dj->enable_limit == 0U) {
+            imp[NPH_GPU_ROW_UPPER] = R(0);
+            if (dj->enable_spring != 0U) {
+                imp[NPH_GPU_ROW_LOCK] = R(0);
+            }
+        }
+        if (dj->enable_motor == 0U) {
+            imp[NPH_GPU_ROW_MOTOR] = R(0);
+        }
+        if (dj->enable_spring == 0U) {
+            imp[NPH_GPU_ROW_SPRING] = R(0);
+        }
+    } else if (jr->type == NPH_GPU_JOINT_SLIDER || jr->type == NPH_GPU_JOINT_D6) {
+        port_axes(jr, j->ax);
+        for (unsigned a = 0U; a < NPH_GPU_D6_AXES; ++a) {
+            REAL *imp = j->axis_impulse[a];
+            const unsigned motion = j->ax[a].motion;
+            if (motion != NPH_GPU_AXIS_LIMITED) {
+                imp[NPH_GPU_ROW_UPPER] = R(0);
+            }
+            if (motion == NPH_GPU_AXIS_FREE) {
+                imp[NPH_GPU_ROW_LOCK] = R(0);
+            }
+            if (motion == NPH_GPU_AXIS_LOCKED || j->ax[a].enable_motor == 0U) {
+                imp[NPH_GPU_ROW_MOTOR] = R(0);
+            }
+            if (motion == NPH_GPU_AXIS_LOCKED || j->ax[a].enable_spring == 0U) {
+                imp[NPH_GPU_ROW_SPRING] = R(0);
+            }
+        }
+        const int rotation = port_all_locked(j->ax, 3U, 3U);
+        const int swing = !rotation && port_all_locked(j->ax, 4U, 2U);
+        const int point = port_all_locked(j->ax, 0U, 3U);
+        const unsigned blocks = (rotation ? NPH_GPU_JOINT_BLOCK_ROTATION : 0U) |
+                                (swing ? NPH_GPU_JOINT_BLOCK_SWING : 0U) |
+                                (point ? NPH_GPU_JOINT_BLOCK_POINT : 0U);
+        const unsigned angular = NPH_GPU_JOINT_BLOCK_ROTATION | NPH_GPU_JOINT_BLOCK_SWING;
+        const unsigned all = angular | NPH_GPU_JOINT_BLOCK_POINT;
+        if ((j->flags & angular) != (blocks & angular)) {
+            j->angular_impulse = FN(v3)(R(0), R(0), R(0));
+        }
+        if ((j->flags & NPH_GPU_JOINT_BLOCK_POINT) != (blocks & NPH_GPU_JOINT_BLOCK_POINT)) {
+            j->linear_impulse = FN(v3)(R(0), R(0), R(0));
+        }
+        j->flags = (j->flags & ~all) | blocks;
+    } else if (jr->type == NPH_GPU_JOINT_BALL) {
         const NphGpuBallJoint *bj = &jr->u.ball;
         if (bj->enable_swing_limit == 0U) {
             j->swing_impulse = R(0);
@@ -1093,17 +1479,26 @@ static void FN(prepare_joint)(FN(Step) *s, const NphGpuJoint *jr, unsigned body_
     }
 }
 
-// joint_solver.c:826-868 (ball and hinge).
+// joint_solver.c:855-868.
 static void FN(joint_warm_start)(FN(Step) *s, FN(Joint) *j)
 {
     FN(JState) st = FN(joint_state)(s, j);
+    if (j->type == NPH_GPU_JOINT_SLIDER || j->type == NPH_GPU_JOINT_D6) {
+        FN(warm_axes)(j, &st);
+        return;
+    }
+    if (j->type == NPH_GPU_JOINT_DISTANCE) {
+        FN(warm_distance)(j, &st);
+        return;
+    }
+    // phys_joint_angular_impulse (joint_solver.c:826-853): the fixed joint's world vector.
     V3 angular = j->angular_impulse;
     if (j->type == NPH_GPU_JOINT_HINGE) {
         angular = FN(add)(FN(scale)(FN(axis_y)(st.qa), j->angular_impulse.x),
                           FN(scale)(FN(axis_z)(st.qa), j->angular_impulse.y));
         const REAL axial = j->lower_impulse - j->upper_impulse + j->motor_impulse + j->spring_impulse;
         angular = FN(mul_add)(angular, FN(axis_x)(st.qa), axial);
-    } else {
+    } else if (j->type == NPH_GPU_JOINT_BALL) {
         angular = j->friction_impulse;
         const V3 xa = FN(axis_x)(st.qa);
         const V3 xb = FN(axis_x)(st.qb);
@@ -1122,14 +1517,27 @@ static void FN(joint_warm_start)(FN(Step) *s, FN(Joint) *j)
     FN(apply_linear)(j, &st, j->linear_impulse);
 }
 
-// joint_solver.c:870-897 (ball and hinge).
+// joint_solver.c:870-897.
 static void FN(joint_solve)(FN(Step) *s, FN(Joint) *j, int use_bias)
 {
     FN(JState) st = FN(joint_state)(s, j);
-    if (j->type == NPH_GPU_JOINT_BALL) {
+    switch (j->type) {
+    case NPH_GPU_JOINT_BALL:
         FN(solve_ball)(s, j, &st, use_bias);
-    } else {
+        break;
+    case NPH_GPU_JOINT_HINGE:
         FN(solve_hinge)(s, j, &st, use_bias);
+        break;
+    case NPH_GPU_JOINT_FIXED:
+        FN(solve_rotation_lock)(s, j, &st, use_bias);
+        break;
+    case NPH_GPU_JOINT_SLIDER:
+    case NPH_GPU_JOINT_D6:
+        FN(solve_axes)(s, j, &st, use_bias);
+        return;
+    default: // NPH_GPU_JOINT_DISTANCE
+        FN(solve_distance)(s, j, &st, use_bias);
+        return;
     }
     FN(solve_point)(s, j, &st, use_bias);
 }

@@ -237,6 +237,43 @@ REF_API u32 nphref_add_joint(RefWorld *r, const NphGpuJoint *j, u32 body_a, u32 
         d.hinge.spring_hertz = j->u.hinge.spring_hertz;
         d.hinge.spring_damping_ratio = j->u.hinge.spring_damping_ratio;
         d.hinge.spring_target = j->u.hinge.spring_target;
+    } else if (j->type == NPH_GPU_JOINT_SLIDER) {
+        d.slider.enable_limit = (b32)j->u.slider.enable_limit;
+        d.slider.lower = j->u.slider.lower;
+        d.slider.upper = j->u.slider.upper;
+        d.slider.enable_motor = (b32)j->u.slider.enable_motor;
+        d.slider.motor_speed = j->u.slider.motor_speed;
+        d.slider.max_motor_force = j->u.slider.max_motor_force;
+        d.slider.enable_spring = (b32)j->u.slider.enable_spring;
+        d.slider.spring_hertz = j->u.slider.spring_hertz;
+        d.slider.spring_damping_ratio = j->u.slider.spring_damping_ratio;
+        d.slider.spring_target = j->u.slider.spring_target;
+    } else if (j->type == NPH_GPU_JOINT_DISTANCE) {
+        d.distance.length = j->u.distance.length;
+        d.distance.enable_limit = (b32)j->u.distance.enable_limit;
+        d.distance.min_length = j->u.distance.min_length;
+        d.distance.max_length = j->u.distance.max_length;
+        d.distance.enable_spring = (b32)j->u.distance.enable_spring;
+        d.distance.spring_hertz = j->u.distance.spring_hertz;
+        d.distance.spring_damping_ratio = j->u.distance.spring_damping_ratio;
+        d.distance.enable_motor = (b32)j->u.distance.enable_motor;
+        d.distance.motor_speed = j->u.distance.motor_speed;
+        d.distance.max_motor_force = j->u.distance.max_motor_force;
+    } else if (j->type == NPH_GPU_JOINT_D6) {
+        for (u32 i = 0U; i < NPH_PHYSICS_D6_AXES; ++i) {
+            const NphGpuD6Axis *x = &j->u.d6[i];
+            NphPhysicsD6Axis *y = &d.d6.axes[i];
+            y->motion = (NphPhysicsAxisMotion)x->motion;
+            y->lower = x->lower;
+            y->upper = x->upper;
+            y->enable_motor = (b32)x->enable_motor;
+            y->motor_speed = x->motor_speed;
+            y->max_motor_force = x->max_motor_force;
+            y->enable_spring = (b32)x->enable_spring;
+            y->spring_hertz = x->spring_hertz;
+            y->spring_damping_ratio = x->spring_damping_ratio;
+            y->spring_target = x->spring_target;
+        }
     }
     NphPhysicsJoint out;
     if (nph_physics_joint_create(r->w, &d, &out) != NPH_RESULT_OK) {
@@ -530,6 +567,10 @@ static void contact_record(RefWorld *r, const PhysContact *c, NphGpuContact *o, 
     }
 }
 
+#define JOINT_BLOCKS (NPH_GPU_JOINT_BLOCK_ROTATION | NPH_GPU_JOINT_BLOCK_SWING | NPH_GPU_JOINT_BLOCK_POINT)
+_Static_assert(sizeof(((PhysJoint *)0)->axis_impulse) == sizeof(((NphGpuJoint *)0)->axis_impulse),
+               "the rows per axis of PhysJoint and of the record");
+
 static void joint_record(RefWorld *r, const PhysJoint *j, NphGpuJoint *o, u32 *fixed_count)
 {
     memset(o, 0, sizeof *o);
@@ -559,7 +600,47 @@ static void joint_record(RefWorld *r, const PhysJoint *j, NphGpuJoint *o, u32 *f
         o->u.hinge.spring_hertz = j->hinge.spring_hertz;
         o->u.hinge.spring_damping_ratio = j->hinge.spring_damping_ratio;
         o->u.hinge.spring_target = j->hinge.spring_target;
+    } else if (j->type == NPH_PHYSICS_JOINT_SLIDER) {
+        o->u.slider.enable_limit = (u32)j->slider.enable_limit;
+        o->u.slider.lower = j->slider.lower;
+        o->u.slider.upper = j->slider.upper;
+        o->u.slider.enable_motor = (u32)j->slider.enable_motor;
+        o->u.slider.motor_speed = j->slider.motor_speed;
+        o->u.slider.max_motor_force = j->slider.max_motor_force;
+        o->u.slider.enable_spring = (u32)j->slider.enable_spring;
+        o->u.slider.spring_hertz = j->slider.spring_hertz;
+        o->u.slider.spring_damping_ratio = j->slider.spring_damping_ratio;
+        o->u.slider.spring_target = j->slider.spring_target;
+    } else if (j->type == NPH_PHYSICS_JOINT_DISTANCE) {
+        o->u.distance.length = j->distance.length;
+        o->u.distance.enable_limit = (u32)j->distance.enable_limit;
+        o->u.distance.min_length = j->distance.min_length;
+        o->u.distance.max_length = j->distance.max_length;
+        o->u.distance.enable_spring = (u32)j->distance.enable_spring;
+        o->u.distance.spring_hertz = j->distance.spring_hertz;
+        o->u.distance.spring_damping_ratio = j->distance.spring_damping_ratio;
+        o->u.distance.enable_motor = (u32)j->distance.enable_motor;
+        o->u.distance.motor_speed = j->distance.motor_speed;
+        o->u.distance.max_motor_force = j->distance.max_motor_force;
+    } else if (j->type == NPH_PHYSICS_JOINT_D6) {
+        for (u32 i = 0U; i < NPH_PHYSICS_D6_AXES; ++i) {
+            const NphPhysicsD6Axis *x = &j->d6.axes[i];
+            NphGpuD6Axis *y = &o->u.d6[i];
+            y->motion = (u32)x->motion;
+            y->lower = x->lower;
+            y->upper = x->upper;
+            y->enable_motor = (u32)x->enable_motor;
+            y->motor_speed = x->motor_speed;
+            y->max_motor_force = x->max_motor_force;
+            y->enable_spring = (u32)x->enable_spring;
+            y->spring_hertz = x->spring_hertz;
+            y->spring_damping_ratio = x->spring_damping_ratio;
+            y->spring_target = x->spring_target;
+        }
     }
+    // The block bits of joint_solver.c:103-112 carry across steps; the others are the step's.
+    o->flags = j->flags & JOINT_BLOCKS;
+    memcpy(o->axis_impulse, j->axis_impulse, sizeof o->axis_impulse);
     memcpy(o->linear_impulse, &j->linear_impulse, sizeof o->linear_impulse);
     memcpy(o->angular_impulse, &j->angular_impulse, sizeof o->angular_impulse);
     memcpy(o->friction_impulse, &j->friction_impulse, sizeof o->friction_impulse);
@@ -656,6 +737,8 @@ REF_API int nphref_import(RefWorld *r, const NphGpuWorldView *v, f32 dt)
             j->swing_impulse = o->swing_impulse;
             j->motor_impulse = o->motor_impulse;
             j->spring_impulse = o->spring_impulse;
+            memcpy(j->axis_impulse, o->axis_impulse, sizeof o->axis_impulse);
+            j->flags = (j->flags & ~(u32)JOINT_BLOCKS) | (o->flags & JOINT_BLOCKS);
         }
     }
     w->last_substep = dt / (f32)w->desc.substeps;

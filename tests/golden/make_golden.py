@@ -59,6 +59,10 @@ def main():
     p8 = abi.WorldParams.default(substeps=8, contact_hertz=45.0, restitution_threshold=0.5)
     save("sphere_pour_substeps8", *cut(ref_scenes.sphere_pour(count=48, extent=6.0, params=p8),
                                        20, p8, dt=1.0 / 120.0), p8, 1.0 / 120.0)
+    save("joint_zoo", *cut(ref_scenes.joint_zoo(seed=5, params=p), 20, p), p, DT)
+    tgs = abi.WorldParams.default(solver=abi.SOLVER_TGS)
+    save("joint_zoo_tgs", *cut(ref_scenes.joint_zoo(seed=6, params=tgs), 20, tgs), tgs, DT)
+    save("box_pile_24_tgs", *cut(ref_scenes.box_pile(count=24, params=tgs), 40, tgs), tgs, DT)
 
 
 def load(path: Path) -> tuple[abi.View, abi.View, abi.WorldParams, float]:

@@ -9,7 +9,8 @@ BODY_OUT = ["center", "origin", "rotation", "linear_velocity", "angular_velocity
             "torque", "sleep_time"]
 POINT_OUT = ["normal_impulse", "max_normal_impulse", "tangent_impulse", "relative_velocity"]
 JOINT_OUT = ["linear_impulse", "angular_impulse", "friction_impulse", "lower_impulse",
-             "upper_impulse", "swing_impulse", "motor_impulse", "spring_impulse"]
+             "upper_impulse", "swing_impulse", "motor_impulse", "spring_impulse", "axis_impulse",
+             "flags"]
 
 
 def _fields(view: abi.View):

@@ -185,3 +185,141 @@ def featured_lattice(edge: int = 8, seed: int = 7, params=None):
     w.add_joints(sc.joints)
     w.inject_contacts(sc.contacts)
     return w
+
+
+def _random_quat(rng):
+    q = rng.normal(size=4)
+    return tuple(q / np.linalg.norm(q))
+
+
+def _d6_axes(rng, joint, kind):
+    """A 6-DOF joint's axes: each locked, limited or free at random, with motors and springs on
+    some free or limited axes; `kind` forces the rotation, swing or point block."""
+    ax = joint["d6_axes"]
+    for i in range(abi.D6_AXES):
+        motion = int(rng.choice([abi.AXIS_LOCKED, abi.AXIS_LIMITED, abi.AXIS_FREE], p=[0.4, 0.35, 0.25]))
+        if kind == "rotation" and i >= 3:
+            motion = abi.AXIS_LOCKED
+        if kind == "swing" and i >= 4:
+            motion = abi.AXIS_LOCKED
+        if kind == "point" and i < 3:
+            motion = abi.AXIS_LOCKED
+        ax["motion"][i] = motion
+        if i < 3:
+            lo, hi = sorted(rng.uniform(-0.4, 0.4, 2))
+        elif i == 3:
+            lo, hi = sorted(rng.uniform(-2.5, 2.5, 2))
+        else:
+            lo, hi = sorted(rng.uniform(-1.2, 1.2, 2))
+        ax["lower"][i], ax["upper"][i] = lo, hi
+        if motion != abi.AXIS_LOCKED and rng.random() < 0.4:
+            ax["enable_motor"][i] = 1
+            ax["motor_speed"][i] = rng.uniform(-1.5, 1.5)
+            ax["max_motor_force"][i] = rng.uniform(5.0, 200.0)
+        if motion != abi.AXIS_LOCKED and rng.random() < 0.4:
+            ax["enable_spring"][i] = 1
+            ax["spring_hertz"][i] = rng.uniform(0.5, 5.0)
+            ax["spring_damping_ratio"][i] = rng.uniform(0.0, 1.5)
+            ax["spring_target"][i] = rng.uniform(-0.2, 0.2)
+
+
+def joint_zoo(seed: int = 5, params=None, types=None):
+    """Every joint type the solver runs, on boxes hanging from static anchors (and from each
+    other), apart so that only the joints act: welded cantilevers (fixed); sliders with
+    limits, motors and springs; distance joints rigid, as ropes, as limited springs and
+    motor-driven; 6-DOF joints with random axes (every block: rotation, swing pair, anchors,
+    none); ball and hinge joints between them."""
+    from oracle.refworld import RefWorld
+    rng = np.random.default_rng(seed)
+    w = RefWorld(params or abi.WorldParams.default(), enable_sleep=False)
+    types = types or ("fixed", "slider", "distance", "d6", "ball", "hinge")
+    joints = []
+    x = 0.0
+
+    def new(jt, a, b, fa=(0.0, 0.0, 0.0), fb=(0.0, 0.0, 0.0), qa=None, qb=None):
+        j = np.zeros(1, abi.JOINT_DTYPE)[0]
+        j["type"] = jt
+        j["body_a"], j["body_b"] = a, b
+        j["frame_a_position"], j["frame_b_position"] = fa, fb
+        j["frame_a_rotation"] = qa if qa is not None else (0.0, 0.0, 0.0, 1.0)
+        j["frame_b_rotation"] = qb if qb is not None else (0.0, 0.0, 0.0, 1.0)
+        joints.append(j)
+        return j
+
+    def box(pos, half=(0.3, 0.2, 0.25)):
+        return w.add_box(pos, half=half, rotation=_random_quat(rng) if rng.random() < 0.5 else (0, 0, 0, 1),
+                         velocity=tuple(rng.uniform(-0.5, 0.5, 3)),
+                         angular_velocity=tuple(rng.uniform(-1.0, 1.0, 3)))
+
+    for kind in types:
+        for variant in range(4):
+            x += 3.0
+            anchor = w.add_body(abi.BODY_STATIC, (x, 10.0, 0.0))
+            if kind == "fixed":
+                prev = anchor
+                for k in range(3):
+                    b = box((x + 0.7 * (k + 1), 10.0, 0.0))
+                    new(abi.JOINT_FIXED, prev, b, fa=(0.35, 0.0, 0.0) if k else (0.0, 0.0, 0.0),
+                        fb=(-0.35, 0.0, 0.0), qa=_random_quat(rng), qb=_random_quat(rng))
+                    prev = b
+            elif kind == "slider":
+                b = box((x + 0.5, 9.5, 0.0))
+                j = new(abi.JOINT_SLIDER, anchor, b, qa=_random_quat(rng), qb=_random_quat(rng))
+                j["slider_enable_limit"] = int(variant > 0)
+                j["slider_lower"], j["slider_upper"] = -0.5, 0.3
+                if variant >= 2:
+                    j["slider_enable_motor"] = 1
+                    j["slider_motor_speed"] = 0.8 if variant == 2 else -0.6
+                    j["slider_max_motor_force"] = 60.0
+                if variant in (1, 3):
+                    j["slider_enable_spring"] = 1
+                    j["slider_spring_hertz"] = 2.0
+                    j["slider_spring_damping_ratio"] = 0.5
+                    j["slider_spring_target"] = 0.1
+            elif kind == "distance":
+                b = box((x + 1.0, 9.2, 0.3))
+                j = new(abi.JOINT_DISTANCE, anchor, b, fb=(0.1, 0.2, 0.0))
+                j["distance_length"] = 1.2
+                if variant == 1:  # a rope
+                    j["distance_enable_limit"] = 1
+                    j["distance_min_length"], j["distance_max_length"] = 0.0, 1.2
+                if variant == 2:  # a limited spring
+                    j["distance_enable_spring"] = 1
+                    j["distance_spring_hertz"] = 3.0
+                    j["distance_spring_damping_ratio"] = 0.3
+                    j["distance_enable_limit"] = 1
+                    j["distance_min_length"], j["distance_max_length"] = 0.8, 1.5
+                if variant == 3:  # motor-driven, rigid otherwise
+                    j["distance_enable_motor"] = 1
+                    j["distance_motor_speed"] = 0.5
+                    j["distance_max_motor_force"] = 30.0
+                # a second box hanging from the first (two dynamic bodies)
+                c = box((x + 1.0, 8.0, 0.3))
+                j2 = new(abi.JOINT_DISTANCE, b, c, fa=(0.0, -0.2, 0.0), fb=(0.0, 0.2, 0.0))
+                j2["distance_length"] = 0.9
+            elif kind == "d6":
+                b = box((x + 0.6, 9.6, 0.0))
+                j = new(abi.JOINT_D6, anchor, b, fb=(-0.3, 0.1, 0.0), qa=_random_quat(rng),
+                        qb=_random_quat(rng))
+                _d6_axes(rng, j, ("rotation", "swing", "point", None)[variant])
+                c = box((x + 1.3, 9.6, 0.0))
+                j2 = new(abi.JOINT_D6, b, c, fa=(0.3, 0.0, 0.0), fb=(-0.3, 0.0, 0.0),
+                         qa=_random_quat(rng), qb=_random_quat(rng))
+                _d6_axes(rng, j2, (None, "point", "swing", "rotation")[variant])
+            elif kind == "ball":
+                b = box((x + 0.6, 10.0, 0.0))
+                j = new(abi.JOINT_BALL, anchor, b, fb=(-0.6, 0.0, 0.0))
+                j["ball_enable_swing_limit"] = variant % 2
+                j["ball_swing_y"], j["ball_swing_z"] = 0.5, 0.3
+                j["ball_enable_twist_limit"] = variant // 2
+                j["ball_twist_lower"], j["ball_twist_upper"] = -0.4, 0.4
+            else:
+                b = box((x + 0.6, 10.0, 0.0))
+                j = new(abi.JOINT_HINGE, anchor, b, fb=(-0.6, 0.0, 0.0), qa=_random_quat(rng),
+                        qb=_random_quat(rng))
+                j["hinge_enable_limit"] = variant % 2
+                j["hinge_lower"], j["hinge_upper"] = -0.5, 0.5
+                j["hinge_enable_motor"] = int(variant >= 2)
+                j["hinge_motor_speed"], j["hinge_max_motor_torque"] = 1.0, 15.0
+    w.add_joints(np.array(joints, abi.JOINT_DTYPE))
+    return w

@@ -12,7 +12,7 @@ from tests import helpers
 from tests.golden.make_golden import load
 
 GOLDEN = sorted((Path(__file__).resolve().parent / "golden").glob("*.npz"))
-ANGLE_ROWS = {"hinge_chain_8"}
+ANGLE_ROWS = {"hinge_chain_8", "joint_zoo", "joint_zoo_tgs"}
 
 
 def ids(p):

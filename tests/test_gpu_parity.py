@@ -237,8 +237,13 @@ def test_unsupported_settings_are_refused(solver):
     p = abi.WorldParams.default(solver=2)
     assert solver.phys_solve_code(view.copy(), p, DT) == abi.UNSUPPORTED
     bad = view.copy()
-    bad.joints["type"][0] = 2
+    bad.joints["type"][0] = 6  # no such joint type
     assert solver.phys_solve_code(bad, abi.WorldParams.default(), DT) == abi.UNSUPPORTED
+    bad = view.copy()
+    bad.joints["type"][0] = abi.JOINT_D6
+    bad.joints["d6_axes"]["motion"][0] = 0
+    bad.joints["d6_axes"]["motion"][0, 2] = 3  # no such motion
+    assert solver.phys_solve_code(bad, abi.WorldParams.default(), DT) == abi.INVALID_ARGUMENT
     assert solver.phys_solve_code(view.copy(), abi.WorldParams.default(), 0.0) == abi.INVALID_ARGUMENT
 
 

@@ -153,7 +153,7 @@ def test_port_rejects_malformed_views():
     assert port32_result(bad, params, DT) == abi.INVALID_ARGUMENT
     bad = v.copy()
     if len(bad.joints):
-        bad.joints["type"][0] = 3
+        bad.joints["type"][0] = 6
         assert port32_result(bad, params, DT) == abi.UNSUPPORTED
 
 
