@@ -47,6 +47,7 @@ struct WorldSlice {
     uint32_t joint_first;
     uint32_t nj;
     uint32_t driven;
+    uint32_t row_joints;    // slider, 6-DOF and distance joints
     uint32_t cfirst[NPH_GPU_COLOR_SLOTS]; // world-relative
     uint32_t ccount[NPH_GPU_COLOR_SLOTS];
     uint32_t jfirst[NPH_GPU_COLOR_SLOTS];
@@ -511,7 +512,7 @@ struct NphGpuBatch {
     bool maps_valid = false;
     bool live_in_merged = false;
     NphGpuWorldView merged_shape{};
-    uint32_t merged_driven = 0;
+    uint32_t merged_driven = 0, merged_row_joints = 0;
     int sms = 148;
     // Device arrays and their capacities (grown, never shrunk, by uploads).
     NphGpuBody *d_bodies = nullptr;
@@ -848,8 +849,10 @@ NphGpuResult build_merge_maps(NphGpuBatch *b)
             shape.joint_color_counts[c] += ws.jcount[c];
         }
     }
+    uint32_t row_joints = 0;
     for (uint32_t w = 0; w < b->world_count; ++w) {
         driven += b->worlds[w].driven;
+        row_joints += b->worlds[w].row_joints;
     }
     if (cmap.size() >= 0xFFFFFFF0ull || b->bodies + b->fixed + 1u >= 0xFFFFFFF0ull) {
         return NPH_GPU_TOO_LARGE;
@@ -883,6 +886,7 @@ NphGpuResult build_merge_maps(NphGpuBatch *b)
     shape.contact_count = (uint32_t)cmap.size();
     shape.joint_count = (uint32_t)jmap.size();
     b->merged_driven = driven;
+    b->merged_row_joints = row_joints;
     const NphGpuResult r = cuda_result(cudaStreamSynchronize(b->stream));
     b->maps_valid = r == NPH_GPU_OK;
     return r;
@@ -910,7 +914,7 @@ NphGpuResult merged_setup(NphGpuBatch *b)
         }
     }
     NphSolverRecords R;
-    r = nph_solver_bind_device(b->merged, &b->merged_shape, b->merged_driven, &R);
+    r = nph_solver_bind_device(b->merged, &b->merged_shape, b->merged_driven, b->merged_row_joints, &R);
     if (r != NPH_GPU_OK) {
         return r;
     }
@@ -1225,6 +1229,7 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_upload(NphGpuBatch *b, const NphGpuWorldV
         for (uint32_t j = 0; j < v.joint_count; ++j) {
             const NphGpuJoint &jr = v.joints[j];
             s.driven += nph_joint_is_driven(&jr) ? 1u : 0u;
+            s.row_joints += (nph_joint_has_axes(jr.type) || jr.type == NPH_GPU_JOINT_DISTANCE) ? 1u : 0u;
         }
         bodies += v.body_count;
         slots += v.body_count + 1u;

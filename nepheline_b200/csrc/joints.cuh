@@ -327,12 +327,23 @@ NPH_D bool joint_has_rows(uint32_t type)
 
 static __device__ __noinline__ void warm_row_joint(const DevSolver &S, uint32_t j);
 
+// Which joints a pass takes: all of them in their order (the overflow's one thread, a batch's
+// worlds), or, within a colour, whose joints share no dynamic body, the ball, hinge and fixed
+// joints in one launch and the slider, 6-DOF and distance joints in another, so that the
+// common launch keeps the registers of its own rows.
+enum JointSet : int { kJointsAll = 0, kJointsPlain = 1, kJointsRows = 2 };
+
 // joint_solver.c:826-868.
+template <int kSet = kJointsAll>
 NPH_D void warm_joint(const DevSolver &S, uint32_t j)
 {
     uint32_t sa, sb, flags;
     joint_head(S, j, sa, sb, flags);
-    if (joint_has_rows(joint_type(flags))) {
+    const bool rows = joint_has_rows(joint_type(flags));
+    if ((kSet == kJointsPlain && rows) || (kSet == kJointsRows && !rows)) {
+        return;
+    }
+    if (kSet != kJointsPlain && rows) {
         warm_row_joint(S, j);
         return;
     }
@@ -813,12 +824,16 @@ static __device__ __noinline__ void warm_row_joint(const DevSolver &S, uint32_t 
 }
 
 // joint_solver.c:870-897, ball (360-394) and hinge (303-336).
-template <bool kUseBias>
+template <bool kUseBias, int kSet = kJointsAll>
 NPH_D void solve_joint(const DevSolver &S, uint32_t j, const StepConsts &K)
 {
     uint32_t sa, sb, flags;
     joint_head(S, j, sa, sb, flags);
-    if (joint_has_rows(joint_type(flags))) {
+    const bool rows = joint_has_rows(joint_type(flags));
+    if ((kSet == kJointsPlain && rows) || (kSet == kJointsRows && !rows)) {
+        return;
+    }
+    if (kSet != kJointsPlain && rows) {
         solve_row_joint<kUseBias>(S, j, K);
         return;
     }

@@ -56,7 +56,6 @@ enum Pass : int { kWarm = 0, kSolve = 1, kRelax = 2, kRestitution = 3 };
 // Record staging: a block copies its records between global and shared memory with 16- or
 // 8-byte accesses covering whole cache lines, and the threads work on the shared copies.
 constexpr uint32_t kStage = 128;
-constexpr uint32_t kJointStage = 64; // joint records are 464 bytes: 29 KB of shared memory
 
 template <typename V, typename Rec>
 __device__ __forceinline__ void stage_in(const Rec *src, uint32_t count, Rec *dst)
@@ -82,7 +81,6 @@ __device__ __forceinline__ void stage_out(const Rec *src, uint32_t count, Rec *d
 
 static_assert(sizeof(NphGpuBody) % 16 == 0, "body records stage in 16-byte words");
 static_assert(sizeof(NphGpuContact) % 16 == 0, "contact records stage in 16-byte words");
-static_assert(sizeof(NphGpuJoint) % 8 == 0, "joint records stage in 8-byte words");
 
 __global__ void __launch_bounds__(kStage) k_prepare_bodies(BodyArrays B, const NphGpuBody *bodies,
                                                            uint32_t n, StepConsts K)
@@ -183,21 +181,18 @@ k_prepare_contacts(DevSolver S, const NphGpuContact *contacts, const NphGpuBody 
     }
 }
 
-__global__ void __launch_bounds__(kJointStage)
+__global__ void __launch_bounds__(kBlock)
 k_prepare_joints(DevSolver S, const NphGpuJoint *joints, const NphGpuBody *bodies,
                  const NphGpuBody *fixed, uint32_t n, uint32_t nf, uint32_t nj, float h, uint32_t *err)
 {
-    __shared__ NphGpuJoint rec[kJointStage];
-    const uint32_t first = blockIdx.x * kJointStage;
-    const uint32_t count = min(kJointStage, nj - first);
-    stage_in<uint2>(joints + first, count, rec);
-    __syncthreads();
-    if (threadIdx.x >= count) {
+    // Each joint reads only what its type uses of its record (a ball or hinge joint about
+    // half of it), straight from global memory: the sectors it touches are its own.
+    const uint32_t j = blockIdx.x * kBlock + threadIdx.x;
+    if (j >= nj) {
         return;
     }
-    const uint32_t j = first + threadIdx.x;
     const uint32_t total = n + nf;
-    const NphGpuJoint &jr = rec[threadIdx.x];
+    const NphGpuJoint &jr = joints[j];
     if (jr.body_a >= total || jr.body_b >= total || nph_joint_check(&jr) != NPH_GPU_OK) {
         atomicOr(err, kErrBadJoint);
         // Inert: both ends the dummy, no impulse, nothing written.
@@ -214,16 +209,22 @@ k_prepare_joints(DevSolver S, const NphGpuJoint *joints, const NphGpuBody *bodie
     prepare_joint(S, j, jr, a, b, jr.body_a < n ? jr.body_a : n, jr.body_b < n ? jr.body_b : n, h);
 }
 
+template <int P, int kSet>
+__device__ __forceinline__ void joint_set_op(const DevSolver &S, uint32_t j, const StepConsts &K)
+{
+    if (P == kWarm) {
+        warm_joint<kSet>(S, j);
+    } else if (P == kSolve) {
+        solve_joint<true, kSet>(S, j, K);
+    } else if (P == kRelax) {
+        solve_joint<false, kSet>(S, j, K);
+    }
+}
+
 template <int P>
 __device__ __forceinline__ void joint_op(const DevSolver &S, uint32_t j, const StepConsts &K)
 {
-    if (P == kWarm) {
-        warm_joint(S, j);
-    } else if (P == kSolve) {
-        solve_joint<true>(S, j, K);
-    } else if (P == kRelax) {
-        solve_joint<false>(S, j, K);
-    }
+    joint_set_op<P, kJointsAll>(S, j, K);
 }
 
 template <int P>
@@ -255,13 +256,13 @@ k_pass(DevSolver S, uint32_t cfirst, uint32_t ccount, StepConsts K)
 
 // One colour's joints in one constraint pass. A colour's joints share no dynamic body with its
 // contacts, so the two kernels run side by side.
-template <int P>
+template <int P, int kSet>
 __global__ void __launch_bounds__(kBlock) k_joint_pass(DevSolver S, uint32_t jfirst, uint32_t jcount,
                                                        StepConsts K)
 {
     const uint32_t j = blockIdx.x * kBlock + threadIdx.x;
     if (j < jcount) {
-        joint_op<P>(S, jfirst + j, K);
+        joint_set_op<P, kSet>(S, jfirst + j, K);
     }
 }
 
@@ -460,18 +461,14 @@ __global__ void __launch_bounds__(kStage) k_store_contacts(DevSolver S, NphGpuCo
 }
 
 // The joints' accumulated impulses back into their records.
-__global__ void __launch_bounds__(kJointStage) k_store_joints(DevSolver S, NphGpuJoint *joints, uint32_t nj)
+// The impulses (and a slider's or 6-DOF joint's rows and blocks) written into the records in
+// place: the settings are not rewritten.
+__global__ void __launch_bounds__(kBlock) k_store_joints(DevSolver S, NphGpuJoint *joints, uint32_t nj)
 {
-    __shared__ NphGpuJoint rec[kJointStage];
-    const uint32_t first = blockIdx.x * kJointStage;
-    const uint32_t count = min(kJointStage, nj - first);
-    stage_in<uint2>(joints + first, count, rec);
-    __syncthreads();
-    if (threadIdx.x < count) {
-        store_joint(S, first + threadIdx.x, rec[threadIdx.x]);
+    const uint32_t j = blockIdx.x * kBlock + threadIdx.x;
+    if (j < nj) {
+        store_joint(S, j, joints[j]);
     }
-    __syncthreads();
-    stage_out<uint2>(rec, count, joints + first);
 }
 
 // finalize_body, solver.c:304-324, on staged records.
@@ -516,10 +513,6 @@ __global__ void __launch_bounds__(kBlock) k_driven(DevSolver S, NphGpuBody *bodi
 
 static uint32_t blocks_for(uint64_t count) { return (uint32_t)((count + kBlock - 1) / kBlock); }
 static uint32_t stage_blocks(uint64_t count) { return (uint32_t)((count + kStage - 1) / kStage); }
-static uint32_t joint_stage_blocks(uint64_t count)
-{
-    return (uint32_t)((count + kJointStage - 1) / kJointStage);
-}
 
 // solver.c:48-65 on the host, in FP32 as the reference.
 static Soft host_make_soft(float hertz, float zeta, float h)
@@ -615,6 +608,7 @@ struct NphGpuSolver {
     uint32_t ccount[NPH_GPU_COLOR_SLOTS] = {}, jcount[NPH_GPU_COLOR_SLOTS] = {};
     uint32_t cfirst[NPH_GPU_COLOR_SLOTS] = {}, jfirst[NPH_GPU_COLOR_SLOTS] = {};
     uint32_t driven = 0;
+    uint32_t row_joints = 0; // slider, 6-DOF and distance joints: their own launch per colour
     // Pass configuration per pass kind (warm, solve, relax, restitution).
     uint32_t pass_config[4] = {2, 7, 7, 0};
     // The step graph and what it was captured for.
@@ -824,7 +818,13 @@ template <int P> void enqueue_pass(NphGpuSolver *s, const StepConsts &K)
                 js = s->side;
             }
             mark_begin(s, kKJoints, jc, 330.0 * jc);
-            k_joint_pass<P><<<blocks_for(jc), kBlock, 0, js>>>(S, s->jfirst[c], jc, K);
+            if (s->row_joints > 0u) {
+                k_joint_pass<P, kJointsPlain><<<blocks_for(jc), kBlock, 0, js>>>(S, s->jfirst[c], jc, K);
+                k_joint_pass<P, kJointsRows><<<blocks_for(jc), kBlock, 0, js>>>(S, s->jfirst[c], jc, K);
+                s->launches++;
+            } else {
+                k_joint_pass<P, kJointsPlain><<<blocks_for(jc), kBlock, 0, js>>>(S, s->jfirst[c], jc, K);
+            }
             mark_end(s);
             s->launches++;
         }
@@ -857,7 +857,7 @@ void enqueue_prepare(NphGpuSolver *s, const StepConsts &K)
     cudaMemsetAsync(s->d_err + 1, 0, NPH_GPU_COLOR_SLOTS * sizeof(uint32_t), s->stream);
     if (s->nj > 0u) {
         mark_begin(s, kKPrepareConstraints, s->nj, 330.0 * s->nj);
-        k_prepare_joints<<<joint_stage_blocks(s->nj), kJointStage, 0, s->stream>>>(
+        k_prepare_joints<<<blocks_for(s->nj), kBlock, 0, s->stream>>>(
             S, s->d_joints, s->d_bodies, s->d_fixed, s->n, s->nf, s->nj, K.h, s->d_err);
         mark_end(s);
         s->launches++;
@@ -938,7 +938,7 @@ void enqueue_step(NphGpuSolver *s, const StepConsts &K, uint32_t substeps)
     }
     if (s->nj > 0u) {
         mark_begin(s, kKStoreFinalize, s->nj, 330.0 * s->nj);
-        k_store_joints<<<joint_stage_blocks(s->nj), kJointStage, 0, s->stream>>>(S, s->d_joints, s->nj);
+        k_store_joints<<<blocks_for(s->nj), kBlock, 0, s->stream>>>(S, s->d_joints, s->nj);
         mark_end(s);
         s->launches++;
     }
@@ -1053,7 +1053,7 @@ NphGpuResult upload(NphGpuSolver *s, const NphGpuWorldView *v)
         return r;
     }
     // The joint records first: a refused view leaves the solver as it was.
-    uint32_t driven = 0;
+    uint32_t driven = 0, row_joints = 0;
     for (uint32_t j = 0; j < v->joint_count; ++j) {
         const NphGpuJoint &jr = v->joints[j];
         const int bad = nph_joint_check(&jr);
@@ -1061,6 +1061,7 @@ NphGpuResult upload(NphGpuSolver *s, const NphGpuWorldView *v)
             return (NphGpuResult)bad;
         }
         driven += nph_joint_is_driven(&jr) ? 1u : 0u;
+        row_joints += (nph_joint_has_axes(jr.type) || jr.type == NPH_GPU_JOINT_DISTANCE) ? 1u : 0u;
     }
     r = ensure_capacity(s, v->body_count, v->fixed_count, v->contact_count, v->joint_count);
     if (r != NPH_GPU_OK) {
@@ -1083,10 +1084,11 @@ NphGpuResult upload(NphGpuSolver *s, const NphGpuWorldView *v)
         cf += s->ccount[c];
         jf += s->jcount[c];
     }
-    if (!same_shape || driven != s->driven) {
+    if (!same_shape || driven != s->driven || (row_joints > 0u) != (s->row_joints > 0u)) {
         drop_graph(s);
     }
     s->driven = driven;
+    s->row_joints = row_joints;
     cudaMemcpyAsync(s->d_bodies, v->bodies, sizeof(NphGpuBody) * s->n, cudaMemcpyHostToDevice, s->stream);
     if (s->nf > 0) {
         cudaMemcpyAsync(s->d_fixed, v->fixed_bodies, sizeof(NphGpuBody) * s->nf, cudaMemcpyHostToDevice,
@@ -1214,7 +1216,7 @@ void enqueue_converge_pass(NphGpuSolver *s, const StepConsts &K, const uint32_t 
 // ------------------------------------------------------------------------------------
 
 NphGpuResult nph_solver_bind_device(NphGpuSolver *s, const NphGpuWorldView *v, uint32_t driven,
-                                    NphSolverRecords *out)
+                                    uint32_t row_joints, NphSolverRecords *out)
 {
     if (s == nullptr || v == nullptr || out == nullptr) {
         return NPH_GPU_INVALID_ARGUMENT;
@@ -1250,10 +1252,11 @@ NphGpuResult nph_solver_bind_device(NphGpuSolver *s, const NphGpuWorldView *v, u
         cf += s->ccount[c];
         jf += s->jcount[c];
     }
-    if (!same_shape || driven != s->driven) {
+    if (!same_shape || driven != s->driven || (row_joints > 0u) != (s->row_joints > 0u)) {
         drop_graph(s);
     }
     s->driven = driven;
+    s->row_joints = row_joints;
     cudaMemsetAsync(s->d_err, 0, 32 * sizeof(uint32_t), s->stream);
     s->uploaded = true;
     return nph_solver_records(s, out);

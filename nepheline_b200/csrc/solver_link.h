@@ -15,9 +15,10 @@ struct NphSolverRecords {
 
 // Sizes the solver for a world of `shape`'s counts and colour tables (its record pointers are
 // not read), marks it uploaded, and gives its device record arrays for the caller to fill on
-// the solver's stream before the next step. `driven`: the view's motor-driven hinges.
+// the solver's stream before the next step. `driven`: the view's motor-driven joints;
+// `row_joints`: its slider, 6-DOF and distance joints.
 NphGpuResult nph_solver_bind_device(NphGpuSolver *s, const NphGpuWorldView *shape, uint32_t driven,
-                                    NphSolverRecords *out);
+                                    uint32_t row_joints, NphSolverRecords *out);
 // The device record arrays of the bound world.
 NphGpuResult nph_solver_records(NphGpuSolver *s, NphSolverRecords *out);
 // The prepare kernels' error word as a result code (NPH_GPU_INVALID_ARGUMENT on a bad record).
