@@ -31,8 +31,7 @@ bool closed_form(uint32_t ta, uint32_t tb)
     if (ta > NPH_GPU_SHAPE_BOX || tb > NPH_GPU_SHAPE_BOX) {
         return false;
     }
-    return !(ta == NPH_GPU_SHAPE_BOX && tb == NPH_GPU_SHAPE_BOX) &&
-           !(ta == NPH_GPU_SHAPE_BOX && tb == NPH_GPU_SHAPE_CAPSULE) &&
+    return !(ta == NPH_GPU_SHAPE_BOX && tb == NPH_GPU_SHAPE_CAPSULE) &&
            !(ta == NPH_GPU_SHAPE_CAPSULE && tb == NPH_GPU_SHAPE_BOX);
 }
 
