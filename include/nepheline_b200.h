@@ -570,12 +570,13 @@ typedef struct NphGpuManifold {
     NphGpuManifoldPoint points[NPH_GPU_MAX_POINTS];
 } NphGpuManifold;
 
-/* nph_physics_collide (collide.c:524-535) for `count` pairs (host arrays), on the device:
- * sphere-sphere, capsule-sphere, capsule-capsule and box-sphere (collide.c:281-458) and box-box
- * (collide_hull.c:1085-1266: the oriented-box axis test, face clipping with the reduction to
- * four points, edge pairs, GJK for boxes apart), in either order; each manifold is the same bits
- * as the reference's. Box-capsule, hulls and meshes are refused (NPH_GPU_UNSUPPORTED), as is an
- * unknown type. Runs on the current device. */
+/* nph_physics_collide (collide.c:524-535) for `count` pairs (host arrays), on the device, for
+ * every pair of spheres, capsules and boxes, in either order: sphere-sphere, capsule-sphere,
+ * capsule-capsule and box-sphere (collide.c:281-458), box-capsule (collide_hull.c:207-378) and
+ * box-box (collide_hull.c:1085-1266: the oriented-box axis test, face clipping with the
+ * reduction to four points, edge pairs, GJK for shapes apart); each manifold is the same bits as
+ * the reference's. An unknown type is refused (NPH_GPU_UNSUPPORTED). Runs on the current
+ * device. */
 NPH_GPU_API NphGpuResult nph_gpu_collide(const NphGpuShape *a, const NphGpuPose *pose_a,
                                          const NphGpuShape *b, const NphGpuPose *pose_b,
                                          const float *speculative, uint32_t count,

@@ -26,14 +26,8 @@ __global__ void __launch_bounds__(256) k_collide(const NphGpuShape *a, const Nph
     out[i] = m;
 }
 
-bool closed_form(uint32_t ta, uint32_t tb)
-{
-    if (ta > NPH_GPU_SHAPE_BOX || tb > NPH_GPU_SHAPE_BOX) {
-        return false;
-    }
-    return !(ta == NPH_GPU_SHAPE_BOX && tb == NPH_GPU_SHAPE_CAPSULE) &&
-           !(ta == NPH_GPU_SHAPE_CAPSULE && tb == NPH_GPU_SHAPE_BOX);
-}
+// Spheres, capsules and boxes, every pair of them.
+bool supported(uint32_t ta, uint32_t tb) { return ta <= NPH_GPU_SHAPE_BOX && tb <= NPH_GPU_SHAPE_BOX; }
 
 template <typename T> NphGpuResult stage(T *&dst, const T *src, uint32_t count, cudaStream_t st)
 {
@@ -63,7 +57,7 @@ NPH_GPU_API NphGpuResult nph_gpu_collide(const NphGpuShape *a, const NphGpuPose 
         return NPH_GPU_INVALID_ARGUMENT;
     }
     for (uint32_t i = 0; i < count; ++i) {
-        if (!closed_form(a[i].type, b[i].type)) {
+        if (!supported(a[i].type, b[i].type)) {
             return NPH_GPU_UNSUPPORTED;
         }
     }

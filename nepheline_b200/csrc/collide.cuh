@@ -3,9 +3,9 @@
 // The narrow phase's closed-form pairs on the device (collide.c:281-458, dispatch
 // collide.c:474-535): sphere-sphere, capsule-sphere, capsule-capsule (with the segment
 // distance of Ericson, "Real-Time Collision Detection" 5.1.9, collide.c:16-59) and
-// box-sphere (the clamp, Ericson 5.1.3), and box-box (collide_box.cuh). Each keeps the
-// reference's operations in its order, so a pair's manifold is the same bits as
-// nph_physics_collide's. Box-capsule and the general hull pairs are not here.
+// box-sphere (the clamp, Ericson 5.1.3), and box-box and box-capsule (collide_box.cuh). Each
+// keeps the reference's operations in its order, so a pair's manifold is the same bits as
+// nph_physics_collide's. Hulls, meshes and heightfields are not here.
 #pragma once
 
 #include "nepheline_b200.h"
@@ -323,6 +323,8 @@ NPH_NC void collide_ordered(const NphGpuShape &a, const NphGpuPose &pa, const Np
         box_sphere(V{a.dims[0], a.dims[1], a.dims[2]}, xa, ra, b.dims[0], xb, spec, out);
     } else if (a.type == NPH_GPU_SHAPE_BOX && b.type == NPH_GPU_SHAPE_BOX) {
         boxes(V{a.dims[0], a.dims[1], a.dims[2]}, xa, ra, V{b.dims[0], b.dims[1], b.dims[2]}, xb, rb, spec, out);
+    } else if (a.type == NPH_GPU_SHAPE_BOX && b.type == NPH_GPU_SHAPE_CAPSULE) {
+        box_capsule(V{a.dims[0], a.dims[1], a.dims[2]}, xa, ra, b.dims[0], b.dims[1], xb, rb, spec, out);
     }
 }
 

@@ -261,12 +261,13 @@ struct GjkSimplex {
 // The identity pose's transforms, kept as operations (gjk.c:40-48).
 NPH_NC V identity_point(V p) { return add(rotate(Q{0.0f, 0.0f, 0.0f, 1.0f}, p), V{0.0f, 0.0f, 0.0f}); }
 
-NPH_NC uint32_t support8(const V *pts, V direction)
+// nph_physics_proxy_support (geometry.c:495-508) along a direction given in the common frame.
+NPH_NC uint32_t support(const V *pts, uint32_t count, V direction)
 {
     const V d = rotate_inverse(Q{0.0f, 0.0f, 0.0f, 1.0f}, direction);
     uint32_t best = 0u;
     float best_dot = dot(pts[0], d);
-    for (uint32_t i = 1u; i < 8u; ++i) {
+    for (uint32_t i = 1u; i < count; ++i) {
         const float x = dot(pts[i], d);
         if (x > best_dot) {
             best_dot = x;
@@ -473,9 +474,9 @@ struct GjkDistance {
     float distance;
 };
 
-// nph_physics_distance (gjk.c:306-420) of two eight-point sets at the identity pose, without
-// radii or a simplex cache.
-NPH_NC GjkDistance gjk_distance(const V *pa, const V *pb)
+// nph_physics_distance (gjk.c:306-420) of two point sets at the identity pose, without radii
+// or a simplex cache.
+NPH_NC GjkDistance gjk_distance(const V *pa, uint32_t na, const V *pb, uint32_t nb)
 {
     GjkSimplex s;
     s.v[0] = make_vertex(pa, 0u, pb, 0u);
@@ -491,8 +492,8 @@ NPH_NC GjkDistance gjk_distance(const V *pa, const V *pb)
             break;
         }
         iterations += 1u;
-        const uint32_t ia = support8(pa, neg(v));
-        const uint32_t ib = support8(pb, v);
+        const uint32_t ia = support(pa, na, neg(v));
+        const uint32_t ib = support(pb, nb, v);
         bool duplicate = false;
         for (uint32_t i = 0u; i < s.count; ++i) {
             duplicate = duplicate || (s.v[i].ia == ia && s.v[i].ib == ib);
@@ -778,7 +779,7 @@ NPH_NC void boxes(V half_a, V pa_p, Q pa_q, V half_b, V pb_p, Q pb_q, float spec
         bp.bv[i] = add(rotate(rel_q, box_vertex(half_b, i)), rel_p);
     }
     if (best > kSlop) {
-        const GjkDistance gd = gjk_distance(bp.av, bp.bv);
+        const GjkDistance gd = gjk_distance(bp.av, 8u, bp.bv, 8u);
         if (gd.distance > speculative) {
             return;
         }
@@ -837,4 +838,162 @@ NPH_NC void boxes(V half_a, V pa_p, Q pa_q, V half_b, V pb_p, Q pb_q, float spec
     for (uint32_t i = 0u; i < count; ++i) {
         push(out, add(rotate(pa_q, pts[i].p), pa_p), pts[i].sep, pts[i].id);
     }
+}
+
+// ---------------------------------------------------------------------------------------
+// Box and capsule (nph_physics_collide_hull_capsule, collide_hull.c:207-378, the box's view)
+// ---------------------------------------------------------------------------------------
+
+// clip_segment_to_face (collide_hull.c:207-249): the segment [p, q] clipped to the prism over
+// face `face`; false when nothing is left.
+NPH_NC bool clip_segment_to_face(V h, uint32_t face, V &p, V &q)
+{
+    const V n = box_plane(h, face).n;
+    float t0 = 0.0f, t1 = 1.0f;
+    const V p0 = p;
+    const V d = sub(q, p);
+    const uint32_t first = box_face_first(face);
+    uint32_t e = first;
+    uint32_t guard = 0u;
+    do {
+        const HalfEdge he = box_edge_of(e);
+        const V a = box_vertex(h, he.origin);
+        const V b = box_vertex(h, box_edge_of(he.next).origin);
+        const V side = cross(sub(b, a), n);
+        const float s0 = dot(side, sub(p0, a));
+        const float sd = dot(side, d);
+        if (sd == 0.0f) {
+            if (s0 > 0.0f) {
+                return false;
+            }
+        } else {
+            const float t = -s0 / sd;
+            if (sd > 0.0f) {
+                t1 = fmin_(t1, t);
+            } else {
+                t0 = fmax_(t0, t);
+            }
+            if (t0 > t1) {
+                return false;
+            }
+        }
+        e = he.next;
+        guard += 1u;
+    } while (e != first && guard < 24u);
+    p = mul_add(p0, d, t0);
+    q = mul_add(p0, d, t1);
+    return true;
+}
+
+NPH_NC void box_capsule(V h, V pa_p, Q pa_q, float half_height, float radius, V pb_p, Q pb_q, float speculative,
+                        NphGpuManifold &out)
+{
+    const V rel_p = rotate_inverse(pa_q, sub(pb_p, pa_p));
+    const Q rel_q = q_mul(Q{-pa_q.x, -pa_q.y, -pa_q.z, pa_q.w}, pb_q);
+    const V axis = scale(axis_y(rel_q), half_height);
+    const V s0 = sub(rel_p, axis);
+    const V s1 = add(rel_p, axis);
+    const float limit = radius + speculative;
+    float face_sep = -3.40282347e38f;
+    uint32_t face = 0u;
+    for (uint32_t f = 0u; f < 6u; ++f) {
+        const Plane pl = box_plane(h, f);
+        const float s = fmin_(dot(pl.n, s0) + pl.d, dot(pl.n, s1) + pl.d);
+        if (s > face_sep) {
+            face_sep = s;
+            face = f;
+        }
+    }
+    if (face_sep > limit) {
+        return;
+    }
+    const V d = sub(s1, s0);
+    const float d_len_sq = length_sq(d);
+    float edge_sep = -3.40282347e38f;
+    uint32_t edge = 0u;
+    V edge_axis = V{0.0f, 1.0f, 0.0f};
+    if (d_len_sq > 1e-12f) {
+        for (uint32_t e = 0u; e < 24u; e += 2u) {
+            const HalfEdge he = box_edge_of(e);
+            const V n1 = box_plane(h, he.face).n;
+            const V n2 = box_plane(h, box_edge_of(e + 1u).face).n;
+            if (dot(n1, d) * dot(n2, d) >= 0.0f) {
+                continue;
+            }
+            const V p = box_vertex(h, he.origin);
+            const V u = sub(box_vertex(h, box_edge_of(he.next).origin), p);
+            V x = cross(u, d);
+            const float len = length(x);
+            if (len < 0.005f * sqrtf(length_sq(u) * d_len_sq)) {
+                continue;
+            }
+            x = scale(x, 1.0f / len);
+            if (dot(x, sub(p, V{0.0f, 0.0f, 0.0f})) < 0.0f) { // the box view's centroid is zero
+                x = neg(x);
+            }
+            const float s = dot(x, sub(s0, p));
+            if (s > edge_sep) {
+                edge_sep = s;
+                edge = e;
+                edge_axis = x;
+            }
+        }
+    }
+    if (edge_sep > limit) {
+        return;
+    }
+    constexpr float kSlop = 0.005f;
+    const bool use_face = face_sep >= edge_sep - 0.5f * kSlop;
+    const float best = use_face ? face_sep : edge_sep;
+    if (best > kSlop) {
+        V av[8];
+        for (uint32_t i = 0u; i < 8u; ++i) {
+            av[i] = box_vertex(h, i);
+        }
+        const V seg[2] = {s0, s1};
+        const GjkDistance gd = gjk_distance(av, 8u, seg, d_len_sq > 0.0f ? 2u : 1u);
+        if (gd.distance > limit) {
+            return;
+        }
+        const V sat_axis = use_face ? box_plane(h, face).n : edge_axis;
+        if (gd.distance > 0.0f && (!use_face || dot(gd.normal, sat_axis) < 0.995f)) {
+            const V surface_b = mul_add(gd.point_b, gd.normal, -radius);
+            const V mid = scale(add(gd.point_a, surface_b), 0.5f);
+            set_normal(out, rotate(pa_q, gd.normal));
+            push(out, add(rotate(pa_q, mid), pa_p), gd.distance - radius, 0x20000u);
+            return;
+        }
+    }
+    if (use_face) {
+        const Plane pl = box_plane(h, face);
+        V p = s0, q = s1;
+        if (!clip_segment_to_face(h, face, p, q)) {
+            p = (dot(pl.n, s0) + pl.d) <= (dot(pl.n, s1) + pl.d) ? s0 : s1;
+            q = p;
+        }
+        set_normal(out, rotate(pa_q, pl.n));
+        const V pts[2] = {p, q};
+        const uint32_t count = length_sq(sub(p, q)) > 1e-12f ? 2u : 1u;
+        for (uint32_t k = 0u; k < count; ++k) {
+            const float dist = dot(pl.n, pts[k]) + pl.d;
+            const float sep = dist - radius;
+            if (sep <= speculative) {
+                const V mid = mul_add(pts[k], pl.n, -0.5f * (dist + radius));
+                push(out, add(rotate(pa_q, mid), pa_p), sep, (face << 8u) | k);
+            }
+        }
+        return;
+    }
+    const HalfEdge he = box_edge_of(edge);
+    const V ep = box_vertex(h, he.origin);
+    const V eq = box_vertex(h, box_edge_of(he.next).origin);
+    const SegmentDistance sd = segment_distance(ep, eq, s0, s1);
+    const float sep = dot(sub(sd.c2, sd.c1), edge_axis) - radius;
+    if (sep > speculative) {
+        return;
+    }
+    const V surface_b = mul_add(sd.c2, edge_axis, -radius);
+    const V mid = scale(add(sd.c1, surface_b), 0.5f);
+    set_normal(out, rotate(pa_q, edge_axis));
+    push(out, add(rotate(pa_q, mid), pa_p), sep, 0x10000u | edge);
 }

@@ -11,7 +11,8 @@ from nepheline_b200 import abi
 KINDS = [(abi.SHAPE_SPHERE, abi.SHAPE_SPHERE), (abi.SHAPE_CAPSULE, abi.SHAPE_SPHERE),
          (abi.SHAPE_SPHERE, abi.SHAPE_CAPSULE), (abi.SHAPE_CAPSULE, abi.SHAPE_CAPSULE),
          (abi.SHAPE_BOX, abi.SHAPE_SPHERE), (abi.SHAPE_SPHERE, abi.SHAPE_BOX),
-         (abi.SHAPE_BOX, abi.SHAPE_BOX)]
+         (abi.SHAPE_BOX, abi.SHAPE_BOX), (abi.SHAPE_BOX, abi.SHAPE_CAPSULE),
+         (abi.SHAPE_CAPSULE, abi.SHAPE_BOX)]
 
 
 def _qmul(x, y):

@@ -45,15 +45,14 @@ def test_stacked_boxes_match_the_reference(ref_lib):
     assert not bad, (len(bad), bad[:5])
 
 
-def test_box_capsule_pairs_are_refused(ref_lib):
+def test_unknown_shape_types_are_refused(ref_lib):
     from nepheline_b200.solver import SolverError, collide
     box = np.zeros(1, abi.SHAPE_DTYPE)
     box["type"] = abi.SHAPE_BOX
     box["dims"] = 0.5
-    cap = np.zeros(1, abi.SHAPE_DTYPE)
-    cap["type"] = abi.SHAPE_CAPSULE
-    cap["dims"][:, :2] = (0.5, 0.2)
+    other = box.copy()
+    other["type"] = 7
     pose = np.zeros(1, abi.POSE_DTYPE)
     pose["rotation"][:, 3] = 1.0
     with pytest.raises(SolverError):
-        collide(box, pose, cap, pose, np.zeros(1, np.float32))
+        collide(box, pose, other, pose, np.zeros(1, np.float32))
