@@ -51,10 +51,12 @@ def parse():
                     help="lattice bodies per axis (128,128,64: 1,048,576 bodies)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=("lattice", "batched", "learned"), default="lattice",
+    ap.add_argument("--workload", choices=("lattice", "batched", "learned", "narrow"), default="lattice",
                     help="lattice: the 1M-body constraint graph (the headline); batched: "
                          "--worlds independent worlds in one persistent launch")
     ap.add_argument("--worlds", type=int, default=4096)
+    ap.add_argument("--pairs", type=int, default=4 * 1024 * 1024,
+                    help="narrow: shape pairs per step (boxes, spheres, capsules near contact)")
     ap.add_argument("--batch-config", default=None,
                     help="batched: fixed launch shape,shared mode,items per thread (no autotuner)")
     ap.add_argument("--pile-worlds", type=int, default=256,
@@ -232,9 +234,146 @@ def cpu_model() -> str:
     return "unknown"
 
 
+NARROW_BYTES_PER_PAIR = 2 * 16 + 2 * 28 + 4 + 96  # two shapes, two poses, speculative, manifold
+
+
+def reference_narrow_sample(sample: int, rounds: int) -> dict:
+    """The reference's nph_physics_collide over `sample` pairs, chunked over every host core
+    (the calls release the interpreter lock), `rounds` times."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from nepheline_b200 import scenes
+    from oracle.refworld import ref_collide
+    a, pa, b, pb, sp = scenes.narrow_pairs(sample, seed=0)
+    cores = os.cpu_count() or 1
+    chunks = [slice(i, min(i + 4096, sample)) for i in range(0, sample, 4096)]
+
+    def run(sl):
+        ref_collide(a[sl], pa[sl], b[sl], pb[sl], sp[sl])
+
+    with ThreadPoolExecutor(max_workers=cores) as ex:
+        list(ex.map(run, chunks))  # warm-up
+        t0 = time.perf_counter()
+        for _ in range(rounds):
+            list(ex.map(run, chunks))
+        sec = (time.perf_counter() - t0) / rounds
+    return {"value": sample / sec, "threads": cores, "ms_per_step": 1e3 * sec}
+
+
+def run_narrow(args):
+    """--workload narrow: the narrow phase (nph_gpu_collide_async) over --pairs pairs of boxes,
+    spheres and capsules near contact, one launch a step; N ranks each collide their own pairs."""
+    import torch
+
+    from nepheline_b200 import abi, scenes
+    from nepheline_b200.solver import collide_async
+
+    rank, world, local, pg = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    dev_name = f"cuda:{local}"
+    n = args.pairs
+    arrays = scenes.narrow_pairs(n, seed=rank)
+    host = [torch.from_numpy(np.ascontiguousarray(x).view(np.uint8).reshape(-1)).pin_memory() for x in arrays]
+    dev = [h.to(dev_name) for h in host]
+    out_bytes = n * abi.MANIFOLD_DTYPE.itemsize
+    out = torch.empty(out_bytes, dtype=torch.uint8, device=dev_name)
+    out_host = torch.empty(out_bytes, dtype=torch.uint8, pin_memory=True)
+    bad = torch.zeros(1, dtype=torch.int32, device=dev_name)
+    stream = torch.cuda.current_stream()
+
+    def launch():
+        collide_async(dev[0].data_ptr(), dev[1].data_ptr(), dev[2].data_ptr(), dev[3].data_ptr(),
+                      dev[4].data_ptr(), n, out.data_ptr(), bad.data_ptr(), stream.cuda_stream)
+
+    clk = Clocks(local).__enter__()
+    for _ in range(args.warmup):
+        launch()
+    torch.cuda.synchronize()
+    barrier(pg)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    clk.lines.clear()
+    e0.record(stream)
+    for _ in range(args.steps):
+        launch()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = clk.summary()
+    clk.__exit__(None, None, None)
+    ms = max_over_ranks(pg, e0.elapsed_time(e1) / args.steps)
+    value = world * n / (ms * 1e-3)
+    if int(bad.item()) != 0:
+        raise RuntimeError("narrow phase: pairs of unknown types")
+
+    # End to end: each step's pairs copied in from pinned host memory, collided, the manifolds
+    # copied back.
+    h2d = sum(h.numel() for h in host)
+    s0 = torch.cuda.Event(enable_timing=True)
+    s1 = torch.cuda.Event(enable_timing=True)
+    barrier(pg)
+    s0.record(stream)
+    for _ in range(args.e2e_steps):
+        for d, h in zip(dev, host):
+            d.copy_(h, non_blocking=True)
+        launch()
+        out_host.copy_(out, non_blocking=True)
+    s1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(pg, s0.elapsed_time(s1) / args.e2e_steps)
+    pk = peaks()
+    achieved = n * NARROW_BYTES_PER_PAIR / (ms * 1e-3) / 1e9
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import refworld
+        if refworld.ref_available():
+            r = reference_narrow_sample(262144, 3)
+            cpu = {"value": r["value"], "unit": "pairs/s", "cores": r["threads"], "kind": "reference",
+                   "sample": f"262,144 pairs of the same mix, 3 rounds of the reference's "
+                             f"nph_physics_collide on {r['threads']} threads; {cpu_model()}"}
+    if rank == 0:
+        print(json.dumps({
+            "metric": "narrow-phase pairs/s", "value": value, "unit": "pairs/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"narrow phase: {n} pairs a step per GPU (60 % box-box resting, "
+                                   f"15 % sphere-sphere, 10 % box-sphere, 10 % box-capsule, "
+                                   f"5 % capsule-capsule), speculative 4 cm",
+                       "pairs": n, "parallelism": f"pairs sharded x{world}",
+                       "l2": f"inputs and manifolds {n * NARROW_BYTES_PER_PAIR / 1e9:.2f} GB, above L2"},
+            "e2e": {"value": world * n / (e2e_ms * 1e-3), "unit": "pairs/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(out_bytes), "ms_per_step": e2e_ms},
+            "gpu_launches": args.steps,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                         "frac": achieved / pk["hbm_gbs"], "traffic": None, "kernel": "k_collide",
+                         "peak_source": pk["source"],
+                         "algorithmic_bytes_per_launch": n * NARROW_BYTES_PER_PAIR},
+            "cpu_baseline": cpu,
+            "clocks": clocks,
+        }))
+    return 0
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
+        return 0
+    if args.workload == "narrow":
+        from oracle import refworld
+        if not refworld.ref_available():
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libnphref.so was not built"}))
+            return 0
+        sample = min(args.pairs, 262144)
+        r = reference_narrow_sample(sample, max(args.steps, 1))
+        txt = f"{sample} pairs of the narrow workload's mix on {r['threads']} threads; {cpu_model()}"
+        print(json.dumps({
+            "impl": "reference", "metric": "narrow-phase pairs/s", "value": r["value"], "unit": "pairs/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": "narrow phase", "pairs": args.pairs, "sample": sample},
+            "cpu_baseline": {"value": r["value"], "unit": "pairs/s", "cores": r["threads"],
+                             "kind": "reference", "sample": txt},
+            "e2e": {"value": r["value"], "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }))
         return 0
     from oracle import refworld
     if not refworld.ref_available():
@@ -528,6 +667,8 @@ def main():
         return run_batched(args)
     if args.workload == "learned":
         return run_learned(args)
+    if args.workload == "narrow":
+        return run_narrow(args)
     import torch
 
     from nepheline_b200 import abi

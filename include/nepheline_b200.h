@@ -577,6 +577,15 @@ typedef struct NphGpuManifold {
  * reduction to four points, edge pairs, GJK for shapes apart); each manifold is the same bits as
  * the reference's. An unknown type is refused (NPH_GPU_UNSUPPORTED). Runs on the current
  * device. */
+/* The same on DEVICE arrays, enqueued on `stream` (a cudaStream_t; NULL: the default stream)
+ * without allocating or waiting: the caller owns the arrays and synchronises the stream. A pair
+ * with an unknown type gets the cleared manifold (+y, no points) and adds one to the device
+ * counter `bad_pairs` when it is not NULL. */
+NPH_GPU_API NphGpuResult nph_gpu_collide_async(const NphGpuShape *a, const NphGpuPose *pose_a,
+                                               const NphGpuShape *b, const NphGpuPose *pose_b,
+                                               const float *speculative, uint32_t count,
+                                               NphGpuManifold *out, uint32_t *bad_pairs, void *stream);
+
 NPH_GPU_API NphGpuResult nph_gpu_collide(const NphGpuShape *a, const NphGpuPose *pose_a,
                                          const NphGpuShape *b, const NphGpuPose *pose_b,
                                          const float *speculative, uint32_t count,

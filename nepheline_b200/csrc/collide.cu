@@ -12,10 +12,26 @@ namespace {
 
 __global__ void __launch_bounds__(256) k_collide(const NphGpuShape *a, const NphGpuPose *pa, const NphGpuShape *b,
                                                  const NphGpuPose *pb, const float *spec, uint32_t count,
-                                                 NphGpuManifold *out)
+                                                 NphGpuManifold *out, uint32_t *bad)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) {
+        return;
+    }
+    if (a[i].type > NPH_GPU_SHAPE_BOX || b[i].type > NPH_GPU_SHAPE_BOX) {
+        // An unknown type: the cleared manifold, and the pair counted.
+        NphGpuManifold m;
+        m.normal[0] = 0.0f;
+        m.normal[1] = 1.0f;
+        m.normal[2] = 0.0f;
+        m.point_count = 0u;
+        for (uint32_t k = 0; k < NPH_GPU_MAX_POINTS; ++k) {
+            m.points[k] = NphGpuManifoldPoint{{0.0f, 0.0f, 0.0f}, 0.0f, 0u};
+        }
+        out[i] = m;
+        if (bad != nullptr) {
+            atomicAdd(bad, 1u);
+        }
         return;
     }
     NphGpuManifold m;
@@ -77,7 +93,7 @@ NPH_GPU_API NphGpuResult nph_gpu_collide(const NphGpuShape *a, const NphGpuPose 
     if (r == NPH_GPU_OK) r = stage(ds, speculative, count, st);
     if (r == NPH_GPU_OK) r = stage(dout, (const NphGpuManifold *)nullptr, count, st);
     if (r == NPH_GPU_OK) {
-        k_collide<<<(count + 255u) / 256u, 256, 0, st>>>(da, dpa, db, dpb, ds, count, dout);
+        k_collide<<<(count + 255u) / 256u, 256, 0, st>>>(da, dpa, db, dpb, ds, count, dout, nullptr);
         cudaMemcpyAsync(out, dout, sizeof(NphGpuManifold) * count, cudaMemcpyDeviceToHost, st);
         const cudaError_t e = cudaStreamSynchronize(st);
         r = e == cudaSuccess ? NPH_GPU_OK : NPH_GPU_DEVICE_LOST;
@@ -90,6 +106,22 @@ NPH_GPU_API NphGpuResult nph_gpu_collide(const NphGpuShape *a, const NphGpuPose 
     cudaFree(dout);
     cudaStreamDestroy(st);
     return r;
+}
+
+NPH_GPU_API NphGpuResult nph_gpu_collide_async(const NphGpuShape *a, const NphGpuPose *pose_a, const NphGpuShape *b,
+                                               const NphGpuPose *pose_b, const float *speculative, uint32_t count,
+                                               NphGpuManifold *out, uint32_t *bad_pairs, void *stream)
+{
+    if (count == 0) {
+        return NPH_GPU_OK;
+    }
+    if (a == nullptr || pose_a == nullptr || b == nullptr || pose_b == nullptr || speculative == nullptr ||
+        out == nullptr) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    k_collide<<<(count + 255u) / 256u, 256, 0, (cudaStream_t)stream>>>(a, pose_a, b, pose_b, speculative, count,
+                                                                     out, bad_pairs);
+    return cudaGetLastError() == cudaSuccess ? NPH_GPU_OK : NPH_GPU_DEVICE_LOST;
 }
 
 } // extern "C"

@@ -714,3 +714,86 @@ def box_pile_batch(worlds: int = 256, seed: int = 0, min_boxes: int = 500,
     rng = np.random.default_rng(seed)
     sizes = rng.integers(min_boxes, max_boxes + 1, worlds)
     return [box_pile_world(int(n), seed * 1_000_003 + i) for i, n in enumerate(sizes)]
+
+
+# ---------------------------------------------------------------------------------------
+# Narrow-phase pairs
+# ---------------------------------------------------------------------------------------
+
+def _unit_quats(rng, n):
+    q = rng.normal(size=(n, 4))
+    return q / np.linalg.norm(q, axis=1, keepdims=True)
+
+
+def _quat_mul(x, y):
+    x1, y1, z1, w1 = x.T
+    x2, y2, z2, w2 = y.T
+    return np.stack([w1 * x2 + x1 * w2 + y1 * z2 - z1 * y2, w1 * y2 - x1 * z2 + y1 * w2 + z1 * x2,
+                     w1 * z2 + x1 * y2 - y1 * x2 + z1 * w2, w1 * w2 - x1 * x2 - y1 * y2 - z1 * z2], 1)
+
+
+def _quat_rotate(q, v):
+    u, w = q[:, :3], q[:, 3:4]
+    t = 2.0 * np.cross(u, v)
+    return v + w * t + np.cross(u, t)
+
+
+def narrow_pairs(n: int, seed: int = 0):
+    """Pairs for the narrow phase in the proportions of the piles, pours and chains the solver
+    steps, near or in contact, as the contact update hands them over (poses relative to the
+    first body, speculative distance per pair): 60 % box on box (one resting on the other,
+    tilted a little, sunk up to 2 cm or up to 3 cm apart), 15 % sphere on sphere, 10 % sphere on
+    a box, 10 % capsule on a box, 5 % capsule on capsule. Returns (a, pose_a, b, pose_b,
+    speculative) as SHAPE_DTYPE / POSE_DTYPE / float32 arrays."""
+    rng = np.random.default_rng(seed)
+    a = np.zeros(n, abi.SHAPE_DTYPE)
+    b = np.zeros(n, abi.SHAPE_DTYPE)
+    pa = np.zeros(n, abi.POSE_DTYPE)
+    pb = np.zeros(n, abi.POSE_DTYPE)
+    kind = rng.choice(5, size=n, p=[0.60, 0.15, 0.10, 0.10, 0.05])
+    qa = _unit_quats(rng, n)
+    half_a = rng.uniform(0.2, 1.0, (n, 3))
+    half_b = rng.uniform(0.2, 1.0, (n, 3))
+    radius_a = rng.uniform(0.1, 0.6, n)
+    radius_b = rng.uniform(0.1, 0.6, n)
+    core = rng.uniform(0.1, 0.8, n)
+    gap = rng.uniform(-0.02, 0.03, n)
+    tilt = rng.normal(0.0, 0.02, (n, 4))
+    tilt[:, 3] = 1.0
+    tilt /= np.linalg.norm(tilt, axis=1, keepdims=True)
+    across = rng.uniform(-0.5, 0.5, (n, 2))
+    off = np.zeros((n, 3))
+    off[:, 0], off[:, 2] = across[:, 0], across[:, 1]
+    qb = _quat_mul(qa, tilt)
+    box_b = kind == 0
+    a["type"][box_b], b["type"][box_b] = abi.SHAPE_BOX, abi.SHAPE_BOX
+    a["dims"][box_b], b["dims"][box_b] = half_a[box_b], half_b[box_b]
+    off[box_b, 1] = half_a[box_b, 1] + half_b[box_b, 1] + gap[box_b]
+    sph = kind == 1
+    a["type"][sph], b["type"][sph] = abi.SHAPE_SPHERE, abi.SHAPE_SPHERE
+    a["dims"][sph, 0], b["dims"][sph, 0] = radius_a[sph], radius_b[sph]
+    off[sph, 0] = off[sph, 2] = 0.0
+    off[sph, 1] = radius_a[sph] + radius_b[sph] + gap[sph]
+    sb = kind == 2
+    a["type"][sb], b["type"][sb] = abi.SHAPE_BOX, abi.SHAPE_SPHERE
+    a["dims"][sb], b["dims"][sb, 0] = half_a[sb], radius_b[sb]
+    off[sb, 1] = half_a[sb, 1] + radius_b[sb] + gap[sb]
+    cb = kind == 3
+    a["type"][cb], b["type"][cb] = abi.SHAPE_BOX, abi.SHAPE_CAPSULE
+    a["dims"][cb] = half_a[cb]
+    b["dims"][cb, 0], b["dims"][cb, 1] = core[cb], radius_b[cb]
+    # A capsule lying on the face: its core along the box's x, then tilted.
+    lie = np.tile(np.array([0.0, 0.0, np.sqrt(0.5), np.sqrt(0.5)]), (int(cb.sum()), 1))
+    qb[cb] = _quat_mul(qb[cb], lie)
+    off[cb, 1] = half_a[cb, 1] + radius_b[cb] + gap[cb]
+    cc = kind == 4
+    a["type"][cc], b["type"][cc] = abi.SHAPE_CAPSULE, abi.SHAPE_CAPSULE
+    a["dims"][cc, 0], a["dims"][cc, 1] = core[cc], radius_a[cc]
+    b["dims"][cc, 0], b["dims"][cc, 1] = core[cc], radius_b[cc]
+    qb[cc] = _unit_quats(rng, int(cc.sum()))
+    off[cc, 1] = radius_a[cc] + radius_b[cc] + gap[cc]
+    pa["rotation"] = qa.astype(np.float32)
+    pb["rotation"] = qb.astype(np.float32)
+    pb["position"] = _quat_rotate(qa, off).astype(np.float32)
+    spec = np.full(n, 0.04, np.float32)
+    return a, pa, b, pb, spec

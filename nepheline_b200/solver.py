@@ -69,6 +69,7 @@ def lib() -> ctypes.CDLL:
                                                     _u32, ctypes.c_float, _u32, ctypes.c_float,
                                                     _vp, _vp, P(abi.ConvergeStats)]),
         "nph_gpu_collide": (ctypes.c_int32, [_vp, _vp, _vp, _vp, _vp, _u32, _vp]),
+        "nph_gpu_collide_async": (ctypes.c_int32, [_vp, _vp, _vp, _vp, _vp, _u32, _vp, _vp, _vp]),
         "nph_gpu_batch_create": (ctypes.c_int32, [P(abi.SolverDesc), P(_vp)]),
         "nph_gpu_batch_destroy": (None, [_vp]),
         "nph_gpu_batch_stream": (_vp, [_vp]),
@@ -399,7 +400,7 @@ class Batch:
 
 def collide(a: np.ndarray, pose_a: np.ndarray, b: np.ndarray, pose_b: np.ndarray,
             speculative: np.ndarray) -> np.ndarray:
-    """The narrow phase's closed-form pairs on the device (nph_gpu_collide)."""
+    """The narrow phase on the device for pairs of spheres, capsules and boxes (nph_gpu_collide)."""
     a = np.ascontiguousarray(a, abi.SHAPE_DTYPE)
     b = np.ascontiguousarray(b, abi.SHAPE_DTYPE)
     pa = np.ascontiguousarray(pose_a, abi.POSE_DTYPE)
@@ -411,6 +412,14 @@ def collide(a: np.ndarray, pose_a: np.ndarray, b: np.ndarray, pose_b: np.ndarray
     _check(lib().nph_gpu_collide(a.ctypes.data, pa.ctypes.data, b.ctypes.data, pb.ctypes.data,
                                  sp.ctypes.data, n, out.ctypes.data), "nph_gpu_collide")
     return out
+
+
+def collide_async(a_ptr: int, pose_a_ptr: int, b_ptr: int, pose_b_ptr: int, speculative_ptr: int,
+                  count: int, out_ptr: int, bad_pairs_ptr: int = 0, stream: int = 0) -> None:
+    """nph_gpu_collide_async on device arrays (raw device pointers), enqueued on `stream`."""
+    _check(lib().nph_gpu_collide_async(a_ptr, pose_a_ptr, b_ptr, pose_b_ptr, speculative_ptr, count,
+                                       out_ptr, bad_pairs_ptr or None, stream or None),
+           "nph_gpu_collide_async")
 
 
 def version() -> str:
