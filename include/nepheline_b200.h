@@ -578,13 +578,19 @@ typedef struct NphGpuManifold {
  * the reference's. An unknown type is refused (NPH_GPU_UNSUPPORTED). Runs on the current
  * device. */
 /* The same on DEVICE arrays, enqueued on `stream` (a cudaStream_t; NULL: the default stream)
- * without allocating or waiting: the caller owns the arrays and synchronises the stream. A pair
- * with an unknown type gets the cleared manifold (+y, no points) and adds one to the device
- * counter `bad_pairs` when it is not NULL. */
+ * without allocating or waiting: the caller owns the arrays and synchronises the stream. With a
+ * device `workspace` of at least nph_gpu_collide_workspace_bytes(count) bytes (4-byte aligned)
+ * the pairs are first sorted by kind on the device, so that each warp runs one pair kind's code
+ * (the results are the same; NULL: unsorted, one launch). A pair with an unknown type gets the
+ * cleared manifold (+y, no points) and adds one to the device counter `bad_pairs` when it is
+ * not NULL. At most 2^28 - 1 pairs a call. */
+NPH_GPU_API uint64_t nph_gpu_collide_workspace_bytes(uint32_t count);
 NPH_GPU_API NphGpuResult nph_gpu_collide_async(const NphGpuShape *a, const NphGpuPose *pose_a,
                                                const NphGpuShape *b, const NphGpuPose *pose_b,
                                                const float *speculative, uint32_t count,
-                                               NphGpuManifold *out, uint32_t *bad_pairs, void *stream);
+                                               NphGpuManifold *out, uint32_t *bad_pairs,
+                                               void *workspace, uint64_t workspace_bytes,
+                                               void *stream);
 
 NPH_GPU_API NphGpuResult nph_gpu_collide(const NphGpuShape *a, const NphGpuPose *pose_a,
                                          const NphGpuShape *b, const NphGpuPose *pose_b,

@@ -10,36 +10,89 @@
 
 namespace {
 
+// One pair's manifold into out[i]: the cleared manifold and a count in `bad` for an unknown type.
+__device__ __forceinline__ void collide_pair(const NphGpuShape *a, const NphGpuPose *pa, const NphGpuShape *b,
+                                             const NphGpuPose *pb, const float *spec, uint32_t i,
+                                             NphGpuManifold *out, uint32_t *bad)
+{
+    NphGpuManifold m;
+    for (uint32_t k = 0; k < NPH_GPU_MAX_POINTS; ++k) {
+        m.points[k] = NphGpuManifoldPoint{{0.0f, 0.0f, 0.0f}, 0.0f, 0u};
+    }
+    if (a[i].type > NPH_GPU_SHAPE_BOX || b[i].type > NPH_GPU_SHAPE_BOX) {
+        m.normal[0] = 0.0f;
+        m.normal[1] = 1.0f;
+        m.normal[2] = 0.0f;
+        m.point_count = 0u;
+        if (bad != nullptr) {
+            atomicAdd(bad, 1u);
+        }
+    } else {
+        nph_nc::collide(a[i], pa[i], b[i], pb[i], spec[i], m);
+    }
+    out[i] = m;
+}
+
 __global__ void __launch_bounds__(256) k_collide(const NphGpuShape *a, const NphGpuPose *pa, const NphGpuShape *b,
                                                  const NphGpuPose *pb, const float *spec, uint32_t count,
                                                  NphGpuManifold *out, uint32_t *bad)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= count) {
-        return;
+    if (i < count) {
+        collide_pair(a, pa, b, pb, spec, i, out, bad);
     }
-    if (a[i].type > NPH_GPU_SHAPE_BOX || b[i].type > NPH_GPU_SHAPE_BOX) {
-        // An unknown type: the cleared manifold, and the pair counted.
-        NphGpuManifold m;
-        m.normal[0] = 0.0f;
-        m.normal[1] = 1.0f;
-        m.normal[2] = 0.0f;
-        m.point_count = 0u;
-        for (uint32_t k = 0; k < NPH_GPU_MAX_POINTS; ++k) {
-            m.points[k] = NphGpuManifoldPoint{{0.0f, 0.0f, 0.0f}, 0.0f, 0u};
+}
+
+// The pair kinds, (type a, type b) in 0..15 (unknown types share kind 15), counted and each pair
+// given its place among its kind's: the warps of the sorted launch then run one kind's code.
+constexpr uint32_t kKinds = 16u;
+
+__device__ __forceinline__ uint32_t pair_kind(const NphGpuShape &a, const NphGpuShape &b)
+{
+    return a.type <= NPH_GPU_SHAPE_BOX && b.type <= NPH_GPU_SHAPE_BOX ? a.type * 3u + b.type : kKinds - 1u;
+}
+
+__global__ void __launch_bounds__(256) k_classify(const NphGpuShape *a, const NphGpuShape *b, uint32_t count,
+                                                  uint32_t *counts, uint32_t *place)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) {
+        const uint32_t k = pair_kind(a[i], b[i]);
+        place[i] = (k << 28u) | atomicAdd(&counts[k], 1u);
+    }
+}
+
+__global__ void k_kind_offsets(uint32_t *counts)
+{
+    if (threadIdx.x == 0u) {
+        uint32_t sum = 0u;
+        for (uint32_t k = 0; k < kKinds; ++k) {
+            const uint32_t c = counts[k];
+            counts[kKinds + k] = sum;
+            sum += c;
         }
-        out[i] = m;
-        if (bad != nullptr) {
-            atomicAdd(bad, 1u);
-        }
-        return;
     }
-    NphGpuManifold m;
-    for (uint32_t k = 0; k < NPH_GPU_MAX_POINTS; ++k) {
-        m.points[k] = NphGpuManifoldPoint{{0.0f, 0.0f, 0.0f}, 0.0f, 0u};
+}
+
+__global__ void __launch_bounds__(256) k_scatter(const uint32_t *counts, const uint32_t *place, uint32_t count,
+                                                 uint32_t *order)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < count) {
+        const uint32_t p = place[i];
+        order[counts[kKinds + (p >> 28u)] + (p & 0x0FFFFFFFu)] = i;
     }
-    nph_nc::collide(a[i], pa[i], b[i], pb[i], spec[i], m);
-    out[i] = m;
+}
+
+__global__ void __launch_bounds__(256) k_collide_sorted(const NphGpuShape *a, const NphGpuPose *pa,
+                                                        const NphGpuShape *b, const NphGpuPose *pb,
+                                                        const float *spec, uint32_t count, const uint32_t *order,
+                                                        NphGpuManifold *out, uint32_t *bad)
+{
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < count) {
+        collide_pair(a, pa, b, pb, spec, order[t], out, bad);
+    }
 }
 
 // Spheres, capsules and boxes, every pair of them.
@@ -86,14 +139,19 @@ NPH_GPU_API NphGpuResult nph_gpu_collide(const NphGpuShape *a, const NphGpuPose 
     NphGpuPose *dpa = nullptr, *dpb = nullptr;
     float *ds = nullptr;
     NphGpuManifold *dout = nullptr;
+    uint32_t *dws = nullptr;
+    const uint64_t ws_words = (2ull * 16u + 2ull * count);
     NphGpuResult r = stage(da, a, count, st);
     if (r == NPH_GPU_OK) r = stage(db, b, count, st);
     if (r == NPH_GPU_OK) r = stage(dpa, pose_a, count, st);
     if (r == NPH_GPU_OK) r = stage(dpb, pose_b, count, st);
     if (r == NPH_GPU_OK) r = stage(ds, speculative, count, st);
     if (r == NPH_GPU_OK) r = stage(dout, (const NphGpuManifold *)nullptr, count, st);
+    if (r == NPH_GPU_OK) r = stage(dws, (const uint32_t *)nullptr, (uint32_t)ws_words, st);
     if (r == NPH_GPU_OK) {
-        k_collide<<<(count + 255u) / 256u, 256, 0, st>>>(da, dpa, db, dpb, ds, count, dout, nullptr);
+        r = nph_gpu_collide_async(da, dpa, db, dpb, ds, count, dout, nullptr, dws, ws_words * sizeof(uint32_t), st);
+    }
+    if (r == NPH_GPU_OK) {
         cudaMemcpyAsync(out, dout, sizeof(NphGpuManifold) * count, cudaMemcpyDeviceToHost, st);
         const cudaError_t e = cudaStreamSynchronize(st);
         r = e == cudaSuccess ? NPH_GPU_OK : NPH_GPU_DEVICE_LOST;
@@ -104,23 +162,45 @@ NPH_GPU_API NphGpuResult nph_gpu_collide(const NphGpuShape *a, const NphGpuPose 
     cudaFree(dpb);
     cudaFree(ds);
     cudaFree(dout);
+    cudaFree(dws);
     cudaStreamDestroy(st);
     return r;
 }
 
+NPH_GPU_API uint64_t nph_gpu_collide_workspace_bytes(uint32_t count)
+{
+    return 2ull * kKinds * sizeof(uint32_t) + 2ull * count * sizeof(uint32_t);
+}
+
 NPH_GPU_API NphGpuResult nph_gpu_collide_async(const NphGpuShape *a, const NphGpuPose *pose_a, const NphGpuShape *b,
                                                const NphGpuPose *pose_b, const float *speculative, uint32_t count,
-                                               NphGpuManifold *out, uint32_t *bad_pairs, void *stream)
+                                               NphGpuManifold *out, uint32_t *bad_pairs, void *workspace,
+                                               uint64_t workspace_bytes, void *stream)
 {
     if (count == 0) {
         return NPH_GPU_OK;
     }
     if (a == nullptr || pose_a == nullptr || b == nullptr || pose_b == nullptr || speculative == nullptr ||
-        out == nullptr) {
+        out == nullptr || count >= (1u << 28)) {
         return NPH_GPU_INVALID_ARGUMENT;
     }
-    k_collide<<<(count + 255u) / 256u, 256, 0, (cudaStream_t)stream>>>(a, pose_a, b, pose_b, speculative, count,
-                                                                     out, bad_pairs);
+    const cudaStream_t st = (cudaStream_t)stream;
+    const uint32_t blocks = (count + 255u) / 256u;
+    if (workspace == nullptr) {
+        k_collide<<<blocks, 256, 0, st>>>(a, pose_a, b, pose_b, speculative, count, out, bad_pairs);
+    } else {
+        if (workspace_bytes < nph_gpu_collide_workspace_bytes(count) || ((uintptr_t)workspace & 3u) != 0u) {
+            return NPH_GPU_INVALID_ARGUMENT;
+        }
+        uint32_t *counts = (uint32_t *)workspace;
+        uint32_t *place = counts + 2u * kKinds;
+        uint32_t *order = place + count;
+        cudaMemsetAsync(counts, 0, kKinds * sizeof(uint32_t), st);
+        k_classify<<<blocks, 256, 0, st>>>(a, b, count, counts, place);
+        k_kind_offsets<<<1, 32, 0, st>>>(counts);
+        k_scatter<<<blocks, 256, 0, st>>>(counts, place, count, order);
+        k_collide_sorted<<<blocks, 256, 0, st>>>(a, pose_a, b, pose_b, speculative, count, order, out, bad_pairs);
+    }
     return cudaGetLastError() == cudaSuccess ? NPH_GPU_OK : NPH_GPU_DEVICE_LOST;
 }
 

@@ -69,7 +69,9 @@ def lib() -> ctypes.CDLL:
                                                     _u32, ctypes.c_float, _u32, ctypes.c_float,
                                                     _vp, _vp, P(abi.ConvergeStats)]),
         "nph_gpu_collide": (ctypes.c_int32, [_vp, _vp, _vp, _vp, _vp, _u32, _vp]),
-        "nph_gpu_collide_async": (ctypes.c_int32, [_vp, _vp, _vp, _vp, _vp, _u32, _vp, _vp, _vp]),
+        "nph_gpu_collide_async": (ctypes.c_int32, [_vp, _vp, _vp, _vp, _vp, _u32, _vp, _vp, _vp,
+                                                   ctypes.c_uint64, _vp]),
+        "nph_gpu_collide_workspace_bytes": (ctypes.c_uint64, [_u32]),
         "nph_gpu_batch_create": (ctypes.c_int32, [P(abi.SolverDesc), P(_vp)]),
         "nph_gpu_batch_destroy": (None, [_vp]),
         "nph_gpu_batch_stream": (_vp, [_vp]),
@@ -414,12 +416,18 @@ def collide(a: np.ndarray, pose_a: np.ndarray, b: np.ndarray, pose_b: np.ndarray
     return out
 
 
+def collide_workspace_bytes(count: int) -> int:
+    return int(lib().nph_gpu_collide_workspace_bytes(count))
+
+
 def collide_async(a_ptr: int, pose_a_ptr: int, b_ptr: int, pose_b_ptr: int, speculative_ptr: int,
-                  count: int, out_ptr: int, bad_pairs_ptr: int = 0, stream: int = 0) -> None:
-    """nph_gpu_collide_async on device arrays (raw device pointers), enqueued on `stream`."""
+                  count: int, out_ptr: int, bad_pairs_ptr: int = 0, workspace_ptr: int = 0,
+                  workspace_bytes: int = 0, stream: int = 0) -> None:
+    """nph_gpu_collide_async on device arrays (raw device pointers), enqueued on `stream`; with a
+    workspace the pairs are sorted by kind on the device first."""
     _check(lib().nph_gpu_collide_async(a_ptr, pose_a_ptr, b_ptr, pose_b_ptr, speculative_ptr, count,
-                                       out_ptr, bad_pairs_ptr or None, stream or None),
-           "nph_gpu_collide_async")
+                                       out_ptr, bad_pairs_ptr or None, workspace_ptr or None,
+                                       workspace_bytes, stream or None), "nph_gpu_collide_async")
 
 
 def version() -> str:
