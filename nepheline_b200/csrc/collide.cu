@@ -57,8 +57,17 @@ __global__ void __launch_bounds__(256) k_classify(const NphGpuShape *a, const Np
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < count) {
+        // One atomic per kind and warp: the lanes of a kind take consecutive places.
         const uint32_t k = pair_kind(a[i], b[i]);
-        place[i] = (k << 28u) | atomicAdd(&counts[k], 1u);
+        const uint32_t lane = threadIdx.x & 31u;
+        const uint32_t group = __match_any_sync(__activemask(), k);
+        const uint32_t leader = __ffs(group) - 1u;
+        uint32_t base = 0u;
+        if (lane == leader) {
+            base = atomicAdd(&counts[k], (uint32_t)__popc(group));
+        }
+        base = __shfl_sync(group, base, leader);
+        place[i] = (k << 28u) | (base + (uint32_t)__popc(group & ((1u << lane) - 1u)));
     }
 }
 
