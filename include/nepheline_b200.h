@@ -675,6 +675,24 @@ NPH_GPU_API NphGpuResult nph_gpu_mlp_train(NphGpuMlp *mlp, const float *features
  *   15   the tangent effective-mass inverse's first entry times kn
  * `scale` is g h / kn, the impulse a network output of 1 stands for; `kind` a
  * NPH_GPU_POINT_* value. */
+/* The island sleep decision of a step (phys_island_sleep_and_split, island.c:675-735; world.c:350-
+ * 358) on the uploaded world, after its step: the bodies' sleep clocks are read on the device.
+ * `island_of` (one per uploaded body, the view's order) gives the place of the body's island in
+ * the world's awake-island list, or NPH_GPU_NULL for a body in no island (kinematic);
+ * `removed` (one per awake island) its constraint_remove_count; `time_to_sleep` the world's
+ * setting. Writes `sleep` (per awake island: 1 when the island falls asleep whole), `*split`
+ * (the awake-island place of the island to split, or NPH_GPU_NULL) and `kinematic_sleep` (per
+ * body: 1 for a kinematic body that falls asleep on its own clock). Each island's clock is its
+ * stillest body's (a body that may not sleep counts as just moved); an island that lost
+ * constraints is not put to sleep, and of those whose sleepiest body is ready, the one most
+ * ready (first in the list on a tie) is split. The caller carries out the list moves
+ * (island_sleep, island_split, the awake list). NPH_GPU_INVALID_ARGUMENT for an island index past
+ * island_count. Host arrays. */
+NPH_GPU_API NphGpuResult nph_gpu_world_sleep_decision(NphGpuSolver *solver, const uint32_t *island_of,
+                                                     uint32_t island_count, const uint32_t *removed,
+                                                     float time_to_sleep, uint8_t *sleep, uint32_t *split,
+                                                     uint8_t *kinematic_sleep);
+
 NPH_GPU_API NphGpuResult nph_gpu_world_features(NphGpuSolver *solver,
                                                 const NphGpuWorldParams *params, float dt,
                                                 float *features, float *scale, uint32_t *kind,

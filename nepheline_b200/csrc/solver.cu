@@ -564,6 +564,84 @@ StepConsts make_step_consts(const NphGpuWorldParams &p, float dt)
     return K;
 }
 
+// ---------------------------------------------------------------------------------------
+// The island sleep decision (phys_island_sleep_and_split, island.c:675-735)
+// ---------------------------------------------------------------------------------------
+
+// Floats as keys that order as the floats do (non-NaN), for atomic min and max.
+__device__ __forceinline__ uint32_t order_key(float f)
+{
+    const uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) != 0u ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float order_value(uint32_t k)
+{
+    return __uint_as_float((k & 0x80000000u) != 0u ? (k & 0x7FFFFFFFu) : ~k);
+}
+
+__global__ void __launch_bounds__(256) k_island_init(uint32_t *tmin, uint32_t *tmax, uint32_t islands,
+                                                     unsigned long long *split)
+{
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < islands) {
+        tmin[k] = order_key(1e30f);
+        tmax[k] = order_key(0.0f);
+    }
+    if (k == 0u) {
+        *split = 0ull;
+    }
+}
+
+// Each island's stillest and sleepiest body clock (a body without sleep counts as just
+// moved), and each kinematic body's own verdict.
+__global__ void __launch_bounds__(256) k_island_bounds(const NphGpuBody *bodies, uint32_t n,
+                                                       const uint32_t *island_of, uint32_t islands,
+                                                       float time_to_sleep, uint32_t *tmin, uint32_t *tmax,
+                                                       uint8_t *kinematic, uint32_t *err)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) {
+        return;
+    }
+    const NphGpuBody &b = bodies[i];
+    const bool may_sleep = (b.flags & NPH_GPU_BODY_ENABLE_SLEEP) != 0u;
+    const uint32_t k = island_of[i];
+    if (k != NPH_GPU_NULL) {
+        if (k >= islands) {
+            atomicOr(err, kErrBadIndex);
+        } else {
+            const uint32_t key = order_key(may_sleep ? b.sleep_time : 0.0f);
+            atomicMin(&tmin[k], key);
+            atomicMax(&tmax[k], key);
+        }
+    }
+    kinematic[i] = (b.type == NPH_GPU_BODY_KINEMATIC && may_sleep && b.sleep_time >= time_to_sleep) ? 1u : 0u;
+}
+
+// Whole islands whose stillest body is ready sleep; of those that lost constraints, the one
+// whose sleepiest body is most ready (the first such in the list) is split instead.
+__global__ void __launch_bounds__(256) k_island_decide(const uint32_t *tmin, const uint32_t *tmax,
+                                                       const uint32_t *removed, uint32_t islands,
+                                                       float time_to_sleep, uint8_t *sleep,
+                                                       unsigned long long *split)
+{
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= islands) {
+        return;
+    }
+    const float t = order_value(tmin[k]);
+    const float sleepiest = order_value(tmax[k]);
+    uint8_t asleep = 0u;
+    if (removed[k] > 0u) {
+        if (sleepiest >= time_to_sleep && sleepiest > 0.0f) {
+            atomicMax(split, ((unsigned long long)order_key(sleepiest) << 32) | (0xFFFFFFFFull - k));
+        }
+    } else if (t >= time_to_sleep) {
+        asleep = 1u;
+    }
+    sleep[k] = asleep;
+}
+
 } // namespace nph
 
 using namespace nph;
@@ -1711,6 +1789,76 @@ NPH_GPU_API NphGpuResult nph_gpu_solver_set_warm_start_model(NphGpuSolver *s, Np
     s->mlp = mlp;
     drop_graph(s);
     return ensure_learned(s);
+}
+
+NPH_GPU_API NphGpuResult nph_gpu_world_sleep_decision(NphGpuSolver *s, const uint32_t *island_of,
+                                                     uint32_t island_count, const uint32_t *removed,
+                                                     float time_to_sleep, uint8_t *sleep, uint32_t *split,
+                                                     uint8_t *kinematic_sleep)
+{
+    if (s == nullptr || split == nullptr || (s->n > 0u && (island_of == nullptr || kinematic_sleep == nullptr)) ||
+        (island_count > 0u && (removed == nullptr || sleep == nullptr))) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    if (!s->uploaded) {
+        return NPH_GPU_INVALID_STATE;
+    }
+    *split = NPH_GPU_NULL;
+    cudaSetDevice(s->device);
+    const uint32_t n = s->n;
+    const uint32_t ni = island_count;
+    uint32_t *d_of = nullptr, *d_removed = nullptr, *d_min = nullptr, *d_max = nullptr;
+    uint8_t *d_sleep = nullptr, *d_kin = nullptr;
+    uint32_t *d_bad = nullptr;
+    unsigned long long *d_split = nullptr;
+    const bool ok = dalloc(d_bad, 1) && dalloc(d_of, std::max<uint32_t>(n, 1u)) && dalloc(d_kin, std::max<uint32_t>(n, 1u)) &&
+                    dalloc(d_removed, std::max<uint32_t>(ni, 1u)) && dalloc(d_min, std::max<uint32_t>(ni, 1u)) &&
+                    dalloc(d_max, std::max<uint32_t>(ni, 1u)) && dalloc(d_sleep, std::max<uint32_t>(ni, 1u)) &&
+                    dalloc(d_split, 1);
+    NphGpuResult r = ok ? NPH_GPU_OK : NPH_GPU_OUT_OF_MEMORY;
+    if (r == NPH_GPU_OK) {
+        cudaMemsetAsync(d_bad, 0, sizeof(uint32_t), s->stream);
+        if (n > 0u) {
+            cudaMemcpyAsync(d_of, island_of, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, s->stream);
+        }
+        if (ni > 0u) {
+            cudaMemcpyAsync(d_removed, removed, sizeof(uint32_t) * ni, cudaMemcpyHostToDevice, s->stream);
+        }
+        k_island_init<<<blocks_for(std::max<uint32_t>(ni, 1u)), kBlock, 0, s->stream>>>(d_min, d_max, ni, d_split);
+        if (n > 0u) {
+            k_island_bounds<<<blocks_for(n), kBlock, 0, s->stream>>>(s->d_bodies, n, d_of, ni, time_to_sleep, d_min,
+                                                                     d_max, d_kin, d_bad);
+        }
+        if (ni > 0u) {
+            k_island_decide<<<blocks_for(ni), kBlock, 0, s->stream>>>(d_min, d_max, d_removed, ni, time_to_sleep,
+                                                                      d_sleep, d_split);
+            cudaMemcpyAsync(sleep, d_sleep, ni, cudaMemcpyDeviceToHost, s->stream);
+        }
+        if (n > 0u) {
+            cudaMemcpyAsync(kinematic_sleep, d_kin, n, cudaMemcpyDeviceToHost, s->stream);
+        }
+        unsigned long long key = 0ull;
+        uint32_t bad = 0u;
+        cudaMemcpyAsync(&key, d_split, sizeof key, cudaMemcpyDeviceToHost, s->stream);
+        cudaMemcpyAsync(&bad, d_bad, sizeof bad, cudaMemcpyDeviceToHost, s->stream);
+        r = check_cuda(cudaStreamSynchronize(s->stream));
+        if (r == NPH_GPU_OK && bad != 0u) {
+            r = NPH_GPU_INVALID_ARGUMENT; // an island index past island_count
+        }
+        if (r == NPH_GPU_OK && key != 0ull) {
+            *split = 0xFFFFFFFFu - (uint32_t)(key & 0xFFFFFFFFull);
+        }
+    }
+    cudaGetLastError();
+    dfree(d_bad);
+    dfree(d_of);
+    dfree(d_kin);
+    dfree(d_removed);
+    dfree(d_min);
+    dfree(d_max);
+    dfree(d_sleep);
+    dfree(d_split);
+    return r;
 }
 
 NPH_GPU_API NphGpuResult nph_gpu_world_features(NphGpuSolver *s, const NphGpuWorldParams *params, float dt,

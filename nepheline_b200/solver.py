@@ -69,6 +69,8 @@ def lib() -> ctypes.CDLL:
                                                     _u32, ctypes.c_float, _u32, ctypes.c_float,
                                                     _vp, _vp, P(abi.ConvergeStats)]),
         "nph_gpu_collide": (ctypes.c_int32, [_vp, _vp, _vp, _vp, _vp, _u32, _vp]),
+        "nph_gpu_world_sleep_decision": (ctypes.c_int32, [_vp, _vp, _u32, _vp, ctypes.c_float, _vp, _vp,
+                                                          _vp]),
         "nph_gpu_collide_async": (ctypes.c_int32, [_vp, _vp, _vp, _vp, _vp, _u32, _vp, _vp, _vp,
                                                    ctypes.c_uint64, _vp]),
         "nph_gpu_collide_workspace_bytes": (ctypes.c_uint64, [_u32]),
@@ -183,6 +185,21 @@ class Solver:
     def set_pass_config(self, pass_kind: int, config: int) -> None:
         _check(self.L.nph_gpu_solver_set_pass_config(self._h, pass_kind, config),
                "nph_gpu_solver_set_pass_config")
+
+    def sleep_decision(self, island_of: np.ndarray, removed: np.ndarray, time_to_sleep: float):
+        """nph_gpu_world_sleep_decision for the uploaded world: (islands that sleep as a bool
+        array, the island to split or None, kinematic bodies that sleep as a bool array)."""
+        island_of = np.ascontiguousarray(island_of, np.uint32)
+        removed = np.ascontiguousarray(removed, np.uint32)
+        sleep = np.zeros(max(len(removed), 1), np.uint8)
+        kin = np.zeros(max(len(island_of), 1), np.uint8)
+        split = _u32()
+        _check(self.L.nph_gpu_world_sleep_decision(self._h, island_of.ctypes.data, len(removed),
+                                                   removed.ctypes.data, time_to_sleep, sleep.ctypes.data,
+                                                   ctypes.byref(split), kin.ctypes.data),
+               "nph_gpu_world_sleep_decision")
+        k = int(split.value)
+        return sleep[:len(removed)] != 0, (None if k == abi.NULL else k), kin[:len(island_of)] != 0
 
     def update_contacts(self, fresh: np.ndarray) -> None:
         """This step's manifolds (one per uploaded contact, same order, impulses zero),

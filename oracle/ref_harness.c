@@ -361,6 +361,57 @@ REF_API int nphref_finish(RefWorld *r)
     return (int)res;
 }
 
+// The island stage in its two halves (world.c:350-358), for a caller that decides between them:
+// the merge of the step's links, then sleep and split.
+REF_API int nphref_merge_islands(RefWorld *r)
+{
+    return (int)phys_island_merge_pending(r->w);
+}
+
+REF_API int nphref_sleep_islands(RefWorld *r)
+{
+    return r->w->desc.enable_sleep != 0 ? (int)phys_island_sleep_and_split(r->w) : 0;
+}
+
+// The islands as the sleep decision reads them (island.c:675-735), after the merge: per awake
+// body (awake-list order: the view's) the place of its island in the awake-island list, or
+// PHYS_NULL for a body in no island (kinematic); per awake island its record index and its
+// constraint_remove_count. Returns the awake-island count (arrays of `cap` islands).
+REF_API u32 nphref_island_view(const RefWorld *r, u32 *island_of, u32 *island_ids, u32 *removed, u32 cap)
+{
+    const NphPhysicsWorld *w = r->w;
+    const u32 n = w->awake_islands.len;
+    for (u32 k = 0U; k < n && k < cap; ++k) {
+        island_ids[k] = w->awake_islands.data[k];
+        removed[k] = w->islands.data[w->awake_islands.data[k]].constraint_remove_count;
+    }
+    for (u32 i = 0U; i < w->awake_bodies.len; ++i) {
+        const PhysBody *b = &w->bodies.data[w->awake_bodies.data[i]];
+        island_of[i] = b->island != PHYS_NULL ? w->islands.data[b->island].awake_slot : PHYS_NULL;
+    }
+    return n;
+}
+
+// An island record's constraint_remove_count and whether it is live and awake.
+REF_API void nphref_island_state(const RefWorld *r, u32 island, u32 *removed, u32 *awake)
+{
+    const PhysIsland *is = &r->w->islands.data[island];
+    *removed = is->constraint_remove_count;
+    *awake = is->live != 0U && is->awake != 0U ? 1U : 0U;
+}
+
+// The creation index of each awake body, in awake-list order.
+REF_API void nphref_awake_creation_ids(const RefWorld *r, u32 *out)
+{
+    const NphPhysicsWorld *w = r->w;
+    for (u32 c = 0U; c < r->body_count; ++c) {
+        const PhysBody *b = phys_body(w, r->bodies[c]);
+        if (b != NULL && b->awake_slot != PHYS_NULL) {
+            out[b->awake_slot] = c;
+        }
+    }
+}
+
 REF_API int nphref_step(RefWorld *r, f32 dt)
 {
     return (int)nph_physics_world_step(r->w, dt, r->js);

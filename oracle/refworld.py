@@ -69,6 +69,11 @@ def _ref_lib():
             "nphref_stats": (None, [_vp, _vp, _vp, _vp, _vp, _vp]),
             "nphref_set_velocity": (None, [_vp, _u32, _vp, _vp]),
             "nphref_collide_pairs": (None, [_vp, _vp, _vp, _vp, _vp, _u32, _vp]),
+            "nphref_merge_islands": (ctypes.c_int, [_vp]),
+            "nphref_sleep_islands": (ctypes.c_int, [_vp]),
+            "nphref_island_view": (_u32, [_vp, _vp, _vp, _vp, _u32]),
+            "nphref_island_state": (None, [_vp, _u32, _vp, _vp]),
+            "nphref_awake_creation_ids": (None, [_vp, _vp]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -206,6 +211,35 @@ class RefWorld:
         r = self.lib.nphref_finish(self._h)
         if r != 0:
             raise RuntimeError(f"reference island stage failed: {r}")
+
+    def merge_islands(self):
+        r = self.lib.nphref_merge_islands(self._h)
+        if r != 0:
+            raise RuntimeError(f"reference island merge failed: {r}")
+
+    def sleep_islands(self):
+        r = self.lib.nphref_sleep_islands(self._h)
+        if r != 0:
+            raise RuntimeError(f"reference sleep and split failed: {r}")
+
+    def island_view(self, awake_bodies: int):
+        """(island_of per awake body, island record ids, constraint_remove_count per awake island)."""
+        cap = max(awake_bodies, 1)
+        island_of = np.zeros(cap, np.uint32)
+        ids = np.zeros(cap, np.uint32)
+        removed = np.zeros(cap, np.uint32)
+        n = self.lib.nphref_island_view(self._h, _p(island_of), _p(ids), _p(removed), cap)
+        return island_of[:awake_bodies], ids[:n], removed[:n]
+
+    def island_state(self, island: int):
+        removed, awake = ctypes.c_uint32(), ctypes.c_uint32()
+        self.lib.nphref_island_state(self._h, island, ctypes.byref(removed), ctypes.byref(awake))
+        return int(removed.value), bool(awake.value)
+
+    def awake_creation_ids(self, awake_bodies: int) -> np.ndarray:
+        out = np.zeros(max(awake_bodies, 1), np.uint32)
+        self.lib.nphref_awake_creation_ids(self._h, _p(out))
+        return out[:awake_bodies]
 
     def step(self, dt: float):
         r = self.lib.nphref_step(self._h, dt)
