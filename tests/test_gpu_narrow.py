@@ -56,3 +56,38 @@ def test_unknown_shape_types_are_refused(ref_lib):
     pose["rotation"][:, 3] = 1.0
     with pytest.raises(SolverError):
         collide(box, pose, other, pose, np.zeros(1, np.float32))
+
+
+def test_async_sorted_and_unsorted_launches_agree(ref_lib):
+    """nph_gpu_collide_async on device arrays: with the workspace (pairs sorted by kind on the
+    device) and without (one launch) the manifolds are the same, and a pair of an unknown type
+    gets the cleared manifold and is counted."""
+    import torch
+
+    from nepheline_b200 import scenes
+    from nepheline_b200.solver import collide_async, collide_workspace_bytes
+    a, pa, b, pb, sp = scenes.narrow_pairs(50000, seed=9)
+    a["type"][123] = 9
+    arrays = [a, pa, b, pb, sp]
+    dev = [torch.from_numpy(np.ascontiguousarray(x).view(np.uint8).reshape(-1)).to("cuda:0") for x in arrays]
+    n = len(a)
+    outs = []
+    for sorted_ in (False, True):
+        out = torch.empty(n * abi.MANIFOLD_DTYPE.itemsize, dtype=torch.uint8, device="cuda:0")
+        bad = torch.zeros(1, dtype=torch.int32, device="cuda:0")
+        ws_bytes = collide_workspace_bytes(n) if sorted_ else 0
+        ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device="cuda:0")
+        collide_async(*[d.data_ptr() for d in dev], n, out.data_ptr(), bad.data_ptr(),
+                      ws.data_ptr() if sorted_ else 0, ws_bytes, torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        assert int(bad.item()) == 1
+        outs.append(out.cpu().numpy().view(abi.MANIFOLD_DTYPE))
+    assert outs[0].tobytes() == outs[1].tobytes()
+    assert outs[0][123]["point_count"] == 0 and tuple(outs[0][123]["normal"]) == (0.0, 1.0, 0.0)
+    from oracle.refworld import ref_collide
+    keep = np.ones(n, bool)
+    keep[123] = False
+    ref = ref_collide(a[keep], pa[keep], b[keep], pb[keep], sp[keep])
+    got = outs[1][keep]
+    bad_rows = [i for i, (x, y) in enumerate(zip(live(got), live(ref))) if x != y]
+    assert not bad_rows, (len(bad_rows), bad_rows[:5])
