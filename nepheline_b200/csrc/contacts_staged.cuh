@@ -178,7 +178,7 @@ NPH_D void warm_manifold_staged(const DevSolver &S, uint32_t g, const Tile<kLane
             im.z = im.z * share;
             im.w = im.w * share;
             *T.at(4u * k + 2u) = im;
-            S.pi[k * S.mcap + g] = im;
+            __stcs(&S.pi[k * S.mcap + g], im);
         }
         hdr.z = bits & ~kHdrImpacted;
         S.hdr[g] = hdr;
@@ -294,7 +294,7 @@ NPH_D void solve_manifold_staged(const DevSolver &S, uint32_t g, const StepConst
         friction_circle(vt1, vt2, friction * im.x, new1, new2);
         im.z = new1;
         im.w = new2;
-        S.pi[k * S.mcap + g] = im;
+        __stcs(&S.pi[k * S.mcap + g], im);
         apply2(sd, a, b, new1 - old1, t1, ra, rb);
         apply2(sd, a, b, new2 - old2, t2, ra, rb);
     }
