@@ -644,7 +644,8 @@ uint32_t class_count_of(uint32_t threads)
 // The queue order for the configuration: each world's size class (the smallest team whose
 // threads cover its largest colour at items_per_thread items a thread; a whole block when
 // items_per_thread is 0), the classes in order, each largest first (a world's work grows with
-// its manifolds, joints and bodies).
+// its manifolds, joints and bodies). A world without awake bodies (every island asleep) is left
+// out: its step does nothing (solver.c:963-966), so it costs the launch nothing.
 void build_order(NphGpuBatch *b)
 {
     const std::vector<WorldSlice> &w = b->worlds;
@@ -665,8 +666,13 @@ void build_order(NphGpuBatch *b)
             cls[i] = c;
         }
     }
-    std::vector<uint32_t> order(w.size());
-    std::iota(order.begin(), order.end(), 0u);
+    std::vector<uint32_t> order;
+    order.reserve(w.size());
+    for (uint32_t i = 0; i < (uint32_t)w.size(); ++i) {
+        if (w[i].n > 0u) {
+            order.push_back(i);
+        }
+    }
     auto work = [&](uint32_t x) { return 4ull * w[x].m + 3ull * w[x].nj + w[x].n; };
     std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
         if (cls[x] != cls[y]) {
@@ -693,7 +699,7 @@ BatchArgs batch_args(const NphGpuBatch *b)
     BatchArgs A;
     A.worlds = b->d_worlds;
     A.order = b->d_order;
-    A.count = b->world_count;
+    A.count = (uint32_t)b->order.size();
     for (uint32_t c = 0; c < kMaxClasses; ++c) {
         A.class_first[c] = b->class_first[c];
         A.class_count[c] = b->class_count[c];
@@ -809,8 +815,10 @@ NphGpuResult apply_order(NphGpuBatch *b)
         return NPH_GPU_OK;
     }
     build_order(b);
-    cudaMemcpyAsync(b->d_order, b->order.data(), sizeof(uint32_t) * b->world_count, cudaMemcpyHostToDevice,
-                    b->stream);
+    if (!b->order.empty()) {
+        cudaMemcpyAsync(b->d_order, b->order.data(), sizeof(uint32_t) * b->order.size(), cudaMemcpyHostToDevice,
+                        b->stream);
+    }
     return cuda_result(cudaStreamSynchronize(b->stream));
 }
 
@@ -1265,7 +1273,10 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_upload(NphGpuBatch *b, const NphGpuWorldV
     b->live_in_merged = false;
     build_order(b);
     cudaMemcpyAsync(b->d_worlds, slices.data(), sizeof(WorldSlice) * count, cudaMemcpyHostToDevice, b->stream);
-    cudaMemcpyAsync(b->d_order, b->order.data(), sizeof(uint32_t) * count, cudaMemcpyHostToDevice, b->stream);
+    if (!b->order.empty()) {
+        cudaMemcpyAsync(b->d_order, b->order.data(), sizeof(uint32_t) * b->order.size(), cudaMemcpyHostToDevice,
+                        b->stream);
+    }
     {
         CopyRun cb(b->stream, cudaMemcpyHostToDevice), cf(b->stream, cudaMemcpyHostToDevice),
             cc(b->stream, cudaMemcpyHostToDevice), cj(b->stream, cudaMemcpyHostToDevice);

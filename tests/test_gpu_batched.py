@@ -246,3 +246,36 @@ def test_merged_packing_refuses_malformed_worlds(solver):
     assert batch.phys_solve_worlds_code([good.copy(), bad], params, DT) == abi.INVALID_ARGUMENT
     assert bad.bodies.tobytes() == before.bodies.tobytes()
     batch.close()
+
+
+def empty_view():
+    """A world whose islands all sleep: no awake body, so no constraint in its view."""
+    z = np.zeros(abi.COLOR_SLOTS, np.uint32)
+    return abi.View(np.zeros(0, abi.BODY_DTYPE), np.zeros(0, abi.BODY_DTYPE),
+                    np.zeros(0, abi.CONTACT_DTYPE), np.zeros(0, abi.JOINT_DTYPE), z, z.copy())
+
+
+@pytest.mark.parametrize("packing", [abi.BATCH_PERSISTENT, abi.BATCH_MERGED])
+def test_sleeping_worlds_are_left_out(solved_alone, packing):
+    """Worlds without awake bodies between the others: the others step as alone, resident or
+    not, and the batch's queue leaves the sleeping ones out (phys_solve does nothing for a
+    world without awake bodies, solver.c:963-966)."""
+    from nepheline_b200.solver import Batch
+    views, alone = solved_alone
+    params = abi.WorldParams.default()
+    mixed, where = [], []
+    for i, v in enumerate(views):
+        mixed.append(empty_view())
+        where.append(len(mixed))
+        mixed.append(v.copy())
+    mixed.append(empty_view())
+    batch = Batch(device=0)
+    batch.set_config(packing=packing)
+    batch.phys_solve_worlds(mixed, params, DT)
+    for i, k in enumerate(where):
+        assert not helpers.mismatches(mixed[k], alone[i]), i
+    for v in mixed:
+        if len(v.bodies) == 0:
+            assert len(v.contacts) == 0 and len(v.joints) == 0
+    assert batch.info()["worlds"] == len(mixed)
+    batch.close()
