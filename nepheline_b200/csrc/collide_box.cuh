@@ -98,6 +98,13 @@ struct CPoint {
     uint32_t id;
 };
 
+// A point of a polygon being clipped: its separation is not known until the clip ends, so the
+// point is its place and feature id only, 16 bytes that move in one vector access.
+struct __align__(16) ClipPoint {
+    V p;
+    uint32_t id;
+};
+
 // ---------------------------------------------------------------------------------------
 // Manifold reduction by catch angle (collide.c:62-277)
 // ---------------------------------------------------------------------------------------
@@ -583,16 +590,14 @@ NPH_NC V face_contact(const BoxPair &bp, bool flip, uint32_t ref, float speculat
             inc = f;
         }
     }
-    CPoint buf[2][kClipCapacity];
+    ClipPoint buf[2][kClipCapacity];
     uint32_t len = 0u;
     {
         const uint32_t first = box_face_first(inc);
         uint32_t e = first;
         do {
             const HalfEdge he = box_edge_of(e);
-            buf[0][len].p = iv[he.origin];
-            buf[0][len].sep = 0.0f;
-            buf[0][len].id = he.origin;
+            buf[0][len] = ClipPoint{iv[he.origin], he.origin};
             len += 1u;
             e = he.next;
         } while (e != first && len < kClipCapacity && len < 24u);
@@ -607,12 +612,12 @@ NPH_NC V face_contact(const BoxPair &bp, bool flip, uint32_t ref, float speculat
         const V b = rv[box_edge_of(he.next).origin];
         const V sn = cross(sub(b, a), n);
         const float so = dot(sn, a);
-        const CPoint *in = buf[cur];
-        CPoint *outp = buf[cur ^ 1u];
+        const ClipPoint *in = buf[cur];
+        ClipPoint *outp = buf[cur ^ 1u];
         uint32_t out_len = 0u;
         for (uint32_t i = 0u; i < len && out_len + 1u < kClipCapacity; ++i) {
-            const CPoint p = in[i];
-            const CPoint q = in[(i + 1u) % len];
+            const ClipPoint p = in[i];
+            const ClipPoint q = in[(i + 1u) % len];
             const float dp = dot(sn, p.p) - so;
             const float dq = dot(sn, q.p) - so;
             if (dp <= 0.0f) {
@@ -620,9 +625,7 @@ NPH_NC V face_contact(const BoxPair &bp, bool flip, uint32_t ref, float speculat
             }
             if ((dp <= 0.0f) != (dq <= 0.0f)) {
                 const float t = dp / (dp - dq);
-                outp[out_len].p = lerp(p.p, q.p, t);
-                outp[out_len].sep = 0.0f;
-                outp[out_len].id = mix_id(mix_id(p.id, q.id), 0x100u + side);
+                outp[out_len] = ClipPoint{lerp(p.p, q.p, t), mix_id(mix_id(p.id, q.id), 0x100u + side)};
                 out_len += 1u;
             }
         }
@@ -632,8 +635,8 @@ NPH_NC V face_contact(const BoxPair &bp, bool flip, uint32_t ref, float speculat
         side += 1u;
     } while (e != first && len > 0u && side < 24u);
     const uint32_t tag = mix_id((flip ? 0x80000000u : 0u) | (ref << 16u), inc);
-    const CPoint *clipped = buf[cur];
-    CPoint *cand = buf[cur ^ 1u];
+    const ClipPoint *clipped = buf[cur];
+    CPoint cand[kClipCapacity];
     uint32_t n_out = 0u;
     for (uint32_t i = 0u; i < len; ++i) {
         const float sep = dot(ref_plane.n, clipped[i].p) + ref_plane.d;
