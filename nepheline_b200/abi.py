@@ -188,6 +188,25 @@ class WorldView(ctypes.Structure):
     ]
 
 
+def _world_view_dtype() -> np.dtype:
+    """A numpy record with NphGpuWorldView's layout, so that a batch's views fill one array."""
+    names, formats, offsets = [], [], []
+    for name, ctype in WorldView._fields_:
+        names.append(name)
+        offsets.append(getattr(WorldView, name).offset)
+        if ctype is ctypes.c_void_p:
+            formats.append(np.uint64)
+        elif ctype is ctypes.c_uint32:
+            formats.append(np.uint32)
+        else:
+            formats.append((np.uint32, (COLOR_SLOTS,)))
+    return np.dtype({"names": names, "formats": formats, "offsets": offsets,
+                     "itemsize": ctypes.sizeof(WorldView)})
+
+
+WORLD_VIEW_DTYPE = _world_view_dtype()
+
+
 class StepStats(ctypes.Structure):
     _fields_ = [
         ("colors_used", ctypes.c_uint32), ("overflow_contacts", ctypes.c_uint32),
@@ -296,6 +315,20 @@ class View:
         v.joint_color_counts[:] = [int(x) for x in self.joint_color_counts]
         return v
 
+    def addresses(self) -> tuple:
+        """(address, count) of the bodies, fixed bodies, manifolds and joints: address 0 for
+        an empty array. Kept while the view holds the same array objects."""
+        key = (self.bodies, self.fixed, self.contacts, self.joints)
+        cached = self.__dict__.get("_addresses")
+        if cached is None or any(x is not y for x, y in zip(cached[0], key)):
+            rec = []
+            for arr in key:
+                assert arr.flags["C_CONTIGUOUS"]
+                rec += [arr.ctypes.data if len(arr) else 0, len(arr)]
+            cached = (key, tuple(rec))
+            self._addresses = cached
+        return cached[1]
+
     @property
     def colors_used(self) -> int:
         return int(np.count_nonzero((self.contact_color_counts[:COLORS] > 0)
@@ -310,6 +343,22 @@ def layout_sizes() -> dict:
     return {"body": BODY_DTYPE.itemsize, "point": POINT_DTYPE.itemsize,
             "contact": CONTACT_DTYPE.itemsize, "joint": JOINT_DTYPE.itemsize,
             "params": ctypes.sizeof(WorldParams), "view": ctypes.sizeof(WorldView)}
+
+
+def views_array(views: list) -> np.ndarray:
+    """The NphGpuWorldView array of a batch's views (at least one record), filled a column at
+    a time: a batch of thousands of worlds costs milliseconds, not a ctypes record each."""
+    n = len(views)
+    out = np.zeros(max(n, 1), WORLD_VIEW_DTYPE)
+    if n == 0:
+        return out
+    rec = np.array([v.addresses() for v in views], dtype=np.uint64).reshape(n, 8)
+    for k, name in enumerate(("bodies", "body_count", "fixed_bodies", "fixed_count", "contacts",
+                              "contact_count", "joints", "joint_count")):
+        out[name][:n] = rec[:, k]
+    out["contact_color_counts"][:n] = np.stack([v.contact_color_counts for v in views])
+    out["joint_color_counts"][:n] = np.stack([v.joint_color_counts for v in views])
+    return out
 
 
 def pack_views(views: list, alloc=None) -> list:

@@ -1250,7 +1250,14 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_upload(NphGpuBatch *b, const NphGpuWorldV
         4ull * contacts >= 0xFFFFFFF0ull || (uint64_t)kJointRows * joints >= 0xFFFFFFF0ull) {
         return NPH_GPU_TOO_LARGE;
     }
-    drop_batch_graph(b);
+    // The same worlds' shapes as the last upload (every count and offset): the arrays keep
+    // their size, so the captured step and the merged lists stay valid; only records move.
+    const bool same_batch = count == b->world_count && b->worlds.size() == count &&
+                            (count == 0 ||
+                             std::memcmp(b->worlds.data(), slices.data(), sizeof(WorldSlice) * count) == 0);
+    if (!same_batch) {
+        drop_batch_graph(b);
+    }
     // The point and joint rows are strided by their capacity: a capacity change reallocates
     // them with the new stride.
     const bool ok = grow(b->d_bodies, b->cap_bodies, bodies) && grow(b->d_fixed, b->cap_fixed, fixed) &&
@@ -1269,7 +1276,7 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_upload(NphGpuBatch *b, const NphGpuWorldV
     b->joints = joints;
     b->max_world_slots = max_slots;
     b->worlds = slices;
-    b->maps_valid = false;
+    b->maps_valid = b->maps_valid && same_batch;
     b->live_in_merged = false;
     build_order(b);
     cudaMemcpyAsync(b->d_worlds, slices.data(), sizeof(WorldSlice) * count, cudaMemcpyHostToDevice, b->stream);

@@ -61,3 +61,37 @@ def test_library_exports_every_declared_entry_point():
     lib = solver.lib()  # loads with its signatures, no device needed
     assert "sm_100a" in solver.version()
     del lib
+
+
+def test_views_array_equals_the_records_one_at_a_time():
+    """The batch's view array, filled column by column, holds the bytes a ctypes record per
+    world would: pointers (0 for empty arrays), counts and colour counts, plain and packed
+    worlds, and a view whose arrays were replaced after a first use."""
+    import ctypes
+
+    import numpy as np
+    rng = np.random.default_rng(1)
+    views = []
+    for _ in range(300):
+        cc = rng.integers(0, 9, abi.COLOR_SLOTS).astype(np.uint32)
+        jc = rng.integers(0, 3, abi.COLOR_SLOTS).astype(np.uint32)
+        views.append(abi.View(np.zeros(rng.integers(0, 12), abi.BODY_DTYPE),
+                              np.zeros(rng.integers(0, 2), abi.BODY_DTYPE),
+                              np.zeros(rng.integers(0, 20), abi.CONTACT_DTYPE),
+                              np.zeros(rng.integers(0, 3), abi.JOINT_DTYPE), cc, jc))
+
+    def one_at_a_time(vs):
+        arr = (abi.WorldView * len(vs))()
+        for i, v in enumerate(vs):
+            arr[i] = v.c_view()
+        return bytes(arr)
+
+    assert abi.WORLD_VIEW_DTYPE.itemsize == ctypes.sizeof(abi.WorldView)
+    for vs in (views, abi.pack_views(views)):
+        assert abi.views_array(vs).tobytes() == one_at_a_time(vs)
+    packed = abi.pack_views(views)
+    abi.views_array(packed)
+    packed[5].contacts = np.zeros(3, abi.CONTACT_DTYPE)
+    packed[7].contact_color_counts[0] += 1
+    assert abi.views_array(packed).tobytes() == one_at_a_time(packed)
+    assert len(abi.views_array([])) == 1

@@ -279,3 +279,38 @@ def test_sleeping_worlds_are_left_out(solved_alone, packing):
             assert len(v.contacts) == 0 and len(v.joints) == 0
     assert batch.info()["worlds"] == len(mixed)
     batch.close()
+
+
+@pytest.mark.parametrize("packing", [abi.BATCH_PERSISTENT, abi.BATCH_MERGED])
+def test_drop_in_steps_with_the_same_shapes(solver, packing):
+    """Consecutive drop-in calls on worlds of unchanged shapes (the step graph and the merged
+    lists are kept between them, only records move) equal each world solved alone as often;
+    a call with two worlds swapped (the same totals) is taken as a new batch."""
+    from nepheline_b200.solver import Batch
+    params = abi.WorldParams.default()
+    views = []
+    for edge, seed in ((4, 5), (7, 6), (6, 7), (2, 8)):
+        sc = scenes.lattice_graph(edge, seed=seed, joint_fraction=0.1)
+        c, s = scenes.host_color(sc)
+        views.append(sc.to_view(c, s))
+    views.append(hub_view(27))
+    batch = Batch(device=0)
+    batch.set_config(packing=packing)
+    mine = abi.pack_views([v.copy() for v in views])
+    want = [v.copy() for v in views]
+    for _ in range(3):
+        batch.phys_solve_worlds(mine, params, DT)
+        for w in want:
+            solver.phys_solve(w, params, DT)
+        for m, w in zip(mine, want):
+            assert not helpers.mismatches(m, w)
+    # The first two worlds swapped: the same totals, other offsets, so a new batch.
+    swapped = [mine[1], mine[0]] + mine[2:]
+    want = [want[1], want[0]] + want[2:]
+    assert len(mine[0].contacts) != len(mine[1].contacts)
+    batch.phys_solve_worlds(swapped, params, DT)
+    for w in want:
+        solver.phys_solve(w, params, DT)
+    for m, w in zip(swapped, want):
+        assert not helpers.mismatches(m, w)
+    batch.close()
