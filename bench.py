@@ -59,6 +59,9 @@ def parse():
                     help="narrow: shape pairs per step (boxes, spheres, capsules near contact)")
     ap.add_argument("--batch-config", default=None,
                     help="batched: fixed launch shape,shared mode,items per thread (no autotuner)")
+    ap.add_argument("--parts", type=int, default=8,
+                    help="batched: the drop-in call's parts (uploads chained, each part's "
+                         "results back while later parts go up; 1: unsplit)")
     ap.add_argument("--pile-worlds", type=int, default=256,
                     help="learned: box-pile worlds per batch (500-5000 boxes each)")
     ap.add_argument("--train-batches", type=int, default=2)
@@ -534,6 +537,7 @@ def run_batched(args):
     pv = abi.pack_views(views, pinned)
     h2d = sum(v.bodies.nbytes + v.contacts.nbytes + v.joints.nbytes + v.fixed.nbytes for v in pv)
     d2h = sum(v.bodies.nbytes + v.contacts.nbytes + v.joints.nbytes for v in pv)
+    batch.set_pipeline(args.parts)
     batch.phys_solve_worlds(pv, params, DT)
     torch.cuda.synchronize()
     barrier(pg)
@@ -571,7 +575,7 @@ def run_batched(args):
                        "l2": "inputs larger than L2"},
             "world_steps_per_s": worlds_all / (ms * 1e-3),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms},
+                    "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms, "parts": args.parts},
             "gpu_launches": args.steps * launches,
             "roofline": roofline,
             "cpu_baseline": cpu,

@@ -489,6 +489,17 @@ NPH_GPU_API NphGpuResult nph_gpu_phys_solve_worlds(NphGpuBatch *batch,
 /* Sets the launch configuration (tuning->ms_per_step and ->threads are ignored). */
 NPH_GPU_API NphGpuResult nph_gpu_batch_set_config(NphGpuBatch *batch,
                                                   const NphGpuBatchTuning *tuning);
+/* Splits nph_gpu_phys_solve_worlds into `parts` (1..NPH_GPU_BATCH_MAX_PARTS; 1, the default,
+ * does not split): consecutive runs of worlds of about equal record bytes, each solved by a
+ * batch of its own on its own stream with this batch's launch configuration. A part's upload
+ * follows the previous part's, its step and its download follow its upload, so the host link
+ * carries one part's results back while later parts' records go up. Results are the same bits
+ * as unsplit (the worlds are independent). Every record the device would refuse is checked on
+ * the host before anything is copied, so a refused batch still has nothing written back. The
+ * parts hold device arrays of their own; the batch's own upload, step and download calls do
+ * not use them. */
+#define NPH_GPU_BATCH_MAX_PARTS 16u
+NPH_GPU_API NphGpuResult nph_gpu_batch_set_pipeline(NphGpuBatch *batch, uint32_t parts);
 NPH_GPU_API uint32_t nph_gpu_batch_config_count(void);
 /* The batch autotuner: times every configuration on the uploaded worlds (`rounds` timed steps
  * each after an untimed one; the worlds advance) and keeps the fastest. */

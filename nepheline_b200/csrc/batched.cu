@@ -20,9 +20,11 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <new>
 #include <numeric>
+#include <thread>
 #include <vector>
 
 #include "nepheline_b200.h"
@@ -541,6 +543,12 @@ struct NphGpuBatch {
     bool graph_valid = false;
     StepConsts graph_consts{};
     uint32_t graph_substeps = 0;
+    // The drop-in call's pipeline: the worlds split into consecutive parts, each a batch on
+    // its own stream, their uploads one after another, so that one part's records come back
+    // while the next parts' go up and step.
+    uint32_t pipeline_parts = 1;
+    std::vector<NphGpuBatch *> parts;
+    std::vector<cudaEvent_t> part_uploaded;
 };
 
 namespace {
@@ -900,8 +908,9 @@ NphGpuResult build_merge_maps(NphGpuBatch *b)
     return r;
 }
 
-// Packed -> the merged solver (the state then lives there).
-NphGpuResult merged_setup(NphGpuBatch *b)
+// Packed -> the merged solver (the state then lives there). Without `sync` the copies are only
+// enqueued on the batch's stream.
+NphGpuResult merged_setup(NphGpuBatch *b, bool sync = true)
 {
     if (b->live_in_merged) {
         return NPH_GPU_OK;
@@ -947,13 +956,13 @@ NphGpuResult merged_setup(NphGpuBatch *b)
         k_merge_joints<<<(mj + 255u) / 256u, 256, 0, b->stream>>>(b->d_joints, b->d_jmap, b->d_jworld, b->d_worlds,
                                                                 n_total, R.joints, mj);
     }
-    r = cuda_result(cudaStreamSynchronize(b->stream));
+    r = cuda_result(sync ? cudaStreamSynchronize(b->stream) : cudaGetLastError());
     b->live_in_merged = r == NPH_GPU_OK;
     return r;
 }
 
 // The merged solver's state -> packed (both then hold it).
-NphGpuResult merged_to_packed(NphGpuBatch *b)
+NphGpuResult merged_to_packed(NphGpuBatch *b, bool sync = true)
 {
     if (!b->live_in_merged) {
         return NPH_GPU_OK;
@@ -973,7 +982,7 @@ NphGpuResult merged_to_packed(NphGpuBatch *b)
     if (mj > 0) {
         k_unmerge_joints<<<(mj + 255u) / 256u, 256, 0, b->stream>>>(R.joints, b->d_jmap, b->d_joints, mj);
     }
-    return cuda_result(cudaStreamSynchronize(b->stream));
+    return cuda_result(sync ? cudaStreamSynchronize(b->stream) : cudaGetLastError());
 }
 
 // Makes the packed arrays the live state (for the persistent packing).
@@ -1177,6 +1186,12 @@ NPH_GPU_API void nph_gpu_batch_destroy(NphGpuBatch *b)
         cudaStreamSynchronize(b->stream);
     }
     free_arrays(b);
+    for (NphGpuBatch *q : b->parts) {
+        nph_gpu_batch_destroy(q);
+    }
+    for (cudaEvent_t e : b->part_uploaded) {
+        cudaEventDestroy(e);
+    }
     if (b->merged != nullptr) {
         nph_gpu_solver_destroy(b->merged);
         b->merged = nullptr;
@@ -1196,18 +1211,13 @@ NPH_GPU_API void *nph_gpu_batch_stream(const NphGpuBatch *b)
     return b != nullptr ? (void *)b->stream : nullptr;
 }
 
-NPH_GPU_API NphGpuResult nph_gpu_batch_upload(NphGpuBatch *b, const NphGpuWorldView *worlds,
-                                              uint32_t count)
+} // extern "C"
+
+namespace {
+
+// The upload of worlds that check_world accepted, enqueued on the batch's stream.
+NphGpuResult upload_begin(NphGpuBatch *b, const NphGpuWorldView *worlds, uint32_t count)
 {
-    if (b == nullptr || (count > 0 && worlds == nullptr)) {
-        return NPH_GPU_INVALID_ARGUMENT;
-    }
-    for (uint32_t w = 0; w < count; ++w) {
-        const NphGpuResult r = check_world(worlds[w]);
-        if (r != NPH_GPU_OK) {
-            return r;
-        }
-    }
     cudaSetDevice(b->device);
     // The slices, then the arrays grown to the batch.
     std::vector<WorldSlice> slices(count);
@@ -1297,7 +1307,241 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_upload(NphGpuBatch *b, const NphGpuWorldV
         }
     }
     cudaMemsetAsync(b->d_counters, 0, 8 * sizeof(uint32_t), b->stream);
-    return cuda_result(cudaStreamSynchronize(b->stream));
+    return cuda_result(cudaGetLastError());
+}
+
+NphGpuResult step_begin(NphGpuBatch *b, const NphGpuWorldParams *params, float dt, uint32_t steps,
+                        bool sync_setup)
+{
+    if (b->world_count == 0) {
+        return NPH_GPU_OK;
+    }
+    cudaSetDevice(b->device);
+    if (b->packing == NPH_GPU_BATCH_MERGED) {
+        const NphGpuResult r = merged_setup(b, sync_setup);
+        return r != NPH_GPU_OK ? r : nph_gpu_world_step_async(b->merged, params, dt, steps);
+    }
+    NphGpuResult r = leave_merged(b);
+    const StepConsts K = make_step_consts(*params, dt);
+    for (uint32_t i = 0; i < steps && r == NPH_GPU_OK; ++i) {
+        r = launch_batch_step(b, K, params->substeps);
+    }
+    return r;
+}
+
+// The packed results' copies into the worlds' records, enqueued on the batch's stream.
+NphGpuResult enqueue_downloads(NphGpuBatch *b, NphGpuWorldView *worlds, uint32_t count)
+{
+    for (uint32_t w = 0; w < count; ++w) {
+        const NphGpuWorldView &v = worlds[w];
+        const WorldSlice &s = b->worlds[w];
+        if (v.body_count != s.n || v.contact_count != s.m || v.joint_count != s.nj ||
+            (s.n > 0 && v.bodies == nullptr) || (s.m > 0 && v.contacts == nullptr) ||
+            (s.nj > 0 && v.joints == nullptr)) {
+            return NPH_GPU_INVALID_STATE;
+        }
+    }
+    CopyRun cb(b->stream, cudaMemcpyDeviceToHost), cc(b->stream, cudaMemcpyDeviceToHost),
+        cj(b->stream, cudaMemcpyDeviceToHost);
+    for (uint32_t w = 0; w < count; ++w) {
+        NphGpuWorldView &v = worlds[w];
+        const WorldSlice &s = b->worlds[w];
+        cb.add(v.bodies, b->d_bodies + s.body_first, sizeof(NphGpuBody) * s.n);
+        cc.add(v.contacts, b->d_contacts + s.contact_first, sizeof(NphGpuContact) * s.m);
+        cj.add(v.joints, b->d_joints + s.joint_first, sizeof(NphGpuJoint) * s.nj);
+    }
+    cb.flush();
+    cc.flush();
+    cj.flush();
+    return cuda_result(cudaGetLastError());
+}
+
+// Waits for the batch's stream and reports a record the device refused.
+NphGpuResult batch_finish(NphGpuBatch *b)
+{
+    cudaSetDevice(b->device);
+    NphGpuResult r = NPH_GPU_OK;
+    if (b->live_in_merged) {
+        r = nph_solver_check(b->merged);
+    }
+    cudaMemcpyAsync(b->h_counters, b->d_counters, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost, b->stream);
+    const NphGpuResult e = cuda_result(cudaStreamSynchronize(b->stream));
+    if (r == NPH_GPU_OK) {
+        r = e;
+    }
+    if (r == NPH_GPU_OK && b->h_counters[6] != 0u) {
+        r = NPH_GPU_INVALID_ARGUMENT;
+    }
+    return r;
+}
+
+// Every record the device would refuse (check_world's and prepare's checks: a joint's or a
+// manifold's body outside its world, a manifold without points or with more than four), on
+// the host, so that a pipelined call refuses a batch before any of it is written back.
+NphGpuResult check_records(const NphGpuWorldView *worlds, uint32_t count)
+{
+    std::atomic<uint32_t> bad{0};
+    auto scan = [&](uint32_t first, uint32_t end) {
+        for (uint32_t w = first; w < end && bad.load(std::memory_order_relaxed) == 0u; ++w) {
+            const NphGpuWorldView &v = worlds[w];
+            const uint32_t total = v.body_count + v.fixed_count;
+            uint32_t worst = 0u;
+            for (uint32_t i = 0; i < v.contact_count; ++i) {
+                const NphGpuContact &c = v.contacts[i];
+                worst |= (c.body_a >= total) | (c.body_b >= total) | (c.point_count < 1u) |
+                         (c.point_count > NPH_GPU_MAX_POINTS);
+            }
+            for (uint32_t j = 0; j < v.joint_count; ++j) {
+                worst |= (v.joints[j].body_a >= total) | (v.joints[j].body_b >= total);
+            }
+            if (worst != 0u) {
+                bad.store(1u, std::memory_order_relaxed);
+            }
+        }
+    };
+    const uint32_t threads = std::max(1u, std::min({8u, std::thread::hardware_concurrency(), count / 64u}));
+    std::vector<std::thread> pool;
+    for (uint32_t t = 1; t < threads; ++t) {
+        pool.emplace_back(scan, (uint32_t)((uint64_t)count * t / threads),
+                          (uint32_t)((uint64_t)count * (t + 1) / threads));
+    }
+    scan(0u, (uint32_t)((uint64_t)count / threads));
+    for (std::thread &t : pool) {
+        t.join();
+    }
+    return bad.load() != 0u ? NPH_GPU_INVALID_ARGUMENT : NPH_GPU_OK;
+}
+
+// The parts' batches and their events, created or released to match the requested count, each
+// part on the parent's launch configuration.
+NphGpuResult ensure_parts(NphGpuBatch *b, uint32_t parts)
+{
+    while (b->parts.size() > parts) {
+        nph_gpu_batch_destroy(b->parts.back());
+        b->parts.pop_back();
+        cudaEventDestroy(b->part_uploaded.back());
+        b->part_uploaded.pop_back();
+    }
+    while (b->parts.size() < parts) {
+        NphGpuSolverDesc d{};
+        d.device = b->device;
+        d.use_graph = b->use_graph ? 1u : 0u;
+        NphGpuBatch *q = nullptr;
+        NphGpuResult r = nph_gpu_batch_create(&d, &q);
+        if (r != NPH_GPU_OK) {
+            return r;
+        }
+        cudaEvent_t e = nullptr;
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+            nph_gpu_batch_destroy(q);
+            return cuda_result(cudaGetLastError());
+        }
+        b->parts.push_back(q);
+        b->part_uploaded.push_back(e);
+    }
+    for (NphGpuBatch *q : b->parts) {
+        if (q->packing != b->packing || q->config != b->config || q->shared_mode != b->shared_mode ||
+            q->items_per_thread != b->items_per_thread) {
+            NphGpuBatchTuning t{};
+            t.config = b->config;
+            t.shared_velocities = b->shared_mode;
+            t.items_per_thread = b->items_per_thread;
+            t.packing = b->packing;
+            const NphGpuResult r = nph_gpu_batch_set_config(q, &t);
+            if (r != NPH_GPU_OK) {
+                return r;
+            }
+        }
+    }
+    return NPH_GPU_OK;
+}
+
+uint64_t record_bytes(const NphGpuWorldView &v)
+{
+    return sizeof(NphGpuBody) * ((uint64_t)v.body_count + v.fixed_count) + sizeof(NphGpuContact) * (uint64_t)v.contact_count +
+           sizeof(NphGpuJoint) * (uint64_t)v.joint_count;
+}
+
+// nph_gpu_phys_solve_worlds in parts: consecutive runs of worlds of about equal record bytes,
+// after the host has checked every record (a refused batch has nothing written back). Each
+// part's stream holds its upload, step and download in turn, and its upload waits for the
+// previous part's, so a part's results come back while the later parts still go up.
+NphGpuResult solve_in_parts(NphGpuBatch *b, const NphGpuWorldParams *params, float dt, NphGpuWorldView *worlds,
+                            uint32_t count)
+{
+    NphGpuResult r = check_records(worlds, count);
+    if (r != NPH_GPU_OK) {
+        return r;
+    }
+    const uint32_t parts = std::min(b->pipeline_parts, count);
+    r = ensure_parts(b, parts);
+    if (r != NPH_GPU_OK) {
+        return r;
+    }
+    std::vector<uint32_t> first(parts + 1u, count);
+    {
+        uint64_t total = 0;
+        for (uint32_t w = 0; w < count; ++w) {
+            total += record_bytes(worlds[w]);
+        }
+        uint64_t sum = 0;
+        uint32_t p = 1;
+        first[0] = 0;
+        for (uint32_t w = 0; w < count && p < parts; ++w) {
+            sum += record_bytes(worlds[w]);
+            while (p < parts && sum * parts >= total * p) {
+                first[p++] = w + 1u;
+            }
+        }
+    }
+    uint32_t started = 0;
+    for (uint32_t p = 0; p < parts && r == NPH_GPU_OK; ++p) {
+        NphGpuBatch *q = b->parts[p];
+        const uint32_t n = first[p + 1u] - first[p];
+        cudaSetDevice(q->device);
+        if (p > 0) {
+            cudaStreamWaitEvent(q->stream, b->part_uploaded[p - 1u], 0);
+        }
+        started = p + 1u;
+        r = upload_begin(q, worlds + first[p], n);
+        cudaEventRecord(b->part_uploaded[p], q->stream);
+        if (r == NPH_GPU_OK) {
+            r = step_begin(q, params, dt, 1u, false);
+        }
+        if (r == NPH_GPU_OK) {
+            r = merged_to_packed(q, false);
+        }
+        if (r == NPH_GPU_OK) {
+            r = enqueue_downloads(q, worlds + first[p], n);
+        }
+    }
+    for (uint32_t p = 0; p < started; ++p) {
+        const NphGpuResult e = batch_finish(b->parts[p]);
+        if (r == NPH_GPU_OK) {
+            r = e;
+        }
+    }
+    return r;
+}
+
+} // namespace
+
+extern "C" {
+
+NPH_GPU_API NphGpuResult nph_gpu_batch_upload(NphGpuBatch *b, const NphGpuWorldView *worlds,
+                                              uint32_t count)
+{
+    if (b == nullptr || (count > 0 && worlds == nullptr)) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    for (uint32_t w = 0; w < count; ++w) {
+        const NphGpuResult r = check_world(worlds[w]);
+        if (r != NPH_GPU_OK) {
+            return r;
+        }
+    }
+    const NphGpuResult r = upload_begin(b, worlds, count);
+    return r != NPH_GPU_OK ? r : cuda_result(cudaStreamSynchronize(b->stream));
 }
 
 NPH_GPU_API NphGpuResult nph_gpu_batch_step_async(NphGpuBatch *b, const NphGpuWorldParams *params,
@@ -1311,20 +1555,7 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_step_async(NphGpuBatch *b, const NphGpuWo
         params->enable_continuous != 0u) {
         return NPH_GPU_UNSUPPORTED;
     }
-    if (b->world_count == 0) {
-        return NPH_GPU_OK;
-    }
-    cudaSetDevice(b->device);
-    if (b->packing == NPH_GPU_BATCH_MERGED) {
-        const NphGpuResult r = merged_setup(b);
-        return r != NPH_GPU_OK ? r : nph_gpu_world_step_async(b->merged, params, dt, steps);
-    }
-    NphGpuResult r = leave_merged(b);
-    const StepConsts K = make_step_consts(*params, dt);
-    for (uint32_t i = 0; i < steps && r == NPH_GPU_OK; ++i) {
-        r = launch_batch_step(b, K, params->substeps);
-    }
-    return r;
+    return step_begin(b, params, dt, steps, true);
 }
 
 NPH_GPU_API NphGpuResult nph_gpu_batch_download(NphGpuBatch *b, NphGpuWorldView *worlds, uint32_t count)
@@ -1351,32 +1582,30 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_download(NphGpuBatch *b, NphGpuWorldView 
     if (b->h_counters[6] != 0u) {
         return NPH_GPU_INVALID_ARGUMENT; // a malformed record: nothing written back
     }
-    for (uint32_t w = 0; w < count; ++w) {
-        const NphGpuWorldView &v = worlds[w];
-        const WorldSlice &s = b->worlds[w];
-        if (v.body_count != s.n || v.contact_count != s.m || v.joint_count != s.nj ||
-            (s.n > 0 && v.bodies == nullptr) || (s.m > 0 && v.contacts == nullptr) ||
-            (s.nj > 0 && v.joints == nullptr)) {
-            return NPH_GPU_INVALID_STATE;
-        }
-    }
-    {
-        CopyRun cb(b->stream, cudaMemcpyDeviceToHost), cc(b->stream, cudaMemcpyDeviceToHost),
-            cj(b->stream, cudaMemcpyDeviceToHost);
-        for (uint32_t w = 0; w < count; ++w) {
-            NphGpuWorldView &v = worlds[w];
-            const WorldSlice &s = b->worlds[w];
-            cb.add(v.bodies, b->d_bodies + s.body_first, sizeof(NphGpuBody) * s.n);
-            cc.add(v.contacts, b->d_contacts + s.contact_first, sizeof(NphGpuContact) * s.m);
-            cj.add(v.joints, b->d_joints + s.joint_first, sizeof(NphGpuJoint) * s.nj);
-        }
-    }
-    return cuda_result(cudaStreamSynchronize(b->stream));
+    r = enqueue_downloads(b, worlds, count);
+    return r != NPH_GPU_OK ? r : cuda_result(cudaStreamSynchronize(b->stream));
 }
 
 NPH_GPU_API NphGpuResult nph_gpu_phys_solve_worlds(NphGpuBatch *b, const NphGpuWorldParams *params,
                                                    float dt, NphGpuWorldView *worlds, uint32_t count)
 {
+    if (b != nullptr && b->pipeline_parts > 1u && count > 1u) {
+        if (worlds == nullptr || params == nullptr || !(dt > 0.0f) || params->substeps == 0u ||
+            params->substeps > 64u) {
+            return NPH_GPU_INVALID_ARGUMENT;
+        }
+        if ((params->solver != NPH_GPU_SOLVER_SOFT_STEP && params->solver != NPH_GPU_SOLVER_TGS) ||
+            params->enable_continuous != 0u) {
+            return NPH_GPU_UNSUPPORTED;
+        }
+        for (uint32_t w = 0; w < count; ++w) {
+            const NphGpuResult r = check_world(worlds[w]);
+            if (r != NPH_GPU_OK) {
+                return r;
+            }
+        }
+        return solve_in_parts(b, params, dt, worlds, count);
+    }
     NphGpuResult r = nph_gpu_batch_upload(b, worlds, count);
     if (r == NPH_GPU_OK) {
         r = nph_gpu_batch_step_async(b, params, dt, 1);
@@ -1405,6 +1634,15 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_set_config(NphGpuBatch *b, const NphGpuBa
     b->shared_mode = t->shared_velocities;
     b->items_per_thread = t->items_per_thread;
     return apply_order(b);
+}
+
+NPH_GPU_API NphGpuResult nph_gpu_batch_set_pipeline(NphGpuBatch *b, uint32_t parts)
+{
+    if (b == nullptr || parts < 1u || parts > NPH_GPU_BATCH_MAX_PARTS) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    b->pipeline_parts = parts;
+    return NPH_GPU_OK;
 }
 
 NPH_GPU_API uint32_t nph_gpu_batch_config_count(void) { return kBatchConfigCount; }

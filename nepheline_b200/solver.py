@@ -84,6 +84,7 @@ def lib() -> ctypes.CDLL:
         "nph_gpu_phys_solve_worlds": (ctypes.c_int32, [_vp, P(abi.WorldParams), ctypes.c_float,
                                                        P(abi.WorldView), _u32]),
         "nph_gpu_batch_set_config": (ctypes.c_int32, [_vp, P(abi.BatchTuning)]),
+        "nph_gpu_batch_set_pipeline": (ctypes.c_int32, [_vp, _u32]),
         "nph_gpu_batch_config_count": (_u32, []),
         "nph_gpu_batch_autotune": (ctypes.c_int32, [_vp, P(abi.WorldParams), ctypes.c_float,
                                                     _u32, P(abi.BatchTuning)]),
@@ -396,6 +397,11 @@ class Batch:
         t.packing = packing
         _check(self.L.nph_gpu_batch_set_config(self._h, ctypes.byref(t)),
                "nph_gpu_batch_set_config")
+
+    def set_pipeline(self, parts: int) -> None:
+        """phys_solve_worlds in `parts` consecutive runs of worlds, each on its own stream, so
+        that one part's results come back while later parts' records go up (1: unsplit)."""
+        _check(self.L.nph_gpu_batch_set_pipeline(self._h, parts), "nph_gpu_batch_set_pipeline")
 
     def config_count(self) -> int:
         return int(self.L.nph_gpu_batch_config_count())

@@ -314,3 +314,64 @@ def test_drop_in_steps_with_the_same_shapes(solver, packing):
     for m, w in zip(swapped, want):
         assert not helpers.mismatches(m, w)
     batch.close()
+
+
+@pytest.mark.parametrize("packing", [abi.BATCH_PERSISTENT, abi.BATCH_MERGED])
+@pytest.mark.parametrize("parts", [2, 3, 8])
+def test_drop_in_in_parts_equals_worlds_solved_alone(solved_alone, packing, parts):
+    """The drop-in call split into parts (each on its own stream, uploads chained) gives each
+    world the bits it has alone, packed or not, twice in a row, with sleeping worlds between."""
+    from nepheline_b200.solver import Batch
+    params = abi.WorldParams.default()
+    views, alone = solved_alone
+    batch = Batch(device=0)
+    batch.set_config(packing=packing)
+    batch.set_pipeline(parts)
+    for packed in (True, False):
+        mixed, where = [], []
+        for v in views:
+            mixed.append(empty_view())
+            where.append(len(mixed))
+            mixed.append(v.copy())
+        worlds = abi.pack_views(mixed) if packed else mixed
+        batch.phys_solve_worlds(worlds, params, DT)
+        for i, k in enumerate(where):
+            assert not helpers.mismatches(worlds[k], alone[i]), (packed, i)
+    batch.close()
+
+
+def test_drop_in_in_parts_refuses_before_writing_back(solver):
+    """A malformed record in the last part: the call is refused and no world, in any part, is
+    written back."""
+    from nepheline_b200.solver import Batch
+    params = abi.WorldParams.default()
+    views = []
+    for edge, seed in ((4, 5), (7, 6), (6, 7), (5, 8)):
+        sc = scenes.lattice_graph(edge, seed=seed, joint_fraction=0.1)
+        c, s = scenes.host_color(sc)
+        views.append(sc.to_view(c, s))
+    batch = Batch(device=0)
+    batch.set_pipeline(4)
+    for field, value in (("body_a", 10_000), ("point_count", 0), ("point_count", 5)):
+        worlds = abi.pack_views([v.copy() for v in views])
+        worlds[-1].contacts[field][3] = value
+        before = [w.copy() for w in worlds]
+        assert batch.phys_solve_worlds_code(worlds, params, DT) == abi.INVALID_ARGUMENT
+        for w, b in zip(worlds, before):
+            assert w.bodies.tobytes() == b.bodies.tobytes()
+            assert w.contacts.tobytes() == b.contacts.tobytes()
+    worlds = abi.pack_views([v.copy() for v in views])
+    worlds[-1].joints["body_b"][0] = 10_000
+    before = worlds[0].copy()
+    assert batch.phys_solve_worlds_code(worlds, params, DT) == abi.INVALID_ARGUMENT
+    assert worlds[0].bodies.tobytes() == before.bodies.tobytes()
+    # And the same batch then solves good worlds.
+    worlds = abi.pack_views([v.copy() for v in views])
+    batch.phys_solve_worlds(worlds, params, DT)
+    for w, v in zip(worlds, views):
+        want = v.copy()
+        solver.phys_solve(want, params, DT)
+        assert not helpers.mismatches(w, want)
+    with pytest.raises(Exception):
+        batch.set_pipeline(0)
+    batch.close()
