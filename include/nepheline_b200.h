@@ -603,6 +603,13 @@ NPH_GPU_API NphGpuResult nph_gpu_collide_async(const NphGpuShape *a, const NphGp
                                                void *workspace, uint64_t workspace_bytes,
                                                void *stream);
 
+/* The same on host arrays, synchronous, on the current device. A pair of an unknown type gets
+ * the cleared manifold and the call returns NPH_GPU_UNSUPPORTED, with every other pair's
+ * manifold written (the types are checked on the device). The pairs go in chunks of about a sixteenth of them
+ * (at least 65,536) through three streams: a chunk's upload follows the previous chunk's, its
+ * collision and the copy of its manifolds back follow its upload, so results come back while
+ * later chunks go up (page-locked host arrays let the copies overlap). The chunks' device arrays
+ * are kept between calls, one set per device; calls are serialised by a lock. */
 NPH_GPU_API NphGpuResult nph_gpu_collide(const NphGpuShape *a, const NphGpuPose *pose_a,
                                          const NphGpuShape *b, const NphGpuPose *pose_b,
                                          const float *speculative, uint32_t count,

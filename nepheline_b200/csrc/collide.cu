@@ -4,6 +4,11 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <mutex>
+#include <new>
+#include <vector>
+
 #include "nepheline_b200.h"
 
 #include "collide.cuh"
@@ -105,18 +110,88 @@ __global__ void __launch_bounds__(256, 3) k_collide_sorted(const NphGpuShape *a,
     }
 }
 
-// Spheres, capsules and boxes, every pair of them.
-bool supported(uint32_t ta, uint32_t tb) { return ta <= NPH_GPU_SHAPE_BOX && tb <= NPH_GPU_SHAPE_BOX; }
+// The host-buffer call's pipeline: the pairs in chunks over three slots, each slot a stream
+// and one chunk's device arrays. A chunk's upload waits for the previous chunk's (uploads go in
+// order over the host link), its sort, collision and download follow on its slot's stream, so
+// one chunk's manifolds come back while later chunks go up and collide. The slots' arrays stay
+// allocated between calls (one set per device, grown to the largest chunk).
+constexpr uint32_t kSlots = 3u;
+constexpr uint32_t kChunkMin = 65536u;
+constexpr uint32_t kChunksWanted = 16u;
 
-template <typename T> NphGpuResult stage(T *&dst, const T *src, uint32_t count, cudaStream_t st)
+struct Slot {
+    NphGpuShape *a = nullptr, *b = nullptr;
+    NphGpuPose *pa = nullptr, *pb = nullptr;
+    float *spec = nullptr;
+    NphGpuManifold *out = nullptr;
+    uint32_t *ws = nullptr;
+    cudaStream_t st = nullptr;
+    cudaEvent_t up = nullptr;
+};
+
+struct Pipe {
+    uint32_t chunk_cap = 0;
+    Slot slot[kSlots];
+    uint32_t *d_bad = nullptr; // pairs of unknown types in the call
+};
+
+std::mutex g_pipe_mutex;
+std::vector<Pipe> *g_pipes = nullptr; // per device; kept to the process's end
+
+void free_slot_arrays(Slot &s)
 {
-    if (cudaMalloc((void **)&dst, sizeof(T) * count) != cudaSuccess) {
+    cudaFree(s.a);
+    cudaFree(s.b);
+    cudaFree(s.pa);
+    cudaFree(s.pb);
+    cudaFree(s.spec);
+    cudaFree(s.out);
+    cudaFree(s.ws);
+    s.a = s.b = nullptr;
+    s.pa = s.pb = nullptr;
+    s.spec = nullptr;
+    s.out = nullptr;
+    s.ws = nullptr;
+}
+
+template <typename T> bool alloc(T *&p, uint64_t count)
+{
+    return cudaMalloc((void **)&p, sizeof(T) * count) == cudaSuccess;
+}
+
+NphGpuResult ensure_pipe(Pipe &pipe, uint32_t chunk)
+{
+    if (pipe.d_bad == nullptr && !alloc(pipe.d_bad, 1)) {
         cudaGetLastError();
         return NPH_GPU_OUT_OF_MEMORY;
     }
-    if (src != nullptr) {
-        cudaMemcpyAsync(dst, src, sizeof(T) * count, cudaMemcpyHostToDevice, st);
+    for (Slot &s : pipe.slot) {
+        if (s.st == nullptr && (cudaStreamCreateWithFlags(&s.st, cudaStreamNonBlocking) != cudaSuccess ||
+                                cudaEventCreateWithFlags(&s.up, cudaEventDisableTiming) != cudaSuccess)) {
+            cudaGetLastError();
+            return NPH_GPU_DEVICE_LOST;
+        }
     }
+    if (chunk <= pipe.chunk_cap) {
+        return NPH_GPU_OK;
+    }
+    for (Slot &s : pipe.slot) {
+        cudaStreamSynchronize(s.st);
+        free_slot_arrays(s);
+    }
+    pipe.chunk_cap = 0;
+    const uint64_t ws_words = nph_gpu_collide_workspace_bytes(chunk) / sizeof(uint32_t);
+    for (Slot &s : pipe.slot) {
+        if (!alloc(s.a, chunk) || !alloc(s.b, chunk) || !alloc(s.pa, chunk) || !alloc(s.pb, chunk) ||
+            !alloc(s.spec, chunk) || !alloc(s.out, chunk) || !alloc(s.ws, ws_words)) {
+            cudaGetLastError();
+            for (Slot &t : pipe.slot) {
+                free_slot_arrays(t);
+            }
+            return NPH_GPU_OUT_OF_MEMORY;
+        }
+    }
+    pipe.chunk_cap = chunk;
     return NPH_GPU_OK;
 }
 
@@ -135,46 +210,60 @@ NPH_GPU_API NphGpuResult nph_gpu_collide(const NphGpuShape *a, const NphGpuPose 
         out == nullptr) {
         return NPH_GPU_INVALID_ARGUMENT;
     }
-    for (uint32_t i = 0; i < count; ++i) {
-        if (!supported(a[i].type, b[i].type)) {
-            return NPH_GPU_UNSUPPORTED;
-        }
-    }
-    cudaStream_t st = nullptr;
-    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) {
         cudaGetLastError();
         return NPH_GPU_DEVICE_LOST;
     }
-    NphGpuShape *da = nullptr, *db = nullptr;
-    NphGpuPose *dpa = nullptr, *dpb = nullptr;
-    float *ds = nullptr;
-    NphGpuManifold *dout = nullptr;
-    uint32_t *dws = nullptr;
-    const uint64_t ws_words = (2ull * 16u + 2ull * count);
-    NphGpuResult r = stage(da, a, count, st);
-    if (r == NPH_GPU_OK) r = stage(db, b, count, st);
-    if (r == NPH_GPU_OK) r = stage(dpa, pose_a, count, st);
-    if (r == NPH_GPU_OK) r = stage(dpb, pose_b, count, st);
-    if (r == NPH_GPU_OK) r = stage(ds, speculative, count, st);
-    if (r == NPH_GPU_OK) r = stage(dout, (const NphGpuManifold *)nullptr, count, st);
-    if (r == NPH_GPU_OK) r = stage(dws, (const uint32_t *)nullptr, (uint32_t)ws_words, st);
-    if (r == NPH_GPU_OK) {
-        r = nph_gpu_collide_async(da, dpa, db, dpb, ds, count, dout, nullptr, dws, ws_words * sizeof(uint32_t), st);
+    std::lock_guard<std::mutex> lock(g_pipe_mutex);
+    if (g_pipes == nullptr) {
+        g_pipes = new (std::nothrow) std::vector<Pipe>();
+        if (g_pipes == nullptr) {
+            return NPH_GPU_OUT_OF_MEMORY;
+        }
     }
-    if (r == NPH_GPU_OK) {
-        cudaMemcpyAsync(out, dout, sizeof(NphGpuManifold) * count, cudaMemcpyDeviceToHost, st);
-        const cudaError_t e = cudaStreamSynchronize(st);
-        r = e == cudaSuccess ? NPH_GPU_OK : NPH_GPU_DEVICE_LOST;
+    if (g_pipes->size() <= (size_t)device) {
+        g_pipes->resize((size_t)device + 1u);
     }
-    cudaFree(da);
-    cudaFree(db);
-    cudaFree(dpa);
-    cudaFree(dpb);
-    cudaFree(ds);
-    cudaFree(dout);
-    cudaFree(dws);
-    cudaStreamDestroy(st);
-    return r;
+    Pipe &pipe = (*g_pipes)[(size_t)device];
+    const uint32_t chunk = std::min(count, std::max(kChunkMin, (count + kChunksWanted - 1u) / kChunksWanted));
+    NphGpuResult r = ensure_pipe(pipe, chunk);
+    if (r != NPH_GPU_OK) {
+        return r;
+    }
+    const uint64_t ws_bytes = nph_gpu_collide_workspace_bytes(chunk);
+    const uint32_t chunks = (count + chunk - 1u) / chunk;
+    // Every later chunk's stream waits for the first chunk's upload, so for this too.
+    cudaMemsetAsync(pipe.d_bad, 0, sizeof(uint32_t), pipe.slot[0].st);
+    for (uint32_t c = 0; c < chunks && r == NPH_GPU_OK; ++c) {
+        Slot &s = pipe.slot[c % kSlots];
+        const uint32_t first = c * chunk;
+        const uint32_t n = std::min(chunk, count - first);
+        if (c > 0) {
+            cudaStreamWaitEvent(s.st, pipe.slot[(c - 1u) % kSlots].up, 0);
+        }
+        cudaMemcpyAsync(s.a, a + first, sizeof(NphGpuShape) * n, cudaMemcpyHostToDevice, s.st);
+        cudaMemcpyAsync(s.pa, pose_a + first, sizeof(NphGpuPose) * n, cudaMemcpyHostToDevice, s.st);
+        cudaMemcpyAsync(s.b, b + first, sizeof(NphGpuShape) * n, cudaMemcpyHostToDevice, s.st);
+        cudaMemcpyAsync(s.pb, pose_b + first, sizeof(NphGpuPose) * n, cudaMemcpyHostToDevice, s.st);
+        cudaMemcpyAsync(s.spec, speculative + first, sizeof(float) * n, cudaMemcpyHostToDevice, s.st);
+        cudaEventRecord(s.up, s.st);
+        r = nph_gpu_collide_async(s.a, s.pa, s.b, s.pb, s.spec, n, s.out, pipe.d_bad, s.ws, ws_bytes, s.st);
+        cudaMemcpyAsync(out + first, s.out, sizeof(NphGpuManifold) * n, cudaMemcpyDeviceToHost, s.st);
+    }
+    for (Slot &s : pipe.slot) {
+        if (cudaStreamSynchronize(s.st) != cudaSuccess && r == NPH_GPU_OK) {
+            r = NPH_GPU_DEVICE_LOST;
+        }
+    }
+    if (r == NPH_GPU_OK && cudaGetLastError() != cudaSuccess) {
+        r = NPH_GPU_DEVICE_LOST;
+    }
+    uint32_t bad = 0;
+    if (r == NPH_GPU_OK && cudaMemcpy(&bad, pipe.d_bad, sizeof bad, cudaMemcpyDeviceToHost) != cudaSuccess) {
+        r = NPH_GPU_DEVICE_LOST;
+    }
+    return r == NPH_GPU_OK && bad != 0u ? NPH_GPU_UNSUPPORTED : r;
 }
 
 NPH_GPU_API uint64_t nph_gpu_collide_workspace_bytes(uint32_t count)

@@ -437,6 +437,14 @@ def collide(a: np.ndarray, pose_a: np.ndarray, b: np.ndarray, pose_b: np.ndarray
     return out
 
 
+def collide_host(a_ptr: int, pose_a_ptr: int, b_ptr: int, pose_b_ptr: int, speculative_ptr: int,
+                 count: int, out_ptr: int) -> None:
+    """nph_gpu_collide on host arrays given by address (page-locked arrays let its chunks'
+    copies overlap); synchronous."""
+    _check(lib().nph_gpu_collide(a_ptr, pose_a_ptr, b_ptr, pose_b_ptr, speculative_ptr, count,
+                                 out_ptr), "nph_gpu_collide")
+
+
 def collide_workspace_bytes(count: int) -> int:
     return int(lib().nph_gpu_collide_workspace_bytes(count))
 

@@ -46,16 +46,29 @@ def test_stacked_boxes_match_the_reference(ref_lib):
 
 
 def test_unknown_shape_types_are_refused(ref_lib):
-    from nepheline_b200.solver import SolverError, collide
-    box = np.zeros(1, abi.SHAPE_DTYPE)
+    """A pair of an unknown type: the host-buffer call returns NPH_GPU_UNSUPPORTED, that pair
+    gets the cleared manifold and every other pair its own."""
+    from nepheline_b200.solver import SolverError, collide, lib
+    box = np.zeros(2, abi.SHAPE_DTYPE)
     box["type"] = abi.SHAPE_BOX
     box["dims"] = 0.5
     other = box.copy()
-    other["type"] = 7
-    pose = np.zeros(1, abi.POSE_DTYPE)
-    pose["rotation"][:, 3] = 1.0
+    other["type"][1] = 7
+    pose_a = np.zeros(2, abi.POSE_DTYPE)
+    pose_a["rotation"][:, 3] = 1.0
+    pose_b = pose_a.copy()
+    pose_b["position"][:, 1] = 0.99
+    spec = np.full(2, 0.04, np.float32)
     with pytest.raises(SolverError):
-        collide(box, pose, other, pose, np.zeros(1, np.float32))
+        collide(box, pose_a, other, pose_b, spec)
+    out = np.zeros(2, abi.MANIFOLD_DTYPE)
+    out["point_count"] = 99
+    code = lib().nph_gpu_collide(box.ctypes.data, pose_a.ctypes.data, other.ctypes.data,
+                                 pose_b.ctypes.data, spec.ctypes.data, 2, out.ctypes.data)
+    assert code == abi.UNSUPPORTED
+    want = collide(box[:1], pose_a[:1], other[:1], pose_b[:1], spec[:1])
+    assert out[:1].tobytes() == want.tobytes() and want[0]["point_count"] == 4
+    assert out[1]["point_count"] == 0 and tuple(out[1]["normal"]) == (0.0, 1.0, 0.0)
 
 
 def test_async_sorted_and_unsorted_launches_agree(ref_lib):
@@ -91,3 +104,33 @@ def test_async_sorted_and_unsorted_launches_agree(ref_lib):
     got = outs[1][keep]
     bad_rows = [i for i, (x, y) in enumerate(zip(live(got), live(ref))) if x != y]
     assert not bad_rows, (len(bad_rows), bad_rows[:5])
+
+
+def test_host_call_in_chunks_equals_one_launch():
+    """nph_gpu_collide on host arrays, in chunks through its three streams (2, 16 and 1 chunks:
+    then slots reused and arrays grown, then a small call), gives the bits of one unsorted
+    launch over all the pairs; from page-locked and from ordinary host memory alike."""
+    import torch
+
+    from nepheline_b200 import scenes
+    from nepheline_b200.solver import collide, collide_async, collide_host
+
+    def one_launch(arrays, n):
+        dev = [torch.from_numpy(np.ascontiguousarray(x).view(np.uint8).reshape(-1)).to("cuda:0")
+               for x in arrays]
+        out = torch.empty(n * abi.MANIFOLD_DTYPE.itemsize, dtype=torch.uint8, device="cuda:0")
+        collide_async(*[d.data_ptr() for d in dev], n, out.data_ptr(), 0, 0, 0,
+                      torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        return out.cpu().numpy().view(abi.MANIFOLD_DTYPE)
+
+    for n, seed in ((131072, 3), (16 * 65536 + 4 * 65536 + 777, 4), (1000, 5)):
+        arrays = scenes.narrow_pairs(n, seed=seed)
+        want = one_launch(arrays, n)
+        got = collide(*arrays)
+        assert got.tobytes() == want.tobytes(), n
+        host = [torch.from_numpy(np.ascontiguousarray(x).view(np.uint8).reshape(-1)).pin_memory()
+                for x in arrays]
+        out = torch.zeros(n * abi.MANIFOLD_DTYPE.itemsize, dtype=torch.uint8).pin_memory()
+        collide_host(*[h.data_ptr() for h in host], n, out.data_ptr())
+        assert out.numpy().tobytes() == want.tobytes(), n
