@@ -496,8 +496,8 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_set_config(NphGpuBatch *batch,
  * carries one part's results back while later parts' records go up. Results are the same bits
  * as unsplit (the worlds are independent). Every record the device would refuse is checked on
  * the host before anything is copied, so a refused batch still has nothing written back. The
- * parts hold device arrays of their own; the batch's own upload, step and download calls do
- * not use them. */
+ * parts hold device arrays of their own (released by setting 1 part); the batch's own upload,
+ * step and download calls do not use them. */
 #define NPH_GPU_BATCH_MAX_PARTS 16u
 NPH_GPU_API NphGpuResult nph_gpu_batch_set_pipeline(NphGpuBatch *batch, uint32_t parts);
 NPH_GPU_API uint32_t nph_gpu_batch_config_count(void);
@@ -614,6 +614,9 @@ NPH_GPU_API NphGpuResult nph_gpu_collide(const NphGpuShape *a, const NphGpuPose 
                                          const NphGpuShape *b, const NphGpuPose *pose_b,
                                          const float *speculative, uint32_t count,
                                          NphGpuManifold *out);
+/* Frees the device arrays and streams nph_gpu_collide keeps between calls, on every device
+ * (the next call makes them again). */
+NPH_GPU_API void nph_gpu_collide_release(void);
 
 /* ------------------------------------------------------------------------------------
  * The contact update on the device

@@ -54,7 +54,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     for src in sources():
         obj = build_dir / (src.stem + ".o")
         cmd = [nvcc(), *ARCH, "-lineinfo", "-O3", "-std=c++17", *EXACT, *HOST,
-               f"-I{INCLUDE}", f"-I{CSRC}", "-dc" if False else "-c", str(src), "-o", str(obj)]
+               f"-I{INCLUDE}", f"-I{CSRC}", "-c", str(src), "-o", str(obj)]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
         subprocess.run(cmd, check=True)

@@ -1642,6 +1642,9 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_set_pipeline(NphGpuBatch *b, uint32_t par
         return NPH_GPU_INVALID_ARGUMENT;
     }
     b->pipeline_parts = parts;
+    if (parts == 1u) {
+        return ensure_parts(b, 0u); // the parts' arrays released
+    }
     return NPH_GPU_OK;
 }
 

@@ -266,6 +266,39 @@ NPH_GPU_API NphGpuResult nph_gpu_collide(const NphGpuShape *a, const NphGpuPose 
     return r == NPH_GPU_OK && bad != 0u ? NPH_GPU_UNSUPPORTED : r;
 }
 
+NPH_GPU_API void nph_gpu_collide_release(void)
+{
+    std::lock_guard<std::mutex> lock(g_pipe_mutex);
+    if (g_pipes == nullptr) {
+        return;
+    }
+    int current = 0;
+    cudaGetDevice(&current);
+    for (size_t d = 0; d < g_pipes->size(); ++d) {
+        Pipe &pipe = (*g_pipes)[d];
+        if (pipe.d_bad == nullptr && pipe.slot[0].st == nullptr) {
+            continue;
+        }
+        cudaSetDevice((int)d);
+        for (Slot &s : pipe.slot) {
+            if (s.st != nullptr) {
+                cudaStreamSynchronize(s.st);
+                cudaStreamDestroy(s.st);
+            }
+            if (s.up != nullptr) {
+                cudaEventDestroy(s.up);
+            }
+            free_slot_arrays(s);
+            s.st = nullptr;
+            s.up = nullptr;
+        }
+        cudaFree(pipe.d_bad);
+        pipe.d_bad = nullptr;
+        pipe.chunk_cap = 0;
+    }
+    cudaSetDevice(current);
+}
+
 NPH_GPU_API uint64_t nph_gpu_collide_workspace_bytes(uint32_t count)
 {
     return 2ull * kKinds * sizeof(uint32_t) + 2ull * count * sizeof(uint32_t);

@@ -69,6 +69,7 @@ def lib() -> ctypes.CDLL:
                                                     _u32, ctypes.c_float, _u32, ctypes.c_float,
                                                     _vp, _vp, P(abi.ConvergeStats)]),
         "nph_gpu_collide": (ctypes.c_int32, [_vp, _vp, _vp, _vp, _vp, _u32, _vp]),
+        "nph_gpu_collide_release": (None, []),
         "nph_gpu_world_sleep_decision": (ctypes.c_int32, [_vp, _vp, _u32, _vp, ctypes.c_float, _vp, _vp,
                                                           _vp]),
         "nph_gpu_collide_async": (ctypes.c_int32, [_vp, _vp, _vp, _vp, _vp, _u32, _vp, _vp, _vp,
@@ -443,6 +444,11 @@ def collide_host(a_ptr: int, pose_a_ptr: int, b_ptr: int, pose_b_ptr: int, specu
     copies overlap); synchronous."""
     _check(lib().nph_gpu_collide(a_ptr, pose_a_ptr, b_ptr, pose_b_ptr, speculative_ptr, count,
                                  out_ptr), "nph_gpu_collide")
+
+
+def collide_release() -> None:
+    """Frees the device arrays nph_gpu_collide keeps between calls."""
+    lib().nph_gpu_collide_release()
 
 
 def collide_workspace_bytes(count: int) -> int:

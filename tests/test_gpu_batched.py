@@ -374,4 +374,12 @@ def test_drop_in_in_parts_refuses_before_writing_back(solver):
         assert not helpers.mismatches(w, want)
     with pytest.raises(Exception):
         batch.set_pipeline(0)
+    # One part: the parts released, the call unsplit, the same bits.
+    batch.set_pipeline(1)
+    worlds = abi.pack_views([v.copy() for v in views])
+    batch.phys_solve_worlds(worlds, params, DT)
+    for w, v in zip(worlds, views):
+        want = v.copy()
+        solver.phys_solve(want, params, DT)
+        assert not helpers.mismatches(w, want)
     batch.close()

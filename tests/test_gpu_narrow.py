@@ -113,7 +113,7 @@ def test_host_call_in_chunks_equals_one_launch():
     import torch
 
     from nepheline_b200 import scenes
-    from nepheline_b200.solver import collide, collide_async, collide_host
+    from nepheline_b200.solver import collide, collide_async, collide_host, collide_release
 
     def one_launch(arrays, n):
         dev = [torch.from_numpy(np.ascontiguousarray(x).view(np.uint8).reshape(-1)).to("cuda:0")
@@ -134,3 +134,7 @@ def test_host_call_in_chunks_equals_one_launch():
         out = torch.zeros(n * abi.MANIFOLD_DTYPE.itemsize, dtype=torch.uint8).pin_memory()
         collide_host(*[h.data_ptr() for h in host], n, out.data_ptr())
         assert out.numpy().tobytes() == want.tobytes(), n
+    # Released, then made again by the next call.
+    collide_release()
+    collide_release()
+    assert collide(*arrays).tobytes() == want.tobytes()
