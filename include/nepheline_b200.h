@@ -586,8 +586,8 @@ typedef struct NphGpuManifold {
  * capsule-capsule and box-sphere (collide.c:281-458), box-capsule (collide_hull.c:207-378) and
  * box-box (collide_hull.c:1085-1266: the oriented-box axis test, face clipping with the
  * reduction to four points, edge pairs, GJK for shapes apart); each manifold is the same bits as
- * the reference's. An unknown type is refused (NPH_GPU_UNSUPPORTED). Runs on the current
- * device. */
+ * the reference's. A pair of an unknown type gets the cleared manifold and makes the call
+ * return NPH_GPU_UNSUPPORTED (nph_gpu_collide, below). */
 /* The same on DEVICE arrays, enqueued on `stream` (a cudaStream_t; NULL: the default stream)
  * without allocating or waiting: the caller owns the arrays and synchronises the stream. With a
  * device `workspace` of at least nph_gpu_collide_workspace_bytes(count) bytes (4-byte aligned)
