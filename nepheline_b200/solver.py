@@ -359,12 +359,12 @@ class Batch:
 
     @staticmethod
     def _c_views(views):
-        arr = abi.views_array(views)
-        return arr, arr.ctypes.data_as(ctypes.POINTER(abi.WorldView))
+        # The pointer keeps the array alive (numpy's data_as holds a reference to it).
+        return abi.views_array(views).ctypes.data_as(ctypes.POINTER(abi.WorldView))
 
     def upload(self, views: list) -> None:
         self._views = views
-        keep, arr = self._c_views(views)
+        arr = self._c_views(views)
         _check(self.L.nph_gpu_batch_upload(self._h, arr, len(views)), "nph_gpu_batch_upload")
 
     def step_async(self, params: abi.WorldParams, dt: float, steps: int = 1) -> None:
@@ -372,16 +372,16 @@ class Batch:
                "nph_gpu_batch_step_async")
 
     def download(self, views: list) -> None:
-        keep, arr = self._c_views(views)
+        arr = self._c_views(views)
         _check(self.L.nph_gpu_batch_download(self._h, arr, len(views)), "nph_gpu_batch_download")
 
     def phys_solve_worlds(self, views: list, params: abi.WorldParams, dt: float) -> None:
-        keep, arr = self._c_views(views)
+        arr = self._c_views(views)
         _check(self.L.nph_gpu_phys_solve_worlds(self._h, ctypes.byref(params), dt, arr,
                                                 len(views)), "nph_gpu_phys_solve_worlds")
 
     def phys_solve_worlds_code(self, views: list, params: abi.WorldParams, dt: float) -> int:
-        keep, arr = self._c_views(views)
+        arr = self._c_views(views)
         return int(self.L.nph_gpu_phys_solve_worlds(self._h, ctypes.byref(params), dt, arr,
                                                     len(views)))
 
