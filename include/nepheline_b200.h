@@ -89,7 +89,9 @@ typedef int32_t NphGpuResult;
 #define NPH_GPU_LOCK_ANGULAR_Z (1u << 5)
 
 /* Contact flag bits the solver stage reads and writes (PHYS_CONTACT_*,
- * world_internal.h:207-213). */
+ * world_internal.h:207-213): HIT in and out; HIT_EVENTS (either shape reports hits) read by
+ * nph_gpu_world_hit_events; the solver keeps every other bit as it came. */
+#define NPH_GPU_CONTACT_HIT_EVENTS (1u << 2)
 #define NPH_GPU_CONTACT_HIT (1u << 4)
 
 /* Constraint bits of nph_gpu_graph_color. */
@@ -196,7 +198,7 @@ typedef struct NphGpuContactPoint {
 typedef struct NphGpuContact {
     uint32_t body_a;
     uint32_t body_b;
-    uint32_t flags;             /* NPH_GPU_CONTACT_HIT: in and out */
+    uint32_t flags;             /* NPH_GPU_CONTACT_HIT: in and out; NPH_GPU_CONTACT_HIT_EVENTS */
     uint32_t point_count;       /* 1..4 */
     float normal[3];            /* from A to B */
     float friction;
@@ -713,6 +715,26 @@ NPH_GPU_API NphGpuResult nph_gpu_world_sleep_decision(NphGpuSolver *solver, cons
                                                      uint32_t island_count, const uint32_t *removed,
                                                      float time_to_sleep, uint8_t *sleep, uint32_t *split,
                                                      uint8_t *kinematic_sleep);
+
+/* A hit of hit_events (solver.c:919-960): the manifold (its index in the view) and its point of
+ * fastest approach. The caller makes NphPhysicsContactHitEvent from it: its shapes, the point
+ * as body A's centre plus the point's anchor_a (nph_dvec3_add_vec3), the manifold's normal. */
+typedef struct NphGpuHitEvent {
+    uint32_t contact;
+    uint32_t point;
+    float approach_speed; /* -relative_velocity, above the threshold */
+    uint32_t pad;
+} NphGpuHitEvent;
+
+/* hit_events after a step, on the device-resident records: for each manifold with
+ * NPH_GPU_CONTACT_HIT_EVENTS, in the view's order (the colour lists, then the overflow: the
+ * reference's order), the point whose approach speed is the largest above `threshold` (the
+ * world's hit_threshold, nph_physics_world_set_hit_threshold) among those with a positive
+ * max_normal_impulse, the first such point on a tie; manifolds with none make no event. Writes
+ * the first min(*count, capacity) events to the host array `events` and the number of events to
+ * `*count`. */
+NPH_GPU_API NphGpuResult nph_gpu_world_hit_events(NphGpuSolver *solver, float threshold, NphGpuHitEvent *events,
+                                                 uint32_t capacity, uint32_t *count);
 
 NPH_GPU_API NphGpuResult nph_gpu_world_features(NphGpuSolver *solver,
                                                 const NphGpuWorldParams *params, float dt,

@@ -36,6 +36,7 @@ BODY_DYNAMIC = 2
 BODY_ENABLE_SLEEP = 1 << 1
 BODY_GYROSCOPIC = 1 << 2
 BODY_BULLET = 1 << 5
+CONTACT_HIT_EVENTS = 1 << 2
 CONTACT_HIT = 1 << 4
 CONSTRAINT_A_DYNAMIC = 1
 CONSTRAINT_B_DYNAMIC = 2
@@ -396,6 +397,25 @@ def pack_views(views: list, alloc=None) -> list:
 # The narrow phase's records (nepheline_b200.h).
 SHAPE_SPHERE, SHAPE_CAPSULE, SHAPE_BOX = 0, 1, 2
 SHAPE_DTYPE = np.dtype([("type", "<u4"), ("dims", "<f4", 3)], align=True)
+HIT_EVENT_DTYPE = np.dtype([("contact", "<u4"), ("point", "<u4"), ("approach_speed", "<f4"),
+                            ("pad", "<u4")])
+
+
+def hit_points(view: "View", events: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """The world points and normals of hit events, from the view the step wrote back: body A's
+    centre plus the point's anchor_a, each component a double sum (nph_dvec3_add_vec3), and the
+    manifold's normal."""
+    c = view.contacts[events["contact"]]
+    a = c["body_a"].astype(np.int64)
+    n = len(view.bodies)
+    centers = np.empty((len(c), 3), np.float64)
+    own = a < n
+    centers[own] = view.bodies["center"][a[own]]
+    centers[~own] = view.fixed["center"][a[~own] - n]
+    anchor = c["points"]["anchor_a"][np.arange(len(c)), events["point"]]
+    return centers + anchor.astype(np.float64), c["normal"].copy()
+
+
 POSE_DTYPE = np.dtype([("position", "<f4", 3), ("rotation", "<f4", 4)], align=True)
 MANIFOLD_POINT_DTYPE = np.dtype([("point", "<f4", 3), ("separation", "<f4"), ("id", "<u4")],
                                 align=True)

@@ -642,6 +642,101 @@ __global__ void __launch_bounds__(256) k_island_decide(const uint32_t *tmin, con
     sleep[k] = asleep;
 }
 
+// hit_events (solver.c:919-960) for one manifold: with NPH_GPU_CONTACT_HIT_EVENTS, its point of
+// fastest approach above the threshold among those with a positive max_normal_impulse (the
+// first on a tie: only a strictly faster point replaces it).
+__device__ __forceinline__ bool hit_point(const NphGpuContact &c, float threshold, uint32_t &point, float &speed)
+{
+    if ((c.flags & NPH_GPU_CONTACT_HIT_EVENTS) == 0u) {
+        return false;
+    }
+    const uint32_t pc = c.point_count <= NPH_GPU_MAX_POINTS ? c.point_count : 0u;
+    float best = threshold;
+    uint32_t found = NPH_GPU_NULL;
+    for (uint32_t k = 0; k < pc; ++k) {
+        const float approach = -c.points[k].relative_velocity;
+        if (approach > best && c.points[k].max_normal_impulse > 0.0f) {
+            best = approach;
+            found = k;
+        }
+    }
+    point = found;
+    speed = best;
+    return found != NPH_GPU_NULL;
+}
+
+constexpr uint32_t kHitBlock = 256;
+constexpr uint32_t kHitScanThreads = 1024;
+
+// The hits of each block of manifolds.
+__global__ void __launch_bounds__(kHitBlock) k_hit_count(const NphGpuContact *contacts, uint32_t m, float threshold,
+                                                         uint32_t *block_hits)
+{
+    const uint32_t g = blockIdx.x * kHitBlock + threadIdx.x;
+    uint32_t point = 0u;
+    float speed = 0.0f;
+    const bool hit = g < m && hit_point(contacts[g], threshold, point, speed);
+    const uint32_t n = (uint32_t)__syncthreads_count(hit ? 1 : 0);
+    if (threadIdx.x == 0u) {
+        block_hits[blockIdx.x] = n;
+    }
+}
+
+// The blocks' hit counts turned into each block's first event, in place, and the total after
+// them: each thread sums a run of blocks, one block-wide scan of the runs, then each run again.
+__global__ void __launch_bounds__(kHitScanThreads) k_hit_scan(uint32_t *block_hits, uint32_t blocks)
+{
+    __shared__ uint32_t part[kHitScanThreads];
+    const uint32_t t = threadIdx.x;
+    const uint32_t per = (blocks + kHitScanThreads - 1u) / kHitScanThreads;
+    const uint32_t first = min(blocks, t * per), end = min(blocks, first + per);
+    uint32_t sum = 0u;
+    for (uint32_t i = first; i < end; ++i) {
+        sum += block_hits[i];
+    }
+    part[t] = sum;
+    __syncthreads();
+    for (uint32_t d = 1u; d < kHitScanThreads; d <<= 1u) {
+        const uint32_t v = t >= d ? part[t - d] : 0u;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    uint32_t run = part[t] - sum;
+    for (uint32_t i = first; i < end; ++i) {
+        const uint32_t h = block_hits[i];
+        block_hits[i] = run;
+        run += h;
+    }
+    if (t == kHitScanThreads - 1u) {
+        block_hits[blocks] = part[t];
+    }
+}
+
+// Each hit at its block's first event plus the hits before it in the block: manifold order.
+__global__ void __launch_bounds__(kHitBlock) k_hit_write(const NphGpuContact *contacts, uint32_t m, float threshold,
+                                                         const uint32_t *block_first, NphGpuHitEvent *out)
+{
+    __shared__ uint32_t warp_hits[kHitBlock / 32u];
+    const uint32_t g = blockIdx.x * kHitBlock + threadIdx.x;
+    uint32_t point = 0u;
+    float speed = 0.0f;
+    const bool hit = g < m && hit_point(contacts[g], threshold, point, speed);
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5u;
+    const uint32_t ballot = __ballot_sync(0xFFFFFFFFu, hit);
+    if (lane == 0u) {
+        warp_hits[warp] = (uint32_t)__popc(ballot);
+    }
+    __syncthreads();
+    uint32_t at = block_first[blockIdx.x] + (uint32_t)__popc(ballot & ((1u << lane) - 1u));
+    for (uint32_t w = 0; w < warp; ++w) {
+        at += warp_hits[w];
+    }
+    if (hit) {
+        out[at] = NphGpuHitEvent{g, point, speed, 0u};
+    }
+}
+
 } // namespace nph
 
 using namespace nph;
@@ -1858,6 +1953,45 @@ NPH_GPU_API NphGpuResult nph_gpu_world_sleep_decision(NphGpuSolver *s, const uin
     dfree(d_max);
     dfree(d_sleep);
     dfree(d_split);
+    return r;
+}
+
+NPH_GPU_API NphGpuResult nph_gpu_world_hit_events(NphGpuSolver *s, float threshold, NphGpuHitEvent *events,
+                                                 uint32_t capacity, uint32_t *count)
+{
+    if (s == nullptr || count == nullptr || (capacity > 0u && events == nullptr)) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    if (!s->uploaded) {
+        return NPH_GPU_INVALID_STATE;
+    }
+    *count = 0u;
+    if (s->m == 0u) {
+        return NPH_GPU_OK;
+    }
+    cudaSetDevice(s->device);
+    const uint32_t blocks = (s->m + kHitBlock - 1u) / kHitBlock;
+    uint32_t *d_blocks = nullptr;
+    NphGpuHitEvent *d_out = nullptr;
+    NphGpuResult r = dalloc(d_blocks, blocks + 1u) && dalloc(d_out, s->m) ? NPH_GPU_OK : NPH_GPU_OUT_OF_MEMORY;
+    uint32_t total = 0u;
+    if (r == NPH_GPU_OK) {
+        k_hit_count<<<blocks, kHitBlock, 0, s->stream>>>(s->d_contacts, s->m, threshold, d_blocks);
+        k_hit_scan<<<1, kHitScanThreads, 0, s->stream>>>(d_blocks, blocks);
+        k_hit_write<<<blocks, kHitBlock, 0, s->stream>>>(s->d_contacts, s->m, threshold, d_blocks, d_out);
+        cudaMemcpyAsync(&total, d_blocks + blocks, sizeof total, cudaMemcpyDeviceToHost, s->stream);
+        r = check_cuda(cudaStreamSynchronize(s->stream));
+    }
+    const uint32_t n = std::min(total, capacity);
+    if (r == NPH_GPU_OK && n > 0u) {
+        r = check_cuda(cudaMemcpy(events, d_out, sizeof(NphGpuHitEvent) * n, cudaMemcpyDeviceToHost));
+    }
+    if (r == NPH_GPU_OK) {
+        *count = total;
+    }
+    cudaGetLastError();
+    dfree(d_blocks);
+    dfree(d_out);
     return r;
 }
 

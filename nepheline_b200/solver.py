@@ -70,6 +70,7 @@ def lib() -> ctypes.CDLL:
                                                     _vp, _vp, P(abi.ConvergeStats)]),
         "nph_gpu_collide": (ctypes.c_int32, [_vp, _vp, _vp, _vp, _vp, _u32, _vp]),
         "nph_gpu_collide_release": (None, []),
+        "nph_gpu_world_hit_events": (ctypes.c_int32, [_vp, ctypes.c_float, _vp, _u32, P(_u32)]),
         "nph_gpu_world_sleep_decision": (ctypes.c_int32, [_vp, _vp, _u32, _vp, ctypes.c_float, _vp, _vp,
                                                           _vp]),
         "nph_gpu_collide_async": (ctypes.c_int32, [_vp, _vp, _vp, _vp, _vp, _u32, _vp, _vp, _vp,
@@ -202,6 +203,16 @@ class Solver:
                "nph_gpu_world_sleep_decision")
         k = int(split.value)
         return sleep[:len(removed)] != 0, (None if k == abi.NULL else k), kin[:len(island_of)] != 0
+
+    def hit_events(self, threshold: float = 1.0, capacity: int | None = None) -> np.ndarray:
+        """nph_gpu_world_hit_events after a step: the hits in the view's order (the contact's
+        index, its point of fastest approach, the approach speed)."""
+        cap = int(self._m) if capacity is None else capacity
+        out = np.zeros(max(cap, 1), abi.HIT_EVENT_DTYPE)
+        count = _u32()
+        _check(self.L.nph_gpu_world_hit_events(self._h, threshold, out.ctypes.data, cap, ctypes.byref(count)),
+               "nph_gpu_world_hit_events")
+        return out[:min(int(count.value), cap)]
 
     def update_contacts(self, fresh: np.ndarray) -> None:
         """This step's manifolds (one per uploaded contact, same order, impulses zero),

@@ -185,6 +185,7 @@ REF_API u32 nphref_add_body(RefWorld *r, u32 type, const f64 position[3], const 
         sd.density = density;
         sd.friction = friction;
         sd.restitution = restitution;
+        sd.hit_events = (flags & 8U) != 0U ? 1 : 0;
         NphPhysicsShape s;
         if (nph_physics_shape_create(r->w, b, &sd, &s) != NPH_RESULT_OK) {
             return PHYS_NULL;
@@ -301,7 +302,7 @@ REF_API u32 nphref_inject_contact(RefWorld *r, const NphGpuContact *in)
     c->shape_b = 0U;
     c->body_a = phys_handle_slot(r->bodies[in->body_a].value);
     c->body_b = phys_handle_slot(r->bodies[in->body_b].value);
-    c->flags = PHYS_CONTACT_TOUCHING | (in->flags & NPH_GPU_CONTACT_HIT);
+    c->flags = PHYS_CONTACT_TOUCHING | (in->flags & (NPH_GPU_CONTACT_HIT | NPH_GPU_CONTACT_HIT_EVENTS));
     c->parent = PHYS_NULL;
     c->child = PHYS_NULL;
     c->prev[0] = c->prev[1] = PHYS_NULL;
@@ -349,8 +350,30 @@ REF_API int nphref_collide(RefWorld *r)
 REF_API int nphref_solve(RefWorld *r, f32 dt)
 {
     r->w->step_dt = dt;
+    NPH_ARRAY_CLEAR(&r->w->hit_events); // as the world step does before its stages (world.c:320)
+    NPH_ARRAY_CLEAR(&r->w->move_events);
     return (int)phys_solve(r->w, dt, r->js);
 }
+
+// The hit events of the last solve (solver.c:919-960), in their order: approach speed, world
+// point and normal; returns how many there are (at most `cap` written).
+REF_API u32 nphref_hit_events(const RefWorld *r, u32 cap, f32 *approach, f64 *point, f32 *normal)
+{
+    const u32 n = r->w->hit_events.len;
+    for (u32 i = 0U; i < n && i < cap; ++i) {
+        const NphPhysicsContactHitEvent *e = &r->w->hit_events.data[i];
+        approach[i] = e->approach_speed;
+        point[3U * i + 0U] = e->point.x;
+        point[3U * i + 1U] = e->point.y;
+        point[3U * i + 2U] = e->point.z;
+        normal[3U * i + 0U] = e->normal.x;
+        normal[3U * i + 1U] = e->normal.y;
+        normal[3U * i + 2U] = e->normal.z;
+    }
+    return n;
+}
+
+REF_API void nphref_set_hit_threshold(RefWorld *r, f32 speed) { nph_physics_world_set_hit_threshold(r->w, speed); }
 
 REF_API int nphref_finish(RefWorld *r)
 {
@@ -599,7 +622,7 @@ static void contact_record(RefWorld *r, const PhysContact *c, NphGpuContact *o, 
     memset(o, 0, sizeof *o);
     o->body_a = view_index(r, c->body_a, fixed_count);
     o->body_b = view_index(r, c->body_b, fixed_count);
-    o->flags = c->flags & PHYS_CONTACT_HIT;
+    o->flags = c->flags & (PHYS_CONTACT_HIT | PHYS_CONTACT_HIT_EVENTS);
     o->point_count = c->point_count;
     memcpy(o->normal, &c->normal, sizeof o->normal);
     o->friction = c->friction;
@@ -619,6 +642,8 @@ static void contact_record(RefWorld *r, const PhysContact *c, NphGpuContact *o, 
 }
 
 #define JOINT_BLOCKS (NPH_GPU_JOINT_BLOCK_ROTATION | NPH_GPU_JOINT_BLOCK_SWING | NPH_GPU_JOINT_BLOCK_POINT)
+_Static_assert(NPH_GPU_CONTACT_HIT == PHYS_CONTACT_HIT && NPH_GPU_CONTACT_HIT_EVENTS == PHYS_CONTACT_HIT_EVENTS,
+               "the contact record's flag bits are the world's");
 _Static_assert(sizeof(((PhysJoint *)0)->axis_impulse) == sizeof(((NphGpuJoint *)0)->axis_impulse),
                "the rows per axis of PhysJoint and of the record");
 

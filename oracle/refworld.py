@@ -54,6 +54,8 @@ def _ref_lib():
             "nphref_inject_contacts": (_u32, [_vp, _u32, _vp]),
             "nphref_collide": (ctypes.c_int, [_vp]),
             "nphref_solve": (ctypes.c_int, [_vp, _f32]),
+            "nphref_hit_events": (_u32, [_vp, _u32, _vp, _vp, _vp]),
+            "nphref_set_hit_threshold": (None, [_vp, _f32]),
             "nphref_finish": (ctypes.c_int, [_vp]),
             "nphref_step": (ctypes.c_int, [_vp, _f32]),
             "nphref_hash": (ctypes.c_uint64, [_vp]),
@@ -149,13 +151,14 @@ class RefWorld:
     def add_body(self, type_, position, rotation=(0, 0, 0, 1), velocity=(0, 0, 0),
                  angular_velocity=(0, 0, 0), shape=0, dims=(0, 0, 0), density=1000.0,
                  friction=0.6, restitution=0.0, gyroscopic=True, enable_sleep=True,
-                 bullet=False) -> int:
+                 bullet=False, hit_events=False) -> int:
         pos = np.asarray(position, np.float64)
         rot = np.asarray(rotation, np.float32)
         v = np.asarray(velocity, np.float32)
         w = np.asarray(angular_velocity, np.float32)
         d = np.asarray(dims, np.float32)
-        flags = (1 if gyroscopic else 0) | (2 if enable_sleep else 0) | (4 if bullet else 0)
+        flags = ((1 if gyroscopic else 0) | (2 if enable_sleep else 0) | (4 if bullet else 0)
+                 | (8 if hit_events else 0))
         idx = self.lib.nphref_add_body(self._h, type_, _p(pos), _p(rot), _p(v), _p(w), shape,
                                        _p(d), density, friction, restitution, flags)
         if idx == abi.NULL:
@@ -200,6 +203,19 @@ class RefWorld:
         r = self.lib.nphref_collide(self._h)
         if r != 0:
             raise RuntimeError(f"reference collide failed: {r}")
+
+    def hit_events(self):
+        """The last solve's hit events (solver.c:919-960): approach speeds, world points (f64)
+        and normals, in the reference's order."""
+        n = int(self.lib.nphref_hit_events(self._h, 0, None, None, None))
+        speed = np.zeros(max(n, 1), np.float32)
+        point = np.zeros((max(n, 1), 3), np.float64)
+        normal = np.zeros((max(n, 1), 3), np.float32)
+        self.lib.nphref_hit_events(self._h, n, speed.ctypes.data, point.ctypes.data, normal.ctypes.data)
+        return speed[:n], point[:n], normal[:n]
+
+    def set_hit_threshold(self, speed: float) -> None:
+        self.lib.nphref_set_hit_threshold(self._h, speed)
 
     def solve(self, dt: float) -> float:
         r = self.lib.nphref_solve(self._h, dt)

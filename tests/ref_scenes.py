@@ -28,9 +28,10 @@ def pyramid(rows: int = 20, jitter: float = 1e-3, seed: int = 1, params=None, wo
 
 
 def sphere_pour(count: int = 512, seed: int = 2, extent: float = 12.0, params=None,
-                workers: int = 0):
+                workers: int = 0, hit_events: bool = False):
     """Spheres of radius 0.5 with density U[500, 2000], friction U[0.2, 0.9], restitution
-    U[0, 0.3], at seeded non-overlapping lattice sites of a box above the ground."""
+    U[0, 0.3], at seeded non-overlapping lattice sites of a box above the ground (every other
+    sphere reporting hits when `hit_events`)."""
     from oracle.refworld import RefWorld
     rng = np.random.default_rng(seed)
     w = RefWorld(params or abi.WorldParams.default(), enable_sleep=False, workers=workers)
@@ -47,7 +48,8 @@ def sphere_pour(count: int = 512, seed: int = 2, extent: float = 12.0, params=No
         w.add_sphere(tuple(p), 0.5, density=float(rng.uniform(500, 2000)),
                      friction=float(rng.uniform(0.2, 0.9)),
                      restitution=float(rng.uniform(0.0, 0.3)),
-                     velocity=tuple(rng.uniform(-1.0, 1.0, 3) + np.array([0, -2.0, 0])))
+                     velocity=tuple(rng.uniform(-1.0, 1.0, 3) + np.array([0, -2.0, 0])),
+                     hit_events=hit_events and (int(s.sum()) % 2 == 0))
     return w
 
 

@@ -1,0 +1,101 @@
+"""Hit events (hit_events, solver.c:919-960): per manifold whose shapes report hits, its point
+of fastest approach above the world's threshold among those that took load, in the colour
+lists' order.
+
+CPU: the restatement (oracle/hits.py) on the records the reference's phys_solve wrote equals
+the reference's own events, approach speed, world point and normal bit for bit, over a sphere
+pour in which half the spheres report hits. GPU: the device's nph_gpu_world_hit_events after
+the device's step equals the reference's events the same way."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from nepheline_b200 import abi
+from tests import helpers, ref_scenes
+
+DT = 1.0 / 60.0
+
+
+def same_events(events, view, ref):
+    speed, point, normal = ref
+    assert len(events) == len(speed)
+    assert events["approach_speed"].tobytes() == speed.tobytes()
+    p, n = abi.hit_points(view, events)
+    assert p.tobytes() == point.tobytes()
+    assert n.tobytes() == normal.tobytes()
+
+
+@pytest.mark.parametrize("threshold", [1.0, 0.25])
+def test_restatement_matches_reference_hit_events(ref_lib, threshold):
+    from oracle.hits import hit_events_of
+    w = ref_scenes.sphere_pour(count=216, hit_events=True)
+    w.set_hit_threshold(threshold)
+    seen = 0
+    for s in range(90):
+        w.collide()
+        w.solve(DT)
+        out = w.export_view()
+        ref = w.hit_events()
+        same_events(hit_events_of(out, threshold), out, ref)
+        seen += len(ref[0])
+        w.finish()
+    assert seen > 20, seen
+    # Contacts of spheres that do not report hits carry no flag: some manifolds have none.
+    flags = w.export_view().contacts["flags"]
+    assert ((flags & abi.CONTACT_HIT_EVENTS) == 0).any() and ((flags & abi.CONTACT_HIT_EVENTS) != 0).any()
+    w.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("threshold", [1.0, 0.25])
+def test_device_hit_events_match_reference(solver, ref_lib, threshold):
+    from oracle.hits import hit_events_of
+    w = ref_scenes.sphere_pour(count=216, hit_events=True)
+    w.set_hit_threshold(threshold)
+    p = abi.WorldParams.default()
+    seen = 0
+    for s in range(90):
+        w.collide()
+        vin = w.export_view()
+        dev = vin.copy()
+        solver.phys_solve(dev, p, DT)
+        events = solver.hit_events(threshold)
+        w.solve(DT)
+        ref_view = w.export_view()
+        assert not helpers.mismatches(dev, ref_view), f"step {s}"
+        same_events(events, dev, w.hit_events())
+        assert events.tobytes() == hit_events_of(dev, threshold).tobytes()
+        seen += len(events)
+        if len(events) > 1:
+            # A smaller buffer takes the first events; the count is all of them.
+            head = solver.hit_events(threshold, capacity=1)
+            assert head.tobytes() == events[:1].tobytes()
+        w.finish()
+    assert seen > 20, seen
+    w.close()
+
+
+@pytest.mark.gpu
+def test_device_hit_events_on_many_manifolds(solver):
+    """Hits spread over many blocks of manifolds (the ordered write across blocks), read from
+    uploaded records whose flags, approach speeds and impulses are set on the host: 70 % of the
+    manifolds report hits, a quarter of the points took no load, ties included."""
+    from oracle.hits import hit_events_of
+    from nepheline_b200 import scenes
+    sc = scenes.lattice_graph(24, seed=3, joint_fraction=0.0)
+    v = sc.to_view(*scenes.host_color(sc))
+    rng = np.random.default_rng(4)
+    c = v.contacts
+    c["flags"] |= np.where(rng.random(len(c)) < 0.7, abi.CONTACT_HIT_EVENTS, 0).astype(np.uint32)
+    pts = c["points"]
+    pts["relative_velocity"] = np.round(rng.uniform(-4.0, 1.0, pts["relative_velocity"].shape), 1)
+    pts["max_normal_impulse"] = np.where(rng.random(pts["max_normal_impulse"].shape) < 0.25, 0.0,
+                                         rng.uniform(0.0, 2.0, pts["max_normal_impulse"].shape))
+    solver.upload(v)
+    for threshold in (0.5, 2.0):
+        events = solver.hit_events(threshold)
+        want = hit_events_of(v, threshold)
+        assert len(want) > 1000
+        assert events.tobytes() == want.tobytes()
+    assert len(solver.hit_events(10.0)) == 0
