@@ -146,10 +146,14 @@ class Solver:
         cv = view.c_view()
         _check(self.L.nph_gpu_phys_solve(self._h, ctypes.byref(params), dt, ctypes.byref(cv)),
                "nph_gpu_phys_solve")
+        self._m = len(view.contacts)
 
     def phys_solve_code(self, view: abi.View, params: abi.WorldParams, dt: float) -> int:
         cv = view.c_view()
-        return int(self.L.nph_gpu_phys_solve(self._h, ctypes.byref(params), dt, ctypes.byref(cv)))
+        code = int(self.L.nph_gpu_phys_solve(self._h, ctypes.byref(params), dt, ctypes.byref(cv)))
+        if code == abi.OK:
+            self._m = len(view.contacts)
+        return code
 
     def upload(self, view: abi.View) -> None:
         cv = view.c_view()
@@ -207,12 +211,15 @@ class Solver:
     def hit_events(self, threshold: float = 1.0, capacity: int | None = None) -> np.ndarray:
         """nph_gpu_world_hit_events after a step: the hits in the view's order (the contact's
         index, its point of fastest approach, the approach speed)."""
-        cap = int(self._m) if capacity is None else capacity
-        out = np.zeros(max(cap, 1), abi.HIT_EVENT_DTYPE)
         count = _u32()
-        _check(self.L.nph_gpu_world_hit_events(self._h, threshold, out.ctypes.data, cap, ctypes.byref(count)),
-               "nph_gpu_world_hit_events")
-        return out[:min(int(count.value), cap)]
+        if capacity is None:  # the count first, then every event
+            _check(self.L.nph_gpu_world_hit_events(self._h, threshold, None, 0, ctypes.byref(count)),
+                   "nph_gpu_world_hit_events")
+            capacity = int(count.value)
+        out = np.zeros(max(capacity, 1), abi.HIT_EVENT_DTYPE)
+        _check(self.L.nph_gpu_world_hit_events(self._h, threshold, out.ctypes.data, capacity,
+                                               ctypes.byref(count)), "nph_gpu_world_hit_events")
+        return out[:min(int(count.value), capacity)]
 
     def update_contacts(self, fresh: np.ndarray) -> None:
         """This step's manifolds (one per uploaded contact, same order, impulses zero),

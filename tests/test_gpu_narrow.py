@@ -138,3 +138,15 @@ def test_host_call_in_chunks_equals_one_launch():
     collide_release()
     collide_release()
     assert collide(*arrays).tobytes() == want.tobytes()
+
+
+def test_host_call_edge_counts():
+    """No pairs: nothing to do; one pair: the one-launch result."""
+    from nepheline_b200 import scenes
+    from nepheline_b200.solver import collide, collide_host
+    a, pa, b, pb, sp = scenes.narrow_pairs(3, seed=6)
+    assert len(collide(a[:0], pa[:0], b[:0], pb[:0], sp[:0])) == 0
+    collide_host(0, 0, 0, 0, 0, 0, 0)
+    one = collide(a[:1], pa[:1], b[:1], pb[:1], sp[:1])
+    three = collide(a, pa, b, pb, sp)
+    assert one.tobytes() == three[:1].tobytes()

@@ -99,3 +99,19 @@ def test_device_hit_events_on_many_manifolds(solver):
         assert len(want) > 1000
         assert events.tobytes() == want.tobytes()
     assert len(solver.hit_events(10.0)) == 0
+
+
+@pytest.mark.gpu
+def test_device_hit_events_edge_cases():
+    """Before any upload the call is refused; a world without manifolds has no hits."""
+    from nepheline_b200 import scenes
+    from nepheline_b200.solver import Solver, SolverError
+    s = Solver(device=0)
+    with pytest.raises(SolverError):
+        s.hit_events(1.0)
+    sc = scenes.lattice_graph(3, seed=1, joint_fraction=0.5)
+    sc.contacts = sc.contacts[:0]
+    v = sc.to_view(*scenes.host_color(sc))
+    s.phys_solve(v, abi.WorldParams.default(), DT)
+    assert len(s.hit_events(0.0)) == 0
+    s.close()
