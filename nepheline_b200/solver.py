@@ -114,6 +114,7 @@ class Solver:
     def __init__(self, device: int = 0, stream: int | None = None, use_graph: bool = True,
                  body_capacity: int = 0, contact_capacity: int = 0, joint_capacity: int = 0):
         L = lib()
+        self._m = 0  # manifolds of the world the device holds
         d = abi.SolverDesc()
         d.device = device
         d.stream = stream
