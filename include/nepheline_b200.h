@@ -720,10 +720,10 @@ NPH_GPU_API NphGpuResult nph_gpu_world_sleep_decision(NphGpuSolver *solver, cons
  * fastest approach. The caller makes NphPhysicsContactHitEvent from it: its shapes, the point
  * as body A's centre plus the point's anchor_a (nph_dvec3_add_vec3), the manifold's normal. */
 typedef struct NphGpuHitEvent {
-    uint32_t contact;
+    uint32_t contact;     /* the manifold's index in its view */
     uint32_t point;
     float approach_speed; /* -relative_velocity, above the threshold */
-    uint32_t pad;
+    uint32_t world;       /* the view's place in a batch (0 for a single world) */
 } NphGpuHitEvent;
 
 /* hit_events after a step, on the device-resident records: for each manifold with
@@ -734,6 +734,11 @@ typedef struct NphGpuHitEvent {
  * the first min(*count, capacity) events to the host array `events` and the number of events to
  * `*count`. */
 NPH_GPU_API NphGpuResult nph_gpu_world_hit_events(NphGpuSolver *solver, float threshold, NphGpuHitEvent *events,
+                                                 uint32_t capacity, uint32_t *count);
+/* The same for every world of a batch after its step (nph_gpu_phys_solve_worlds, split or not,
+ * or resident steps): world by world in the batch's order, each world's hits in its view's
+ * order, `world` its place in the batch. */
+NPH_GPU_API NphGpuResult nph_gpu_batch_hit_events(NphGpuBatch *batch, float threshold, NphGpuHitEvent *events,
                                                  uint32_t capacity, uint32_t *count);
 
 NPH_GPU_API NphGpuResult nph_gpu_world_features(NphGpuSolver *solver,

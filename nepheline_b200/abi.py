@@ -398,7 +398,7 @@ def pack_views(views: list, alloc=None) -> list:
 SHAPE_SPHERE, SHAPE_CAPSULE, SHAPE_BOX = 0, 1, 2
 SHAPE_DTYPE = np.dtype([("type", "<u4"), ("dims", "<f4", 3)], align=True)
 HIT_EVENT_DTYPE = np.dtype([("contact", "<u4"), ("point", "<u4"), ("approach_speed", "<f4"),
-                            ("pad", "<u4")])
+                            ("world", "<u4")])
 
 
 def hit_points(view: "View", events: np.ndarray) -> tuple[np.ndarray, np.ndarray]:

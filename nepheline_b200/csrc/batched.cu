@@ -549,6 +549,10 @@ struct NphGpuBatch {
     uint32_t pipeline_parts = 1;
     std::vector<NphGpuBatch *> parts;
     std::vector<cudaEvent_t> part_uploaded;
+    // Where the last results live: the parts (after a split call, part p's worlds starting at
+    // part_first[p]) or the batch itself.
+    bool results_in_parts = false;
+    std::vector<uint32_t> part_first;
 };
 
 namespace {
@@ -1521,6 +1525,8 @@ NphGpuResult solve_in_parts(NphGpuBatch *b, const NphGpuWorldParams *params, flo
             r = e;
         }
     }
+    b->results_in_parts = r == NPH_GPU_OK;
+    b->part_first.assign(first.begin(), first.begin() + parts);
     return r;
 }
 
@@ -1540,6 +1546,7 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_upload(NphGpuBatch *b, const NphGpuWorldV
             return r;
         }
     }
+    b->results_in_parts = false;
     const NphGpuResult r = upload_begin(b, worlds, count);
     return r != NPH_GPU_OK ? r : cuda_result(cudaStreamSynchronize(b->stream));
 }
@@ -1634,6 +1641,54 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_set_config(NphGpuBatch *b, const NphGpuBa
     b->shared_mode = t->shared_velocities;
     b->items_per_thread = t->items_per_thread;
     return apply_order(b);
+}
+
+NPH_GPU_API NphGpuResult nph_gpu_batch_hit_events(NphGpuBatch *b, float threshold, NphGpuHitEvent *events,
+                                                 uint32_t capacity, uint32_t *count)
+{
+    if (b == nullptr || count == nullptr || (capacity > 0u && events == nullptr)) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    *count = 0u;
+    std::vector<std::pair<NphGpuBatch *, uint32_t>> sources; // a batch, its first world
+    if (b->results_in_parts) {
+        for (size_t p = 0; p < b->part_first.size() && p < b->parts.size(); ++p) {
+            sources.emplace_back(b->parts[p], b->part_first[p]);
+        }
+    } else {
+        sources.emplace_back(b, 0u);
+    }
+    uint32_t total = 0u;
+    for (const auto &src : sources) {
+        NphGpuBatch *q = src.first;
+        if (q->world_count == 0u) {
+            continue;
+        }
+        cudaSetDevice(q->device);
+        NphGpuResult r = merged_to_packed(q);
+        if (r != NPH_GPU_OK) {
+            return r;
+        }
+        const uint32_t room = total < capacity ? capacity - total : 0u;
+        uint32_t n = 0u;
+        r = nph_hits_scan(q->d_contacts, (uint32_t)q->contacts, threshold, q->stream,
+                          room > 0u ? events + total : nullptr, room, &n);
+        if (r != NPH_GPU_OK) {
+            return r;
+        }
+        // A packed index into its world: the last world starting at or before it.
+        for (uint32_t i = 0; i < std::min(n, room); ++i) {
+            NphGpuHitEvent &e = events[total + i];
+            const auto it = std::upper_bound(q->worlds.begin(), q->worlds.end(), e.contact,
+                                             [](uint32_t x, const WorldSlice &w) { return x < w.contact_first; });
+            const uint32_t w = (uint32_t)(it - q->worlds.begin()) - 1u;
+            e.contact -= q->worlds[w].contact_first;
+            e.world = src.second + w;
+        }
+        total += n;
+    }
+    *count = total;
+    return NPH_GPU_OK;
 }
 
 NPH_GPU_API NphGpuResult nph_gpu_batch_set_pipeline(NphGpuBatch *b, uint32_t parts)

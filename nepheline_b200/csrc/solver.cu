@@ -733,7 +733,7 @@ __global__ void __launch_bounds__(kHitBlock) k_hit_write(const NphGpuContact *co
         at += warp_hits[w];
     }
     if (hit) {
-        out[at] = NphGpuHitEvent{g, point, speed, 0u};
+        out[at] = NphGpuHitEvent{g, point, speed, 0u}; // world 0: the caller numbers batches' worlds
     }
 }
 
@@ -1456,6 +1456,38 @@ NphGpuResult nph_solver_check(NphGpuSolver *s)
     return read_error(s);
 }
 
+NphGpuResult nph_hits_scan(const NphGpuContact *contacts, uint32_t m, float threshold, cudaStream_t st,
+                           NphGpuHitEvent *events, uint32_t capacity, uint32_t *count)
+{
+    *count = 0u;
+    if (m == 0u) {
+        return NPH_GPU_OK;
+    }
+    const uint32_t blocks = (m + kHitBlock - 1u) / kHitBlock;
+    uint32_t *d_blocks = nullptr;
+    NphGpuHitEvent *d_out = nullptr;
+    NphGpuResult r = dalloc(d_blocks, blocks + 1u) && dalloc(d_out, m) ? NPH_GPU_OK : NPH_GPU_OUT_OF_MEMORY;
+    uint32_t total = 0u;
+    if (r == NPH_GPU_OK) {
+        k_hit_count<<<blocks, kHitBlock, 0, st>>>(contacts, m, threshold, d_blocks);
+        k_hit_scan<<<1, kHitScanThreads, 0, st>>>(d_blocks, blocks);
+        k_hit_write<<<blocks, kHitBlock, 0, st>>>(contacts, m, threshold, d_blocks, d_out);
+        cudaMemcpyAsync(&total, d_blocks + blocks, sizeof total, cudaMemcpyDeviceToHost, st);
+        r = check_cuda(cudaStreamSynchronize(st));
+    }
+    const uint32_t n = std::min(total, capacity);
+    if (r == NPH_GPU_OK && n > 0u) {
+        r = check_cuda(cudaMemcpy(events, d_out, sizeof(NphGpuHitEvent) * n, cudaMemcpyDeviceToHost));
+    }
+    if (r == NPH_GPU_OK) {
+        *count = total;
+    }
+    cudaGetLastError();
+    dfree(d_blocks);
+    dfree(d_out);
+    return r;
+}
+
 // ------------------------------------------------------------------------------------
 // The C ABI
 // ------------------------------------------------------------------------------------
@@ -1962,37 +1994,12 @@ NPH_GPU_API NphGpuResult nph_gpu_world_hit_events(NphGpuSolver *s, float thresho
     if (s == nullptr || count == nullptr || (capacity > 0u && events == nullptr)) {
         return NPH_GPU_INVALID_ARGUMENT;
     }
+    *count = 0u;
     if (!s->uploaded) {
         return NPH_GPU_INVALID_STATE;
     }
-    *count = 0u;
-    if (s->m == 0u) {
-        return NPH_GPU_OK;
-    }
     cudaSetDevice(s->device);
-    const uint32_t blocks = (s->m + kHitBlock - 1u) / kHitBlock;
-    uint32_t *d_blocks = nullptr;
-    NphGpuHitEvent *d_out = nullptr;
-    NphGpuResult r = dalloc(d_blocks, blocks + 1u) && dalloc(d_out, s->m) ? NPH_GPU_OK : NPH_GPU_OUT_OF_MEMORY;
-    uint32_t total = 0u;
-    if (r == NPH_GPU_OK) {
-        k_hit_count<<<blocks, kHitBlock, 0, s->stream>>>(s->d_contacts, s->m, threshold, d_blocks);
-        k_hit_scan<<<1, kHitScanThreads, 0, s->stream>>>(d_blocks, blocks);
-        k_hit_write<<<blocks, kHitBlock, 0, s->stream>>>(s->d_contacts, s->m, threshold, d_blocks, d_out);
-        cudaMemcpyAsync(&total, d_blocks + blocks, sizeof total, cudaMemcpyDeviceToHost, s->stream);
-        r = check_cuda(cudaStreamSynchronize(s->stream));
-    }
-    const uint32_t n = std::min(total, capacity);
-    if (r == NPH_GPU_OK && n > 0u) {
-        r = check_cuda(cudaMemcpy(events, d_out, sizeof(NphGpuHitEvent) * n, cudaMemcpyDeviceToHost));
-    }
-    if (r == NPH_GPU_OK) {
-        *count = total;
-    }
-    cudaGetLastError();
-    dfree(d_blocks);
-    dfree(d_out);
-    return r;
+    return nph_hits_scan(s->d_contacts, s->m, threshold, s->stream, events, capacity, count);
 }
 
 NPH_GPU_API NphGpuResult nph_gpu_world_features(NphGpuSolver *s, const NphGpuWorldParams *params, float dt,

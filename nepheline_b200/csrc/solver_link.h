@@ -4,6 +4,8 @@
 // packed as one world hands its records to a single-world solver on the device.
 #pragma once
 
+#include <cuda_runtime.h>
+
 #include "nepheline_b200.h"
 
 struct NphSolverRecords {
@@ -23,3 +25,8 @@ NphGpuResult nph_solver_bind_device(NphGpuSolver *s, const NphGpuWorldView *shap
 NphGpuResult nph_solver_records(NphGpuSolver *s, NphSolverRecords *out);
 // The prepare kernels' error word as a result code (NPH_GPU_INVALID_ARGUMENT on a bad record).
 NphGpuResult nph_solver_check(NphGpuSolver *s);
+// hit_events over `m` device-resident contact records on stream `st` (nph_gpu_world_hit_events'
+// scan): the first min(total, capacity) events to the host array `events`, in record order, with
+// `contact` the record's index and `world` 0; the total to `*count`.
+NphGpuResult nph_hits_scan(const NphGpuContact *contacts, uint32_t m, float threshold, cudaStream_t st,
+                           NphGpuHitEvent *events, uint32_t capacity, uint32_t *count);

@@ -71,6 +71,7 @@ def lib() -> ctypes.CDLL:
         "nph_gpu_collide": (ctypes.c_int32, [_vp, _vp, _vp, _vp, _vp, _u32, _vp]),
         "nph_gpu_collide_release": (None, []),
         "nph_gpu_world_hit_events": (ctypes.c_int32, [_vp, ctypes.c_float, _vp, _u32, P(_u32)]),
+        "nph_gpu_batch_hit_events": (ctypes.c_int32, [_vp, ctypes.c_float, _vp, _u32, P(_u32)]),
         "nph_gpu_world_sleep_decision": (ctypes.c_int32, [_vp, _vp, _u32, _vp, ctypes.c_float, _vp, _vp,
                                                           _vp]),
         "nph_gpu_collide_async": (ctypes.c_int32, [_vp, _vp, _vp, _vp, _vp, _u32, _vp, _vp, _vp,
@@ -417,6 +418,18 @@ class Batch:
         t.packing = packing
         _check(self.L.nph_gpu_batch_set_config(self._h, ctypes.byref(t)),
                "nph_gpu_batch_set_config")
+
+    def hit_events(self, threshold: float = 1.0) -> np.ndarray:
+        """nph_gpu_batch_hit_events after a step: every world's hits, world by world (`world`
+        its place in the batch, `contact` the manifold's index in its view)."""
+        count = _u32()
+        _check(self.L.nph_gpu_batch_hit_events(self._h, threshold, None, 0, ctypes.byref(count)),
+               "nph_gpu_batch_hit_events")
+        cap = int(count.value)
+        out = np.zeros(max(cap, 1), abi.HIT_EVENT_DTYPE)
+        _check(self.L.nph_gpu_batch_hit_events(self._h, threshold, out.ctypes.data, cap, ctypes.byref(count)),
+               "nph_gpu_batch_hit_events")
+        return out[:min(int(count.value), cap)]
 
     def set_pipeline(self, parts: int) -> None:
         """phys_solve_worlds in `parts` consecutive runs of worlds, each on its own stream, so

@@ -383,3 +383,26 @@ def test_drop_in_in_parts_refuses_before_writing_back(solver):
         solver.phys_solve(want, params, DT)
         assert not helpers.mismatches(w, want)
     batch.close()
+
+
+def test_drop_in_in_parts_follows_the_batch(solver):
+    """The parts take the batch's packing when it changes between calls, and TGS steps as alone."""
+    from nepheline_b200.solver import Batch
+    views = []
+    for edge, seed in ((4, 5), (7, 6), (6, 7), (5, 8), (3, 9)):
+        sc = scenes.lattice_graph(edge, seed=seed, joint_fraction=0.1)
+        views.append(sc.to_view(*scenes.host_color(sc)))
+    batch = Batch(device=0)
+    batch.set_pipeline(3)
+    mine = abi.pack_views([v.copy() for v in views])
+    want = [v.copy() for v in views]
+    for packing, solver_kind in ((abi.BATCH_PERSISTENT, abi.SOLVER_SOFT_STEP), (abi.BATCH_MERGED, abi.SOLVER_TGS),
+                                 (abi.BATCH_PERSISTENT, abi.SOLVER_TGS)):
+        params = abi.WorldParams.default(solver=solver_kind)
+        batch.set_config(packing=packing)
+        batch.phys_solve_worlds(mine, params, DT)
+        for w in want:
+            solver.phys_solve(w, params, DT)
+        for m, w in zip(mine, want):
+            assert not helpers.mismatches(m, w), (packing, solver_kind)
+    batch.close()

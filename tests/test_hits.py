@@ -115,3 +115,41 @@ def test_device_hit_events_edge_cases():
     s.phys_solve(v, abi.WorldParams.default(), DT)
     assert len(s.hit_events(0.0)) == 0
     s.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("parts", [1, 2])
+@pytest.mark.parametrize("packing", [abi.BATCH_PERSISTENT, abi.BATCH_MERGED])
+def test_batch_hit_events_equal_each_world_alone(solver, ref_lib, parts, packing):
+    """A batch of sphere pours (and a world without hits between them), split or not: the
+    batch's hits are each world's own hits, world by world, tagged with the world."""
+    from nepheline_b200.solver import Batch
+    p = abi.WorldParams.default()
+    views = []
+    for seed in (2, 5, 7):
+        w = ref_scenes.sphere_pour(count=125, seed=seed, hit_events=True)
+        for _ in range(20):
+            w.step(DT)
+        w.collide()
+        views.append(w.export_view())
+        w.close()
+    quiet = ref_scenes.sphere_pour(count=27, seed=9)  # no step yet: bodies, no manifolds
+    views.insert(1, quiet.export_view())
+    quiet.close()
+    batch = Batch(device=0)
+    batch.set_config(packing=packing)
+    batch.set_pipeline(parts)
+    mine = abi.pack_views([v.copy() for v in views])
+    batch.phys_solve_worlds(mine, p, DT)
+    got = batch.hit_events(0.25)
+    want = []
+    for i, v in enumerate(views):
+        alone = v.copy()
+        solver.phys_solve(alone, p, DT)
+        e = solver.hit_events(0.25)
+        e["world"] = i
+        want.append(e)
+    want = np.concatenate(want)
+    assert len(want) > 5
+    assert got.tobytes() == want.tobytes()
+    batch.close()
