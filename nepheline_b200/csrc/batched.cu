@@ -1388,7 +1388,7 @@ NphGpuResult check_records(const NphGpuWorldView *worlds, uint32_t count)
     auto scan = [&](uint32_t first, uint32_t end) {
         for (uint32_t w = first; w < end && bad.load(std::memory_order_relaxed) == 0u; ++w) {
             const NphGpuWorldView &v = worlds[w];
-            const uint32_t total = v.body_count + v.fixed_count;
+            const uint64_t total = (uint64_t)v.body_count + v.fixed_count;
             uint32_t worst = 0u;
             for (uint32_t i = 0; i < v.contact_count; ++i) {
                 const NphGpuContact &c = v.contacts[i];
@@ -1406,8 +1406,13 @@ NphGpuResult check_records(const NphGpuWorldView *worlds, uint32_t count)
     const uint32_t threads = std::max(1u, std::min({8u, std::thread::hardware_concurrency(), count / 64u}));
     std::vector<std::thread> pool;
     for (uint32_t t = 1; t < threads; ++t) {
-        pool.emplace_back(scan, (uint32_t)((uint64_t)count * t / threads),
-                          (uint32_t)((uint64_t)count * (t + 1) / threads));
+        const uint32_t first = (uint32_t)((uint64_t)count * t / threads);
+        const uint32_t end = (uint32_t)((uint64_t)count * (t + 1) / threads);
+        try {
+            pool.emplace_back(scan, first, end);
+        } catch (...) { // no thread to be had: this one scans the run
+            scan(first, end);
+        }
     }
     scan(0u, (uint32_t)((uint64_t)count / threads));
     for (std::thread &t : pool) {

@@ -223,7 +223,11 @@ NPH_GPU_API NphGpuResult nph_gpu_collide(const NphGpuShape *a, const NphGpuPose 
         }
     }
     if (g_pipes->size() <= (size_t)device) {
-        g_pipes->resize((size_t)device + 1u);
+        try {
+            g_pipes->resize((size_t)device + 1u);
+        } catch (...) {
+            return NPH_GPU_OUT_OF_MEMORY;
+        }
     }
     Pipe &pipe = (*g_pipes)[(size_t)device];
     const uint32_t chunk = std::min(count, std::max(kChunkMin, (count + kChunksWanted - 1u) / kChunksWanted));
