@@ -57,13 +57,47 @@ __device__ __forceinline__ uint32_t pair_kind(const NphGpuShape &a, const NphGpu
     return a.type <= NPH_GPU_SHAPE_BOX && b.type <= NPH_GPU_SHAPE_BOX ? a.type * 3u + b.type : kKinds - 1u;
 }
 
-__global__ void __launch_bounds__(256) k_classify(const NphGpuShape *a, const NphGpuShape *b, uint32_t count,
-                                                  uint32_t *counts, uint32_t *place)
+// Box pairs apart along a face axis by more than the slop take the GJK path (or none), the rest
+// the face clip: an estimate from the six face axes gives the apart ones a kind of their own
+// (kind 9), so that a warp runs one of the two paths. Only the order of the pairs depends on it.
+constexpr uint32_t kKindBoxesApart = 9u;
+
+__device__ __forceinline__ bool boxes_apart(const NphGpuShape &a, const NphGpuPose &pa, const NphGpuShape &b,
+                                            const NphGpuPose &pb)
+{
+    using namespace nph_nc;
+    const Q qa{pa.rotation[0], pa.rotation[1], pa.rotation[2], pa.rotation[3]};
+    const Q qb{pb.rotation[0], pb.rotation[1], pb.rotation[2], pb.rotation[3]};
+    const V t = rotate_inverse(qa, V{pb.position[0] - pa.position[0], pb.position[1] - pa.position[1],
+                                     pb.position[2] - pa.position[2]});
+    const Q rq = q_mul(Q{-qa.x, -qa.y, -qa.z, qa.w}, qb);
+    const V c[3] = {axis_x(rq), axis_y(rq), axis_z(rq)}; // B's axes in A's frame
+    float worst = -3.4e38f;
+#pragma unroll
+    for (uint32_t i = 0; i < 3u; ++i) {
+        const float ra = a.dims[i];
+        const float rb = b.dims[0] * fabsf(at(c[0], i)) + b.dims[1] * fabsf(at(c[1], i)) + b.dims[2] * fabsf(at(c[2], i));
+        worst = fmaxf(worst, fabsf(at(t, i)) - (ra + rb));
+    }
+#pragma unroll
+    for (uint32_t j = 0; j < 3u; ++j) {
+        const float ra = a.dims[0] * fabsf(c[j].x) + a.dims[1] * fabsf(c[j].y) + a.dims[2] * fabsf(c[j].z);
+        worst = fmaxf(worst, fabsf(dot(t, c[j])) - (ra + b.dims[j]));
+    }
+    return worst > 0.005f;
+}
+
+__global__ void __launch_bounds__(256) k_classify(const NphGpuShape *a, const NphGpuPose *pa, const NphGpuShape *b,
+                                                  const NphGpuPose *pb, uint32_t count, uint32_t *counts,
+                                                  uint32_t *place)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < count) {
         // One atomic per kind and warp: the lanes of a kind take consecutive places.
-        const uint32_t k = pair_kind(a[i], b[i]);
+        uint32_t k = pair_kind(a[i], b[i]);
+        if (k == NPH_GPU_SHAPE_BOX * 4u && boxes_apart(a[i], pa[i], b[i], pb[i])) {
+            k = kKindBoxesApart;
+        }
         const uint32_t lane = threadIdx.x & 31u;
         const uint32_t group = __match_any_sync(__activemask(), k);
         const uint32_t leader = __ffs(group) - 1u;
@@ -332,7 +366,7 @@ NPH_GPU_API NphGpuResult nph_gpu_collide_async(const NphGpuShape *a, const NphGp
         uint32_t *place = counts + 2u * kKinds;
         uint32_t *order = place + count;
         cudaMemsetAsync(counts, 0, kKinds * sizeof(uint32_t), st);
-        k_classify<<<blocks, 256, 0, st>>>(a, b, count, counts, place);
+        k_classify<<<blocks, 256, 0, st>>>(a, pose_a, b, pose_b, count, counts, place);
         k_kind_offsets<<<1, 32, 0, st>>>(counts);
         k_scatter<<<blocks, 256, 0, st>>>(counts, place, count, order);
         k_collide_sorted<<<blocks, 256, 0, st>>>(a, pose_a, b, pose_b, speculative, count, order, out, bad_pairs);
