@@ -523,7 +523,12 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_info(const NphGpuBatch *batch, NphGpuBatc
  * bit 2 that the constraint is a joint (joints and contacts share the colours' body sets,
  * but each colour keeps a contact list and a joint list: island.c:77-88, 106-118). Writes
  * each constraint's colour and its slot in its colour's list of its kind (the list order
- * is the insertion order). The result equals the sequential first-fit bit for bit. */
+ * is the insertion order). The result equals the sequential first-fit bit for bit.
+ * Cost: one launch per round of the parallel fixpoint, as many rounds as the longest chain of
+ * constraints each sharing a dynamic body with an earlier one (about 320 for the 1,048,576-body
+ * lattice); a longer chain (a rope or stack inserted in order) is finished after
+ * max(512, count / 512) rounds by the sequential rule on one warp, about 60 ns a constraint.
+ * Counts at or above 2^30 and body_slots at or above 2^31 - 1 return NPH_GPU_TOO_LARGE. */
 NPH_GPU_API NphGpuResult nph_gpu_graph_color(NphGpuSolver *solver, const uint32_t *body_a,
                                              const uint32_t *body_b, const uint8_t *dynamic_bits,
                                              uint32_t count, uint32_t body_slots,
@@ -537,10 +542,13 @@ NPH_GPU_API NphGpuResult nph_gpu_graph_color(NphGpuSolver *solver, const uint32_
  * arrays, as in nph_gpu_graph_color. At most NPH_GPU_GRAPH_COLOR_STATIC_MAX_CONSTRAINTS
  * constraints over NPH_GPU_GRAPH_COLOR_STATIC_MAX_BODY_SLOTS body slots: larger inputs
  * return NPH_GPU_TOO_LARGE. Runs on the current device, on `stream` (a cudaStream_t, NULL for
- * the default stream). The first call on a device looks the array's address up and should
- * come before any stream capture. All calls share the one array: calls that overlap on the
- * GPU (other threads, other streams of the device) race and must be serialised by the
- * caller. The result equals nph_gpu_graph_color's. */
+ * the default stream). Each call looks the array's address up in the current context (so a
+ * context reset or a context the caller makes current is followed); the first call in a
+ * context also loads the library's device code and should come before any stream capture.
+ * All calls share the one array and it keeps the last call's contents (what must start at
+ * zero is cleared by each call): calls that overlap on the GPU (other threads, other streams
+ * of the device) race and must be serialised by the caller. The result equals
+ * nph_gpu_graph_color's. */
 #define NPH_GPU_GRAPH_COLOR_STATIC_MAX_CONSTRAINTS 131072u
 #define NPH_GPU_GRAPH_COLOR_STATIC_MAX_BODY_SLOTS 131072u
 #define NPH_GPU_GRAPH_COLOR_STATIC_SCRATCH_BYTES (8u << 20)

@@ -20,13 +20,14 @@ COLOR_SLOTS = 25
 OK = 0
 OUT_OF_MEMORY = 1
 INVALID_ARGUMENT = 2
+TOO_LARGE = 7
 UNSUPPORTED = 8
 DEVICE_LOST = 17
 INVALID_STATE = 18
 UNKNOWN = 19
 RESULT_NAMES = {
     OK: "OK", OUT_OF_MEMORY: "OUT_OF_MEMORY", INVALID_ARGUMENT: "INVALID_ARGUMENT",
-    UNSUPPORTED: "UNSUPPORTED", DEVICE_LOST: "DEVICE_LOST", INVALID_STATE: "INVALID_STATE",
+    TOO_LARGE: "TOO_LARGE", UNSUPPORTED: "UNSUPPORTED", DEVICE_LOST: "DEVICE_LOST", INVALID_STATE: "INVALID_STATE",
     UNKNOWN: "UNKNOWN",
 }
 

@@ -1875,6 +1875,12 @@ NPH_GPU_API void *nph_gpu_solver_stream(const NphGpuSolver *s)
     return s != nullptr ? (void *)s->stream : nullptr;
 }
 
+} // extern "C"
+
+int nph_solver_device(const NphGpuSolver *s) { return s != nullptr ? s->device : 0; }
+
+extern "C" {
+
 NPH_GPU_API NphGpuResult nph_gpu_world_update_contacts(NphGpuSolver *s, const NphGpuContact *fresh,
                                                        uint32_t count)
 {

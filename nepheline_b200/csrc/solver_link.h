@@ -30,3 +30,5 @@ NphGpuResult nph_solver_check(NphGpuSolver *s);
 // `contact` the record's index and `world` 0; the total to `*count`.
 NphGpuResult nph_hits_scan(const NphGpuContact *contacts, uint32_t m, float threshold, cudaStream_t st,
                            NphGpuHitEvent *events, uint32_t capacity, uint32_t *count);
+// The CUDA device a solver was created on.
+int nph_solver_device(const NphGpuSolver *s);

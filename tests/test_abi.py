@@ -95,3 +95,18 @@ def test_views_array_equals_the_records_one_at_a_time():
     packed[7].contact_color_counts[0] += 1
     assert abi.views_array(packed).tobytes() == one_at_a_time(packed)
     assert len(abi.views_array([])) == 1
+
+
+def test_colouring_refuses_counts_beyond_the_sort_without_touching_arrays():
+    """Counts the device sort cannot index (it counts items in int) are refused before the
+    solver, the arrays or the device are touched: no device is needed."""
+    import ctypes
+
+    from nepheline_b200 import solver
+    if not solver.LIB_PATH.exists():
+        pytest.skip("library not built")
+    fn = solver.lib().nph_gpu_graph_color
+    dummy = ctypes.create_string_buffer(64)
+    p = ctypes.addressof(dummy)
+    assert fn(p, p, p, p, 0x7FFFFFFF, 16, p, p) == abi.TOO_LARGE
+    assert fn(p, p, p, p, 16, 0x7FFFFFFF, p, p) == abi.TOO_LARGE

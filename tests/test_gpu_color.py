@@ -56,3 +56,37 @@ def test_colouring_refuses_bad_slots(solver):
     with pytest.raises(SolverError):
         solver.graph_color(np.array([0, 5], np.uint32), np.array([1, 2], np.uint32),
                            np.array([3, 3], np.uint8), 4)
+
+
+def rope(links: int, seed: int):
+    """A chain inserted in order: constraint i joins bodies i and i + 1, so each constraint's
+    colour waits on the one before it (the longest chain of lower-index neighbours is the whole
+    rope). Every seventh link is a joint, every eleventh body static."""
+    rng = np.random.default_rng(seed)
+    slots = links + 1
+    dynamic = np.ones(slots, bool)
+    dynamic[::11] = False
+    a = np.arange(links, dtype=np.uint32)
+    b = a + 1
+    keep = dynamic[a] | dynamic[b]
+    a, b = a[keep], b[keep]
+    d = dynamic[a].astype(np.uint8) | (dynamic[b].astype(np.uint8) << 1)
+    d[::7] |= abi.CONSTRAINT_JOINT
+    order = np.arange(len(a))
+    rng.shuffle(order[len(a) // 2:])  # the second half out of order: shorter chains there
+    return a[order], b[order], d[order], slots
+
+
+@pytest.mark.parametrize("links", [600, 100_000])
+def test_long_chain_colouring_matches_port(solver, links):
+    """A rope longer than the rounds' cap goes to the sequential first-fit on one warp; a
+    shorter one converges in rounds. Both equal the sequential rule."""
+    import time
+    from oracle.refworld import port_graph_color
+    a, b, d, slots = rope(links, seed=links)
+    t = time.perf_counter()
+    color, slot = solver.graph_color(a, b, d, slots)
+    ms = 1e3 * (time.perf_counter() - t)
+    pc, ps = port_graph_color(a, b, d, slots)
+    assert np.array_equal(color, pc) and np.array_equal(slot, ps)
+    print(f"rope of {links} links coloured in {ms:.1f} ms")

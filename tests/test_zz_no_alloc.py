@@ -81,6 +81,24 @@ def test_static_colouring_equals_allocating_colouring_two_calls_in_a_row(allocat
         assert np.array_equal(slot, want_slot)
 
 
+def test_static_colouring_takes_no_device_memory_after_its_first_call():
+    """Once the library is loaded on the device (its first call), further calls leave the
+    device's free memory where it was: nothing is allocated, by the entry point or a library
+    it calls."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    args = (*random_graph(12, 5000, 60000), 5000)
+    assert color_static(*args)[0] == abi.OK
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info(0)
+    for _ in range(3):
+        assert color_static(*args)[0] == abi.OK
+    torch.cuda.synchronize()
+    free_after, _ = torch.cuda.mem_get_info(0)
+    assert free_after == free_before
+
+
 def test_static_colouring_at_its_capacity(allocating):
     a, b, d = random_graph(3, MAX_BODY_SLOTS, MAX_CONSTRAINTS + 4000)
     a, b, d = a[:MAX_CONSTRAINTS], b[:MAX_CONSTRAINTS], d[:MAX_CONSTRAINTS]
