@@ -8,12 +8,12 @@
 // (207-230) last where the type has one. The reference keeps joints scalar, so every formula
 // here is its scalar formula in its order. Joints of a colour share no dynamic body with each
 // other or with the colour's contacts, so a colour's joints run in parallel. Every angle (a
-// hinge limit or spring, a ball cone or twist limit, a 6-DOF twist or swing) is the correctly
-// rounded FP32 arctangent (the double-precision atan2 rounded once to FP32): the reference's
-// is the host C library's atan2f, which is not correctly rounded, so those rows match the
-// reference within floating-point tolerance, the others bit for bit.
+// hinge limit or spring, a ball cone or twist limit, a 6-DOF twist or swing) goes through
+// nph_atan2f (atan2f.h), the reference's C library arctangent restated in FP32 operations, so
+// the angle rows round to the reference's bits like every other row.
 #pragma once
 
+#include "atan2f.h"
 #include "joint_config.h"
 #include "layout.cuh"
 
@@ -56,9 +56,6 @@ NPH_D float axial_mass(const JointBodies &jb, V3 axis)
     return k > 0.0f ? 1.0f / k : 0.0f;
 }
 
-// atan2(y, x) rounded once to FP32 from the double-precision value.
-NPH_D float atan2_rn(float y, float x) { return (float)atan2((double)y, (double)x); }
-
 // joint_solver.c:77-84.
 NPH_D float twist_angle(Q4 qa, Q4 qb)
 {
@@ -66,7 +63,7 @@ NPH_D float twist_angle(Q4 qa, Q4 qb)
     if (r.w < 0.0f) {
         r = Q4{-r.x, -r.y, -r.z, -r.w};
     }
-    return 2.0f * atan2_rn(r.x, r.w);
+    return 2.0f * nph_atan2f(r.x, r.w);
 }
 
 // joint_solver.c:86-96.
@@ -640,12 +637,12 @@ NPH_D AxesNow axes_of(Q4 qa, Q4 qb, V3 d)
     if (r.w < 0.0f) {
         r = Q4{-r.x, -r.y, -r.z, -r.w};
     }
-    n.value[3] = 2.0f * atan2_rn(r.x, r.w);
+    n.value[3] = 2.0f * nph_atan2f(r.x, r.w);
     const float tl = sqrtf(r.x * r.x + r.w * r.w);
     const Q4 twist = tl > 1e-9f ? Q4{r.x / tl, 0.0f, 0.0f, r.w / tl} : q_identity();
     const Q4 swing = q_mul(r, q_conj(twist));
-    n.value[4] = 2.0f * atan2_rn(swing.y, swing.w);
-    n.value[5] = 2.0f * atan2_rn(swing.z, swing.w);
+    n.value[4] = 2.0f * nph_atan2f(swing.y, swing.w);
+    n.value[5] = 2.0f * nph_atan2f(swing.z, swing.w);
     n.axis[3] = normalize_or(add(n.axis[0], axis_x(qb)), n.axis[0]);
     n.axis[4] = n.axis[1];
     n.axis[5] = n.axis[2];
@@ -904,7 +901,7 @@ NPH_D void solve_joint(const DevSolver &S, uint32_t j, const StepConsts &K)
                 const float ey = local.y / set_a.x;
                 const float ez = local.z / set_a.y;
                 const float limit = 1.0f / sqrtf(ey * ey + ez * ez);
-                const float phi = atan2_rn(sin_phi, dot(xa, xb));
+                const float phi = nph_atan2f(sin_phi, dot(xa, xb));
                 solve_angular_limit(jb, axis, limit - phi, fric.w, K, kUseBias);
             }
         }

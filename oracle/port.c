@@ -60,22 +60,6 @@ static int port_all_locked(const NphGpuD6Axis *ax, unsigned first, unsigned coun
 #undef ATAN2
 #undef ABS
 
-// FP32 with the correctly rounded arctangent (the double-precision atan2 rounded once to FP32),
-// the device solver's angle: the device must equal this instance bit for bit, and this
-// instance differs from the reference only through the host C library's atan2f rounding.
-static float atan2_cr(float y, float x) { return (float)atan2((double)y, (double)x); }
-#define REAL float
-#define SUF _f32cr
-#define SQRT sqrtf
-#define ATAN2 atan2_cr
-#define ABS fabsf
-#include "port_impl.h"
-#undef REAL
-#undef SUF
-#undef SQRT
-#undef ATAN2
-#undef ABS
-
 #define REAL double
 #define SUF _f64
 #define SQRT sqrt
@@ -178,8 +162,7 @@ PORT_API int nph_port32_solve(const NphGpuWorldParams *wp, float dt, NphGpuWorld
     return NPH_GPU_OK;
 }
 
-// The residual-driven mode (nph_gpu_world_converge) in FP32 with the correctly rounded
-// arctangent, the residual in double: residuals[0..passes], 1 + max_passes doubles.
+// The residual-driven mode (nph_gpu_world_converge) in FP32, the residual in double: residuals[0..passes], 1 + max_passes doubles.
 PORT_API int nph_port32_converge(const NphGpuWorldParams *wp, float dt, const NphGpuWorldView *v,
                                  const float *init, double tol, unsigned max_passes, double ref,
                                  double *residuals, unsigned *passes, unsigned *cold, float *impulses)
@@ -191,7 +174,7 @@ PORT_API int nph_port32_converge(const NphGpuWorldParams *wp, float dt, const Np
     if (wp->solver != NPH_GPU_SOLVER_SOFT_STEP) {
         return NPH_GPU_UNSUPPORTED; // the residual-driven mode is the soft step's
     }
-    return converge_f32cr(wp, dt, v, init, tol, max_passes, ref, residuals, passes, cold, impulses);
+    return converge_f32(wp, dt, v, init, tol, max_passes, ref, residuals, passes, cold, impulses);
 }
 
 // The contact update's warm start for pairs of convex shapes (contact.c:332-380, 516-565),
@@ -267,25 +250,6 @@ PORT_API int nph_port_warm_update(const NphGpuContact *old, const NphGpuContact 
         }
         out[g] = c;
     }
-    return NPH_GPU_OK;
-}
-
-// The same with the correctly rounded arctangent in the joints' angle rows.
-PORT_API int nph_port32cr_solve(const NphGpuWorldParams *wp, float dt, NphGpuWorldView *v)
-{
-    const int bad = check_view(wp, v);
-    if (bad != NPH_GPU_OK) {
-        return bad;
-    }
-    Result_f32cr rc;
-    const int res = run_f32cr(wp, dt, v, &rc);
-    if (res != NPH_GPU_OK) {
-        return res;
-    }
-    // The two FP32 instances have the same layout: only their angle function differs.
-    Result_f32 r;
-    memcpy(&r, &rc, sizeof r);
-    write_back_f32(&r, dt, v);
     return NPH_GPU_OK;
 }
 

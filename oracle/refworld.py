@@ -92,9 +92,6 @@ def _port_lib():
         lib.nph_port32_solve.restype = ctypes.c_int
         lib.nph_port32_solve.argtypes = [ctypes.POINTER(abi.WorldParams), _f32,
                                          ctypes.POINTER(abi.WorldView)]
-        lib.nph_port32cr_solve.restype = ctypes.c_int
-        lib.nph_port32cr_solve.argtypes = [ctypes.POINTER(abi.WorldParams), _f32,
-                                           ctypes.POINTER(abi.WorldView)]
         lib.nph_port64_solve.restype = ctypes.c_int
         lib.nph_port64_solve.argtypes = [ctypes.POINTER(abi.WorldParams), _f32,
                                          ctypes.POINTER(abi.WorldView), _vp]
@@ -335,17 +332,6 @@ def port32(view: abi.View, params: abi.WorldParams, dt: float) -> abi.View:
     r = _port_lib().nph_port32_solve(ctypes.byref(params), dt, ctypes.byref(cv))
     if r != 0:
         raise RuntimeError(f"port32 failed: {abi.RESULT_NAMES.get(r, r)}")
-    return out
-
-
-def port32cr(view: abi.View, params: abi.WorldParams, dt: float) -> abi.View:
-    """FP32 solve of a copy of `view` with the correctly rounded arctangent in the joints'
-    angle rows (the device solver's): otherwise the reference's arithmetic."""
-    out = view.copy()
-    cv = out.c_view()
-    r = _port_lib().nph_port32cr_solve(ctypes.byref(params), dt, ctypes.byref(cv))
-    if r != 0:
-        raise RuntimeError(f"port32cr failed: {abi.RESULT_NAMES.get(r, r)}")
     return out
 
 

@@ -4,11 +4,8 @@ Every scene is cut at the solver stage: the reference's world exports the solver
 view; the device solves a copy through nph_gpu_phys_solve; the reference's own phys_solve
 (or the CPU restatement pinned to it) solves the same input. Outputs must agree value for
 value (IEEE equality, so +0 and -0 are equal). The joint rows whose angle goes through an
-arctangent (hinge limits and springs, ball cones and twists) use the correctly rounded angle
-on the device; the reference's glibc 2.39 atan2f is not correctly rounded (it differs from
-the correctly rounded value in about a fifth of random inputs), so those scenes are compared
-exactly against the CPU restatement with the correctly rounded angle, and against the
-reference within what the one-ulp angles make of the limit rows.
+arctangent (hinge limits and springs, ball cones and twists) take it from nph_atan2f, the
+reference's C library atan2f restated in FP32 operations, so they are compared exactly too.
 """
 from __future__ import annotations
 
@@ -22,10 +19,6 @@ pytestmark = pytest.mark.gpu
 
 DT = 1.0 / 60.0
 ANGLE_TOL = 1e-5
-# The reference's atan2f rounding against the correctly rounded one, as the limit rows of the
-# jointed-chain scene amplify it (measured with the CPU restatement: 4.8e-4 of the field's
-# scale at worst over 120 steps).
-ANGLE_ROUNDING_TOL = 1e-3
 
 
 def gpu_solve(solver, view, params, dt=DT):
@@ -93,28 +86,14 @@ def test_lattice_with_joints_matches_reference(solver, ref_lib):
         assert not bad, f"step {s}: {bad}"
 
 
-def test_jointed_chain_matches_restatement_with_rounded_angles(solver, ref_lib):
-    """Hinge limits, motors and springs, ball cones, twists and friction. The device's angle is
-    the correctly rounded arctangent; against the CPU restatement that uses the same, every
-    value agrees. Against the reference, whose atan2f (glibc 2.39) is not correctly rounded,
-    the difference is what one-ulp angles make of the limit rows, and it equals the
-    restatement's own difference from the reference exactly."""
-    from oracle.refworld import port32cr
+def test_jointed_chain_matches_reference_every_step(solver, ref_lib):
+    """Hinge limits, motors and springs, ball cones, twists and friction: every step the device
+    solves the reference's own input and every value equals the reference's output, angle rows
+    included (the arctangent is the reference's, restated)."""
     params = abi.WorldParams.default()
     w = ref_scenes.hinge_chain(links=12)
-    worst = 0.0
-    for s in range(120):
-        w.collide()
-        vin = w.export_view()
-        dev = gpu_solve(solver, vin, params)
-        cr = port32cr(vin, params, DT)
-        assert not helpers.mismatches(dev, cr), f"step {s}"
-        w.solve(DT)
-        w.finish()
-        if s % 3 == 0:
-            err = helpers.max_normwise_err(dev, w.export_view())
-            worst = max(worst, max(err.values()))
-    assert worst < ANGLE_ROUNDING_TOL, worst
+    cut_and_compare(solver, w, 120, params)
+    w.close()
 
 
 def test_other_settings_match_reference(solver, ref_lib):
@@ -258,7 +237,7 @@ def test_every_pass_configuration_gives_the_same_bits(ref_lib):
     kernels) for every pass kind: the same bits as the restatement, on a jointed lattice large
     enough for the pipelined passes' blocks to walk several chunks, and on a batch world."""
     from nepheline_b200.solver import Solver
-    from oracle.refworld import port32cr
+    from oracle.refworld import port32
     params = abi.WorldParams.default()
     views = []
     sc = scenes.lattice_graph((80, 80, 24), seed=3, joint_fraction=0.1)
@@ -267,7 +246,7 @@ def test_every_pass_configuration_gives_the_same_bits(ref_lib):
     sc = scenes.mixed_world(800, 5)
     c, s_ = scenes.host_color(sc)
     views.append(sc.to_view(c, s_))
-    want = [port32cr(v, params, DT) for v in views]
+    want = [port32(v, params, DT) for v in views]
     solver = Solver(device=0)
     for config in range(solver.pass_config_count()):
         for kind in range(4):
@@ -305,20 +284,14 @@ def test_sphere_pour_configuration_65536_spheres(solver, ref_lib):
 
 def test_every_body_feature_matches(solver, ref_lib):
     """Kinematic bodies, locks, damping, gravity scale, forces and torques, unequal inertias
-    (the gyroscopic step) and both speed caps: the device equals the restatement with the
-    correctly rounded angle value for value, and the reference on bodies and contacts (its
-    joint rows differ only by its atan2f rounding)."""
-    from oracle.refworld import port32cr
+    (the gyroscopic step) and both speed caps, with joints: the device equals the reference
+    value for value every step."""
     params = abi.WorldParams.default()
     w = ref_scenes.featured_lattice(edge=9, seed=11)
     for s in range(12):
         vin = w.export_view()
         dev = gpu_solve(solver, vin, params)
-        assert not helpers.mismatches(dev, port32cr(vin, params, DT)), f"step {s}"
         w.solve(DT)
-        ref = w.export_view()
-        bad = {k: v for k, v in helpers.mismatches(dev, ref).items() if not k.startswith("joint.")}
+        bad = helpers.mismatches(dev, w.export_view())
         assert not bad, f"step {s}: {bad}"
-        err = helpers.max_normwise_err(dev, ref)
-        assert max(err.values()) < ANGLE_ROUNDING_TOL, f"step {s}: {err}"
     w.close()

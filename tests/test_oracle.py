@@ -223,19 +223,16 @@ def test_port_warm_update_matches_the_reference_contact_update(ref_lib):
 
 def test_port_matches_reference_with_every_body_feature(ref_lib):
     """Kinematic bodies, locks, damping, gravity scale, forces and torques, the gyroscopic step
-    and both speed caps."""
-    from oracle.refworld import port32cr
+    and both speed caps, with joints: value for value every step."""
+    from oracle.refworld import port32
     params = abi.WorldParams.default()
     w = ref_scenes.featured_lattice(edge=7, seed=7)
     v0 = w.export_view()
     assert (v0.bodies["type"] == abi.BODY_KINEMATIC).any() and v0.bodies["locks"].any()
     for s in range(12):
         vin = w.export_view()
-        mine = port32cr(vin, params, DT)
+        mine = port32(vin, params, DT)
         w.solve(DT)
-        err = helpers.max_normwise_err(mine, w.export_view())
-        assert max(err.values()) < 1e-3, f"step {s}: {err}"
-        bad = {k: v for k, v in helpers.mismatches(mine, w.export_view()).items()
-               if not k.startswith("joint.")}
+        bad = helpers.mismatches(mine, w.export_view())
         assert not bad, f"step {s}: {bad}"
     w.close()
