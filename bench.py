@@ -227,6 +227,103 @@ def reference_sample(dims, steps: int, warmup: int, workers: int, params) -> dic
             "manifolds": manifolds, "bodies": len(sc.bodies), "dims": tuple(dims)}
 
 
+# The solve pass's DRAM bytes per launch on the 128 x 128 x 64 lattice: an ncu capture of the
+# same kernel (dram__bytes_read.sum + dram__bytes_write.sum) on the 96 x 96 x 64 lattice, scaled
+# to this workload's launches by their manifolds (profiles/solve_traffic_lattice.md).
+SOLVE_TRAFFIC_PER_LAUNCH = 149_700_000
+SOLVE_TRAFFIC_SOURCE = ("ncu capture of the solve pass on the 96x96x64 lattice scaled by "
+                        "manifolds to this workload's launches; a constant, not measured in "
+                        "this run")
+
+def _out_fields(view) -> dict:
+    """The outputs phys_solve writes, per field (contact points within each manifold's count)."""
+    import numpy as np
+    out = {}
+    for f in ("center", "rotation", "linear_velocity", "angular_velocity", "sleep_time"):
+        out["body." + f] = view.bodies[f]
+    mask = np.arange(4)[None, :] < view.contacts["point_count"][:, None]
+    for f in ("normal_impulse", "max_normal_impulse", "tangent_impulse", "relative_velocity"):
+        out["point." + f] = view.contacts["points"][f][mask]
+    for f in ("linear_impulse", "angular_impulse", "friction_impulse", "lower_impulse",
+              "upper_impulse", "swing_impulse", "motor_impulse", "spring_impulse"):
+        out["joint." + f] = view.joints[f]
+    return out
+
+
+def reference_leg(dims, view, solver, params, steps: int) -> dict:
+    """Outside every timed region, on the bench's own workload: the lattice built in the
+    reference (bodies created, joints made, manifolds injected in insertion order and coloured
+    by its phys_graph_add); its exported input must equal the bench's (the device's colouring
+    against the reference's, record for record). Then one step of the reference's phys_solve
+    against one drop-in step of the device on that input, value for value; the FP64
+    restatement of the same step as the error baseline of both FP32 results; and the
+    reference's phys_solve timed on its job system over `steps` more steps (the CPU baseline)."""
+    import numpy as np
+
+    from oracle import refworld
+    w, _ = refworld.lattice_world(dims, seed=0, joint_fraction=0.1, params=params, workers=-1)
+    vin = w.export_view()
+    same_input = (vin.bodies.tobytes() == view.bodies.tobytes()
+                  and vin.contacts.tobytes() == view.contacts.tobytes()
+                  and vin.joints.tobytes() == view.joints.tobytes()
+                  and np.array_equal(vin.contact_color_counts, view.contact_color_counts)
+                  and np.array_equal(vin.joint_color_counts, view.joint_color_counts))
+    dev = vin.copy()
+    solver.phys_solve(dev, params, DT)
+    w.solve(DT)
+    ref = w.export_view()
+    fd, fr = _out_fields(dev), _out_fields(ref)
+    compared = mismatched = 0
+    max_abs = max_rel = 0.0
+    for k in fr:
+        a = np.asarray(fd[k], np.float64)
+        b = np.asarray(fr[k], np.float64)
+        if a.size == 0:
+            continue
+        compared += a.size
+        mismatched += int(np.count_nonzero(a != b))
+        d = np.abs(a - b)
+        max_abs = max(max_abs, float(d.max()))
+        max_rel = max(max_rel, float((d / np.maximum(np.abs(b), 1e-30)).max()))
+    # The FP64 restatement of the same step: each FP32 result's error per field, as the largest
+    # difference over the field's largest FP64 magnitude.
+    f64 = refworld.port64(vin, params, DT)
+    mask = np.arange(4)[None, :] < vin.contacts["point_count"][:, None]
+    pairs = {
+        "body.linear_velocity": ("linear_velocity", None), "body.angular_velocity":
+        ("angular_velocity", None), "body.rotation": ("rotation", None), "body.center":
+        ("center", None), "point.normal_impulse": ("normal_impulse", mask),
+        "point.tangent_impulse": ("tangent_impulse", mask), "point.relative_velocity":
+        ("relative_velocity", mask), "joint.linear_impulse": ("joint_linear_impulse", None),
+        "joint.angular_impulse": ("joint_angular_impulse", None)}
+    fp64 = {}
+    for k, (name, m) in pairs.items():
+        ref64 = f64[name][m] if m is not None else f64[name]
+        scale = float(np.abs(ref64).max()) if ref64.size else 0.0
+        if scale == 0.0:
+            continue
+        fp64[k] = {"device": float(np.abs(np.asarray(fd[k], np.float64) - ref64).max()) / scale,
+                   "reference": float(np.abs(np.asarray(fr[k], np.float64) - ref64).max()) / scale}
+    # The CPU baseline: more steps of the same world on the reference's job system.
+    w.solve(DT)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        w.solve(DT)
+    sec = (time.perf_counter() - t0) / max(steps, 1)
+    threads = w.workers + 1 if w.workers > 0 else 1
+    w.close()
+    return {
+        "parity": {"against": "the reference's phys_solve, one step, on the same lattice built and "
+                              "coloured by the reference", "input_equal": bool(same_input),
+                   "values_compared": compared, "values_differing": mismatched,
+                   "max_abs_diff": max_abs, "max_rel_diff": max_rel},
+        "fp64_error": {"measure": "max |f32 - f64| / max |f64| per field, one step, FP64 "
+                                  "restatement of the same step", "fields": fp64},
+        "cpu": {"value": passes_per_step(params) * len(vin.contacts) / sec, "ms_per_step": 1e3 * sec,
+                "threads": threads, "steps": steps},
+    }
+
+
 def cpu_model() -> str:
     try:
         for line in Path("/proc/cpuinfo").read_text().splitlines():
@@ -737,14 +834,13 @@ def main():
     per_launch_ms = top[1]["total_ms"] / top[1]["launches"]
     per_launch_bytes = top[1]["bytes"] / top[1]["launches"]
     achieved = per_launch_bytes / (per_launch_ms * 1e-3) / 1e9
-    traffic = None
-    tf = ROOT / "profiles" / "solve_traffic_lattice.md"
-    if top[0] == "solve" and tf.exists():
-        import re
-        m = re.search(r"traffic bytes per launch at full size: (\d+)", tf.read_text())
-        traffic = int(m.group(1)) if m else None
+    # DRAM bytes per launch of the dominant kernel cannot be counted inside this run (that
+    # takes a profiler): the figure is this build's ncu capture of the same kernel, scaled to
+    # this workload's launches, and the line says so.
+    traffic = SOLVE_TRAFFIC_PER_LAUNCH if top[0] == "solve" and tuple(dims) == (128, 128, 64) else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
-                "frac": achieved / pk["hbm_gbs"], "traffic": traffic, "kernel": top[0],
+                "frac": achieved / pk["hbm_gbs"], "traffic": traffic,
+                "traffic_source": SOLVE_TRAFFIC_SOURCE if traffic else None, "kernel": top[0],
                 "peak_source": pk["source"], "launches_per_step": top[1]["launches"] // 3,
                 "ms_per_launch": per_launch_ms, "algorithmic_bytes_per_launch": per_launch_bytes,
                 "kernel_share": top[1]["total_ms"] / sum(v["total_ms"] for v in kinds.values())}
@@ -770,15 +866,17 @@ def main():
     e2e_value = world * solves_per_step / (e2e_ms * 1e-3)
 
     cpu = None
+    leg = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         from oracle import refworld
         if refworld.ref_available():
-            r = reference_sample((128, 128, 16), steps=8, warmup=1, workers=-1, params=params)
+            leg = reference_leg(dims, view, solver, params, steps=6)
             r1 = reference_sample((128, 128, 8), steps=4, warmup=1, workers=0, params=params)
-            cpu = {"value": r["value"], "unit": UNIT, "cores": r["threads"], "kind": "reference",
-                   "sample": f"128x128x16 slab of the lattice ({r['bodies']} bodies, "
-                             f"{r['manifolds']} manifolds), 8 steps of the reference phys_solve "
-                             f"on its job system; {cpu_model()}",
+            cpu = {"value": leg["cpu"]["value"], "unit": UNIT, "cores": leg["cpu"]["threads"],
+                   "kind": "reference",
+                   "sample": f"the bench's lattice itself ({len(view.bodies)} bodies, {manifolds} "
+                             f"manifolds), {leg['cpu']['steps']} steps of the reference "
+                             f"phys_solve on its job system after one; {cpu_model()}",
                    "single_thread": {"value": r1["value"], "unit": UNIT, "cores": 1,
                                      "sample": f"128x128x8 slab ({r1['bodies']} bodies), 4 "
                                                f"steps without a job system"}}
@@ -814,10 +912,15 @@ def main():
             "gpu_launches": int(stats.launches) * args.steps,
             "roofline": roofline,
             "cpu_baseline": cpu,
+            "parity": leg["parity"] if leg else None,
+            "fp64_error": leg["fp64_error"] if leg else None,
             "clocks": clocks,
             "points_solved_per_s": value * 4,
             "kernels": {k: {"launches": v["launches"] // 3, "ms": v["total_ms"] / 3}
                         for k, v in kinds.items()},
+            "kernels_source": "CUDA events around every launch of three steps run launch by "
+                              "launch outside the step's graph (roofline.ms_per_launch too); "
+                              "ms_per_step is the graph's",
         }
         print(json.dumps(out))
     solver.close()
