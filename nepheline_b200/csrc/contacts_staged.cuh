@@ -8,6 +8,10 @@
 // once whatever its register budget. The tile is [slot][lane]: a warp's 32 lanes read 512
 // contiguous bytes per slot, free of bank conflicts. The arithmetic is contacts.cuh's, in
 // its order: the staged and unstaged passes give the same bits.
+//
+// The lean form (kBodies = false) stages only the point rows, which the arithmetic reads
+// again and again, and loads the body rows straight into registers, where they stay for the
+// whole manifold anyway: its tile is 16 slots instead of 30, so an SM holds more warps.
 #pragma once
 
 #include <cuda_pipeline_primitives.h>
@@ -21,6 +25,7 @@ constexpr uint32_t kSlotVa = 16, kSlotWa = 17, kSlotVb = 18, kSlotWb = 19;
 constexpr uint32_t kSlotDpa = 20, kSlotDqa = 21, kSlotDpb = 22, kSlotDqb = 23;
 constexpr uint32_t kSlotIa = 24, kSlotIb = 27; // three columns each
 constexpr uint32_t kSlots = 30;
+constexpr uint32_t kPointSlots = 16; // the lean form's tile: the point rows only
 
 template <uint32_t kLanes> struct Tile {
     float4 *base;
@@ -53,12 +58,23 @@ NPH_D uint64_t policy_evict_last()
     return p;
 }
 
+// A 16-byte load into registers with an L2 eviction policy (the lean form's body rows).
+NPH_D float4 ld_policy(const float4 *src, uint64_t policy)
+{
+    float4 v;
+    asm volatile("ld.global.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;\n"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+                 : "l"(src), "l"(policy));
+    return v;
+}
+
 // Issues the manifold's loads into the lane's column: the rows of its own points (pt only
-// when `tangents`), the velocities of both bodies, their displacements and rotations when
-// `poses`, and the inertia of the sides that take results. The copies are not committed.
+// when `tangents`), and when `bodies` the velocities of both bodies, their displacements and
+// rotations when `poses`, and the inertia of the sides that take results. The copies are not
+// committed.
 template <uint32_t kLanes>
 NPH_D void issue_manifold(const DevSolver &S, uint32_t g, uint4 hdr, const Tile<kLanes> &T,
-                          bool tangents, bool poses)
+                          bool tangents, bool poses, bool bodies = true)
 {
     const uint32_t bits = hdr.z;
     const uint32_t pc = bits & kHdrPointsMask;
@@ -74,6 +90,9 @@ NPH_D void issue_manifold(const DevSolver &S, uint32_t g, uint4 hdr, const Tile<
                 copy16_policy(T.at(4u * k + 3u), &S.pt[row], stream);
             }
         }
+    }
+    if (!bodies) {
+        return;
     }
     copy16_policy(T.at(kSlotVa), &S.vel[2u * hdr.x], keep);
     copy16_policy(T.at(kSlotWa), &S.vel[2u * hdr.x + 1u], keep);
@@ -107,6 +126,56 @@ NPH_D void stage_manifold(const DevSolver &S, uint32_t g, uint4 hdr, const Tile<
     __pipeline_wait_prior(0);
 }
 
+// The two bodies of a manifold as the passes use them.
+struct ManifoldBodies {
+    Sides sd;
+    BodyState a, b;
+    BodyPose pa, pb;
+};
+
+// The lean form's body rows, loaded into registers (the poses only when `poses`).
+NPH_D ManifoldBodies load_bodies(const DevSolver &S, uint4 hdr, bool poses)
+{
+    const uint64_t keep = policy_evict_last();
+    const uint32_t bits = hdr.z;
+    ManifoldBodies m;
+    m.sd.wa = (bits & kHdrWriteA) != 0u;
+    m.sd.wb = (bits & kHdrWriteB) != 0u;
+    const float4 va = ld_policy(&S.vel[2u * hdr.x], keep);
+    const float4 wa = ld_policy(&S.vel[2u * hdr.x + 1u], keep);
+    const float4 vb = ld_policy(&S.vel[2u * hdr.y], keep);
+    const float4 wb = ld_policy(&S.vel[2u * hdr.y + 1u], keep);
+    m.a = BodyState{v3(va), v3(wa)};
+    m.b = BodyState{v3(vb), v3(wb)};
+    if (poses) {
+        const float4 pa = ld_policy(&S.pos[2u * hdr.x], keep);
+        const float4 qa = ld_policy(&S.pos[2u * hdr.x + 1u], keep);
+        const float4 pb = ld_policy(&S.pos[2u * hdr.y], keep);
+        const float4 qb = ld_policy(&S.pos[2u * hdr.y + 1u], keep);
+        m.pa = BodyPose{v3(pa), q4(qa)};
+        m.pb = BodyPose{v3(pb), q4(qb)};
+    }
+    m.sd.ma = 0.0f;
+    m.sd.mb = 0.0f;
+    m.sd.ia = m_zero();
+    m.sd.ib = m_zero();
+    if (m.sd.wa) {
+        const float4 c0 = ld_policy(&S.prm[3u * hdr.x], keep);
+        const float4 c1 = ld_policy(&S.prm[3u * hdr.x + 1u], keep);
+        const float4 c2 = ld_policy(&S.prm[3u * hdr.x + 2u], keep);
+        m.sd.ma = c0.w;
+        m.sd.ia = M3{v3(c0), v3(c1), v3(c2)};
+    }
+    if (m.sd.wb) {
+        const float4 c0 = ld_policy(&S.prm[3u * hdr.y], keep);
+        const float4 c1 = ld_policy(&S.prm[3u * hdr.y + 1u], keep);
+        const float4 c2 = ld_policy(&S.prm[3u * hdr.y + 2u], keep);
+        m.sd.mb = c0.w;
+        m.sd.ib = M3{v3(c0), v3(c1), v3(c2)};
+    }
+    return m;
+}
+
 template <uint32_t kLanes> NPH_D Sides staged_sides(const Tile<kLanes> &T, uint32_t bits)
 {
     Sides s;
@@ -131,8 +200,8 @@ template <uint32_t kLanes> NPH_D Sides staged_sides(const Tile<kLanes> &T, uint3
 
 // warm_manifold (solver_impl.h:181-258) on the staged loads.
 // kIssued: the lane's column already holds the manifold's loads (a pipelined pass issued and
-// waited for them).
-template <uint32_t kLanes, bool kIssued = false>
+// waited for them). kBodies: the tile holds the body rows (else they are loaded into registers).
+template <uint32_t kLanes, bool kIssued = false, bool kBodies = true>
 NPH_D void warm_manifold_staged(const DevSolver &S, uint32_t g, const Tile<kLanes> &T)
 {
     uint4 hdr = S.hdr[g];
@@ -142,12 +211,24 @@ NPH_D void warm_manifold_staged(const DevSolver &S, uint32_t g, const Tile<kLane
     if (pc == 0u) {
         return;
     }
-    if (!kIssued) {
-        stage_manifold(S, g, hdr, T, false, false);
+    Sides sd;
+    BodyState a, b;
+    if (kBodies) {
+        if (!kIssued) {
+            stage_manifold(S, g, hdr, T, false, false);
+        }
+        sd = staged_sides(T, bits);
+        a = BodyState{v3(T.get(kSlotVa)), v3(T.get(kSlotWa))};
+        b = BodyState{v3(T.get(kSlotVb)), v3(T.get(kSlotWb))};
+    } else {
+        issue_manifold(S, g, hdr, T, false, false, false);
+        __pipeline_commit();
+        const ManifoldBodies m = load_bodies(S, hdr, false);
+        __pipeline_wait_prior(0);
+        sd = m.sd;
+        a = m.a;
+        b = m.b;
     }
-    const Sides sd = staged_sides(T, bits);
-    BodyState a = BodyState{v3(T.get(kSlotVa)), v3(T.get(kSlotWa))};
-    BodyState b = BodyState{v3(T.get(kSlotVb)), v3(T.get(kSlotWb))};
     const V3 t1 = perpendicular(n);
     const V3 t2 = cross(n, t1);
     if ((bits & kHdrImpacted) != 0u) {
@@ -199,7 +280,7 @@ NPH_D void warm_manifold_staged(const DevSolver &S, uint32_t g, const Tile<kLane
 }
 
 // solve_manifold (solver_impl.h:484-602) on the staged loads.
-template <bool kUseBias, uint32_t kLanes, bool kIssued = false>
+template <bool kUseBias, uint32_t kLanes, bool kIssued = false, bool kBodies = true>
 NPH_D void solve_manifold_staged(const DevSolver &S, uint32_t g, const StepConsts &K,
                                  const Tile<kLanes> &T)
 {
@@ -210,14 +291,29 @@ NPH_D void solve_manifold_staged(const DevSolver &S, uint32_t g, const StepConst
     if (pc == 0u) {
         return;
     }
-    if (!kIssued) {
-        stage_manifold(S, g, hdr, T, true, true);
+    Sides sd;
+    BodyState a, b;
+    BodyPose pa_, pb_;
+    if (kBodies) {
+        if (!kIssued) {
+            stage_manifold(S, g, hdr, T, true, true);
+        }
+        sd = staged_sides(T, bits);
+        a = BodyState{v3(T.get(kSlotVa)), v3(T.get(kSlotWa))};
+        b = BodyState{v3(T.get(kSlotVb)), v3(T.get(kSlotWb))};
+        pa_ = BodyPose{v3(T.get(kSlotDpa)), q4(T.get(kSlotDqa))};
+        pb_ = BodyPose{v3(T.get(kSlotDpb)), q4(T.get(kSlotDqb))};
+    } else {
+        issue_manifold(S, g, hdr, T, true, true, false);
+        __pipeline_commit();
+        const ManifoldBodies m = load_bodies(S, hdr, true);
+        __pipeline_wait_prior(0);
+        sd = m.sd;
+        a = m.a;
+        b = m.b;
+        pa_ = m.pa;
+        pb_ = m.pb;
     }
-    const Sides sd = staged_sides(T, bits);
-    BodyState a = BodyState{v3(T.get(kSlotVa)), v3(T.get(kSlotWa))};
-    BodyState b = BodyState{v3(T.get(kSlotVb)), v3(T.get(kSlotWb))};
-    const BodyPose pa_ = BodyPose{v3(T.get(kSlotDpa)), q4(T.get(kSlotDqa))};
-    const BodyPose pb_ = BodyPose{v3(T.get(kSlotDpb)), q4(T.get(kSlotDqb))};
     const V3 n = v3(nf);
     const float friction = nf.w;
     const Soft soft = (bits & kHdrStaticSoft) != 0u ? K.static_soft : K.contact_soft;
