@@ -358,7 +358,8 @@ NPH_GPU_API void nph_gpu_solver_destroy(NphGpuSolver *solver);
  * overflow first; then restitution, store, finalize) and writes the results back into the
  * view's arrays. Returns NPH_GPU_INVALID_ARGUMENT for a malformed view (an index out of
  * range, a point count outside 1..4, colour counts that do not add up, an axis motion other
- * than NPH_GPU_AXIS_*), NPH_GPU_UNSUPPORTED for a setting the device solver does not run
+ * than NPH_GPU_AXIS_*, a body record with a value the stage reads that is not finite: NaN or
+ * infinite), NPH_GPU_UNSUPPORTED for a setting the device solver does not run
  * (XPBD, continuous collision, an unknown joint type), NPH_GPU_OUT_OF_MEMORY when the device buffers
  * cannot grow (the view is then untouched: the step did not happen), and
  * NPH_GPU_DEVICE_LOST when a device wait gave up or the device reported an error. */
@@ -378,6 +379,15 @@ NPH_GPU_API NphGpuResult nph_gpu_solver_synchronize(NphGpuSolver *solver);
 NPH_GPU_API NphGpuResult nph_gpu_solver_stats(const NphGpuSolver *solver, NphGpuStepStats *out);
 /* The stream the solver launches on (a cudaStream_t). */
 NPH_GPU_API void *nph_gpu_solver_stream(const NphGpuSolver *solver);
+
+/* A budget for the solver's record and row arrays, in bytes (0, the default: none). A call
+ * whose view would grow them beyond it returns NPH_GPU_OUT_OF_MEMORY before any array or the
+ * view is touched, as an allocation failure does (world.h:163-165: the step did not happen;
+ * the reference's failing-allocator test, test_sensor.c:342-392, fails its steps this way).
+ * An engine that gives the solver a fixed share of device memory sets it. */
+NPH_GPU_API NphGpuResult nph_gpu_solver_set_memory_limit(NphGpuSolver *solver, uint64_t bytes);
+/* The bytes the solver's record and row arrays hold now (the figure the budget limits). */
+NPH_GPU_API uint64_t nph_gpu_solver_memory(const NphGpuSolver *solver);
 
 /* One kind of kernel in a profiled step. */
 typedef struct NphGpuKernelTime {

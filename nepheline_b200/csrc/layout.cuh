@@ -94,6 +94,7 @@ enum : uint32_t {
 constexpr uint32_t kErrBadIndex = 1u << 0;
 constexpr uint32_t kErrBadPoints = 1u << 1;
 constexpr uint32_t kErrBadJoint = 1u << 2;
+constexpr uint32_t kErrBadBody = 1u << 3; // a value the stage reads is not finite
 
 // The step's constants (StepContext, solver.c:67-85), computed on the host in FP32 with the
 // reference's operations.

@@ -15,6 +15,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cstddef>
 #include <cstdio>
 #include <cstdlib>
 #include <algorithm>
@@ -82,8 +83,23 @@ __device__ __forceinline__ void stage_out(const Rec *src, uint32_t count, Rec *d
 static_assert(sizeof(NphGpuBody) % 16 == 0, "body records stage in 16-byte words");
 static_assert(sizeof(NphGpuContact) % 16 == 0, "contact records stage in 16-byte words");
 
+// Whether every value of a body record that the stage reads is finite: the centre, the rotation,
+// the velocities, force and torque, the mass properties and the integration settings.
+__device__ bool body_finite(const NphGpuBody &b)
+{
+    bool ok = isfinite(b.center[0]) && isfinite(b.center[1]) && isfinite(b.center[2]);
+    const float *f = b.rotation; // rotation .. max_extent: 44 consecutive floats
+    static_assert(offsetof(NphGpuBody, type) - offsetof(NphGpuBody, rotation) == 44 * sizeof(float),
+                  "the record's float block");
+#pragma unroll 4
+    for (uint32_t k = 0; k < 44u; ++k) {
+        ok = ok && isfinite(f[k]);
+    }
+    return ok;
+}
+
 __global__ void __launch_bounds__(kStage) k_prepare_bodies(BodyArrays B, const NphGpuBody *bodies,
-                                                           uint32_t n, StepConsts K)
+                                                           uint32_t n, StepConsts K, uint32_t *err)
 {
     __shared__ NphGpuBody rec[kStage];
     const uint32_t first = blockIdx.x * kStage;
@@ -92,7 +108,22 @@ __global__ void __launch_bounds__(kStage) k_prepare_bodies(BodyArrays B, const N
         stage_in<uint4>(bodies + first, count, rec);
         __syncthreads();
         if (threadIdx.x < count) {
-            prepare_body(B, first + threadIdx.x, rec[threadIdx.x], K);
+            if (body_finite(rec[threadIdx.x])) {
+                prepare_body(B, first + threadIdx.x, rec[threadIdx.x], K);
+            } else {
+                // Refused: the call returns before anything is written back. Meanwhile the body
+                // is inert (a static body at rest), so nothing it touches takes a non-finite value.
+                atomicOr(err, kErrBadBody);
+                NphGpuBody inert = rec[threadIdx.x];
+                inert.type = NPH_GPU_BODY_STATIC;
+                for (uint32_t k = 0; k < 3u; ++k) {
+                    inert.linear_velocity[k] = 0.0f;
+                    inert.angular_velocity[k] = 0.0f;
+                }
+                inert.rotation[0] = inert.rotation[1] = inert.rotation[2] = 0.0f;
+                inert.rotation[3] = 1.0f;
+                prepare_body(B, first + threadIdx.x, inert, K);
+            }
         }
     }
     if (first + threadIdx.x == n) {
@@ -266,8 +297,9 @@ __global__ void __launch_bounds__(kBlock) k_joint_pass(DevSolver S, uint32_t jfi
     }
 }
 
-// The same pass with the manifold's loads staged through shared memory (contacts_staged.cuh).
-template <int P, uint32_t kLanes, int kMinBlocks>
+// The same pass with the manifold's loads staged through shared memory (contacts_staged.cuh);
+// kBodies false: the lean form, only the point rows staged.
+template <int P, uint32_t kLanes, int kMinBlocks, bool kBodies = true>
 __global__ void __launch_bounds__(kLanes, kMinBlocks)
 k_pass_staged(DevSolver S, uint32_t cfirst, uint32_t ccount, StepConsts K)
 {
@@ -278,11 +310,11 @@ k_pass_staged(DevSolver S, uint32_t cfirst, uint32_t ccount, StepConsts K)
     }
     const Tile<kLanes> T{tile, threadIdx.x};
     if (P == kWarm) {
-        warm_manifold_staged(S, cfirst + g, T);
+        warm_manifold_staged<kLanes, false, kBodies>(S, cfirst + g, T);
     } else if (P == kSolve) {
-        solve_manifold_staged<true>(S, cfirst + g, K, T);
+        solve_manifold_staged<true, kLanes, false, kBodies>(S, cfirst + g, K, T);
     } else if (P == kRelax) {
-        solve_manifold_staged<false>(S, cfirst + g, K, T);
+        solve_manifold_staged<false, kLanes, false, kBodies>(S, cfirst + g, K, T);
     } else {
         restitution_manifold(S, cfirst + g, K);
     }
@@ -349,14 +381,16 @@ k_pass_pipelined(DevSolver S, uint32_t cfirst, uint32_t ccount, StepConsts K)
 }
 
 // The pass configurations: threads per block and the blocks per SM the register budget
-// allows (65,536 registers / (threads x blocks)); the last two stage the loads through
-// shared memory (kSlots x threads x 16 bytes per block).
+// allows (65,536 registers / (threads x blocks)); `staged`: 0 plain loads, 1 the loads staged
+// through shared memory (kSlots x threads x 16 bytes per block), 2 staged and pipelined, 3 the
+// lean staged form (kPointSlots x threads x 16 bytes per block).
 struct PassConfig {
     uint32_t threads, min_blocks, staged;
 };
 constexpr PassConfig kPassConfigs[] = {{256, 1, 0}, {256, 2, 0}, {128, 4, 0}, {256, 3, 0},
                                        {64, 6, 1},  {64, 7, 1},  {128, 3, 1}, {32, 14, 1},
-                                       {32, 7, 2},  {64, 3, 2}};
+                                       {32, 7, 2},  {64, 3, 2},  {32, 18, 3}, {32, 24, 3},
+                                       {64, 9, 3},  {64, 12, 3}, {128, 6, 3}};
 constexpr uint32_t kPassConfigCount = sizeof(kPassConfigs) / sizeof(kPassConfigs[0]);
 
 template <int P>
@@ -365,7 +399,8 @@ void launch_pass(uint32_t config, uint32_t cc, cudaStream_t st, const DevSolver 
 {
     const uint32_t t = kPassConfigs[config].threads;
     const uint32_t grid = (cc + t - 1) / t;
-    const size_t tile = kPassConfigs[config].staged ? (size_t)kSlots * t * sizeof(float4) : 0;
+    const uint32_t slots = kPassConfigs[config].staged == 3u ? kPointSlots : kSlots;
+    const size_t tile = kPassConfigs[config].staged ? (size_t)slots * t * sizeof(float4) : 0;
     if (kPassConfigs[config].staged == 2u) {
         if (P == kRestitution) { // no loads worth pipelining: the plain kernel
             k_pass<P, 128, 4><<<(cc + 127u) / 128u, 128, 0, st>>>(S, cfirst, cc, K);
@@ -394,7 +429,12 @@ void launch_pass(uint32_t config, uint32_t cc, cudaStream_t st, const DevSolver 
     case 4: k_pass_staged<P, 64, 6><<<grid, 64, tile, st>>>(S, cfirst, cc, K); break;
     case 5: k_pass_staged<P, 64, 7><<<grid, 64, tile, st>>>(S, cfirst, cc, K); break;
     case 6: k_pass_staged<P, 128, 3><<<grid, 128, tile, st>>>(S, cfirst, cc, K); break;
-    default: k_pass_staged<P, 32, 14><<<grid, 32, tile, st>>>(S, cfirst, cc, K); break;
+    case 7: k_pass_staged<P, 32, 14><<<grid, 32, tile, st>>>(S, cfirst, cc, K); break;
+    case 10: k_pass_staged<P, 32, 18, false><<<grid, 32, tile, st>>>(S, cfirst, cc, K); break;
+    case 11: k_pass_staged<P, 32, 24, false><<<grid, 32, tile, st>>>(S, cfirst, cc, K); break;
+    case 12: k_pass_staged<P, 64, 9, false><<<grid, 64, tile, st>>>(S, cfirst, cc, K); break;
+    case 13: k_pass_staged<P, 64, 12, false><<<grid, 64, tile, st>>>(S, cfirst, cc, K); break;
+    default: k_pass_staged<P, 128, 6, false><<<grid, 128, tile, st>>>(S, cfirst, cc, K); break;
     }
 }
 
@@ -750,6 +790,7 @@ struct NphGpuSolver {
     bool use_graph = true;
     // Capacities of the device arrays.
     uint32_t bcap = 0, fcap = 0, mcap = 0, jcap = 0;
+    uint64_t memory_limit = 0; // bytes the record and row arrays may take (0: no limit)
     // Records (device copies of the view's arrays).
     NphGpuBody *d_bodies = nullptr;
     NphGpuBody *d_fixed = nullptr;
@@ -835,9 +876,28 @@ void drop_graph(NphGpuSolver *s)
     s->graph_valid = false;
 }
 
-// Grows the device arrays to hold the view (between steps only).
+// Device bytes of the record and row arrays at these capacities.
+uint64_t array_bytes(uint64_t bcap, uint64_t fcap, uint64_t mcap, uint64_t jcap)
+{
+    return bcap * (sizeof(NphGpuBody) + 13u * sizeof(float4)) + fcap * sizeof(NphGpuBody) +
+           mcap * (sizeof(NphGpuContact) + sizeof(uint4) + sizeof(float4) + sizeof(float) +
+                   16u * sizeof(float4)) +
+           jcap * (sizeof(NphGpuJoint) + (uint64_t)kJointRows * sizeof(float4));
+}
+
+// Grows the device arrays to hold the view (between steps only). A growth the solver's memory
+// limit does not allow is refused before any array is touched: the world stays as it was.
 NphGpuResult ensure_capacity(NphGpuSolver *s, uint32_t n, uint32_t nf, uint32_t m, uint32_t nj)
 {
+    if (s->memory_limit != 0u) {
+        const uint64_t bcap = n + 1u > s->bcap ? (uint64_t)(n + 1u) + (n + 1u) / 8u : s->bcap;
+        const uint64_t fcap = nf > s->fcap ? (uint64_t)nf + nf / 8u + 1u : s->fcap;
+        const uint64_t mcap = m > s->mcap ? (uint64_t)m + m / 8u + 1u : s->mcap;
+        const uint64_t jcap = nj > s->jcap ? (uint64_t)nj + nj / 8u + 1u : s->jcap;
+        if (array_bytes(bcap, fcap, mcap, jcap) > s->memory_limit) {
+            return NPH_GPU_OUT_OF_MEMORY;
+        }
+    }
     bool ok = true;
     if (n + 1u > s->bcap) {
         const uint32_t cap = n + 1u + (n + 1u) / 8u;
@@ -1021,7 +1081,8 @@ void enqueue_prepare(NphGpuSolver *s, const StepConsts &K)
     const BodyArrays B = body_arrays(s);
     const double n = s->n;
     mark_begin(s, kKPrepareBodies, s->n, 368.0 * n);
-    k_prepare_bodies<<<stage_blocks(s->n + 1u), kStage, 0, s->stream>>>(B, s->d_bodies, s->n, K);
+    k_prepare_bodies<<<stage_blocks(s->n + 1u), kStage, 0, s->stream>>>(B, s->d_bodies, s->n, K,
+                                                                         s->d_err);
     mark_end(s);
     s->launches++;
     ColorTable T;
@@ -1873,6 +1934,20 @@ NPH_GPU_API NphGpuResult nph_gpu_solver_stats(const NphGpuSolver *s, NphGpuStepS
 NPH_GPU_API void *nph_gpu_solver_stream(const NphGpuSolver *s)
 {
     return s != nullptr ? (void *)s->stream : nullptr;
+}
+
+NPH_GPU_API NphGpuResult nph_gpu_solver_set_memory_limit(NphGpuSolver *s, uint64_t bytes)
+{
+    if (s == nullptr) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    s->memory_limit = bytes;
+    return NPH_GPU_OK;
+}
+
+NPH_GPU_API uint64_t nph_gpu_solver_memory(const NphGpuSolver *s)
+{
+    return s != nullptr ? array_bytes(s->bcap, s->fcap, s->mcap, s->jcap) : 0u;
 }
 
 } // extern "C"

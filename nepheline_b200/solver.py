@@ -46,6 +46,8 @@ def lib() -> ctypes.CDLL:
         "nph_gpu_solver_synchronize": (ctypes.c_int32, [_vp]),
         "nph_gpu_solver_stats": (ctypes.c_int32, [_vp, P(abi.StepStats)]),
         "nph_gpu_solver_stream": (_vp, [_vp]),
+        "nph_gpu_solver_set_memory_limit": (ctypes.c_int32, [_vp, ctypes.c_uint64]),
+        "nph_gpu_solver_memory": (ctypes.c_uint64, [_vp]),
         "nph_gpu_graph_color": (ctypes.c_int32, [_vp, _vp, _vp, _vp, _u32, _u32, _vp, _vp]),
         "nph_gpu_version": (ctypes.c_char_p, []),
         "nph_gpu_world_profile_step": (ctypes.c_int32, [_vp, P(abi.WorldParams), ctypes.c_float,
@@ -172,6 +174,16 @@ class Solver:
 
     def synchronize(self) -> None:
         _check(self.L.nph_gpu_solver_synchronize(self._h), "nph_gpu_solver_synchronize")
+
+    def set_memory_limit(self, nbytes: int) -> None:
+        """A budget for the record and row arrays (0: none); growth beyond it fails with
+        OUT_OF_MEMORY before anything is touched."""
+        _check(self.L.nph_gpu_solver_set_memory_limit(self._h, int(nbytes)),
+               "nph_gpu_solver_set_memory_limit")
+
+    def memory(self) -> int:
+        """Bytes the record and row arrays hold now."""
+        return int(self.L.nph_gpu_solver_memory(self._h))
 
     def stats(self) -> abi.StepStats:
         st = abi.StepStats()
