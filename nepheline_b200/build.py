@@ -65,9 +65,17 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     return LIB
 
 
+# Where the reference's sources lie in the build container (NPH_REFERENCE overrides); the GPU
+# machines only use the libraries built from them.
+REFERENCE = Path(os.environ.get("NPH_REFERENCE", "/root/reference"))
+
+
 def build_oracle() -> None:
     """The checkers under oracle/ (the reference library only where its sources exist)."""
-    subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "-j8"], check=True)
+    cmd = ["make", "-s", "-C", str(ROOT / "oracle"), "-j8"]
+    if (REFERENCE / "engine" / "physics" / "src" / "solver.c").exists():
+        cmd.append(f"REF={REFERENCE}")
+    subprocess.run(cmd, check=True)
 
 
 if __name__ == "__main__":
