@@ -30,6 +30,7 @@
 #include "world_internal.h"
 
 #include "nepheline_b200.h"
+#include "world_view.h" // the binding's world <-> view conversion (nepheline_b200/binding)
 
 #include <stdlib.h>
 #include <string.h>
@@ -48,9 +49,7 @@ typedef struct RefWorld {
     u32 *records;
     u32 constraint_count;
     u32 constraint_cap;
-    u32 *fixed_of_slot; // per body slot: its fixed-body index in the last view, or PHYS_NULL
-    u32 fixed_cap;
-    u32 *fixed_slots; // per fixed-body index: its body slot
+    NphViewMap map; // the last view's fixed bodies
 } RefWorld;
 
 static void *grow(void *p, u32 *cap, u32 need, size_t elem)
@@ -116,8 +115,7 @@ REF_API void nphref_world_destroy(RefWorld *r)
     free(r->bodies);
     free(r->kinds);
     free(r->records);
-    free(r->fixed_of_slot);
-    free(r->fixed_slots);
+    nph_view_map_release(&r->map);
     free(r);
 }
 
@@ -517,249 +515,19 @@ REF_API u32 nphref_body_slots(const RefWorld *r)
 }
 
 // ---------------------------------------------------------------------------
-// World <-> view
+// World <-> view (the conversion is the binding's, nepheline_b200/binding/world_view.h)
 // ---------------------------------------------------------------------------
-
-static const NphArrayU32 *contact_list(const NphPhysicsWorld *w, u32 c)
-{
-    return c == PHYS_GRAPH_OVERFLOW ? &w->overflow : &w->colors[c].contacts;
-}
-
-static const NphArrayU32 *joint_list(const NphPhysicsWorld *w, u32 c)
-{
-    return c == PHYS_GRAPH_OVERFLOW ? &w->overflow_joints : &w->colors[c].joints;
-}
-
-static void body_record(const PhysBody *b, NphGpuBody *o)
-{
-    memset(o, 0, sizeof *o);
-    o->center[0] = b->center.x;
-    o->center[1] = b->center.y;
-    o->center[2] = b->center.z;
-    o->origin[0] = b->origin.x;
-    o->origin[1] = b->origin.y;
-    o->origin[2] = b->origin.z;
-    memcpy(o->rotation, &b->rotation, sizeof o->rotation);
-    memcpy(o->local_center, &b->local_center, sizeof o->local_center);
-    memcpy(o->linear_velocity, &b->linear_velocity, sizeof o->linear_velocity);
-    memcpy(o->angular_velocity, &b->angular_velocity, sizeof o->angular_velocity);
-    memcpy(o->force, &b->force, sizeof o->force);
-    memcpy(o->torque, &b->torque, sizeof o->torque);
-    memcpy(o->inertia, &b->inertia, sizeof o->inertia);
-    memcpy(o->inv_inertia, &b->inv_inertia, sizeof o->inv_inertia);
-    o->inv_mass = b->inv_mass;
-    o->linear_damping = b->linear_damping;
-    o->angular_damping = b->angular_damping;
-    o->gravity_scale = b->gravity_scale;
-    o->sleep_threshold = b->sleep_threshold;
-    o->sleep_time = b->sleep_time;
-    o->max_extent = b->max_extent;
-    o->type = b->type;
-    o->flags = b->flags;
-    o->locks = b->locks;
-}
-
-// The view index of body slot `slot`: its awake slot, or a fixed body's index after them.
-static u32 view_index(RefWorld *r, u32 slot, u32 *fixed_count)
-{
-    const PhysBody *b = &r->w->bodies.data[slot];
-    if (b->awake_slot != PHYS_NULL) {
-        return b->awake_slot;
-    }
-    if (r->fixed_of_slot[slot] == PHYS_NULL) {
-        r->fixed_slots[*fixed_count] = slot;
-        r->fixed_of_slot[slot] = (*fixed_count)++;
-    }
-    return r->w->awake_bodies.len + r->fixed_of_slot[slot];
-}
-
-static void map_fixed(RefWorld *r, u32 *fixed_count)
-{
-    const NphPhysicsWorld *w = r->w;
-    u32 cap = r->fixed_cap;
-    r->fixed_of_slot = (u32 *)grow(r->fixed_of_slot, &cap, w->bodies.len + 1U, sizeof(u32));
-    cap = r->fixed_cap;
-    r->fixed_slots = (u32 *)grow(r->fixed_slots, &cap, w->bodies.len + 1U, sizeof(u32));
-    r->fixed_cap = cap;
-    for (u32 i = 0U; i < w->bodies.len; ++i) {
-        r->fixed_of_slot[i] = PHYS_NULL;
-    }
-    *fixed_count = 0U;
-    for (u32 c = 0U; c <= PHYS_GRAPH_COLORS; ++c) {
-        const NphArrayU32 *list = contact_list(w, c);
-        for (u32 i = 0U; i < list->len; ++i) {
-            const PhysContact *ct = &w->contacts.data[list->data[i]];
-            (void)view_index(r, ct->body_a, fixed_count);
-            (void)view_index(r, ct->body_b, fixed_count);
-        }
-        const NphArrayU32 *jl = joint_list(w, c);
-        for (u32 i = 0U; i < jl->len; ++i) {
-            const PhysJoint *j = &w->joints.data[jl->data[i]];
-            (void)view_index(r, j->body_a, fixed_count);
-            (void)view_index(r, j->body_b, fixed_count);
-        }
-    }
-}
 
 // The sizes a view of the world needs.
 REF_API void nphref_view_sizes(RefWorld *r, u32 *bodies, u32 *fixed, u32 *contacts, u32 *joints)
 {
-    const NphPhysicsWorld *w = r->w;
-    map_fixed(r, fixed);
-    *bodies = w->awake_bodies.len;
-    u32 nc = 0U;
-    u32 nj = 0U;
-    for (u32 c = 0U; c <= PHYS_GRAPH_COLORS; ++c) {
-        nc += contact_list(w, c)->len;
-        nj += joint_list(w, c)->len;
+    if (nph_view_sizes(r->w, &r->map, bodies, fixed, contacts, joints) != NPH_RESULT_OK) {
+        abort();
     }
-    *contacts = nc;
-    *joints = nj;
-}
-
-static void contact_record(RefWorld *r, const PhysContact *c, NphGpuContact *o, u32 *fixed_count)
-{
-    memset(o, 0, sizeof *o);
-    o->body_a = view_index(r, c->body_a, fixed_count);
-    o->body_b = view_index(r, c->body_b, fixed_count);
-    o->flags = c->flags & (PHYS_CONTACT_HIT | PHYS_CONTACT_HIT_EVENTS);
-    o->point_count = c->point_count;
-    memcpy(o->normal, &c->normal, sizeof o->normal);
-    o->friction = c->friction;
-    o->restitution = c->restitution;
-    for (u32 k = 0U; k < c->point_count; ++k) {
-        const PhysContactPoint *p = &c->points[k];
-        NphGpuContactPoint *q = &o->points[k];
-        memcpy(q->anchor_a, &p->anchor_a, sizeof q->anchor_a);
-        memcpy(q->anchor_b, &p->anchor_b, sizeof q->anchor_b);
-        q->separation = p->separation;
-        q->normal_impulse = p->normal_impulse;
-        q->max_normal_impulse = p->max_normal_impulse;
-        memcpy(q->tangent_impulse, &p->tangent_impulse, sizeof q->tangent_impulse);
-        q->relative_velocity = p->relative_velocity;
-        q->id = p->id;
-    }
-}
-
-#define JOINT_BLOCKS (NPH_GPU_JOINT_BLOCK_ROTATION | NPH_GPU_JOINT_BLOCK_SWING | NPH_GPU_JOINT_BLOCK_POINT)
-_Static_assert(NPH_GPU_CONTACT_HIT == PHYS_CONTACT_HIT && NPH_GPU_CONTACT_HIT_EVENTS == PHYS_CONTACT_HIT_EVENTS,
-               "the contact record's flag bits are the world's");
-_Static_assert(sizeof(((PhysJoint *)0)->axis_impulse) == sizeof(((NphGpuJoint *)0)->axis_impulse),
-               "the rows per axis of PhysJoint and of the record");
-
-static void joint_record(RefWorld *r, const PhysJoint *j, NphGpuJoint *o, u32 *fixed_count)
-{
-    memset(o, 0, sizeof *o);
-    o->type = j->type;
-    o->body_a = view_index(r, j->body_a, fixed_count);
-    o->body_b = view_index(r, j->body_b, fixed_count);
-    memcpy(o->frame_a_position, &j->frame_a.position, sizeof o->frame_a_position);
-    memcpy(o->frame_a_rotation, &j->frame_a.rotation, sizeof o->frame_a_rotation);
-    memcpy(o->frame_b_position, &j->frame_b.position, sizeof o->frame_b_position);
-    memcpy(o->frame_b_rotation, &j->frame_b.rotation, sizeof o->frame_b_rotation);
-    if (j->type == NPH_PHYSICS_JOINT_BALL) {
-        o->u.ball.enable_swing_limit = (u32)j->ball.enable_swing_limit;
-        o->u.ball.swing_y = j->ball.swing_y;
-        o->u.ball.swing_z = j->ball.swing_z;
-        o->u.ball.enable_twist_limit = (u32)j->ball.enable_twist_limit;
-        o->u.ball.twist_lower = j->ball.twist_lower;
-        o->u.ball.twist_upper = j->ball.twist_upper;
-        o->u.ball.friction_torque = j->ball.friction_torque;
-    } else if (j->type == NPH_PHYSICS_JOINT_HINGE) {
-        o->u.hinge.enable_limit = (u32)j->hinge.enable_limit;
-        o->u.hinge.lower = j->hinge.lower;
-        o->u.hinge.upper = j->hinge.upper;
-        o->u.hinge.enable_motor = (u32)j->hinge.enable_motor;
-        o->u.hinge.motor_speed = j->hinge.motor_speed;
-        o->u.hinge.max_motor_torque = j->hinge.max_motor_torque;
-        o->u.hinge.enable_spring = (u32)j->hinge.enable_spring;
-        o->u.hinge.spring_hertz = j->hinge.spring_hertz;
-        o->u.hinge.spring_damping_ratio = j->hinge.spring_damping_ratio;
-        o->u.hinge.spring_target = j->hinge.spring_target;
-    } else if (j->type == NPH_PHYSICS_JOINT_SLIDER) {
-        o->u.slider.enable_limit = (u32)j->slider.enable_limit;
-        o->u.slider.lower = j->slider.lower;
-        o->u.slider.upper = j->slider.upper;
-        o->u.slider.enable_motor = (u32)j->slider.enable_motor;
-        o->u.slider.motor_speed = j->slider.motor_speed;
-        o->u.slider.max_motor_force = j->slider.max_motor_force;
-        o->u.slider.enable_spring = (u32)j->slider.enable_spring;
-        o->u.slider.spring_hertz = j->slider.spring_hertz;
-        o->u.slider.spring_damping_ratio = j->slider.spring_damping_ratio;
-        o->u.slider.spring_target = j->slider.spring_target;
-    } else if (j->type == NPH_PHYSICS_JOINT_DISTANCE) {
-        o->u.distance.length = j->distance.length;
-        o->u.distance.enable_limit = (u32)j->distance.enable_limit;
-        o->u.distance.min_length = j->distance.min_length;
-        o->u.distance.max_length = j->distance.max_length;
-        o->u.distance.enable_spring = (u32)j->distance.enable_spring;
-        o->u.distance.spring_hertz = j->distance.spring_hertz;
-        o->u.distance.spring_damping_ratio = j->distance.spring_damping_ratio;
-        o->u.distance.enable_motor = (u32)j->distance.enable_motor;
-        o->u.distance.motor_speed = j->distance.motor_speed;
-        o->u.distance.max_motor_force = j->distance.max_motor_force;
-    } else if (j->type == NPH_PHYSICS_JOINT_D6) {
-        for (u32 i = 0U; i < NPH_PHYSICS_D6_AXES; ++i) {
-            const NphPhysicsD6Axis *x = &j->d6.axes[i];
-            NphGpuD6Axis *y = &o->u.d6[i];
-            y->motion = (u32)x->motion;
-            y->lower = x->lower;
-            y->upper = x->upper;
-            y->enable_motor = (u32)x->enable_motor;
-            y->motor_speed = x->motor_speed;
-            y->max_motor_force = x->max_motor_force;
-            y->enable_spring = (u32)x->enable_spring;
-            y->spring_hertz = x->spring_hertz;
-            y->spring_damping_ratio = x->spring_damping_ratio;
-            y->spring_target = x->spring_target;
-        }
-    }
-    // The block bits of joint_solver.c:103-112 carry across steps; the others are the step's.
-    o->flags = j->flags & JOINT_BLOCKS;
-    memcpy(o->axis_impulse, j->axis_impulse, sizeof o->axis_impulse);
-    memcpy(o->linear_impulse, &j->linear_impulse, sizeof o->linear_impulse);
-    memcpy(o->angular_impulse, &j->angular_impulse, sizeof o->angular_impulse);
-    memcpy(o->friction_impulse, &j->friction_impulse, sizeof o->friction_impulse);
-    o->lower_impulse = j->lower_impulse;
-    o->upper_impulse = j->upper_impulse;
-    o->swing_impulse = j->swing_impulse;
-    o->motor_impulse = j->motor_impulse;
-    o->spring_impulse = j->spring_impulse;
 }
 
 // Fills a view whose arrays the caller sized by nphref_view_sizes.
-REF_API int nphref_export(RefWorld *r, NphGpuWorldView *v)
-{
-    const NphPhysicsWorld *w = r->w;
-    u32 fixed = 0U;
-    map_fixed(r, &fixed);
-    v->body_count = w->awake_bodies.len;
-    for (u32 i = 0U; i < w->awake_bodies.len; ++i) {
-        body_record(&w->bodies.data[w->awake_bodies.data[i]], &v->bodies[i]);
-    }
-    v->fixed_count = fixed;
-    for (u32 i = 0U; i < fixed; ++i) {
-        body_record(&w->bodies.data[r->fixed_slots[i]], (NphGpuBody *)&v->fixed_bodies[i]);
-    }
-    u32 nc = 0U;
-    u32 nj = 0U;
-    u32 again = fixed;
-    for (u32 c = 0U; c <= PHYS_GRAPH_COLORS; ++c) {
-        const NphArrayU32 *list = contact_list(w, c);
-        v->contact_color_counts[c] = list->len;
-        for (u32 i = 0U; i < list->len; ++i) {
-            contact_record(r, &w->contacts.data[list->data[i]], &v->contacts[nc++], &again);
-        }
-        const NphArrayU32 *jl = joint_list(w, c);
-        v->joint_color_counts[c] = jl->len;
-        for (u32 i = 0U; i < jl->len; ++i) {
-            joint_record(r, &w->joints.data[jl->data[i]], &v->joints[nj++], &again);
-        }
-    }
-    v->contact_count = nc;
-    v->joint_count = nj;
-    return again == fixed ? 0 : 1;
-}
+REF_API int nphref_export(RefWorld *r, NphGpuWorldView *v) { return nph_view_export(r->w, &r->map, v); }
 
 // Writes a solved view back into the world: what phys_solve's stages write
 // (finalize_body, store_group, the joints' impulses), then the finalize pass's box refresh
@@ -768,76 +536,11 @@ REF_API int nphref_export(RefWorld *r, NphGpuWorldView *v)
 REF_API int nphref_import(RefWorld *r, const NphGpuWorldView *v, f32 dt)
 {
     NphPhysicsWorld *w = r->w;
-    if (v->body_count != w->awake_bodies.len) {
-        return (int)NPH_RESULT_INVALID_STATE;
+    NphResult res = nph_view_import(w, v, dt);
+    for (u32 i = 0U; res == NPH_RESULT_OK && i < w->awake_bodies.len; ++i) {
+        res = nph_view_grow_proxies(w, &w->bodies.data[w->awake_bodies.data[i]]);
     }
-    for (u32 i = 0U; i < v->body_count; ++i) {
-        PhysBody *b = &w->bodies.data[w->awake_bodies.data[i]];
-        const NphGpuBody *o = &v->bodies[i];
-        b->center = nph_dvec3(o->center[0], o->center[1], o->center[2]);
-        b->origin = nph_dvec3(o->origin[0], o->origin[1], o->origin[2]);
-        memcpy(&b->rotation, o->rotation, sizeof o->rotation);
-        memcpy(&b->linear_velocity, o->linear_velocity, sizeof o->linear_velocity);
-        memcpy(&b->angular_velocity, o->angular_velocity, sizeof o->angular_velocity);
-        b->force = nph_vec3_zero();
-        b->torque = nph_vec3_zero();
-        b->sleep_time = o->sleep_time;
-        phys_body_refresh_boxes(w, b);
-    }
-    u32 nc = 0U;
-    u32 nj = 0U;
-    for (u32 c = 0U; c <= PHYS_GRAPH_COLORS; ++c) {
-        const NphArrayU32 *list = contact_list(w, c);
-        for (u32 i = 0U; i < list->len; ++i) {
-            PhysContact *ct = &w->contacts.data[list->data[i]];
-            const NphGpuContact *o = &v->contacts[nc++];
-            ct->flags = (ct->flags & ~(u32)PHYS_CONTACT_HIT) | (o->flags & PHYS_CONTACT_HIT);
-            for (u32 k = 0U; k < ct->point_count; ++k) {
-                PhysContactPoint *p = &ct->points[k];
-                p->normal_impulse = o->points[k].normal_impulse;
-                p->max_normal_impulse = o->points[k].max_normal_impulse;
-                p->relative_velocity = o->points[k].relative_velocity;
-                memcpy(&p->tangent_impulse, o->points[k].tangent_impulse,
-                       sizeof o->points[k].tangent_impulse);
-            }
-        }
-        const NphArrayU32 *jl = joint_list(w, c);
-        for (u32 i = 0U; i < jl->len; ++i) {
-            PhysJoint *j = &w->joints.data[jl->data[i]];
-            const NphGpuJoint *o = &v->joints[nj++];
-            memcpy(&j->linear_impulse, o->linear_impulse, sizeof o->linear_impulse);
-            memcpy(&j->angular_impulse, o->angular_impulse, sizeof o->angular_impulse);
-            memcpy(&j->friction_impulse, o->friction_impulse, sizeof o->friction_impulse);
-            j->lower_impulse = o->lower_impulse;
-            j->upper_impulse = o->upper_impulse;
-            j->swing_impulse = o->swing_impulse;
-            j->motor_impulse = o->motor_impulse;
-            j->spring_impulse = o->spring_impulse;
-            memcpy(j->axis_impulse, o->axis_impulse, sizeof o->axis_impulse);
-            j->flags = (j->flags & ~(u32)JOINT_BLOCKS) | (o->flags & JOINT_BLOCKS);
-        }
-    }
-    w->last_substep = dt / (f32)w->desc.substeps;
-    for (u32 i = 0U; i < w->awake_bodies.len; ++i) {
-        PhysBody *b = &w->bodies.data[w->awake_bodies.data[i]];
-        if ((b->flags & PHYS_BODY_ENLARGED) == 0U) {
-            continue;
-        }
-        b->flags &= ~(u32)PHYS_BODY_ENLARGED;
-        for (u32 s = b->shape_head; s != PHYS_NULL; s = w->shapes.data[s].next) {
-            PhysShape *shape = &w->shapes.data[s];
-            if ((shape->flags & PHYS_SHAPE_ENLARGED) != 0U) {
-                shape->flags &= ~(u32)PHYS_SHAPE_ENLARGED;
-                nph_aabb_tree_enlarge_proxy(&w->trees[shape->tree], shape->proxy,
-                                            shape->fat_aabb);
-                const NphResult res = phys_move_buffer_push(w, s);
-                if (res != NPH_RESULT_OK) {
-                    return (int)res;
-                }
-            }
-        }
-    }
-    return 0;
+    return (int)res;
 }
 
 // The world's statistics the scenes report.
