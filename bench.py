@@ -209,6 +209,69 @@ def pinned_copy(view):
     return v
 
 
+
+def pinned_alloc(n, dtype):
+    """A page-locked numpy record array (the end-to-end legs' host buffers)."""
+    import numpy as np
+    import torch
+    t = torch.empty(max(n, 1) * dtype.itemsize, dtype=torch.uint8, pin_memory=True)
+    a = t.numpy().view(dtype)[:n]
+    a[...] = np.zeros(1, dtype)
+    _PINNED.append(t)
+    return a
+
+
+_PINNED: list = []
+
+
+def _timed_calls(call, steps: int, pg) -> float:
+    """ms per call: each call timed alone (wall clock, which covers its copies both ways and the
+    step; the call returns after the download), the largest over ranks."""
+    import torch
+    total = 0.0
+    for _ in range(steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        call()
+        total += time.perf_counter() - t0
+    return max_over_ranks(pg, 1e3 * total / max(steps, 1))
+
+
+def e2e_whole(solver, pv, params, steps: int, pg) -> float:
+    """The whole-record drop-in, its records updated in place call after call."""
+    solver.phys_solve(pv, params, DT)
+    barrier(pg)
+    return _timed_calls(lambda: solver.phys_solve(pv, params, DT), steps, pg)
+
+
+def e2e_packed(solver, pk, params, steps: int, pg) -> float:
+    """The packed drop-in; between calls (outside the timing) the outputs become the next call's
+    inputs, as a caller's world carries them from step to step."""
+    def carry():
+        for f in ("center", "rotation", "linear_velocity", "angular_velocity", "sleep_time"):
+            pk.bodies[f] = pk.out_bodies[f]
+        pk.bodies["force"] = 0.0
+        pk.bodies["torque"] = 0.0
+        pk.contacts["flags"] = pk.out_contacts["flags"]
+        pk.contacts["points"]["normal_impulse"] = pk.out_contacts["points"]["normal_impulse"]
+        pk.contacts["points"]["tangent_impulse"] = pk.out_contacts["points"]["tangent_impulse"]
+        for f in abi_joint_outputs():
+            pk.joints[f] = pk.out_joints[f]
+
+    solver.phys_solve_packed(pk, params, DT)
+    carry()
+    barrier(pg)
+    total = 0.0
+    for _ in range(steps):
+        total += _timed_calls(lambda: solver.phys_solve_packed(pk, params, DT), 1, None)
+        carry()
+    return max_over_ranks(pg, total / max(steps, 1))
+
+
+def abi_joint_outputs():
+    from nepheline_b200 import abi
+    return abi.JOINT_OUTPUT_DTYPE.names
+
 def reference_sample(dims, steps: int, warmup: int, workers: int, params) -> dict:
     """The reference's phys_solve on its job system over a dims lattice (the same scene)."""
     from oracle.refworld import lattice_world
@@ -845,24 +908,15 @@ def main():
                 "ms_per_launch": per_launch_ms, "algorithmic_bytes_per_launch": per_launch_bytes,
                 "kernel_share": top[1]["total_ms"] / sum(v["total_ms"] for v in kinds.values())}
 
-    # End to end through the drop-in call on pinned host records.
+    # End to end through the drop-in call on pinned host records: the packed call (the fields
+    # the stage reads up, the fields it writes back), and the whole-record call beside it.
     pv = pinned_copy(view)
-    h2d = pv.bodies.nbytes + pv.contacts.nbytes + pv.joints.nbytes + pv.fixed.nbytes
-    d2h = pv.bodies.nbytes + pv.contacts.nbytes + pv.joints.nbytes
-    solver.phys_solve(pv, params, DT)
-    torch.cuda.synchronize()
-    barrier(pg)
-    s0 = torch.cuda.Event(enable_timing=True)
-    s1 = torch.cuda.Event(enable_timing=True)
-    t0 = time.perf_counter()
-    s0.record(stream)
-    for _ in range(args.e2e_steps):
-        solver.phys_solve(pv, params, DT)
-    s1.record(stream)
-    torch.cuda.synchronize()
-    wall = (time.perf_counter() - t0) / args.e2e_steps
-    e2e_ms = max(s0.elapsed_time(s1) / args.e2e_steps, wall * 1e3)
-    e2e_ms = max_over_ranks(pg, e2e_ms)
+    h2d_whole = pv.bodies.nbytes + pv.contacts.nbytes + pv.joints.nbytes + pv.fixed.nbytes
+    d2h_whole = pv.bodies.nbytes + pv.contacts.nbytes + pv.joints.nbytes
+    whole_ms = e2e_whole(solver, pv, params, args.e2e_steps, pg)
+    pk = abi.Packed(view, alloc=pinned_alloc)
+    h2d, d2h = pk.input_bytes(), pk.output_bytes()
+    e2e_ms = e2e_packed(solver, pk, params, args.e2e_steps, pg)
     e2e_value = world * solves_per_step / (e2e_ms * 1e-3)
 
     cpu = None
@@ -908,7 +962,12 @@ def main():
                        "pass_configs": tuned,
                        "l2": "inputs larger than L2 (about 2 GB of manifold rows per step)"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms},
+                    "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms,
+                    "call": "nph_gpu_phys_solve_packed on page-locked host records"},
+            "e2e_whole_records": {"value": world * solves_per_step / (whole_ms * 1e-3), "unit": UNIT,
+                                  "h2d_bytes_per_step": int(h2d_whole),
+                                  "d2h_bytes_per_step": int(d2h_whole), "ms_per_step": whole_ms,
+                                  "call": "nph_gpu_phys_solve on page-locked host records"},
             "gpu_launches": int(stats.launches) * args.steps,
             "roofline": roofline,
             "cpu_baseline": cpu,

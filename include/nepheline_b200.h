@@ -319,6 +319,108 @@ typedef struct NphGpuWorldView {
     uint32_t joint_color_counts[NPH_GPU_COLOR_SLOTS];
 } NphGpuWorldView;
 
+/* The packed records of nph_gpu_phys_solve_packed: the fields the solver stage reads of a
+ * body and of a contact (NphGpuBody and NphGpuContact without what the stage only writes or
+ * never reads), and the fields it writes of a body, a contact and a joint. */
+typedef struct NphGpuBodyInput {
+    double center[3];
+    float rotation[4];
+    float local_center[3];
+    float linear_velocity[3];
+    float angular_velocity[3];
+    float force[3];
+    float torque[3];
+    float inertia[9];
+    float inv_inertia[9];
+    float inv_mass;
+    float linear_damping;
+    float angular_damping;
+    float gravity_scale;
+    float sleep_threshold;
+    float sleep_time;
+    float max_extent;
+    uint32_t type;
+    uint32_t flags;
+    uint32_t locks;
+    uint32_t pad;
+} NphGpuBodyInput;
+
+typedef struct NphGpuContactPointInput {
+    float anchor_a[3];
+    float anchor_b[3];
+    float separation;
+    float normal_impulse;      /* the warm start */
+    float tangent_impulse[3];  /* the warm start: world vector */
+    uint32_t id;               /* kept on the device for a later nph_gpu_world_update_contacts */
+} NphGpuContactPointInput;
+
+typedef struct NphGpuContactInput {
+    uint32_t body_a;
+    uint32_t body_b;
+    uint32_t flags;
+    uint32_t point_count;
+    float normal[3];
+    float friction;
+    float restitution;
+    NphGpuContactPointInput points[NPH_GPU_MAX_POINTS];
+} NphGpuContactInput;
+
+/* After the step: force and torque are zero, as phys_solve leaves them (the caller clears its
+ * own; they are not sent back). */
+typedef struct NphGpuBodyOutput {
+    double center[3];
+    double origin[3];
+    float rotation[4];
+    float linear_velocity[3];
+    float angular_velocity[3];
+    float sleep_time;
+    uint32_t pad;
+} NphGpuBodyOutput;
+
+typedef struct NphGpuContactPointOutput {
+    float normal_impulse;
+    float max_normal_impulse;
+    float tangent_impulse[3];
+    float relative_velocity;
+} NphGpuContactPointOutput;
+
+typedef struct NphGpuContactOutput {
+    uint32_t flags; /* the input's flags with NPH_GPU_CONTACT_HIT as the step leaves it */
+    NphGpuContactPointOutput points[NPH_GPU_MAX_POINTS]; /* the first point_count are live */
+} NphGpuContactOutput;
+
+typedef struct NphGpuJointOutput {
+    float linear_impulse[3];
+    float angular_impulse[3];
+    float friction_impulse[3];
+    float lower_impulse;
+    float upper_impulse;
+    float swing_impulse;
+    float motor_impulse;
+    float spring_impulse;
+    float axis_impulse[NPH_GPU_D6_AXES][4];
+    uint32_t flags; /* NPH_GPU_JOINT_BLOCK_* as the step leaves them */
+} NphGpuJointOutput;
+
+typedef struct NphGpuPackedInput {
+    const NphGpuBodyInput *bodies;      /* awake bodies, awake-list order */
+    uint32_t body_count;
+    uint32_t fixed_count;
+    const NphGpuBody *fixed_bodies;     /* bodies without a solver slot, read only */
+    const NphGpuContactInput *contacts; /* colour order */
+    uint32_t contact_count;
+    uint32_t joint_count;
+    const NphGpuJoint *joints;          /* colour order, whole records (settings and impulses) */
+    uint32_t contact_color_counts[NPH_GPU_COLOR_SLOTS];
+    uint32_t joint_color_counts[NPH_GPU_COLOR_SLOTS];
+} NphGpuPackedInput;
+
+typedef struct NphGpuPackedOutput {
+    NphGpuBodyOutput *bodies;       /* body_count records */
+    NphGpuContactOutput *contacts;  /* contact_count records */
+    NphGpuJointOutput *joints;      /* joint_count records */
+} NphGpuPackedOutput;
+
 /* What a step reports (a subset of NphPhysicsStats, world.h:250-278). */
 typedef struct NphGpuStepStats {
     uint32_t colors_used;           /* colours holding contacts or joints */
@@ -365,6 +467,17 @@ NPH_GPU_API void nph_gpu_solver_destroy(NphGpuSolver *solver);
  * NPH_GPU_DEVICE_LOST when a device wait gave up or the device reported an error. */
 NPH_GPU_API NphGpuResult nph_gpu_phys_solve(NphGpuSolver *solver, const NphGpuWorldParams *params,
                                             float dt, NphGpuWorldView *view);
+
+/* nph_gpu_phys_solve on packed records: the host arrays hold only the fields the stage reads
+ * (in) and writes (out), so each step moves about 1.5 GB over PCIe for the 1,048,576-body
+ * lattice instead of 2.5 GB of whole records. The records are expanded and packed on the
+ * device; the results equal nph_gpu_phys_solve's field for field. The same refusals, with the
+ * outputs untouched. A caller that keeps its world in other records (the engine's own) gathers
+ * the inputs from them and scatters the outputs back, as it would for the whole records. */
+NPH_GPU_API NphGpuResult nph_gpu_phys_solve_packed(NphGpuSolver *solver,
+                                                   const NphGpuWorldParams *params, float dt,
+                                                   const NphGpuPackedInput *in,
+                                                   NphGpuPackedOutput *out);
 
 /* Device-resident stepping: the view's records are uploaded once, stepped `steps` times on
  * the device (each step the whole solver stage over the resident records: the manifolds'

@@ -341,10 +341,139 @@ class View:
         return int(self.contacts["point_count"].sum())
 
 
+# The packed drop-in's records (nph_gpu_phys_solve_packed): the fields the stage reads, and the
+# fields it writes.
+BODY_INPUT_DTYPE = np.dtype([
+    ("center", "<f8", 3), ("rotation", "<f4", 4), ("local_center", "<f4", 3),
+    ("linear_velocity", "<f4", 3), ("angular_velocity", "<f4", 3), ("force", "<f4", 3),
+    ("torque", "<f4", 3), ("inertia", "<f4", 9), ("inv_inertia", "<f4", 9), ("inv_mass", "<f4"),
+    ("linear_damping", "<f4"), ("angular_damping", "<f4"), ("gravity_scale", "<f4"),
+    ("sleep_threshold", "<f4"), ("sleep_time", "<f4"), ("max_extent", "<f4"), ("type", "<u4"),
+    ("flags", "<u4"), ("locks", "<u4"), ("pad", "<u4"),
+], align=True)
+POINT_INPUT_DTYPE = np.dtype([
+    ("anchor_a", "<f4", 3), ("anchor_b", "<f4", 3), ("separation", "<f4"),
+    ("normal_impulse", "<f4"), ("tangent_impulse", "<f4", 3), ("id", "<u4"),
+])
+CONTACT_INPUT_DTYPE = np.dtype([
+    ("body_a", "<u4"), ("body_b", "<u4"), ("flags", "<u4"), ("point_count", "<u4"),
+    ("normal", "<f4", 3), ("friction", "<f4"), ("restitution", "<f4"),
+    ("points", POINT_INPUT_DTYPE, MAX_POINTS),
+])
+BODY_OUTPUT_DTYPE = np.dtype([
+    ("center", "<f8", 3), ("origin", "<f8", 3), ("rotation", "<f4", 4),
+    ("linear_velocity", "<f4", 3), ("angular_velocity", "<f4", 3), ("sleep_time", "<f4"),
+    ("pad", "<u4"),
+], align=True)
+POINT_OUTPUT_DTYPE = np.dtype([
+    ("normal_impulse", "<f4"), ("max_normal_impulse", "<f4"), ("tangent_impulse", "<f4", 3),
+    ("relative_velocity", "<f4"),
+])
+CONTACT_OUTPUT_DTYPE = np.dtype([("flags", "<u4"), ("points", POINT_OUTPUT_DTYPE, MAX_POINTS)])
+JOINT_OUTPUT_DTYPE = np.dtype([
+    ("linear_impulse", "<f4", 3), ("angular_impulse", "<f4", 3), ("friction_impulse", "<f4", 3),
+    ("lower_impulse", "<f4"), ("upper_impulse", "<f4"), ("swing_impulse", "<f4"),
+    ("motor_impulse", "<f4"), ("spring_impulse", "<f4"), ("axis_impulse", "<f4", (D6_AXES, 4)),
+    ("flags", "<u4"),
+])
+
+
+class PackedInput(ctypes.Structure):
+    """NphGpuPackedInput."""
+
+    _fields_ = [
+        ("bodies", ctypes.c_void_p), ("body_count", ctypes.c_uint32),
+        ("fixed_count", ctypes.c_uint32), ("fixed_bodies", ctypes.c_void_p),
+        ("contacts", ctypes.c_void_p), ("contact_count", ctypes.c_uint32),
+        ("joint_count", ctypes.c_uint32), ("joints", ctypes.c_void_p),
+        ("contact_color_counts", ctypes.c_uint32 * COLOR_SLOTS),
+        ("joint_color_counts", ctypes.c_uint32 * COLOR_SLOTS),
+    ]
+
+
+class PackedOutput(ctypes.Structure):
+    """NphGpuPackedOutput."""
+
+    _fields_ = [("bodies", ctypes.c_void_p), ("contacts", ctypes.c_void_p),
+                ("joints", ctypes.c_void_p)]
+
+
+class Packed:
+    """A view's packed records: the stage's inputs gathered from the whole records, and the
+    output arrays a packed solve fills (`alloc` makes the arrays, e.g. in page-locked memory)."""
+
+    def __init__(self, view: "View", alloc=None):
+        alloc = alloc or (lambda n, dt: np.zeros(n, dt))
+        self.bodies = alloc(len(view.bodies), BODY_INPUT_DTYPE)
+        self.contacts = alloc(len(view.contacts), CONTACT_INPUT_DTYPE)
+        self.fixed = alloc(len(view.fixed), BODY_DTYPE)
+        self.fixed[...] = view.fixed
+        self.joints = alloc(len(view.joints), JOINT_DTYPE)
+        self.counts = (view.contact_color_counts.copy(), view.joint_color_counts.copy())
+        self.out_bodies = alloc(len(view.bodies), BODY_OUTPUT_DTYPE)
+        self.out_contacts = alloc(len(view.contacts), CONTACT_OUTPUT_DTYPE)
+        self.out_joints = alloc(len(view.joints), JOINT_OUTPUT_DTYPE)
+        self.gather(view)
+
+    def gather(self, view: "View") -> None:
+        for f in BODY_INPUT_DTYPE.names:
+            if f != "pad":
+                self.bodies[f] = view.bodies[f]
+        for f in ("body_a", "body_b", "flags", "point_count", "normal", "friction", "restitution"):
+            self.contacts[f] = view.contacts[f]
+        for f in POINT_INPUT_DTYPE.names:
+            self.contacts["points"][f] = view.contacts["points"][f]
+        self.joints[...] = view.joints
+
+    def scatter(self, view: "View") -> None:
+        """The outputs into the whole records, as a whole-record solve leaves them."""
+        for f in ("center", "origin", "rotation", "linear_velocity", "angular_velocity", "sleep_time"):
+            view.bodies[f] = self.out_bodies[f]
+        view.bodies["force"] = 0.0
+        view.bodies["torque"] = 0.0
+        view.contacts["flags"] = self.out_contacts["flags"]
+        for f in POINT_OUTPUT_DTYPE.names:
+            view.contacts["points"][f] = self.out_contacts["points"][f]
+        for f in JOINT_OUTPUT_DTYPE.names:
+            view.joints[f] = self.out_joints[f]
+
+    def c_input(self) -> PackedInput:
+        c = PackedInput()
+        c.bodies = _ptr(self.bodies)
+        c.body_count = len(self.bodies)
+        c.fixed_bodies = _ptr(self.fixed)
+        c.fixed_count = len(self.fixed)
+        c.contacts = _ptr(self.contacts)
+        c.contact_count = len(self.contacts)
+        c.joints = _ptr(self.joints)
+        c.joint_count = len(self.joints)
+        c.contact_color_counts[:] = [int(x) for x in self.counts[0]]
+        c.joint_color_counts[:] = [int(x) for x in self.counts[1]]
+        return c
+
+    def c_output(self) -> PackedOutput:
+        c = PackedOutput()
+        c.bodies = _ptr(self.out_bodies)
+        c.contacts = _ptr(self.out_contacts)
+        c.joints = _ptr(self.out_joints)
+        return c
+
+    def input_bytes(self) -> int:
+        return self.bodies.nbytes + self.contacts.nbytes + self.joints.nbytes + self.fixed.nbytes
+
+    def output_bytes(self) -> int:
+        return self.out_bodies.nbytes + self.out_contacts.nbytes + self.out_joints.nbytes
+
+
 def layout_sizes() -> dict:
     return {"body": BODY_DTYPE.itemsize, "point": POINT_DTYPE.itemsize,
             "contact": CONTACT_DTYPE.itemsize, "joint": JOINT_DTYPE.itemsize,
-            "params": ctypes.sizeof(WorldParams), "view": ctypes.sizeof(WorldView)}
+            "params": ctypes.sizeof(WorldParams), "view": ctypes.sizeof(WorldView),
+            "body_input": BODY_INPUT_DTYPE.itemsize, "contact_input": CONTACT_INPUT_DTYPE.itemsize,
+            "body_output": BODY_OUTPUT_DTYPE.itemsize,
+            "contact_output": CONTACT_OUTPUT_DTYPE.itemsize,
+            "joint_output": JOINT_OUTPUT_DTYPE.itemsize,
+            "packed_input": ctypes.sizeof(PackedInput), "packed_output": ctypes.sizeof(PackedOutput)}
 
 
 def views_array(views: list) -> np.ndarray:

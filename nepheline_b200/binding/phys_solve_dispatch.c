@@ -7,7 +7,8 @@
 //
 // so the solver stage's one call (world.c:346) comes here, with no edit to the engine's
 // sources. phys_solve_dispatch does what phys_solve (solver.c:961-1105) does, in its order:
-// the stage's arithmetic on the device (nph_gpu_phys_solve over the world's view), its results
+// the stage's arithmetic on the device (nph_gpu_phys_solve_packed over the world's packed
+// records: only the fields the stage reads go up, only those it writes come back), its results
 // written back into the world (finalize_body, store_group, the joints' impulses, the box
 // refresh), then the host work after the arithmetic: post_finalize (solver.c:847-917: driven
 // joints keep their bodies awake, the CCD flags cleared, enlarged proxies grown, one move event
@@ -24,16 +25,19 @@
 #include <nepheline/physics/world.h>
 #include <nepheline/platform/time.h>
 
-// The view's arrays, kept between steps and grown as the world grows.
+// The packed records' arrays, kept between steps and grown as the world grows.
 typedef struct Binding {
     NphGpuSolver *solver;
     NphViewMap map;
-    NphGpuBody *bodies;
+    NphGpuBodyInput *bodies;
     NphGpuBody *fixed;
-    NphGpuContact *contacts;
+    NphGpuContactInput *contacts;
     NphGpuJoint *joints;
+    NphGpuBodyOutput *out_bodies;
+    NphGpuContactOutput *out_contacts;
+    NphGpuJointOutput *out_joints;
     NphGpuHitEvent *hits;
-    u32 body_cap, fixed_cap, contact_cap, joint_cap, hit_cap;
+    u32 body_cap, fixed_cap, contact_cap, joint_cap, out_body_cap, out_contact_cap, out_joint_cap, hit_cap;
 } Binding;
 
 static Binding g_binding;
@@ -50,6 +54,9 @@ void nph_gpu_binding_release(void)
     free(g_binding.fixed);
     free(g_binding.contacts);
     free(g_binding.joints);
+    free(g_binding.out_bodies);
+    free(g_binding.out_contacts);
+    free(g_binding.out_joints);
     free(g_binding.hits);
     memset(&g_binding, 0, sizeof g_binding);
 }
@@ -190,26 +197,28 @@ NphResult phys_solve_dispatch(NphPhysicsWorld *w, f32 dt, NphJobSystem *js)
     }
     u32 nb = 0U, nf = 0U, nc = 0U, nj = 0U;
     NPH_TRY(nph_view_sizes(w, &g->map, &nb, &nf, &nc, &nj));
-    NPH_TRY(reserve((void **)&g->bodies, &g->body_cap, nb, sizeof(NphGpuBody)));
+    NPH_TRY(reserve((void **)&g->bodies, &g->body_cap, nb, sizeof(NphGpuBodyInput)));
     NPH_TRY(reserve((void **)&g->fixed, &g->fixed_cap, nf, sizeof(NphGpuBody)));
-    NPH_TRY(reserve((void **)&g->contacts, &g->contact_cap, nc, sizeof(NphGpuContact)));
+    NPH_TRY(reserve((void **)&g->contacts, &g->contact_cap, nc, sizeof(NphGpuContactInput)));
     NPH_TRY(reserve((void **)&g->joints, &g->joint_cap, nj, sizeof(NphGpuJoint)));
+    NPH_TRY(reserve((void **)&g->out_bodies, &g->out_body_cap, nb, sizeof(NphGpuBodyOutput)));
+    NPH_TRY(reserve((void **)&g->out_contacts, &g->out_contact_cap, nc, sizeof(NphGpuContactOutput)));
+    NPH_TRY(reserve((void **)&g->out_joints, &g->out_joint_cap, nj, sizeof(NphGpuJointOutput)));
     NPH_TRY(reserve((void **)&g->hits, &g->hit_cap, nc, sizeof(NphGpuHitEvent)));
-    NphGpuWorldView v;
-    memset(&v, 0, sizeof v);
-    v.bodies = g->bodies;
-    v.fixed_bodies = g->fixed;
-    v.contacts = g->contacts;
-    v.joints = g->joints;
-    if (nph_view_export(w, &g->map, &v) != 0) {
+    NphGpuPackedInput in;
+    if (nph_view_export_packed(w, &g->map, g->bodies, g->fixed, g->contacts, g->joints, &in) != 0) {
         return NPH_RESULT_INVALID_STATE;
     }
+    NphGpuPackedOutput out;
+    out.bodies = g->out_bodies;
+    out.contacts = g->out_contacts;
+    out.joints = g->out_joints;
     const NphGpuWorldParams p = params_from_desc(&w->desc);
-    const NphGpuResult r = nph_gpu_phys_solve(g->solver, &p, dt, &v);
+    const NphGpuResult r = nph_gpu_phys_solve_packed(g->solver, &p, dt, &in, &out);
     if (r != NPH_GPU_OK) {
         return (NphResult)r; // the world is untouched: the step did not happen
     }
-    NPH_TRY(nph_view_import(w, &v, dt));
+    NPH_TRY(nph_view_import_packed(w, &out, in.body_count, dt));
     w->stats.workers = 1U;
     const u64 t = nph_time_now_ns();
     NPH_TRY(post_finalize(w));

@@ -352,6 +352,157 @@ static inline NphResult nph_view_import(NphPhysicsWorld *w, const NphGpuWorldVie
     return NPH_RESULT_OK;
 }
 
+// The packed records of nph_gpu_phys_solve_packed, gathered straight from the world: the fields
+// the stage reads.
+static inline void nph_view_body_input(const PhysBody *b, NphGpuBodyInput *o)
+{
+    o->center[0] = b->center.x;
+    o->center[1] = b->center.y;
+    o->center[2] = b->center.z;
+    memcpy(o->rotation, &b->rotation, sizeof o->rotation);
+    memcpy(o->local_center, &b->local_center, sizeof o->local_center);
+    memcpy(o->linear_velocity, &b->linear_velocity, sizeof o->linear_velocity);
+    memcpy(o->angular_velocity, &b->angular_velocity, sizeof o->angular_velocity);
+    memcpy(o->force, &b->force, sizeof o->force);
+    memcpy(o->torque, &b->torque, sizeof o->torque);
+    memcpy(o->inertia, &b->inertia, sizeof o->inertia);
+    memcpy(o->inv_inertia, &b->inv_inertia, sizeof o->inv_inertia);
+    o->inv_mass = b->inv_mass;
+    o->linear_damping = b->linear_damping;
+    o->angular_damping = b->angular_damping;
+    o->gravity_scale = b->gravity_scale;
+    o->sleep_threshold = b->sleep_threshold;
+    o->sleep_time = b->sleep_time;
+    o->max_extent = b->max_extent;
+    o->type = b->type;
+    o->flags = b->flags;
+    o->locks = b->locks;
+    o->pad = 0U;
+}
+
+static inline void nph_view_contact_input(const NphPhysicsWorld *w, NphViewMap *m, const PhysContact *c,
+                                          NphGpuContactInput *o, u32 *fixed_count)
+{
+    memset(o, 0, sizeof *o);
+    o->body_a = nph_view_index(w, m, c->body_a, fixed_count);
+    o->body_b = nph_view_index(w, m, c->body_b, fixed_count);
+    o->flags = c->flags & (PHYS_CONTACT_HIT | PHYS_CONTACT_HIT_EVENTS);
+    o->point_count = c->point_count;
+    memcpy(o->normal, &c->normal, sizeof o->normal);
+    o->friction = c->friction;
+    o->restitution = c->restitution;
+    for (u32 k = 0U; k < c->point_count; ++k) {
+        const PhysContactPoint *p = &c->points[k];
+        NphGpuContactPointInput *q = &o->points[k];
+        memcpy(q->anchor_a, &p->anchor_a, sizeof q->anchor_a);
+        memcpy(q->anchor_b, &p->anchor_b, sizeof q->anchor_b);
+        q->separation = p->separation;
+        q->normal_impulse = p->normal_impulse;
+        memcpy(q->tangent_impulse, &p->tangent_impulse, sizeof q->tangent_impulse);
+        q->id = p->id;
+    }
+}
+
+// Fills the packed input (its arrays sized by nph_view_sizes with the same map; joints and fixed
+// bodies as whole records). Returns 0, or 1 when the world changed since the sizes were taken.
+static inline int nph_view_export_packed(const NphPhysicsWorld *w, NphViewMap *m, NphGpuBodyInput *bodies,
+                                         NphGpuBody *fixed_bodies, NphGpuContactInput *contacts,
+                                         NphGpuJoint *joints, NphGpuPackedInput *in)
+{
+    u32 fixed = 0U;
+    if (nph_view_map_fixed(w, m, &fixed) != NPH_RESULT_OK) {
+        return 1;
+    }
+    memset(in, 0, sizeof *in);
+    in->bodies = bodies;
+    in->fixed_bodies = fixed_bodies;
+    in->contacts = contacts;
+    in->joints = joints;
+    in->body_count = w->awake_bodies.len;
+    for (u32 i = 0U; i < w->awake_bodies.len; ++i) {
+        nph_view_body_input(&w->bodies.data[w->awake_bodies.data[i]], &bodies[i]);
+    }
+    in->fixed_count = fixed;
+    for (u32 i = 0U; i < fixed; ++i) {
+        nph_view_body_record(&w->bodies.data[m->fixed_slots[i]], &fixed_bodies[i]);
+    }
+    u32 nc = 0U;
+    u32 nj = 0U;
+    u32 again = fixed;
+    for (u32 c = 0U; c <= PHYS_GRAPH_COLORS; ++c) {
+        const NphArrayU32 *list = nph_view_contact_list(w, c);
+        in->contact_color_counts[c] = list->len;
+        for (u32 i = 0U; i < list->len; ++i) {
+            nph_view_contact_input(w, m, &w->contacts.data[list->data[i]], &contacts[nc++], &again);
+        }
+        const NphArrayU32 *jl = nph_view_joint_list(w, c);
+        in->joint_color_counts[c] = jl->len;
+        for (u32 i = 0U; i < jl->len; ++i) {
+            nph_view_joint_record(w, m, &w->joints.data[jl->data[i]], &joints[nj++], &again);
+        }
+    }
+    in->contact_count = nc;
+    in->joint_count = nj;
+    return again == fixed ? 0 : 1;
+}
+
+// Writes the packed outputs back into the world, as nph_view_import does the whole records'.
+static inline NphResult nph_view_import_packed(NphPhysicsWorld *w, const NphGpuPackedOutput *out,
+                                               u32 body_count, f32 dt)
+{
+    if (body_count != w->awake_bodies.len) {
+        return NPH_RESULT_INVALID_STATE;
+    }
+    for (u32 i = 0U; i < body_count; ++i) {
+        PhysBody *b = &w->bodies.data[w->awake_bodies.data[i]];
+        const NphGpuBodyOutput *o = &out->bodies[i];
+        b->center = nph_dvec3(o->center[0], o->center[1], o->center[2]);
+        b->origin = nph_dvec3(o->origin[0], o->origin[1], o->origin[2]);
+        memcpy(&b->rotation, o->rotation, sizeof o->rotation);
+        memcpy(&b->linear_velocity, o->linear_velocity, sizeof o->linear_velocity);
+        memcpy(&b->angular_velocity, o->angular_velocity, sizeof o->angular_velocity);
+        b->force = nph_vec3_zero();
+        b->torque = nph_vec3_zero();
+        b->sleep_time = o->sleep_time;
+        phys_body_refresh_boxes(w, b);
+    }
+    u32 nc = 0U;
+    u32 nj = 0U;
+    for (u32 c = 0U; c <= PHYS_GRAPH_COLORS; ++c) {
+        const NphArrayU32 *list = nph_view_contact_list(w, c);
+        for (u32 i = 0U; i < list->len; ++i) {
+            PhysContact *ct = &w->contacts.data[list->data[i]];
+            const NphGpuContactOutput *o = &out->contacts[nc++];
+            ct->flags = (ct->flags & ~(u32)PHYS_CONTACT_HIT) | (o->flags & PHYS_CONTACT_HIT);
+            for (u32 k = 0U; k < ct->point_count; ++k) {
+                PhysContactPoint *p = &ct->points[k];
+                p->normal_impulse = o->points[k].normal_impulse;
+                p->max_normal_impulse = o->points[k].max_normal_impulse;
+                p->relative_velocity = o->points[k].relative_velocity;
+                memcpy(&p->tangent_impulse, o->points[k].tangent_impulse,
+                       sizeof o->points[k].tangent_impulse);
+            }
+        }
+        const NphArrayU32 *jl = nph_view_joint_list(w, c);
+        for (u32 i = 0U; i < jl->len; ++i) {
+            PhysJoint *j = &w->joints.data[jl->data[i]];
+            const NphGpuJointOutput *o = &out->joints[nj++];
+            memcpy(&j->linear_impulse, o->linear_impulse, sizeof o->linear_impulse);
+            memcpy(&j->angular_impulse, o->angular_impulse, sizeof o->angular_impulse);
+            memcpy(&j->friction_impulse, o->friction_impulse, sizeof o->friction_impulse);
+            j->lower_impulse = o->lower_impulse;
+            j->upper_impulse = o->upper_impulse;
+            j->swing_impulse = o->swing_impulse;
+            j->motor_impulse = o->motor_impulse;
+            j->spring_impulse = o->spring_impulse;
+            memcpy(j->axis_impulse, o->axis_impulse, sizeof o->axis_impulse);
+            j->flags = (j->flags & ~(u32)NPH_VIEW_JOINT_BLOCKS) | (o->flags & NPH_VIEW_JOINT_BLOCKS);
+        }
+    }
+    w->last_substep = dt / (f32)w->desc.substeps;
+    return NPH_RESULT_OK;
+}
+
 // The finalize pass's proxy growth (solver.c:867-878) for one awake body: shapes whose boxes
 // left their proxies get them enlarged and pushed onto the move buffer.
 static inline NphResult nph_view_grow_proxies(NphPhysicsWorld *w, PhysBody *b)

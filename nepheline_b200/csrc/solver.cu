@@ -527,6 +527,159 @@ __global__ void __launch_bounds__(kStage) k_finalize(BodyArrays B, NphGpuBody *b
     stage_out<uint4>(rec, count, bodies + first);
 }
 
+// The packed drop-in's conversions (nph_gpu_phys_solve_packed): a block stages its records
+// through shared memory in 4-byte words both ways, so the global reads and writes are
+// coalesced whatever the records' sizes.
+constexpr uint32_t kConvert = 64;
+static_assert(sizeof(NphGpuBodyInput) % 4 == 0 && sizeof(NphGpuContactInput) % 4 == 0 &&
+                  sizeof(NphGpuBodyOutput) % 4 == 0 && sizeof(NphGpuContactOutput) % 4 == 0 &&
+                  sizeof(NphGpuJointOutput) % 4 == 0 && sizeof(NphGpuJoint) % 4 == 0,
+              "packed records stage in 4-byte words");
+
+__device__ void expand_body(const NphGpuBodyInput &i, NphGpuBody &o)
+{
+    for (uint32_t k = 0; k < 3u; ++k) {
+        o.center[k] = i.center[k];
+        o.origin[k] = 0.0;
+        o.local_center[k] = i.local_center[k];
+        o.linear_velocity[k] = i.linear_velocity[k];
+        o.angular_velocity[k] = i.angular_velocity[k];
+        o.force[k] = i.force[k];
+        o.torque[k] = i.torque[k];
+    }
+    for (uint32_t k = 0; k < 4u; ++k) {
+        o.rotation[k] = i.rotation[k];
+    }
+    for (uint32_t k = 0; k < 9u; ++k) {
+        o.inertia[k] = i.inertia[k];
+        o.inv_inertia[k] = i.inv_inertia[k];
+    }
+    o.inv_mass = i.inv_mass;
+    o.linear_damping = i.linear_damping;
+    o.angular_damping = i.angular_damping;
+    o.gravity_scale = i.gravity_scale;
+    o.sleep_threshold = i.sleep_threshold;
+    o.sleep_time = i.sleep_time;
+    o.max_extent = i.max_extent;
+    o.type = i.type;
+    o.flags = i.flags;
+    o.locks = i.locks;
+    o.pad = 0u;
+}
+
+__device__ void expand_contact(const NphGpuContactInput &i, NphGpuContact &o)
+{
+    o.body_a = i.body_a;
+    o.body_b = i.body_b;
+    o.flags = i.flags;
+    o.point_count = i.point_count;
+    for (uint32_t k = 0; k < 3u; ++k) {
+        o.normal[k] = i.normal[k];
+    }
+    o.friction = i.friction;
+    o.restitution = i.restitution;
+    o.pad[0] = o.pad[1] = o.pad[2] = 0u;
+    for (uint32_t p = 0; p < NPH_GPU_MAX_POINTS; ++p) {
+        const NphGpuContactPointInput &a = i.points[p];
+        NphGpuContactPoint &b = o.points[p];
+        for (uint32_t k = 0; k < 3u; ++k) {
+            b.anchor_a[k] = a.anchor_a[k];
+            b.anchor_b[k] = a.anchor_b[k];
+            b.tangent_impulse[k] = a.tangent_impulse[k];
+        }
+        b.separation = a.separation;
+        b.normal_impulse = a.normal_impulse;
+        b.max_normal_impulse = 0.0f;
+        b.relative_velocity = 0.0f;
+        b.id = a.id;
+    }
+}
+
+__device__ void pack_body(const NphGpuBody &i, NphGpuBodyOutput &o)
+{
+    for (uint32_t k = 0; k < 3u; ++k) {
+        o.center[k] = i.center[k];
+        o.origin[k] = i.origin[k];
+        o.linear_velocity[k] = i.linear_velocity[k];
+        o.angular_velocity[k] = i.angular_velocity[k];
+    }
+    for (uint32_t k = 0; k < 4u; ++k) {
+        o.rotation[k] = i.rotation[k];
+    }
+    o.sleep_time = i.sleep_time;
+    o.pad = 0u;
+}
+
+__device__ void pack_contact(const NphGpuContact &i, NphGpuContactOutput &o)
+{
+    o.flags = i.flags;
+    for (uint32_t p = 0; p < NPH_GPU_MAX_POINTS; ++p) {
+        const NphGpuContactPoint &a = i.points[p];
+        NphGpuContactPointOutput &b = o.points[p];
+        b.normal_impulse = a.normal_impulse;
+        b.max_normal_impulse = a.max_normal_impulse;
+        for (uint32_t k = 0; k < 3u; ++k) {
+            b.tangent_impulse[k] = a.tangent_impulse[k];
+        }
+        b.relative_velocity = a.relative_velocity;
+    }
+}
+
+__device__ void pack_joint(const NphGpuJoint &i, NphGpuJointOutput &o)
+{
+    for (uint32_t k = 0; k < 3u; ++k) {
+        o.linear_impulse[k] = i.linear_impulse[k];
+        o.angular_impulse[k] = i.angular_impulse[k];
+        o.friction_impulse[k] = i.friction_impulse[k];
+    }
+    o.lower_impulse = i.lower_impulse;
+    o.upper_impulse = i.upper_impulse;
+    o.swing_impulse = i.swing_impulse;
+    o.motor_impulse = i.motor_impulse;
+    o.spring_impulse = i.spring_impulse;
+    for (uint32_t a = 0; a < NPH_GPU_D6_AXES; ++a) {
+        for (uint32_t r = 0; r < 4u; ++r) {
+            o.axis_impulse[a][r] = i.axis_impulse[a][r];
+        }
+    }
+    o.flags = i.flags;
+}
+
+// Records of type In to records of type Out, kConvert a block.
+template <typename In, typename Out, int kKind>
+__global__ void __launch_bounds__(kConvert) k_convert(const In *in, Out *out, uint32_t count)
+{
+    __shared__ In src[kConvert];
+    __shared__ Out dst[kConvert];
+    const uint32_t first = blockIdx.x * kConvert;
+    const uint32_t n = min(kConvert, count - first);
+    stage_in<uint32_t>(in + first, n, src);
+    __syncthreads();
+    if (threadIdx.x < n) {
+        if constexpr (kKind == 0) {
+            expand_body(src[threadIdx.x], dst[threadIdx.x]);
+        } else if constexpr (kKind == 1) {
+            expand_contact(src[threadIdx.x], dst[threadIdx.x]);
+        } else if constexpr (kKind == 2) {
+            pack_body(src[threadIdx.x], dst[threadIdx.x]);
+        } else if constexpr (kKind == 3) {
+            pack_contact(src[threadIdx.x], dst[threadIdx.x]);
+        } else {
+            pack_joint(src[threadIdx.x], dst[threadIdx.x]);
+        }
+    }
+    __syncthreads();
+    stage_out<uint32_t>(dst, n, out + first);
+}
+
+template <typename In, typename Out, int kKind>
+void launch_convert(const In *in, Out *out, uint32_t count, cudaStream_t st)
+{
+    if (count > 0u) {
+        k_convert<In, Out, kKind><<<(count + kConvert - 1u) / kConvert, kConvert, 0, st>>>(in, out, count);
+    }
+}
+
 // post_finalize, solver.c:851-857: a driven joint's bodies stay awake.
 __global__ void __launch_bounds__(kBlock) k_driven(DevSolver S, NphGpuBody *bodies, uint32_t n,
                                                    uint32_t nj)
@@ -791,6 +944,13 @@ struct NphGpuSolver {
     // Capacities of the device arrays.
     uint32_t bcap = 0, fcap = 0, mcap = 0, jcap = 0;
     uint64_t memory_limit = 0; // bytes the record and row arrays may take (0: no limit)
+    // The packed drop-in's device arrays (allocated by its first call).
+    NphGpuBodyInput *in_bodies = nullptr;
+    NphGpuContactInput *in_contacts = nullptr;
+    NphGpuBodyOutput *out_bodies = nullptr;
+    NphGpuContactOutput *out_contacts = nullptr;
+    NphGpuJointOutput *out_joints = nullptr;
+    uint32_t pbcap = 0, pmcap = 0, pjcap = 0;
     // Records (device copies of the view's arrays).
     NphGpuBody *d_bodies = nullptr;
     NphGpuBody *d_fixed = nullptr;
@@ -885,20 +1045,51 @@ uint64_t array_bytes(uint64_t bcap, uint64_t fcap, uint64_t mcap, uint64_t jcap)
            jcap * (sizeof(NphGpuJoint) + (uint64_t)kJointRows * sizeof(float4));
 }
 
-// Grows the device arrays to hold the view (between steps only). A growth the solver's memory
-// limit does not allow is refused before any array is touched: the world stays as it was.
-NphGpuResult ensure_capacity(NphGpuSolver *s, uint32_t n, uint32_t nf, uint32_t m, uint32_t nj)
+// Device bytes of the packed drop-in's arrays at these capacities.
+uint64_t packed_bytes(uint64_t bcap, uint64_t mcap, uint64_t jcap)
+{
+    return bcap * (sizeof(NphGpuBodyInput) + sizeof(NphGpuBodyOutput)) +
+           mcap * (sizeof(NphGpuContactInput) + sizeof(NphGpuContactOutput)) + jcap * sizeof(NphGpuJointOutput);
+}
+
+uint64_t grown(uint32_t need, uint32_t cap) { return need > cap ? (uint64_t)need + need / 8u + 1u : cap; }
+
+// Grows the device arrays to hold the view (between steps only), and the packed drop-in's when
+// `packed`. A growth the solver's memory limit does not allow is refused before any array is
+// touched: the world stays as it was.
+NphGpuResult ensure_capacity(NphGpuSolver *s, uint32_t n, uint32_t nf, uint32_t m, uint32_t nj,
+                             bool packed = false)
 {
     if (s->memory_limit != 0u) {
         const uint64_t bcap = n + 1u > s->bcap ? (uint64_t)(n + 1u) + (n + 1u) / 8u : s->bcap;
         const uint64_t fcap = nf > s->fcap ? (uint64_t)nf + nf / 8u + 1u : s->fcap;
         const uint64_t mcap = m > s->mcap ? (uint64_t)m + m / 8u + 1u : s->mcap;
         const uint64_t jcap = nj > s->jcap ? (uint64_t)nj + nj / 8u + 1u : s->jcap;
-        if (array_bytes(bcap, fcap, mcap, jcap) > s->memory_limit) {
+        uint64_t total = array_bytes(bcap, fcap, mcap, jcap);
+        if (packed || s->pbcap > 0u) {
+            total += packed_bytes(packed ? grown(n, s->pbcap) : s->pbcap, packed ? grown(m, s->pmcap) : s->pmcap,
+                                  packed ? grown(nj, s->pjcap) : s->pjcap);
+        }
+        if (total > s->memory_limit) {
             return NPH_GPU_OUT_OF_MEMORY;
         }
     }
     bool ok = true;
+    if (packed && n > s->pbcap) {
+        const uint32_t cap = (uint32_t)grown(n, 0u);
+        ok = dalloc(s->in_bodies, cap) && dalloc(s->out_bodies, cap);
+        s->pbcap = ok ? cap : 0;
+    }
+    if (ok && packed && m > s->pmcap) {
+        const uint32_t cap = (uint32_t)grown(m, 0u);
+        ok = dalloc(s->in_contacts, cap) && dalloc(s->out_contacts, cap);
+        s->pmcap = ok ? cap : 0;
+    }
+    if (ok && packed && nj > s->pjcap) {
+        const uint32_t cap = (uint32_t)grown(nj, 0u);
+        ok = dalloc(s->out_joints, cap);
+        s->pjcap = ok ? cap : 0;
+    }
     if (n + 1u > s->bcap) {
         const uint32_t cap = n + 1u + (n + 1u) / 8u;
         // vel, pos and prm in one allocation: the body rows the constraint passes gather.
@@ -1280,7 +1471,9 @@ NphGpuResult validate_view(const NphGpuWorldView *v)
     return NPH_GPU_OK;
 }
 
-NphGpuResult upload(NphGpuSolver *s, const NphGpuWorldView *v)
+// Checks a view's counts and joint records, grows the arrays, and takes the view's shape
+// (its counts and colour tables); the records are the caller's to copy.
+NphGpuResult upload_shape(NphGpuSolver *s, const NphGpuWorldView *v, bool packed)
 {
     NphGpuResult r = validate_view(v);
     if (r != NPH_GPU_OK) {
@@ -1297,7 +1490,7 @@ NphGpuResult upload(NphGpuSolver *s, const NphGpuWorldView *v)
         driven += nph_joint_is_driven(&jr) ? 1u : 0u;
         row_joints += (nph_joint_has_axes(jr.type) || jr.type == NPH_GPU_JOINT_DISTANCE) ? 1u : 0u;
     }
-    r = ensure_capacity(s, v->body_count, v->fixed_count, v->contact_count, v->joint_count);
+    r = ensure_capacity(s, v->body_count, v->fixed_count, v->contact_count, v->joint_count, packed);
     if (r != NPH_GPU_OK) {
         return r;
     }
@@ -1323,6 +1516,15 @@ NphGpuResult upload(NphGpuSolver *s, const NphGpuWorldView *v)
     }
     s->driven = driven;
     s->row_joints = row_joints;
+    return NPH_GPU_OK;
+}
+
+NphGpuResult upload(NphGpuSolver *s, const NphGpuWorldView *v)
+{
+    const NphGpuResult r = upload_shape(s, v, false);
+    if (r != NPH_GPU_OK) {
+        return r;
+    }
     cudaMemcpyAsync(s->d_bodies, v->bodies, sizeof(NphGpuBody) * s->n, cudaMemcpyHostToDevice, s->stream);
     if (s->nf > 0) {
         cudaMemcpyAsync(s->d_fixed, v->fixed_bodies, sizeof(NphGpuBody) * s->nf, cudaMemcpyHostToDevice,
@@ -1354,6 +1556,68 @@ NphGpuResult download(NphGpuSolver *s, NphGpuWorldView *v)
     }
     if (s->nj > 0) {
         cudaMemcpyAsync(v->joints, s->d_joints, sizeof(NphGpuJoint) * s->nj, cudaMemcpyDeviceToHost,
+                        s->stream);
+    }
+    return check_cuda(cudaStreamSynchronize(s->stream));
+}
+
+// The packed drop-in's upload: the packed records up, expanded into the solver's records on the
+// device (the fields the stage only writes start at zero).
+NphGpuResult upload_packed(NphGpuSolver *s, const NphGpuPackedInput *in)
+{
+    if (in == nullptr) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    NphGpuWorldView shape;
+    std::memset(&shape, 0, sizeof shape);
+    shape.bodies = (NphGpuBody *)in->bodies; // for the null checks only: never read as records
+    shape.body_count = in->body_count;
+    shape.fixed_count = in->fixed_count;
+    shape.fixed_bodies = in->fixed_bodies;
+    shape.contacts = (NphGpuContact *)in->contacts;
+    shape.contact_count = in->contact_count;
+    shape.joint_count = in->joint_count;
+    shape.joints = (NphGpuJoint *)in->joints;
+    std::memcpy(shape.contact_color_counts, in->contact_color_counts, sizeof shape.contact_color_counts);
+    std::memcpy(shape.joint_color_counts, in->joint_color_counts, sizeof shape.joint_color_counts);
+    const NphGpuResult r = upload_shape(s, &shape, true);
+    if (r != NPH_GPU_OK) {
+        return r;
+    }
+    cudaMemcpyAsync(s->in_bodies, in->bodies, sizeof(NphGpuBodyInput) * s->n, cudaMemcpyHostToDevice, s->stream);
+    if (s->nf > 0) {
+        cudaMemcpyAsync(s->d_fixed, in->fixed_bodies, sizeof(NphGpuBody) * s->nf, cudaMemcpyHostToDevice,
+                        s->stream);
+    }
+    if (s->m > 0) {
+        cudaMemcpyAsync(s->in_contacts, in->contacts, sizeof(NphGpuContactInput) * s->m,
+                        cudaMemcpyHostToDevice, s->stream);
+    }
+    if (s->nj > 0) {
+        cudaMemcpyAsync(s->d_joints, in->joints, sizeof(NphGpuJoint) * s->nj, cudaMemcpyHostToDevice,
+                        s->stream);
+    }
+    launch_convert<NphGpuBodyInput, NphGpuBody, 0>(s->in_bodies, s->d_bodies, s->n, s->stream);
+    launch_convert<NphGpuContactInput, NphGpuContact, 1>(s->in_contacts, s->d_contacts, s->m, s->stream);
+    cudaMemsetAsync(s->d_err, 0, 32 * sizeof(uint32_t), s->stream);
+    s->uploaded = true;
+    return check_cuda(cudaGetLastError());
+}
+
+// The packed drop-in's download: the written fields packed on the device, one copy per kind.
+NphGpuResult download_packed(NphGpuSolver *s, NphGpuPackedOutput *out)
+{
+    launch_convert<NphGpuBody, NphGpuBodyOutput, 2>(s->d_bodies, s->out_bodies, s->n, s->stream);
+    launch_convert<NphGpuContact, NphGpuContactOutput, 3>(s->d_contacts, s->out_contacts, s->m, s->stream);
+    launch_convert<NphGpuJoint, NphGpuJointOutput, 4>(s->d_joints, s->out_joints, s->nj, s->stream);
+    cudaMemcpyAsync(out->bodies, s->out_bodies, sizeof(NphGpuBodyOutput) * s->n, cudaMemcpyDeviceToHost,
+                    s->stream);
+    if (s->m > 0) {
+        cudaMemcpyAsync(out->contacts, s->out_contacts, sizeof(NphGpuContactOutput) * s->m,
+                        cudaMemcpyDeviceToHost, s->stream);
+    }
+    if (s->nj > 0) {
+        cudaMemcpyAsync(out->joints, s->out_joints, sizeof(NphGpuJointOutput) * s->nj, cudaMemcpyDeviceToHost,
                         s->stream);
     }
     return check_cuda(cudaStreamSynchronize(s->stream));
@@ -1652,6 +1916,11 @@ NPH_GPU_API void nph_gpu_solver_destroy(NphGpuSolver *s)
     dfree(s->r_ref);
     dfree(s->r_state);
     dfree(s->d_err);
+    dfree(s->in_bodies);
+    dfree(s->in_contacts);
+    dfree(s->out_bodies);
+    dfree(s->out_contacts);
+    dfree(s->out_joints);
     if (s->h_err != nullptr) {
         cudaFreeHost(s->h_err);
     }
@@ -1768,6 +2037,59 @@ NPH_GPU_API NphGpuResult nph_gpu_phys_solve(NphGpuSolver *s, const NphGpuWorldPa
     }
     cudaEventRecord(s->ev[3], s->stream);
     r = download(s, view);
+    if (r != NPH_GPU_OK) {
+        return r;
+    }
+    cudaEventRecord(s->ev[4], s->stream);
+    cudaEventSynchronize(s->ev[4]);
+    cudaEventElapsedTime(&s->stats.upload_ms, s->ev[0], s->ev[1]);
+    cudaEventElapsedTime(&s->stats.device_ms, s->ev[1], s->ev[2]);
+    cudaEventElapsedTime(&s->stats.download_ms, s->ev[3], s->ev[4]);
+    fill_stats(s);
+    return NPH_GPU_OK;
+}
+
+NPH_GPU_API NphGpuResult nph_gpu_phys_solve_packed(NphGpuSolver *s, const NphGpuWorldParams *params, float dt,
+                                                   const NphGpuPackedInput *in, NphGpuPackedOutput *out)
+{
+    if (s == nullptr || in == nullptr || out == nullptr) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    NphGpuResult r = validate_params(params, dt);
+    if (r != NPH_GPU_OK) {
+        return r;
+    }
+    if ((in->body_count > 0 && out->bodies == nullptr) || (in->contact_count > 0 && out->contacts == nullptr) ||
+        (in->joint_count > 0 && out->joints == nullptr)) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    cudaSetDevice(s->device);
+    if (in->body_count == 0u) {
+        uint64_t nc = 0, nj = 0;
+        for (uint32_t c = 0; c < NPH_GPU_COLOR_SLOTS; ++c) {
+            nc += in->contact_color_counts[c];
+            nj += in->joint_color_counts[c];
+        }
+        return nc == in->contact_count && nj == in->joint_count ? NPH_GPU_OK : NPH_GPU_INVALID_ARGUMENT;
+    }
+    cudaEventRecord(s->ev[0], s->stream);
+    r = upload_packed(s, in);
+    if (r != NPH_GPU_OK) {
+        return r;
+    }
+    cudaEventRecord(s->ev[1], s->stream);
+    const StepConsts K = make_step_consts(*params, dt);
+    r = launch_step(s, K, params->substeps);
+    if (r != NPH_GPU_OK) {
+        return r;
+    }
+    cudaEventRecord(s->ev[2], s->stream);
+    r = read_error(s);
+    if (r != NPH_GPU_OK) {
+        return r; // the outputs are untouched: the step did not happen
+    }
+    cudaEventRecord(s->ev[3], s->stream);
+    r = download_packed(s, out);
     if (r != NPH_GPU_OK) {
         return r;
     }

@@ -39,6 +39,8 @@ def lib() -> ctypes.CDLL:
         "nph_gpu_solver_destroy": (None, [_vp]),
         "nph_gpu_phys_solve": (ctypes.c_int32, [_vp, P(abi.WorldParams), ctypes.c_float,
                                                 P(abi.WorldView)]),
+        "nph_gpu_phys_solve_packed": (ctypes.c_int32, [_vp, P(abi.WorldParams), ctypes.c_float,
+                                                       P(abi.PackedInput), P(abi.PackedOutput)]),
         "nph_gpu_world_upload": (ctypes.c_int32, [_vp, P(abi.WorldView)]),
         "nph_gpu_world_step_async": (ctypes.c_int32, [_vp, P(abi.WorldParams), ctypes.c_float,
                                                       _u32]),
@@ -174,6 +176,12 @@ class Solver:
 
     def synchronize(self) -> None:
         _check(self.L.nph_gpu_solver_synchronize(self._h), "nph_gpu_solver_synchronize")
+
+    def phys_solve_packed(self, packed: abi.Packed, params: abi.WorldParams, dt: float) -> None:
+        """nph_gpu_phys_solve_packed: the packed inputs in, the packed outputs filled."""
+        cin, cout = packed.c_input(), packed.c_output()
+        _check(self.L.nph_gpu_phys_solve_packed(self._h, ctypes.byref(params), dt, ctypes.byref(cin),
+                                                ctypes.byref(cout)), "nph_gpu_phys_solve_packed")
 
     def set_memory_limit(self, nbytes: int) -> None:
         """A budget for the record and row arrays (0: none); growth beyond it fails with
