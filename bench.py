@@ -64,7 +64,12 @@ def parse():
                          "results back while later parts go up; 1: unsplit)")
     ap.add_argument("--pile-worlds", type=int, default=256,
                     help="learned: box-pile worlds per batch (500-5000 boxes each)")
-    ap.add_argument("--train-batches", type=int, default=2)
+    ap.add_argument("--train-steps", type=int, default=200,
+                    help="learned: steps the plain solver runs the training piles")
+    ap.add_argument("--sample-every", type=int, default=20,
+                    help="learned: steps between kept training samples")
+    ap.add_argument("--eval-steps", default="20,40,60,90",
+                    help="learned: steps of the held-out piles judged")
     ap.add_argument("--max-passes", type=int, default=2000)
     ap.add_argument("--epochs", type=int, default=30)
     ap.add_argument("--solver", choices=("soft_step", "tgs"), default="soft_step",
@@ -749,14 +754,21 @@ def run_batched(args):
 
 
 def run_learned(args):
-    """--workload learned: the learned warm start on collapsing box piles. Training data: the
-    cold points of --train-batches batches of --pile-worlds piles (500-5000 boxes each), their
-    targets the impulses the plain solver converged to; the network trained on the device;
-    judged on a held-out batch by the residual-driven mode (passes to each tolerance of the
-    plain start's initial residual, learned against plain). Rank 0 only."""
+    """--workload learned: the learned warm start on collapsing box piles, as configured:
+    --pile-worlds worlds of 500-5000 boxes (half extents 0.2-1.0 m) dropped from seeded random
+    orientations and collided every step by the library's own stages (nepheline_b200.piles:
+    device broad phase, narrow phase, warm start, colouring, solver stage).
+
+    Training: the plain solver steps a training set of piles for --train-steps steps (worlds x
+    steps world-steps); every --sample-every steps the cold points' features and the impulses
+    the plain solver converges to (to 1e-4 of the plain start's initial residual) are kept; the
+    network trains on the device. Evaluation: a held-out set of piles stepped the same way; at
+    each of --eval-steps the plain start, the learned start and the exact start (cold points at
+    the impulses the plain run converges to, which no predictor can beat) run the
+    residual-driven mode: passes and device time to each tolerance. Rank 0 only."""
     import torch
 
-    from nepheline_b200 import abi, learned, scenes
+    from nepheline_b200 import abi, learned, piles
     from nepheline_b200.solver import Mlp, Solver
 
     rank = int(os.environ.get("RANK", "0"))
@@ -768,52 +780,78 @@ def run_learned(args):
     clk = Clocks(local).__enter__()
     solver = Solver(device=local)
     mlp = Mlp(device=local, seed=0)
+    eval_steps = sorted(int(x) for x in args.eval_steps.split(","))
+
     t0 = time.perf_counter()
-    xs, ts, passes = [], [], []
-    for b in range(args.train_batches):
-        view = learned.merged_view(solver, scenes.box_pile_batch(args.pile_worlds, seed=100 + b))
-        x, t, run = learned.samples(solver, view, params, DT, tolerance=1e-4,
-                                    max_passes=args.max_passes)
-        xs.append(x)
-        ts.append(t)
-        passes.append(int(run["passes"]))
+    train = piles.Piles(piles.pile_sizes(args.pile_worlds, seed=1), seed=1)
+    xs, ts, sampled = [], [], []
+    step_s = 0.0
+    for s in range(args.train_steps):
+        view, where, keys = train.view(solver, DT)
+        if s > 0 and s % args.sample_every == 0:
+            x, t, run = learned.samples(solver, view, params, DT, tolerance=1e-4,
+                                        max_passes=args.max_passes)
+            xs.append(x)
+            ts.append(t)
+            sampled.append({"step": s, "manifolds": len(view.contacts), "cold_points": len(x),
+                            "passes": int(run["passes"]), "converged": bool(run["converged"])})
+        t1 = time.perf_counter()
+        solver.phys_solve(view, params, DT)
+        step_s += time.perf_counter() - t1
+        train.finish(view, where, keys)
+    data_s = time.perf_counter() - t0
     x = np.concatenate(xs)
     t = np.concatenate(ts)
-    data_s = time.perf_counter() - t0
     t1 = time.perf_counter()
     fit = learned.train(mlp, x, t, epochs=args.epochs, batch=4096, lr=1e-3, seed=1)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t1
-    scs = scenes.box_pile_batch(args.pile_worlds, seed=0)
-    view = learned.merged_view(solver, scs)
+
+    held = piles.Piles(piles.pile_sizes(args.pile_worlds, seed=2), seed=2)
+    evals = []
     clk.lines.clear()
-    cmp = learned.compare(solver, mlp, view, params, DT, tolerances=(1e-2, 1e-3, 1e-4),
-                          max_passes=args.max_passes)
+    for s in range(eval_steps[-1] + 1):
+        view, where, keys = held.view(solver, DT)
+        if s in eval_steps:
+            j = learned.judge(solver, mlp, view, params, DT, max_passes=args.max_passes)
+            j.update({"step": s, "bodies": len(view.bodies), "manifolds": len(view.contacts),
+                      "new_pairs": held._new})
+            evals.append(j)
+        solver.phys_solve(view, params, DT)
+        held.finish(view, where, keys)
     clocks = clk.summary()
     clk.__exit__(None, None, None)
-    tight = cmp["tolerances"]["0.0001"]
-    value = tight["learned"] if tight["learned"] is not None else args.max_passes
-    plain = tight["plain"] if tight["plain"] is not None else args.max_passes
+
+    def total(name, tol):
+        vals = [e["tolerances"][tol][name] for e in evals]
+        return None if any(v is None for v in vals) else int(sum(vals))
+
+    tight = "0.0001"
+    value = total("learned", tight)
+    plain = total("plain", tight)
     out = {
-        "metric": "iters to 1e-4 residual, learned vs plain init", "value": value,
-        "unit": "passes", "n_gpus": 1, "steps": 1, "warmup": 0,
-        "ms_per_step": tight["learned_ms"], "higher_is_better": False, "scaling": "weak",
-        "vs_baseline": None, "dtype": "bf16 network, f32 solver", "data": "synthetic",
-        "config": {"workload": f"collapsing box piles: {args.pile_worlds} worlds of 500-5000 "
-                               f"boxes (half extents 0.2-1.0 m), columns of 1-8 on a ground, "
-                               f"top boxes just dropped, a seeded share of contacts new",
-                   "bodies": len(view.bodies), "manifolds": len(view.contacts),
-                   "cold_points": cmp["cold_points"], "max_passes": args.max_passes,
-                   "training": dict(fit, batches=args.train_batches, epochs=args.epochs,
-                                    data_s=data_s, train_s=train_s,
-                                    plain_passes_on_training_data=passes)},
-        "plain": plain, "reached": {"plain": tight["plain"] is not None,
-                                    "learned": tight["learned"] is not None},
-        "comparison": cmp,
-        "e2e": {"value": value, "unit": "passes", "h2d_bytes_per_step":
-                int(view.bodies.nbytes + view.contacts.nbytes + view.fixed.nbytes),
-                "d2h_bytes_per_step": 4 * (args.max_passes + 1)},
-        "gpu_launches": int(plain + value) * 8,
+        "metric": "iters to 1e-4 residual, learned vs plain init",
+        "value": value if value is not None else args.max_passes * len(evals),
+        "unit": "passes", "n_gpus": 1, "steps": len(evals), "warmup": 0,
+        "ms_per_step": sum(e["tolerances"][tight]["learned_ms"] for e in evals) / len(evals),
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16 network, f32 solver", "data": "synthetic",
+        "config": {"workload": f"collapsing box piles: {args.pile_worlds} worlds of 500-5000 boxes "
+                               f"(half extents 0.2-1.0 m, seeded random orientations) dropped on a "
+                               f"ground, collided every step by the library's broad and narrow "
+                               f"phases",
+                   "bodies": int(held.n), "eval_steps": eval_steps, "max_passes": args.max_passes,
+                   "training": dict(fit, world_steps=args.pile_worlds * args.train_steps,
+                                    world_steps_asked=50000, steps=args.train_steps,
+                                    samples=sampled, data_s=data_s, plain_step_s=step_s,
+                                    train_s=train_s, epochs=args.epochs)},
+        "plain": plain if plain is not None else args.max_passes * len(evals),
+        "summary": {tol: {name: total(name, tol) for name in ("plain", "learned", "exact")}
+                    for tol in evals[0]["tolerances"]},
+        "evaluations": evals,
+        "e2e": {"value": value if value is not None else args.max_passes * len(evals),
+                "unit": "passes", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "gpu_launches": None,
         "clocks": clocks,
     }
     print(json.dumps(out))

@@ -751,6 +751,26 @@ NPH_GPU_API NphGpuResult nph_gpu_collide(const NphGpuShape *a, const NphGpuPose 
  * (the next call makes them again). */
 NPH_GPU_API void nph_gpu_collide_release(void);
 
+/* The broad phase for worlds the caller steps with the library's own stages: the pairs (a < b,
+ * by index) of boxes of the same group whose axis-aligned boxes overlap (closed intervals, as
+ * boxes_overlap, contact.c:286-290; the reference pairs its fattened boxes from AABB trees,
+ * phys_update_pairs, contact.c:811). `lo`/`hi`: count x 3 floats; `group`: a world number per
+ * box; `cell`: a grid spacing no smaller than any box's extent on any axis. The first
+ * min(total, capacity) pairs in (a, b) order go to pair_a/pair_b, the total to *pair_count (a
+ * caller with too small a capacity calls again). Host arrays; device arrays per call. */
+NPH_GPU_API NphGpuResult nph_gpu_broad_phase(const float *lo, const float *hi, const uint32_t *group,
+                                             uint32_t count, float cell, uint32_t *pair_a,
+                                             uint32_t *pair_b, uint32_t capacity, uint32_t *pair_count);
+
+/* phys_contact_update's warm start (contact.c:516-565) for `count` contacts on host arrays:
+ * out[i] is fresh[i] (the narrow phase's manifold as a contact record: anchors from each body's
+ * centre, separation, feature ids, impulses zero) with the pair and flags of old[i] and the
+ * impulses of old[i]'s points carried over by feature id, then by place (warm_by_id,
+ * warm_by_place, contact.c:332-380). A pair new this step passes an old record with its bodies,
+ * flags 0 and no points. On the device; device arrays per call. */
+NPH_GPU_API NphGpuResult nph_gpu_warm_start_contacts(const NphGpuContact *old, const NphGpuContact *fresh,
+                                                     uint32_t count, NphGpuContact *out);
+
 /* ------------------------------------------------------------------------------------
  * The contact update on the device
  * ---------------------------------------------------------------------------------- */

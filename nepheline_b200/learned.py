@@ -7,6 +7,8 @@
   compare()   the residual-driven comparison that judges the network: the plain start and the
               learned start on the same world, passes to each tolerance of the plain start's
               initial residual, and device time
+  judge()     the same with the exact start beside them: the cold points started at the very
+              impulses the plain run converges to, which no predictor can beat
 
 The reference has no counterpart (its new contact points start at zero impulse,
 engine/physics/src/contact.c:547-565).
@@ -80,4 +82,72 @@ def compare(solver, mlp, view: abi.View, params: abi.WorldParams, dt: float,
         out["learned_initial_over_plain"] = float(learned["initial_residual"]) / ref if ref > 0 else None
         out["plain_lowest"] = float(plain["residuals"].min()) / ref if ref > 0 else None
         out["learned_lowest"] = float(learned["residuals"].min()) / ref if ref > 0 else None
+    return out
+
+
+def tangents(normal: np.ndarray):
+    """t1 = nph_vec3_perpendicular(n) (vec.h:460-469: n crossed with the axis it is least
+    aligned with, normalised) and t2 = n x t1, in FP32, for (m, 3) unit normals."""
+    n = np.asarray(normal, np.float32)
+    a = np.abs(n)
+    axis = np.zeros_like(n)
+    use_x = (a[:, 0] <= a[:, 1]) & (a[:, 0] <= a[:, 2])
+    use_y = ~use_x & (a[:, 1] <= a[:, 2])
+    axis[use_x, 0] = 1.0
+    axis[use_y, 1] = 1.0
+    axis[~use_x & ~use_y, 2] = 1.0
+    t1 = np.cross(n, axis)
+    t1 /= np.linalg.norm(t1, axis=1, keepdims=True)
+    return t1.astype(np.float32), np.cross(n, t1).astype(np.float32)
+
+
+def exact_start(view: abi.View, kind: np.ndarray, impulses: np.ndarray) -> abi.View:
+    """`view` with its cold points' warm start set to `impulses` (4 x (normal, t1, t2) per
+    manifold, as nph_gpu_world_converge returns them): the exact start of the new points."""
+    out = view.copy()
+    cold = (np.asarray(kind).reshape(-1, 4) == abi.POINT_COLD)
+    t1, t2 = tangents(out.contacts["normal"])
+    imp = np.asarray(impulses, np.float32).reshape(-1, 4, 3)
+    pts = out.contacts["points"]
+    pts["normal_impulse"] = np.where(cold, imp[..., 0], pts["normal_impulse"])
+    world = imp[..., 1:2] * t1[:, None, :] + imp[..., 2:3] * t2[:, None, :]
+    pts["tangent_impulse"] = np.where(cold[..., None], world, pts["tangent_impulse"])
+    return out
+
+
+def judge(solver, mlp, view: abi.View, params: abi.WorldParams, dt: float,
+          tolerances=(1e-1, 1e-2, 1e-3, 1e-4), max_passes: int = 2000) -> dict:
+    """Passes and device time to each tolerance of the plain start's initial residual, for the
+    plain start, the learned start and the exact start, on one world (each run stops at its
+    tolerance, so each time is the run's own)."""
+    solver.upload(view)
+    _, _, kind = solver.features(params, dt)
+    full = solver.converge(params, dt, tolerance=min(tolerances), max_passes=max_passes,
+                           impulses=True)
+    ref = float(full["reference_residual"])
+    exact = exact_start(view, kind, full["impulses"])
+    out = {"reference_residual": ref, "cold_points": int(full["cold_points"]),
+           "points": int((np.asarray(kind) != abi.POINT_NONE).sum()),
+           "plain_lowest": float(full["residuals"].min()) / ref if ref > 0 else None,
+           "tolerances": {}}
+    for tol in sorted(tolerances, reverse=True):
+        row = {}
+        for name in ("plain", "learned", "exact"):
+            if name == "exact":
+                solver.upload(exact)
+            else:
+                solver.upload(view)
+            if name == "learned":
+                solver.set_warm_start_model(mlp)
+            try:
+                r = solver.converge(params, dt, learned=name == "learned", tolerance=tol,
+                                    max_passes=max_passes, reference_residual=ref)
+            finally:
+                if name == "learned":
+                    solver.set_warm_start_model(None)
+            row[name] = int(r["passes"]) if r["converged"] else None
+            row[name + "_ms"] = float(r["ms"])
+            if tol == max(tolerances):
+                out[name + "_initial_over_plain"] = float(r["initial_residual"]) / ref if ref > 0 else None
+        out["tolerances"][f"{tol:g}"] = row
     return out

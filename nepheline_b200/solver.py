@@ -81,6 +81,9 @@ def lib() -> ctypes.CDLL:
         "nph_gpu_collide_async": (ctypes.c_int32, [_vp, _vp, _vp, _vp, _vp, _u32, _vp, _vp, _vp,
                                                    ctypes.c_uint64, _vp]),
         "nph_gpu_collide_workspace_bytes": (ctypes.c_uint64, [_u32]),
+        "nph_gpu_broad_phase": (ctypes.c_int32, [_vp, _vp, _vp, _u32, ctypes.c_float, _vp, _vp, _u32,
+                                                 P(_u32)]),
+        "nph_gpu_warm_start_contacts": (ctypes.c_int32, [_vp, _vp, _u32, _vp]),
         "nph_gpu_batch_create": (ctypes.c_int32, [P(abi.SolverDesc), P(_vp)]),
         "nph_gpu_batch_destroy": (None, [_vp]),
         "nph_gpu_batch_stream": (_vp, [_vp]),
@@ -519,3 +522,33 @@ def collide_async(a_ptr: int, pose_a_ptr: int, b_ptr: int, pose_b_ptr: int, spec
 
 def version() -> str:
     return lib().nph_gpu_version().decode()
+
+
+def broad_phase(lo: np.ndarray, hi: np.ndarray, group: np.ndarray, cell: float):
+    """nph_gpu_broad_phase: (pair_a, pair_b) of the boxes whose bounds overlap, within groups."""
+    L = lib()
+    lo = np.ascontiguousarray(lo, np.float32)
+    hi = np.ascontiguousarray(hi, np.float32)
+    group = np.ascontiguousarray(group, np.uint32)
+    cap = max(16, 8 * len(lo))
+    while True:
+        a = np.zeros(cap, np.uint32)
+        b = np.zeros(cap, np.uint32)
+        n = _u32()
+        _check(L.nph_gpu_broad_phase(lo.ctypes.data, hi.ctypes.data, group.ctypes.data, len(lo),
+                                     float(cell), a.ctypes.data, b.ctypes.data, cap, ctypes.byref(n)),
+               "nph_gpu_broad_phase")
+        if n.value <= cap:
+            return a[: n.value], b[: n.value]
+        cap = n.value
+
+
+def warm_start_contacts(old: np.ndarray, fresh: np.ndarray) -> np.ndarray:
+    """nph_gpu_warm_start_contacts over aligned record arrays."""
+    old = np.ascontiguousarray(old, abi.CONTACT_DTYPE)
+    fresh = np.ascontiguousarray(fresh, abi.CONTACT_DTYPE)
+    assert len(old) == len(fresh)
+    out = np.zeros_like(fresh)
+    _check(lib().nph_gpu_warm_start_contacts(old.ctypes.data, fresh.ctypes.data, len(out),
+                                             out.ctypes.data), "nph_gpu_warm_start_contacts")
+    return out
