@@ -67,16 +67,22 @@ def test_warm_start_contacts_equals_the_restatement(ref_lib):
 
 
 def test_dropped_piles_come_to_rest(solver):
+    """270 boxes in three worlds dropped from layers up to 13 m: the piles collapse and come to
+    rest within 10 s, as the reference engine's world step does with the same boxes (measured:
+    8 boxes still above 1 m/s after 4 s, none above 0.2 m/s from 9 s on)."""
     from nepheline_b200 import piles
     params = abi.WorldParams.default()
     p = piles.Piles([60, 120, 90], seed=5)
     speeds = []
-    for _ in range(240):
+    for s in range(600):
         view = p.step(solver, params, DT)
         assert np.isfinite(view.bodies["linear_velocity"]).all()
-        speeds.append(float(np.abs(view.bodies["linear_velocity"]).max()))
+        v = np.linalg.norm(view.bodies["linear_velocity"], axis=1)
+        speeds.append(float(v.max()))
+        if s % 60 == 59:
+            print(f"step {s}: max |v| {v.max():.3f}, above 1 m/s {int((v > 1).sum())}")
     assert len(p.records) > p.n // 2  # boxes rest on the ground and on each other
-    assert speeds[-1] < 0.5 and speeds[-1] < max(speeds)
+    assert max(speeds) > 5.0 and speeds[-1] < 0.5
     # No box sank through its ground (the slab's top is y = 0).
     lowest = p.bodies["center"][:, 1] - np.linalg.norm(p.half, axis=1)
     assert lowest.min() > -0.1
