@@ -4,9 +4,15 @@
 // 2.39's atan2f (joint_solver.c:77-84, 303-394 through nph_f32_atan2, scalar.h:239-242),
 // restated so the device's joint angles round to the same bits as the reference's.
 //
-// glibc 2.39 computes atan2f in single precision by fdlibm's method (Sun Microsystems'
-// freely distributable math library, 1993: "Permission to use, copy, modify, and distribute
-// this software is freely granted, provided that this notice is preserved."):
+// glibc 2.39 computes atan2f in single precision by fdlibm's method. fdlibm's notice, kept as
+// it asks for the method and coefficients restated here:
+//
+//   Copyright (C) 1993 by Sun Microsystems, Inc. All rights reserved.
+//   Developed at SunPro, a Sun Microsystems, Inc. business.
+//   Permission to use, copy, modify, and distribute this software is freely granted, provided
+//   that this notice is preserved.
+//
+// The method:
 //
 //   atan(t), t >= 0: reduce to |u| < 7/16 around a breakpoint b in {0, 1/2, 1, 3/2, inf},
 //     atan(t) = atan(b) + atan(u) with u = (t - b) / (1 + b t)  (u = -1/t for b = inf),
