@@ -340,6 +340,8 @@ k_pass_pair(DevSolver S, uint32_t cfirst, uint32_t ccount, StepConsts K)
         solve_manifold_pair<true, kStaged>(S, cfirst + g, p, K, T);
     } else if (P == kRelax) {
         solve_manifold_pair<false, kStaged>(S, cfirst + g, p, K, T);
+    } else if (P == kWarm) {
+        warm_manifold_pair(S, cfirst + g, p);
     }
 }
 
@@ -407,8 +409,9 @@ k_pass_pipelined(DevSolver S, uint32_t cfirst, uint32_t ccount, StepConsts K)
 // allows (65,536 registers / (threads x blocks)); `staged`: 0 plain loads, 1 the loads staged
 // through shared memory (kSlots x threads x 16 bytes per block), 2 staged and pipelined, 3 the
 // lean staged form (kPointSlots x threads x 16 bytes per block), 4 two lanes a manifold for
-// the solve and relax passes (contacts_pair.cuh; the other pass kinds run the plain kernel), 5
-// the same with the point rows staged (kPointSlots x threads / 2 x 16 bytes per block).
+// the warm start, solve and relax passes (contacts_pair.cuh; restitution runs the plain
+// kernel), 5 the same with the solve and relax passes' point rows staged (kPointSlots x threads
+// / 2 x 16 bytes per block; the warm start reads its rows once and stays unstaged).
 struct PassConfig {
     uint32_t threads, min_blocks, staged;
 };
@@ -429,7 +432,7 @@ void launch_pass(uint32_t config, uint32_t cc, cudaStream_t st, const DevSolver 
     if (kPassConfigs[config].staged >= 4u) {
         const uint32_t pair_grid = (2u * cc + t - 1) / t;
         const size_t pair_tile = (size_t)kPointSlots * (t / 2u) * sizeof(float4);
-        if (P == kSolve || P == kRelax) {
+        if (P == kSolve || P == kRelax || P == kWarm) {
             switch (config) {
             case 15: k_pass_pair<P, 128, 6, false><<<pair_grid, 128, 0, st>>>(S, cfirst, cc, K); break;
             case 16: k_pass_pair<P, 128, 8, false><<<pair_grid, 128, 0, st>>>(S, cfirst, cc, K); break;
