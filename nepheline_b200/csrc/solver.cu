@@ -321,28 +321,17 @@ k_pass_staged(DevSolver S, uint32_t cfirst, uint32_t ccount, StepConsts K)
     }
 }
 
-// The solve and relax passes with two lanes a manifold (contacts_pair.cuh): lanes 2i and 2i + 1
-// of the grid take manifold i, bodies A and B. kStaged: the point rows through a shared-memory
-// tile of kPointSlots slots x threads / 2 manifolds.
-template <int P, int kThreads, int kMinBlocks, bool kStaged>
-__global__ void __launch_bounds__(kThreads, kMinBlocks)
-k_pass_pair(DevSolver S, uint32_t cfirst, uint32_t ccount, StepConsts K)
+// The warm start with two lanes a manifold (contacts_pair.cuh): lanes 2i and 2i + 1 of the
+// grid take manifold i, bodies A and B.
+template <int kThreads, int kMinBlocks>
+__global__ void __launch_bounds__(kThreads, kMinBlocks) k_warm_pair(DevSolver S, uint32_t cfirst, uint32_t ccount)
 {
-    extern __shared__ float4 pair_tile[];
     const uint32_t g = (blockIdx.x * kThreads + threadIdx.x) >> 1;
     if (g >= ccount) {
         return;
     }
     const uint32_t lane = threadIdx.x & 31u;
-    const Pair p{3u << (lane & ~1u), (lane & 1u) != 0u};
-    const PairTile T{pair_tile, kThreads / 2u, threadIdx.x >> 1};
-    if (P == kSolve) {
-        solve_manifold_pair<true, kStaged>(S, cfirst + g, p, K, T);
-    } else if (P == kRelax) {
-        solve_manifold_pair<false, kStaged>(S, cfirst + g, p, K, T);
-    } else if (P == kWarm) {
-        warm_manifold_pair(S, cfirst + g, p);
-    }
+    warm_manifold_pair(S, cfirst + g, Pair{3u << (lane & ~1u), (lane & 1u) != 0u});
 }
 
 // The contact update for the next step (contact.c:516-565): each contact's record becomes the
@@ -409,9 +398,7 @@ k_pass_pipelined(DevSolver S, uint32_t cfirst, uint32_t ccount, StepConsts K)
 // allows (65,536 registers / (threads x blocks)); `staged`: 0 plain loads, 1 the loads staged
 // through shared memory (kSlots x threads x 16 bytes per block), 2 staged and pipelined, 3 the
 // lean staged form (kPointSlots x threads x 16 bytes per block), 4 two lanes a manifold for
-// the warm start, solve and relax passes (contacts_pair.cuh; restitution runs the plain
-// kernel), 5 the same with the solve and relax passes' point rows staged (kPointSlots x threads
-// / 2 x 16 bytes per block; the warm start reads its rows once and stays unstaged).
+// the warm start (contacts_pair.cuh; the other pass kinds run the plain kernel).
 struct PassConfig {
     uint32_t threads, min_blocks, staged;
 };
@@ -419,8 +406,7 @@ constexpr PassConfig kPassConfigs[] = {{256, 1, 0}, {256, 2, 0}, {128, 4, 0}, {2
                                        {64, 6, 1},  {64, 7, 1},  {128, 3, 1}, {32, 14, 1},
                                        {32, 7, 2},  {64, 3, 2},  {32, 18, 3}, {32, 24, 3},
                                        {64, 9, 3},  {64, 12, 3}, {128, 6, 3}, {128, 6, 4},
-                                       {128, 8, 4}, {64, 14, 4}, {256, 4, 4}, {128, 8, 5},
-                                       {128, 7, 5}, {64, 16, 5}, {128, 6, 5}};
+                                       {128, 8, 4}, {64, 14, 4}, {256, 4, 4}};
 constexpr uint32_t kPassConfigCount = sizeof(kPassConfigs) / sizeof(kPassConfigs[0]);
 
 template <int P>
@@ -429,19 +415,14 @@ void launch_pass(uint32_t config, uint32_t cc, cudaStream_t st, const DevSolver 
 {
     const uint32_t t = kPassConfigs[config].threads;
     const uint32_t grid = (cc + t - 1) / t;
-    if (kPassConfigs[config].staged >= 4u) {
-        const uint32_t pair_grid = (2u * cc + t - 1) / t;
-        const size_t pair_tile = (size_t)kPointSlots * (t / 2u) * sizeof(float4);
-        if (P == kSolve || P == kRelax || P == kWarm) {
+    if (kPassConfigs[config].staged == 4u) {
+        if (P == kWarm) {
+            const uint32_t pair_grid = (2u * cc + t - 1) / t;
             switch (config) {
-            case 15: k_pass_pair<P, 128, 6, false><<<pair_grid, 128, 0, st>>>(S, cfirst, cc, K); break;
-            case 16: k_pass_pair<P, 128, 8, false><<<pair_grid, 128, 0, st>>>(S, cfirst, cc, K); break;
-            case 17: k_pass_pair<P, 64, 14, false><<<pair_grid, 64, 0, st>>>(S, cfirst, cc, K); break;
-            case 18: k_pass_pair<P, 256, 4, false><<<pair_grid, 256, 0, st>>>(S, cfirst, cc, K); break;
-            case 19: k_pass_pair<P, 128, 8, true><<<pair_grid, 128, pair_tile, st>>>(S, cfirst, cc, K); break;
-            case 20: k_pass_pair<P, 128, 7, true><<<pair_grid, 128, pair_tile, st>>>(S, cfirst, cc, K); break;
-            case 21: k_pass_pair<P, 64, 16, true><<<pair_grid, 64, pair_tile, st>>>(S, cfirst, cc, K); break;
-            default: k_pass_pair<P, 128, 6, true><<<pair_grid, 128, pair_tile, st>>>(S, cfirst, cc, K); break;
+            case 15: k_warm_pair<128, 6><<<pair_grid, 128, 0, st>>>(S, cfirst, cc); break;
+            case 16: k_warm_pair<128, 8><<<pair_grid, 128, 0, st>>>(S, cfirst, cc); break;
+            case 17: k_warm_pair<64, 14><<<pair_grid, 64, 0, st>>>(S, cfirst, cc); break;
+            default: k_warm_pair<256, 4><<<pair_grid, 256, 0, st>>>(S, cfirst, cc); break;
             }
         } else {
             k_pass<P, 128, 4><<<(cc + 127u) / 128u, 128, 0, st>>>(S, cfirst, cc, K);
