@@ -406,3 +406,26 @@ def test_drop_in_in_parts_follows_the_batch(solver):
         for m, w in zip(mine, want):
             assert not helpers.mismatches(m, w), (packing, solver_kind)
     batch.close()
+
+
+@pytest.mark.parametrize("packing", [abi.BATCH_PERSISTENT, abi.BATCH_MERGED])
+def test_batched_worlds_match_the_restatement(packing):
+    """Worlds of the batched configuration's generator (box pyramids, piles and capsule chains on
+    hinges, 8 to 600 bodies) solved in one batch, three steps, against the CPU restatement
+    pinned to the reference, world by world: a direct check, not through the single-world
+    device solver."""
+    from nepheline_b200.solver import Batch
+    from oracle.refworld import port32
+    params = abi.WorldParams.default()
+    worlds = [w.to_view(*scenes.host_color(w))
+              for w in scenes.batched_worlds(12, seed=9, max_bodies=600)]
+    batch = Batch(device=0)
+    batch.set_config(packing=packing)
+    mine = [v.copy() for v in worlds]
+    want = [v.copy() for v in worlds]
+    for _ in range(3):
+        batch.phys_solve_worlds(mine, params, DT)
+        want = [port32(v, params, DT) for v in want]
+    for i, (m, r) in enumerate(zip(mine, want)):
+        assert not helpers.mismatches(m, r), f"world {i}"
+    batch.close()
