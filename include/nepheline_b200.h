@@ -573,6 +573,8 @@ typedef struct NphGpuBatchTuning {
     uint32_t packing;           /* NPH_GPU_BATCH_PERSISTENT or NPH_GPU_BATCH_MERGED; the fields
                                    above apply to the persistent packing */
     float ms_per_step;          /* the autotuner's time for it (filled in) */
+    float persistent_ms_per_step; /* the autotuner's best persistent configuration's time */
+    float merged_ms_per_step;     /* the autotuner's time for the merged packing */
 } NphGpuBatchTuning;
 
 typedef struct NphGpuBatchInfo {
@@ -903,9 +905,18 @@ NPH_GPU_API NphGpuResult nph_gpu_world_features(NphGpuSolver *solver,
  * zero. */
 NPH_GPU_API NphGpuResult nph_gpu_solver_set_warm_start_model(NphGpuSolver *solver, NphGpuMlp *mlp);
 
+/* The starts of the residual-driven mode: cold points at zero (the reference's start); at the
+ * attached network's predictions; or at the network's predictions with the plain start as the
+ * fallback, kept only when the residual after the warm start is no larger than the plain
+ * start's (the reference residual when one is given, else a plain start run first), otherwise
+ * the plain start runs again from the records. Every start's device time counts in `ms`. */
+#define NPH_GPU_START_PLAIN 0u
+#define NPH_GPU_START_LEARNED 1u
+#define NPH_GPU_START_GATED 2u
+
 /* The residual-driven mode that judges a warm start. On the uploaded world: prepare, the
- * first substep's velocity integration and warm start (plain, or learned when `learned` and a
- * network is attached), then rigid passes (the relax pass: no softness, speculative rows for
+ * first substep's velocity integration and warm start (`learned`: an NPH_GPU_START_* value; a
+ * network must be attached unless plain), then rigid passes (the relax pass: no softness, speculative rows for
  * separated points) over every colour until the velocity-constraint residual falls to
  * `tolerance` x the reference residual, or `max_passes`. The residual is the L2 norm over
  * points of r_n = |vn + b| where the normal impulse is positive, max(-(vn + b), 0) where not
@@ -922,7 +933,8 @@ typedef struct NphGpuConvergeStats {
     float initial_residual;    /* after the warm start */
     float final_residual;
     float reference_residual;  /* the denominator */
-    float ms;                  /* device time from prepare to the last pass */
+    float ms;                  /* device time from the first prepare to the last pass */
+    uint32_t fell_back;        /* NPH_GPU_START_GATED: 1 when the plain start replaced the network's */
 } NphGpuConvergeStats;
 NPH_GPU_API NphGpuResult nph_gpu_world_converge(NphGpuSolver *solver,
                                                 const NphGpuWorldParams *params, float dt,

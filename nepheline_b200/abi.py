@@ -230,6 +230,7 @@ class KernelTime(ctypes.Structure):
 
 BATCH_SHARED_NONE, BATCH_SHARED_SMALL, BATCH_SHARED_LARGE = 0, 1, 2
 BATCH_PERSISTENT, BATCH_MERGED = 0, 1
+START_PLAIN, START_LEARNED, START_GATED = 0, 1, 2
 
 # The learned warm start's network and point slots (nepheline_b200.h).
 MLP_INPUTS, MLP_HIDDEN, MLP_OUTPUTS = 16, 64, 3
@@ -242,13 +243,15 @@ class ConvergeStats(ctypes.Structure):
     _fields_ = [("passes", ctypes.c_uint32), ("converged", ctypes.c_uint32),
                 ("cold_points", ctypes.c_uint32), ("predicted_points", ctypes.c_uint32),
                 ("initial_residual", ctypes.c_float), ("final_residual", ctypes.c_float),
-                ("reference_residual", ctypes.c_float), ("ms", ctypes.c_float)]
+                ("reference_residual", ctypes.c_float), ("ms", ctypes.c_float),
+                ("fell_back", ctypes.c_uint32)]
 
 
 class BatchTuning(ctypes.Structure):
     _fields_ = [("config", ctypes.c_uint32), ("threads", ctypes.c_uint32),
                 ("shared_velocities", ctypes.c_uint32), ("items_per_thread", ctypes.c_uint32),
-                ("packing", ctypes.c_uint32), ("ms_per_step", ctypes.c_float)]
+                ("packing", ctypes.c_uint32), ("ms_per_step", ctypes.c_float),
+                ("persistent_ms_per_step", ctypes.c_float), ("merged_ms_per_step", ctypes.c_float)]
 
 
 class BatchInfo(ctypes.Structure):

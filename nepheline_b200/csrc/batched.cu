@@ -1727,7 +1727,8 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_autotune(NphGpuBatch *b, const NphGpuWorl
     static const uint32_t kSplits[] = {0u, 1u, 2u, 4u, 8u};
     float best = 1e30f;
     NphGpuBatchTuning chosen{b->config, kBatchConfigs[b->config].threads, b->shared_mode, b->items_per_thread,
-                             b->packing, 0.0f};
+                             b->packing, 0.0f, 0.0f, 0.0f};
+    float best_persistent = 0.0f, merged_ms = 0.0f;
     rounds = rounds == 0u ? 1u : rounds;
     auto timed = [&](auto &&step) -> float {
         cudaEventRecord(e0, b->stream);
@@ -1767,8 +1768,9 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_autotune(NphGpuBatch *b, const NphGpuWorl
                 const float ms = timed([&] { return launch_batch_step(b, K, params->substeps); });
                 if (ms < best) {
                     best = ms;
+                    best_persistent = ms / (float)rounds;
                     chosen = NphGpuBatchTuning{c, kBatchConfigs[c].threads, shared, split, NPH_GPU_BATCH_PERSISTENT,
-                                               ms / (float)rounds};
+                                               ms / (float)rounds, 0.0f, 0.0f};
                 }
             }
         }
@@ -1786,10 +1788,12 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_autotune(NphGpuBatch *b, const NphGpuWorl
         }
         if (r == NPH_GPU_OK) {
             const float ms = timed([&] { return nph_gpu_world_step_async(b->merged, params, dt, 1); });
+            merged_ms = ms / (float)rounds;
             if (ms < best) {
                 best = ms;
                 chosen = NphGpuBatchTuning{b->config, kBatchConfigs[b->config].threads, b->shared_mode,
-                                           b->items_per_thread, NPH_GPU_BATCH_MERGED, ms / (float)rounds};
+                                           b->items_per_thread, NPH_GPU_BATCH_MERGED, ms / (float)rounds, 0.0f,
+                                           0.0f};
             }
         }
     }
@@ -1806,6 +1810,8 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_autotune(NphGpuBatch *b, const NphGpuWorl
     if (ro == NPH_GPU_OK) {
         ro = apply_order(b);
     }
+    chosen.persistent_ms_per_step = best_persistent;
+    chosen.merged_ms_per_step = merged_ms;
     if (out != nullptr) {
         *out = chosen;
     }

@@ -252,8 +252,9 @@ NPH_D float manifold_residual_sq(const DevSolver &S, uint32_t g, float inv_h)
     return sum;
 }
 
-// The residual's square, summed over the manifolds into acc[0] (one atomic per block).
-__global__ void __launch_bounds__(256) k_residual(DevSolver S, uint32_t m, float inv_h, float *acc,
+// The residual's square: each block's sum over its manifolds into partials[blockIdx.x].
+constexpr uint32_t kResidualBlocks = 148u * 8u; // the most blocks a residual launch has
+__global__ void __launch_bounds__(256) k_residual(DevSolver S, uint32_t m, float inv_h, float *partials,
                                                   const uint32_t *done)
 {
     if (*done != 0u) {
@@ -277,19 +278,38 @@ __global__ void __launch_bounds__(256) k_residual(DevSolver S, uint32_t m, float
         for (uint32_t w = 0; w < blockDim.x / 32u; ++w) {
             t += part[w];
         }
-        atomicAdd(acc, t);
+        partials[blockIdx.x] = t;
     }
 }
 
-// After pass p (0: the warm start): the residual, the reference residual at p = 0, and the
-// stop test. state[0] done, state[1] the passes run.
-__global__ void k_residual_check(const float *res_sq, float *residuals, float *ref, uint32_t p, float tolerance,
-                                 float ref_in, uint32_t *state)
+// After pass p (0: the warm start), one block of 256 threads: the blocks' partial sums added
+// in a fixed order (so a run's residuals are the same bits every time), the residual, the
+// reference residual at p = 0, and the stop test. state[0] done, state[1] the passes run.
+__global__ void __launch_bounds__(256) k_residual_check(const float *partials, uint32_t nparts, float *res_sq,
+                                                        float *residuals, float *ref, uint32_t p,
+                                                        float tolerance, float ref_in, uint32_t *state)
 {
-    if (state[0] != 0u) {
+    if (state[0] != 0u) { // read by every thread before any thread writes it
         return;
     }
-    const float r = sqrtf(res_sq[p]);
+    __shared__ float sh[256];
+    float v = 0.0f;
+    for (uint32_t i = threadIdx.x; i < nparts; i += 256u) {
+        v += partials[i];
+    }
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (uint32_t half = 128u; half > 0u; half >>= 1) {
+        if (threadIdx.x < half) {
+            sh[threadIdx.x] += sh[threadIdx.x + half];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x != 0u) {
+        return;
+    }
+    res_sq[p] = sh[0];
+    const float r = sqrtf(sh[0]);
     residuals[p] = r;
     if (p == 0u) {
         ref[0] = ref_in > 0.0f ? ref_in : r;

@@ -1034,7 +1034,7 @@ struct NphGpuSolver {
     uint32_t *l_counts = nullptr; // [0] cold points, [1] features written
     // The residual-driven mode's buffers.
     uint32_t rcap = 0;            // residual slots (passes + 1)
-    float *r_sq = nullptr, *r_val = nullptr, *r_ref = nullptr;
+    float *r_sq = nullptr, *r_val = nullptr, *r_ref = nullptr, *r_part = nullptr;
     uint32_t *r_state = nullptr;  // [0] done, [1] passes, [2] cold points, [3] predicted
 };
 
@@ -1705,7 +1705,7 @@ NphGpuResult ensure_residuals(NphGpuSolver *s, uint32_t slots)
         return NPH_GPU_OK;
     }
     const bool ok = dalloc(s->r_sq, slots) && dalloc(s->r_val, slots) && dalloc(s->r_ref, 1) &&
-                    dalloc(s->r_state, 4);
+                    dalloc(s->r_state, 4) && dalloc(s->r_part, kResidualBlocks);
     if (!ok) {
         s->rcap = 0;
         cudaGetLastError();
@@ -1942,6 +1942,7 @@ NPH_GPU_API void nph_gpu_solver_destroy(NphGpuSolver *s)
     dfree(s->l_slot);
     dfree(s->l_counts);
     dfree(s->r_sq);
+    dfree(s->r_part);
     dfree(s->r_val);
     dfree(s->r_ref);
     dfree(s->r_state);
@@ -2489,14 +2490,15 @@ NPH_GPU_API NphGpuResult nph_gpu_world_converge(NphGpuSolver *s, const NphGpuWor
                                                 float reference_residual, float *residuals, float *impulses,
                                                 NphGpuConvergeStats *out)
 {
-    if (s == nullptr || out == nullptr || !(tolerance > 0.0f) || max_passes > 1000000u) {
+    if (s == nullptr || out == nullptr || !(tolerance > 0.0f) || max_passes > 1000000u ||
+        learned > NPH_GPU_START_GATED) {
         return NPH_GPU_INVALID_ARGUMENT;
     }
     NphGpuResult r = validate_soft_params(params, dt);
     if (r != NPH_GPU_OK) {
         return r;
     }
-    if (!s->uploaded || (learned != 0u && s->mlp == nullptr)) {
+    if (!s->uploaded || (learned != NPH_GPU_START_PLAIN && s->mlp == nullptr)) {
         return NPH_GPU_INVALID_STATE;
     }
     std::memset(out, 0, sizeof *out);
@@ -2516,33 +2518,63 @@ NPH_GPU_API NphGpuResult nph_gpu_world_converge(NphGpuSolver *s, const NphGpuWor
     cudaEventCreate(&e1);
     cudaMemsetAsync(s->r_sq, 0, (max_passes + 1u) * sizeof(float), s->stream);
     cudaMemsetAsync(s->r_val, 0, (max_passes + 1u) * sizeof(float), s->stream);
-    cudaMemsetAsync(s->r_state, 0, 4 * sizeof(uint32_t), s->stream);
     s->marks = nullptr;
     const uint32_t *done = s->r_state;
-    const uint32_t res_blocks = std::max<uint32_t>(1u, std::min<uint32_t>(blocks_for(s->m), 148u * 8u));
-    cudaEventRecord(e0, s->stream);
-    enqueue_prepare(s, K);
-    // Cold points: counted (plain), or counted and started by the network (learned).
-    const bool use = learned != 0u && s->lcap > 0u;
-    if (s->m > 0u) {
-        k_cold_features<<<blocks_for(s->m), 256, 0, s->stream>>>(S, s->m, feature_consts(K), s->l_feat, s->l_scale,
-                                                                 s->l_slot, s->r_state + 2, use ? s->lcap : 0u,
-                                                                 use ? 1u : 0u);
-        if (use) {
-            nph_mlp_forward_device_count(s->mlp, s->l_feat, s->r_state + 3, s->lcap, s->l_pred, s->stream);
-            k_apply_predictions<<<blocks_for(s->lcap), 256, 0, s->stream>>>(S, s->l_pred, s->l_scale, s->l_slot,
-                                                                            s->r_state + 2, s->lcap);
+    const uint32_t res_blocks = std::max<uint32_t>(1u, std::min<uint32_t>(blocks_for(s->m), kResidualBlocks));
+    // The start: prepare from the uploaded records, the cold points counted (and started by the
+    // network when `net`), the first substep's velocity integration and warm start, and the
+    // residual after it against `ref_in` (<= 0: its own). Prepare rebuilds every row the passes
+    // use from the records, so a second start replaces the first.
+    auto start = [&](bool net, float ref_in) {
+        cudaMemsetAsync(s->r_state, 0, 4 * sizeof(uint32_t), s->stream);
+        enqueue_prepare(s, K);
+        if (s->m > 0u) {
+            k_cold_features<<<blocks_for(s->m), 256, 0, s->stream>>>(S, s->m, feature_consts(K), s->l_feat,
+                                                                     s->l_scale, s->l_slot, s->r_state + 2,
+                                                                     net ? s->lcap : 0u, net ? 1u : 0u);
+            if (net) {
+                nph_mlp_forward_device_count(s->mlp, s->l_feat, s->r_state + 3, s->lcap, s->l_pred, s->stream);
+                k_apply_predictions<<<blocks_for(s->lcap), 256, 0, s->stream>>>(S, s->l_pred, s->l_scale,
+                                                                                s->l_slot, s->r_state + 2, s->lcap);
+            }
         }
+        k_integrate_velocity<<<blocks_for(s->n), kBlock, 0, s->stream>>>(B, s->n, K.h);
+        enqueue_pass<kWarm>(s, K);
+        k_residual<<<res_blocks, 256, 0, s->stream>>>(S, s->m, K.inv_h, s->r_part, done);
+        k_residual_check<<<1, 256, 0, s->stream>>>(s->r_part, res_blocks, s->r_sq, s->r_val, s->r_ref, 0u,
+                                                   tolerance, ref_in, s->r_state);
+    };
+    auto initial = [&](float &v) {
+        cudaMemcpyAsync(&v, s->r_val, sizeof v, cudaMemcpyDeviceToHost, s->stream);
+        return check_cuda(cudaStreamSynchronize(s->stream));
+    };
+    const bool use = learned != NPH_GPU_START_PLAIN && s->lcap > 0u;
+    bool fell_back = false;
+    float reference = reference_residual;
+    cudaEventRecord(e0, s->stream);
+    if (use && learned == NPH_GPU_START_GATED) {
+        // The plain start is the fallback: the network's start is kept only when the plain
+        // solver's residual after it is no larger than after the plain start.
+        if (!(reference > 0.0f)) {
+            start(false, 0.0f);
+            r = initial(reference);
+        }
+        float learned_initial = 0.0f;
+        if (r == NPH_GPU_OK) {
+            start(true, reference);
+            r = initial(learned_initial);
+        }
+        if (r == NPH_GPU_OK && learned_initial > reference) {
+            start(false, reference);
+            fell_back = true;
+        }
+    } else {
+        start(use, reference);
     }
-    k_integrate_velocity<<<blocks_for(s->n), kBlock, 0, s->stream>>>(B, s->n, K.h);
-    enqueue_pass<kWarm>(s, K);
-    k_residual<<<res_blocks, 256, 0, s->stream>>>(S, s->m, K.inv_h, s->r_sq, done);
-    k_residual_check<<<1, 1, 0, s->stream>>>(s->r_sq, s->r_val, s->r_ref, 0u, tolerance, reference_residual,
-                                             s->r_state);
     // Passes in chunks of eight; the host stops issuing once the residual reached the tolerance.
     uint32_t state[4] = {0u, 0u, 0u, 0u};
     uint32_t issued = 0;
-    while (issued < max_passes) {
+    while (r == NPH_GPU_OK && issued < max_passes) {
         cudaMemcpyAsync(state, s->r_state, sizeof state, cudaMemcpyDeviceToHost, s->stream);
         r = check_cuda(cudaStreamSynchronize(s->stream));
         if (r != NPH_GPU_OK || state[0] != 0u) {
@@ -2552,9 +2584,9 @@ NPH_GPU_API NphGpuResult nph_gpu_world_converge(NphGpuSolver *s, const NphGpuWor
         for (uint32_t q = 0; q < chunk; ++q) {
             const uint32_t p = ++issued;
             enqueue_converge_pass(s, K, done);
-            k_residual<<<res_blocks, 256, 0, s->stream>>>(S, s->m, K.inv_h, s->r_sq + p, done);
-            k_residual_check<<<1, 1, 0, s->stream>>>(s->r_sq, s->r_val, s->r_ref, p, tolerance, reference_residual,
-                                                     s->r_state);
+            k_residual<<<res_blocks, 256, 0, s->stream>>>(S, s->m, K.inv_h, s->r_part, done);
+            k_residual_check<<<1, 256, 0, s->stream>>>(s->r_part, res_blocks, s->r_sq, s->r_val, s->r_ref, p,
+                                                       tolerance, reference, s->r_state);
         }
     }
     cudaEventRecord(e1, s->stream);
@@ -2596,7 +2628,8 @@ NPH_GPU_API NphGpuResult nph_gpu_world_converge(NphGpuSolver *s, const NphGpuWor
     out->passes = passes;
     out->converged = state[0];
     out->cold_points = state[2];
-    out->predicted_points = use ? std::min(state[3], s->lcap) : 0u;
+    out->predicted_points = use && !fell_back ? std::min(state[3], s->lcap) : 0u;
+    out->fell_back = fell_back ? 1u : 0u;
     out->initial_residual = vals[0];
     out->final_residual = vals[passes];
     out->reference_residual = ref;

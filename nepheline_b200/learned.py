@@ -118,7 +118,8 @@ def exact_start(view: abi.View, kind: np.ndarray, impulses: np.ndarray) -> abi.V
 def judge(solver, mlp, view: abi.View, params: abi.WorldParams, dt: float,
           tolerances=(1e-1, 1e-2, 1e-3, 1e-4), max_passes: int = 2000) -> dict:
     """Passes and device time to each tolerance of the plain start's initial residual, for the
-    plain start, the learned start and the exact start, on one world (each run stops at its
+    plain start, the network's start, the gated start (the network's start with the plain start
+    as its fallback, abi.START_GATED) and the exact start, on one world (each run stops at its
     tolerance, so each time is the run's own)."""
     solver.upload(view)
     _, _, kind = solver.features(params, dt)
@@ -132,21 +133,24 @@ def judge(solver, mlp, view: abi.View, params: abi.WorldParams, dt: float,
            "tolerances": {}}
     for tol in sorted(tolerances, reverse=True):
         row = {}
-        for name in ("plain", "learned", "exact"):
+        for name in ("plain", "learned", "gated", "exact"):
             if name == "exact":
                 solver.upload(exact)
             else:
                 solver.upload(view)
-            if name == "learned":
+            start = {"learned": abi.START_LEARNED, "gated": abi.START_GATED}.get(name, abi.START_PLAIN)
+            if start != abi.START_PLAIN:
                 solver.set_warm_start_model(mlp)
             try:
-                r = solver.converge(params, dt, learned=name == "learned", tolerance=tol,
+                r = solver.converge(params, dt, learned=start, tolerance=tol,
                                     max_passes=max_passes, reference_residual=ref)
             finally:
-                if name == "learned":
+                if start != abi.START_PLAIN:
                     solver.set_warm_start_model(None)
             row[name] = int(r["passes"]) if r["converged"] else None
             row[name + "_ms"] = float(r["ms"])
+            if name == "gated":
+                row["gated_fell_back"] = bool(r["fell_back"])
             if tol == max(tolerances):
                 out[name + "_initial_over_plain"] = float(r["initial_residual"]) / ref if ref > 0 else None
         out["tolerances"][f"{tol:g}"] = row

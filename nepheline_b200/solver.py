@@ -270,10 +270,12 @@ class Solver:
                                                           else mlp.handle),
                "nph_gpu_solver_set_warm_start_model")
 
-    def converge(self, params: abi.WorldParams, dt: float, learned: bool = False,
+    def converge(self, params: abi.WorldParams, dt: float, learned=False,
                  tolerance: float = 1e-4, max_passes: int = 2000,
                  reference_residual: float = 0.0, impulses: bool = False) -> dict:
-        """The residual-driven mode on the uploaded world (nph_gpu_world_converge)."""
+        """The residual-driven mode on the uploaded world (nph_gpu_world_converge). `learned`:
+        False/True (the plain or the network's start) or an abi.START_* value (START_GATED: the
+        network's start with the plain start as its fallback)."""
         res = np.zeros(max_passes + 1, np.float32)
         imp = np.zeros(12 * int(self._m), np.float32) if impulses else None
         st = abi.ConvergeStats()
@@ -469,7 +471,8 @@ class Batch:
         return {"config": t.config, "threads": t.threads,
                 "shared_velocities": t.shared_velocities, "items_per_thread": t.items_per_thread,
                 "packing": t.packing,
-                "ms_per_step": t.ms_per_step}
+                "ms_per_step": t.ms_per_step, "persistent_ms_per_step": t.persistent_ms_per_step,
+                "merged_ms_per_step": t.merged_ms_per_step}
 
     def info(self) -> dict:
         i = abi.BatchInfo()

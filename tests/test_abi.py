@@ -36,9 +36,9 @@ def test_record_layouts_match_the_header(tmp_path):
         'offsetof(NphGpuJoint,linear_impulse),offsetof(NphGpuContact,points),'
         'sizeof(NphGpuKernelTime),sizeof(NphGpuBatchTuning),sizeof(NphGpuBatchInfo),'
         'sizeof(NphGpuStepStats),sizeof(NphGpuSolverDesc));'
-        'printf("%zu %zu %zu %zu %zu %zu %zu\\n",sizeof(NphGpuBodyInput),sizeof(NphGpuContactInput),'
+        'printf("%zu %zu %zu %zu %zu %zu %zu %zu\\n",sizeof(NphGpuBodyInput),sizeof(NphGpuContactInput),'
         'sizeof(NphGpuBodyOutput),sizeof(NphGpuContactOutput),sizeof(NphGpuJointOutput),'
-        'sizeof(NphGpuPackedInput),sizeof(NphGpuPackedOutput));return 0;}\n')
+        'sizeof(NphGpuPackedInput),sizeof(NphGpuPackedOutput),sizeof(NphGpuConvergeStats));return 0;}\n')
     exe = tmp_path / "sizes"
     subprocess.run(["gcc", f"-I{HEADER.parent}", str(src), "-o", str(exe)], check=True)
     got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True,
@@ -51,7 +51,8 @@ def test_record_layouts_match_the_header(tmp_path):
                    ctypes.sizeof(abi.BatchTuning), ctypes.sizeof(abi.BatchInfo),
                    ctypes.sizeof(abi.StepStats), ctypes.sizeof(abi.SolverDesc),
                    sz["body_input"], sz["contact_input"], sz["body_output"], sz["contact_output"],
-                   sz["joint_output"], sz["packed_input"], sz["packed_output"]]
+                   sz["joint_output"], sz["packed_input"], sz["packed_output"],
+                   ctypes.sizeof(abi.ConvergeStats)]
 
 
 def test_library_exports_every_declared_entry_point():

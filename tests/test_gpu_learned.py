@@ -174,6 +174,50 @@ def test_learned_converge_matches_the_restatement(solver):
     net.close()
 
 
+def gated_against_plain_and_learned(solver, net, view, params, tol=1e-4, max_passes=3000):
+    """The gated start beside the plain and the network's own start on one world: the gate
+    keeps the network's start exactly when its initial residual is no larger than the plain
+    start's, and the run it keeps is that start's run, bit for bit. Given no reference, the
+    gated start runs the plain start first and judges by its residual the same way."""
+    solver.upload(view)
+    plain = solver.converge(params, DT, tolerance=tol, max_passes=max_passes, impulses=True)
+    ref = float(plain["reference_residual"])
+    solver.set_warm_start_model(net)
+    try:
+        learned = solver.converge(params, DT, learned=abi.START_LEARNED, tolerance=tol,
+                                  max_passes=max_passes, reference_residual=ref, impulses=True)
+        gated = solver.converge(params, DT, learned=abi.START_GATED, tolerance=tol,
+                                max_passes=max_passes, reference_residual=ref, impulses=True)
+        alone = solver.converge(params, DT, learned=abi.START_GATED, tolerance=tol,
+                                max_passes=max_passes, impulses=True)
+    finally:
+        solver.set_warm_start_model(None)
+    keep = learned["initial_residual"] <= ref
+    want = learned if keep else plain
+    for run in (gated, alone):
+        assert run["fell_back"] == (0 if keep else 1)
+        assert run["passes"] == want["passes"] and run["converged"] == want["converged"]
+        assert np.array_equal(run["residuals"], want["residuals"])
+        assert np.array_equal(run["impulses"], want["impulses"])
+        assert run["predicted_points"] == (learned["predicted_points"] if keep else 0)
+        assert run["reference_residual"] == ref
+    assert plain["fell_back"] == learned["fell_back"] == 0
+    return keep
+
+
+def test_gated_start_falls_back_to_the_plain_start(solver):
+    """A network whose starts push every new contact far too hard (an untrained network with
+    its weights scaled up): the gate sees the larger residual and the plain start runs."""
+    from nepheline_b200.solver import Mlp
+    params = abi.WorldParams.default()
+    net = Mlp(seed=11)
+    net.set_weights(net.get_weights() * 8.0)
+    try:
+        assert not gated_against_plain_and_learned(solver, net, moving_world(seed=8), params)
+    finally:
+        net.close()
+
+
 def test_attached_model_changes_only_cold_points(solver):
     """With every point warm, a step with a network attached is the plain step bit for bit; with
     cold points it differs; detached, the plain step again."""
@@ -233,5 +277,8 @@ def test_trained_network_gains_over_the_zero_start(solver):
         assert cmp["learned_initial_over_plain"] < 0.5
         plain += cmp["tolerances"]["0.001"]["plain"]
         learned_total += cmp["tolerances"]["0.001"]["learned"]
+        # The gate keeps this network's start.
+        assert gated_against_plain_and_learned(solver, net, ground_drop(seed), params, tol=1e-3,
+                                               max_passes=500)
     assert learned_total < plain
     net.close()
