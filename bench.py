@@ -11,9 +11,11 @@ solve, integrate, relax) over every colour, restitution, store, finalize. One co
 is one manifold in one solve or relax pass: 2 x substeps x manifolds per step.
 
   value   device time of K resident steps (CUDA events on the solver's stream, max over ranks)
-  e2e     the same metric through the drop-in call nph_gpu_phys_solve on pinned host
-          records: host->device upload, the step, device->host download, every step
-  roofline the dominant kernel (the solve pass) against the measured HBM bandwidth
+  e2e     the same metric through the packed drop-in call nph_gpu_phys_solve_packed on pinned
+          host records: host->device upload, the step, device->host download, every step
+          (the whole-record call nph_gpu_phys_solve beside it)
+  roofline the dominant kernel (the solve or the relax pass, whichever takes longer) against
+          the HBM bandwidth
   cpu_baseline the reference's own phys_solve (oracle/_ref, built from its sources) on the
           host's cores, on a bounded sample of the same workload
 
@@ -51,7 +53,8 @@ def parse():
                     help="lattice bodies per axis (128,128,64: 1,048,576 bodies)")
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=("lattice", "batched", "learned", "narrow"), default="lattice",
+    ap.add_argument("--workload", choices=("lattice", "batched", "learned", "narrow", "network"),
+                    default="lattice",
                     help="lattice: the 1M-body constraint graph (the headline); batched: "
                          "--worlds independent worlds in one persistent launch")
     ap.add_argument("--worlds", type=int, default=4096)
@@ -71,6 +74,8 @@ def parse():
     ap.add_argument("--eval-steps", default="20,40,60,90",
                     help="learned: steps of the held-out piles judged")
     ap.add_argument("--max-passes", type=int, default=2000)
+    ap.add_argument("--rows", type=int, default=4 * 1024 * 1024,
+                    help="network: feature rows a launch (the learned start's cold points)")
     ap.add_argument("--epochs", type=int, default=30)
     ap.add_argument("--solver", choices=("soft_step", "tgs"), default="soft_step",
                     help="the world's solver (lattice and batched workloads; learned: soft step)")
@@ -874,6 +879,65 @@ def run_learned(args):
     return 0
 
 
+# The network's work per feature row: 16 -> 64 -> 64 -> 64 -> 3 multiply-adds, and the bytes of
+# a row in (16 floats) and out (3 floats; the gradient pass reads 3 target floats instead).
+NETWORK_MACS = 16 * 64 + 64 * 64 + 64 * 64 + 64 * 3
+NETWORK_BYTES = 4 * (16 + 3)
+
+
+def run_network(args):
+    """--workload network: the learned start's network on --rows device-resident feature rows
+    (a seeded pattern): one forward launch and one gradient launch (forward, backward and the
+    weight gradients summed over the rows) a step, timed with CUDA events. Rank 0 only."""
+    import torch
+
+    from nepheline_b200.solver import Mlp
+
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    net = Mlp(device=local, seed=0)
+    net.time_kernels(args.rows, reps=max(1, args.warmup))
+    clk = Clocks(local).__enter__()
+    t = net.time_kernels(args.rows, reps=args.steps)
+    clocks = clk.summary()
+    clk.__exit__(None, None, None)
+    net.close()
+    fwd_flops = 2.0 * NETWORK_MACS * args.rows
+    # Backward: the activations' gradients through layers 4..2 and every layer's weight gradient.
+    grad_flops = fwd_flops + 2.0 * args.rows * (2 * NETWORK_MACS - 16 * 64)
+    fwd_tf = fwd_flops / (t["forward_ms"] * 1e-3) / 1e12
+    grad_tf = grad_flops / (t["gradients_ms"] * 1e-3) / 1e12
+    gbs = NETWORK_BYTES * args.rows / (t["forward_ms"] * 1e-3) / 1e9
+    pk = peaks()
+    tensor_peak, tensor_src = 1590.0, "fallback"
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        tensor_peak, tensor_src = float(json.loads(p.read_text())["bf16_tflops"]), "measured"
+    rows_s = args.rows / (t["forward_ms"] * 1e-3)
+    print(json.dumps({
+        "metric": "network feature rows/s (forward)", "value": rows_s, "unit": "rows/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t["forward_ms"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16 weights and activations, f32 accumulate", "data": "synthetic",
+        "config": {"workload": f"the learned start's network 16-64-64-64-3 on {args.rows} "
+                               f"device-resident feature rows (seeded pattern)",
+                   "rows": args.rows, "l2": "inputs larger than L2" if args.rows * 76 > 126e6
+                   else "inputs smaller than L2"},
+        "gradients": {"ms_per_launch": t["gradients_ms"], "tflops": grad_tf,
+                      "rows_per_s": args.rows / (t["gradients_ms"] * 1e-3)},
+        "roofline": {"bound": "tensor", "achieved": fwd_tf, "peak": tensor_peak, "unit": "TFLOP/s",
+                     "frac": fwd_tf / tensor_peak, "traffic": None, "peak_source": tensor_src,
+                     "kernel": "k_mlp_forward", "hbm_gbs": gbs, "hbm_frac": gbs / pk["hbm_gbs"]},
+        "e2e": None,
+        "gpu_launches": 2 * args.steps,
+        "clocks": clocks,
+    }))
+    return 0
+
+
 def workload_name(dims) -> str:
     n = dims[0] * dims[1] * dims[2]
     return f"synthetic constraint graph, {dims[0]}x{dims[1]}x{dims[2]} lattice, {n} bodies"
@@ -889,6 +953,8 @@ def main():
         return run_learned(args)
     if args.workload == "narrow":
         return run_narrow(args)
+    if args.workload == "network":
+        return run_network(args)
     import torch
 
     from nepheline_b200 import abi

@@ -830,6 +830,13 @@ NPH_GPU_API NphGpuResult nph_gpu_mlp_train(NphGpuMlp *mlp, const float *features
                                            uint32_t batch, float lr, uint64_t shuffle_seed,
                                            float *final_loss);
 
+/* Times the network's kernels on `count` device-resident rows (at most 2^31): features and
+ * targets a seeded pattern in [-1, 1) written on the device, then `reps` forward launches and
+ * `reps` gradient launches over all rows, each timed with CUDA events on the network's stream;
+ * writes the average milliseconds of one launch of each. The weights are not changed. */
+NPH_GPU_API NphGpuResult nph_gpu_mlp_time_kernels(NphGpuMlp *mlp, uint64_t count, uint32_t reps,
+                                                  float *forward_ms, float *gradients_ms);
+
 /* Point slots: manifold g's point k is slot 4 g + k (g in the uploaded colour order). */
 #define NPH_GPU_POINT_NONE 0u /* k >= the manifold's point count */
 #define NPH_GPU_POINT_WARM 1u /* starts at a persisted (non-zero) impulse */

@@ -120,6 +120,9 @@ __device__ DevSolver world_solver(const BatchArgs &A, const WorldSlice &W, float
     S.mcap = A.mcap;
     S.jw = A.jw + W.joint_first;
     S.jcap = A.jcap;
+    S.cmask = nullptr;
+    S.done = nullptr;
+    S.jrank = nullptr;
     return S;
 }
 

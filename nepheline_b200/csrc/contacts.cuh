@@ -168,7 +168,15 @@ NPH_D void prepare_manifold(const DevSolver &S, uint32_t g, const NphGpuContact 
 // once (__ldcs / __stcs: evicted first), so the body rows every manifold of a body reads stay in
 // L2 (measured 0.8 % and 0.3 % off the lattice step).
 
-NPH_D void warm_manifold(const DevSolver &S, uint32_t g)
+// Where a pass reads a manifold's body velocities it first calls gate(hdr): a dependency-driven
+// pass (solver.cu k_pass_flow) waits there for the constraints of earlier colours on the
+// bodies; a pass that runs a colour a launch reads them straight away.
+struct NoGate {
+    NPH_D void operator()(uint4) const {}
+};
+
+template <class Gate = NoGate>
+NPH_D void warm_manifold(const DevSolver &S, uint32_t g, const Gate &gate = Gate())
 {
     uint4 hdr = S.hdr[g];
     const V3 n = v3(S.nrm[g]);
@@ -190,6 +198,7 @@ NPH_D void warm_manifold(const DevSolver &S, uint32_t g)
         }
     }
     const Sides sd = load_sides(S.prm, hdr.x, hdr.y, bits);
+    gate(hdr);
     BodyState a = load_state(S.vel, hdr.x);
     BodyState b = load_state(S.vel, hdr.y);
     const V3 t1 = perpendicular(n);

@@ -68,6 +68,7 @@ NPH_D float4 ld_policy(const float4 *src, uint64_t policy)
     return v;
 }
 
+
 // Issues the manifold's loads into the lane's column: the rows of its own points (pt only
 // when `tangents`), and when `bodies` the velocities of both bodies, their displacements and
 // rotations when `poses`, and the inertia of the sides that take results. The copies are not
@@ -133,20 +134,18 @@ struct ManifoldBodies {
     BodyPose pa, pb;
 };
 
-// The lean form's body rows, loaded into registers (the poses only when `poses`).
-NPH_D ManifoldBodies load_bodies(const DevSolver &S, uint4 hdr, bool poses)
+// The lean form's body rows, loaded into registers (the poses only when `poses`). The
+// velocities come last, after `gate(hdr)`: a dependency-driven pass waits there for the
+// constraints of earlier colours on the bodies (the poses and inertias do not change during a
+// pass).
+template <class Gate = NoGate>
+NPH_D ManifoldBodies load_bodies(const DevSolver &S, uint4 hdr, bool poses, const Gate &gate = Gate())
 {
     const uint64_t keep = policy_evict_last();
     const uint32_t bits = hdr.z;
     ManifoldBodies m;
     m.sd.wa = (bits & kHdrWriteA) != 0u;
     m.sd.wb = (bits & kHdrWriteB) != 0u;
-    const float4 va = ld_policy(&S.vel[2u * hdr.x], keep);
-    const float4 wa = ld_policy(&S.vel[2u * hdr.x + 1u], keep);
-    const float4 vb = ld_policy(&S.vel[2u * hdr.y], keep);
-    const float4 wb = ld_policy(&S.vel[2u * hdr.y + 1u], keep);
-    m.a = BodyState{v3(va), v3(wa)};
-    m.b = BodyState{v3(vb), v3(wb)};
     if (poses) {
         const float4 pa = ld_policy(&S.pos[2u * hdr.x], keep);
         const float4 qa = ld_policy(&S.pos[2u * hdr.x + 1u], keep);
@@ -173,6 +172,13 @@ NPH_D ManifoldBodies load_bodies(const DevSolver &S, uint4 hdr, bool poses)
         m.sd.mb = c0.w;
         m.sd.ib = M3{v3(c0), v3(c1), v3(c2)};
     }
+    gate(hdr);
+    const float4 va = ld_policy(&S.vel[2u * hdr.x], keep);
+    const float4 wa = ld_policy(&S.vel[2u * hdr.x + 1u], keep);
+    const float4 vb = ld_policy(&S.vel[2u * hdr.y], keep);
+    const float4 wb = ld_policy(&S.vel[2u * hdr.y + 1u], keep);
+    m.a = BodyState{v3(va), v3(wa)};
+    m.b = BodyState{v3(vb), v3(wb)};
     return m;
 }
 
@@ -279,10 +285,11 @@ NPH_D void warm_manifold_staged(const DevSolver &S, uint32_t g, const Tile<kLane
     }
 }
 
-// solve_manifold (solver_impl.h:484-602) on the staged loads.
-template <bool kUseBias, uint32_t kLanes, bool kIssued = false, bool kBodies = true>
+// solve_manifold (solver_impl.h:484-602) on the staged loads; the lean form waits at `gate`
+// before it reads the velocities (load_bodies).
+template <bool kUseBias, uint32_t kLanes, bool kIssued = false, bool kBodies = true, class Gate = NoGate>
 NPH_D void solve_manifold_staged(const DevSolver &S, uint32_t g, const StepConsts &K,
-                                 const Tile<kLanes> &T)
+                                 const Tile<kLanes> &T, const Gate &gate = Gate())
 {
     const uint4 hdr = S.hdr[g];
     const float4 nf = S.nrm[g];
@@ -306,7 +313,7 @@ NPH_D void solve_manifold_staged(const DevSolver &S, uint32_t g, const StepConst
     } else {
         issue_manifold(S, g, hdr, T, true, true, false);
         __pipeline_commit();
-        const ManifoldBodies m = load_bodies(S, hdr, true);
+        const ManifoldBodies m = load_bodies(S, hdr, true, gate);
         __pipeline_wait_prior(0);
         sd = m.sd;
         a = m.a;

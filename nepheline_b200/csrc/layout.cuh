@@ -32,6 +32,11 @@
 
 namespace nph {
 
+// A constraint's rank on a body it writes, in hdr.w for a manifold (A in bits 0-7, B in bits
+// 8-15): how many constraints of earlier colours write that body (at most the colours).
+constexpr uint32_t kRankBits = 8u;
+constexpr uint32_t kRankMask = 0xFFu;
+
 // Manifold header bits (hdr.z).
 constexpr uint32_t kHdrPointsMask = 7u;        // the manifold's own point count, 0..4
 constexpr uint32_t kHdrGroupShift = 3u;        // its eight-lane group's largest point count
@@ -95,6 +100,7 @@ constexpr uint32_t kErrBadIndex = 1u << 0;
 constexpr uint32_t kErrBadPoints = 1u << 1;
 constexpr uint32_t kErrBadJoint = 1u << 2;
 constexpr uint32_t kErrBadBody = 1u << 3; // a value the stage reads is not finite
+constexpr uint32_t kErrWait = 1u << 4;    // a dependency-driven pass gave up a wait
 
 // The step's constants (StepContext, solver.c:67-85), computed on the host in FP32 with the
 // reference's operations.
@@ -130,6 +136,12 @@ struct DevSolver {
     uint32_t mcap;
     float4 *jw;                // joint rows, stride jcap
     uint32_t jcap;
+    // The dependency-driven passes (solver.cu k_pass_flow): per body slot, the colours whose
+    // constraints write it (bit c) and how many of them have finished the current pass; per
+    // joint, its rank on each body it writes (the manifolds' ranks are in hdr.w).
+    const uint32_t *cmask;
+    uint32_t *done;
+    uint32_t *jrank;
 };
 
 NPH_D M3 load_inv_inertia(const float4 *prm, uint32_t i, float *inv_mass)

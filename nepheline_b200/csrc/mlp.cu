@@ -54,23 +54,29 @@ static_assert(kParams == NPH_GPU_MLP_PARAMS, "parameter count");
 constexpr int kWarps = 4;            // per block
 constexpr int kThreads = 32 * kWarps;
 constexpr int kTile = 16;            // samples per warp tile
+// Shared-memory rows are padded by 8 bf16 (16 bytes): a fragment's eight rows then start in
+// eight different groups of four banks, so a warp's 32 fragment loads hit 32 banks (unpadded,
+// rows of 64 bf16 are 32 words apart and eight lanes share each bank).
+constexpr int kPad = 8;
+constexpr int kInRow = kIn + kPad;
+constexpr int kHidRow = kHid + kPad;
 
 // Shared memory of a block: the bf16 weights (and transposes), fp32 biases.
 struct SmemWeights {
-    __nv_bfloat16 w1[kHid][kIn];       // [out][in]
-    __nv_bfloat16 w2[kHid][kHid];
-    __nv_bfloat16 w3[kHid][kHid];
-    __nv_bfloat16 w4[kOutPad][kHid];   // rows >= 3 zero
-    __nv_bfloat16 w2t[kHid][kHid];     // [in][out]
-    __nv_bfloat16 w3t[kHid][kHid];
-    __nv_bfloat16 w4t[kHid][16];       // [in][out], out padded to one k-step
+    __nv_bfloat16 w1[kHid][kInRow];      // [out][in]
+    __nv_bfloat16 w2[kHid][kHidRow];
+    __nv_bfloat16 w3[kHid][kHidRow];
+    __nv_bfloat16 w4[kOutPad][kHidRow];  // rows >= 3 zero
+    __nv_bfloat16 w2t[kHid][kHidRow];    // [in][out]
+    __nv_bfloat16 w3t[kHid][kHidRow];
+    __nv_bfloat16 w4t[kHid][16 + kPad];  // [in][out], out padded to one k-step
     float b1[kHid], b2[kHid], b3[kHid], b4[kOutPad];
 };
 
 // A warp's scratch for the backward pass: a layer's dZ and input, bf16, [sample][unit].
 struct SmemTile {
-    __nv_bfloat16 dz[kTile][kHid];
-    __nv_bfloat16 h[kTile][kHid];
+    __nv_bfloat16 dz[kTile][kHidRow];
+    __nv_bfloat16 h[kTile][kHidRow];
 };
 
 __device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
@@ -102,7 +108,7 @@ __device__ __forceinline__ void mma(float d[4], const uint32_t a[4], uint32_t b0
 }
 
 // B fragment of rows [16 kt, 16 kt + 16) (the k index) and columns [8 nt, 8 nt + 8) (the n
-// index) of a matrix stored [n][k] (row-major by n), K columns wide.
+// index) of a matrix stored [n][k] (row-major by n), rows K bf16 apart.
 template <int K>
 __device__ __forceinline__ void b_frag(const __nv_bfloat16 (*w)[K], int nt, int kt, int g, int t,
                                        uint32_t &b0, uint32_t &b1)
@@ -166,7 +172,7 @@ __device__ __forceinline__ void forward(const SmemWeights &W, const float *x, ui
     for (int nt = 0; nt < 8; ++nt) {
         d[nt][0] = d[nt][1] = d[nt][2] = d[nt][3] = 0.0f;
         uint32_t b0, b1;
-        b_frag<kIn>(W.w1, nt, 0, g, t, b0, b1);
+        b_frag<kInRow>(W.w1, nt, 0, g, t, b0, b1);
         mma(d[nt], F.a0, b0, b1);
     }
     relu_to_a(d, W.b1, t, F.a1, F.m1);
@@ -176,7 +182,7 @@ __device__ __forceinline__ void forward(const SmemWeights &W, const float *x, ui
 #pragma unroll
         for (int kt = 0; kt < 4; ++kt) {
             uint32_t b0, b1;
-            b_frag<kHid>(W.w2, nt, kt, g, t, b0, b1);
+            b_frag<kHidRow>(W.w2, nt, kt, g, t, b0, b1);
             mma(d[nt], F.a1[kt], b0, b1);
         }
     }
@@ -187,7 +193,7 @@ __device__ __forceinline__ void forward(const SmemWeights &W, const float *x, ui
 #pragma unroll
         for (int kt = 0; kt < 4; ++kt) {
             uint32_t b0, b1;
-            b_frag<kHid>(W.w3, nt, kt, g, t, b0, b1);
+            b_frag<kHidRow>(W.w3, nt, kt, g, t, b0, b1);
             mma(d[nt], F.a2[kt], b0, b1);
         }
     }
@@ -196,7 +202,7 @@ __device__ __forceinline__ void forward(const SmemWeights &W, const float *x, ui
 #pragma unroll
     for (int kt = 0; kt < 4; ++kt) {
         uint32_t b0, b1;
-        b_frag<kHid>(W.w4, 0, kt, g, t, b0, b1);
+        b_frag<kHidRow>(W.w4, 0, kt, g, t, b0, b1);
         mma(F.y, F.a3[kt], b0, b1);
     }
     const int c = 2 * t;
@@ -209,12 +215,12 @@ __device__ __forceinline__ void forward(const SmemWeights &W, const float *x, ui
 __device__ void load_weights(SmemWeights &W, const __nv_bfloat16 *wb, const float *master)
 {
     for (int i = threadIdx.x; i < kHid * kIn; i += blockDim.x) {
-        (&W.w1[0][0])[i] = wb[kW1 + i];
+        W.w1[i / kIn][i % kIn] = wb[kW1 + i];
     }
     for (int i = threadIdx.x; i < kHid * kHid; i += blockDim.x) {
         const int o = i / kHid, k = i % kHid;
-        (&W.w2[0][0])[i] = wb[kW2 + i];
-        (&W.w3[0][0])[i] = wb[kW3 + i];
+        W.w2[o][k] = wb[kW2 + i];
+        W.w3[o][k] = wb[kW3 + i];
         W.w2t[k][o] = wb[kW2 + i];
         W.w3t[k][o] = wb[kW3 + i];
     }
@@ -278,7 +284,7 @@ __global__ void __launch_bounds__(kThreads) k_mlp_forward(const float *x, uint32
 }
 
 // dZ (accumulators of 8 n-tiles) to shared memory as bf16 [sample][unit].
-__device__ __forceinline__ void store_tile(__nv_bfloat16 (*dst)[kHid], const float d[8][4], int g, int t)
+__device__ __forceinline__ void store_tile(__nv_bfloat16 (*dst)[kHidRow], const float d[8][4], int g, int t)
 {
 #pragma unroll
     for (int nt = 0; nt < 8; ++nt) {
@@ -291,7 +297,7 @@ __device__ __forceinline__ void store_tile(__nv_bfloat16 (*dst)[kHid], const flo
 }
 
 // An A-fragment set (4 k-steps, 16 samples x 64 units) to shared memory [sample][unit].
-__device__ __forceinline__ void store_a(__nv_bfloat16 (*dst)[kHid], const uint32_t a[4][4], int g, int t)
+__device__ __forceinline__ void store_a(__nv_bfloat16 (*dst)[kHidRow], const uint32_t a[4][4], int g, int t)
 {
 #pragma unroll
     for (int kt = 0; kt < 4; ++kt) {
@@ -306,7 +312,7 @@ __device__ __forceinline__ void store_a(__nv_bfloat16 (*dst)[kHid], const uint32
 // grad[o][i] += sum over the tile's 16 samples of dz[s][o] h[s][i], for O outputs x I inputs,
 // on the tensor cores (A = dz^T, B = h), accumulated into fp32 shared memory.
 template <int O, int I>
-__device__ void weight_grad(const __nv_bfloat16 (*dz)[kHid], const __nv_bfloat16 (*h)[kHid], float *grad,
+__device__ void weight_grad(const __nv_bfloat16 (*dz)[kHidRow], const __nv_bfloat16 (*h)[kHidRow], float *grad,
                             int g, int t)
 {
     for (int mt = 0; mt < (O + 15) / 16; ++mt) {
@@ -340,7 +346,7 @@ __device__ void weight_grad(const __nv_bfloat16 (*dz)[kHid], const __nv_bfloat16
 }
 
 // dH = dZ W: dz fragments (A, 4 k-steps over the layer's outputs) times the transposed weights.
-__device__ __forceinline__ void back_mm(const uint32_t dz[4][4], const __nv_bfloat16 (*wt)[kHid], int g,
+__device__ __forceinline__ void back_mm(const uint32_t dz[4][4], const __nv_bfloat16 (*wt)[kHidRow], int g,
                                         int t, float d[8][4])
 {
 #pragma unroll
@@ -349,7 +355,7 @@ __device__ __forceinline__ void back_mm(const uint32_t dz[4][4], const __nv_bflo
 #pragma unroll
         for (int kt = 0; kt < 4; ++kt) {
             uint32_t b0, b1;
-            b_frag<kHid>(wt, nt, kt, g, t, b0, b1);
+            b_frag<kHidRow>(wt, nt, kt, g, t, b0, b1);
             mma(d[nt], dz[kt], b0, b1);
         }
     }
@@ -419,7 +425,7 @@ k_mlp_gradients(const float *x, const float *target, uint32_t count, float norm,
         }
         // Output layer: dW4 = dY^T h3, db4 = sum dY; dH3 = dY W4.
         __syncwarp();
-        for (int i = lane; i < kTile * kHid; i += 32) {
+        for (int i = lane; i < kTile * kHidRow; i += 32) {
             (&S.dz[0][0])[i] = __float2bfloat16(0.0f);
         }
         __syncwarp();
@@ -482,7 +488,7 @@ k_mlp_gradients(const float *x, const float *target, uint32_t count, float norm,
         mask_to_a(d, F.m1, dz1);
         __syncwarp();
         store_tile(S.dz, d, g, t);
-        for (int i = lane; i < kTile * kHid; i += 32) {
+        for (int i = lane; i < kTile * kHidRow; i += 32) {
             (&S.h[0][0])[i] = __float2bfloat16(0.0f);
         }
         __syncwarp();
@@ -631,6 +637,18 @@ void init_weights(std::vector<float> &w, uint64_t seed)
 }
 
 } // namespace
+
+// A seeded pattern in [-1, 1): a splitmix64 hash of (seed, i).
+__global__ void k_fill_pattern(float *p, uint64_t n, uint64_t seed)
+{
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t z = (seed + i + 1u) * 0x9E3779B97F4A7C15ull;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        p[i] = (float)(z >> 40) * (2.0f / 16777216.0f) - 1.0f;
+    }
+}
 
 // The network's inference on device features (the solver's learned warm start).
 void nph_mlp_forward_device(const NphGpuMlp *n, const float *x, uint32_t count, float *y, cudaStream_t st)
@@ -789,6 +807,51 @@ NPH_GPU_API NphGpuResult nph_gpu_mlp_gradients(NphGpuMlp *n, const float *featur
     if (loss != nullptr) {
         *loss = sq / (float)count;
     }
+    return r;
+}
+
+NPH_GPU_API NphGpuResult nph_gpu_mlp_time_kernels(NphGpuMlp *n, uint64_t count, uint32_t reps, float *forward_ms,
+                                                  float *gradients_ms)
+{
+    if (n == nullptr || count == 0 || count > 0x80000000ull || reps == 0 || forward_ms == nullptr ||
+        gradients_ms == nullptr) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    cudaSetDevice(n->device);
+    NphGpuResult r = ensure_samples(n, count);
+    if (r != NPH_GPU_OK) {
+        return r;
+    }
+    const uint32_t fill_blocks = (uint32_t)n->sms * 8u;
+    k_fill_pattern<<<fill_blocks, 256, 0, n->stream>>>(n->x, count * kIn, 1u);
+    k_fill_pattern<<<fill_blocks, 256, 0, n->stream>>>(n->tgt, count * kOut, 2u);
+    cudaEvent_t e[3];
+    for (cudaEvent_t &ev : e) {
+        cudaEventCreate(&ev);
+    }
+    const uint32_t c = (uint32_t)count;
+    nph_mlp_forward_device(n, n->x, c, n->y, n->stream); // warm-up launches
+    enqueue_gradients(n, n->x, n->tgt, c, (float)count);
+    cudaEventRecord(e[0], n->stream);
+    for (uint32_t i = 0; i < reps; ++i) {
+        nph_mlp_forward_device(n, n->x, c, n->y, n->stream);
+    }
+    cudaEventRecord(e[1], n->stream);
+    for (uint32_t i = 0; i < reps; ++i) {
+        enqueue_gradients(n, n->x, n->tgt, c, (float)count);
+    }
+    cudaEventRecord(e[2], n->stream);
+    r = mlp_cuda(cudaStreamSynchronize(n->stream));
+    float f = 0.0f, g = 0.0f;
+    if (r == NPH_GPU_OK) {
+        cudaEventElapsedTime(&f, e[0], e[1]);
+        cudaEventElapsedTime(&g, e[1], e[2]);
+    }
+    for (cudaEvent_t &ev : e) {
+        cudaEventDestroy(ev);
+    }
+    *forward_ms = f / (float)reps;
+    *gradients_ms = g / (float)reps;
     return r;
 }
 

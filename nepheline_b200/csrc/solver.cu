@@ -398,7 +398,9 @@ k_pass_pipelined(DevSolver S, uint32_t cfirst, uint32_t ccount, StepConsts K)
 // allows (65,536 registers / (threads x blocks)); `staged`: 0 plain loads, 1 the loads staged
 // through shared memory (kSlots x threads x 16 bytes per block), 2 staged and pipelined, 3 the
 // lean staged form (kPointSlots x threads x 16 bytes per block), 4 two lanes a manifold for
-// the warm start (contacts_pair.cuh; the other pass kinds run the plain kernel).
+// the warm start (contacts_pair.cuh; the other pass kinds run the plain kernel), 5 the whole
+// pass in one dependency-driven launch of one-warp blocks (k_pass_flow: the warm start's
+// contacts plain, the solve and relax passes' lean staged; restitution runs the plain kernel).
 struct PassConfig {
     uint32_t threads, min_blocks, staged;
 };
@@ -406,7 +408,8 @@ constexpr PassConfig kPassConfigs[] = {{256, 1, 0}, {256, 2, 0}, {128, 4, 0}, {2
                                        {64, 6, 1},  {64, 7, 1},  {128, 3, 1}, {32, 14, 1},
                                        {32, 7, 2},  {64, 3, 2},  {32, 18, 3}, {32, 24, 3},
                                        {64, 9, 3},  {64, 12, 3}, {128, 6, 3}, {128, 6, 4},
-                                       {128, 8, 4}, {64, 14, 4}, {256, 4, 4}};
+                                       {128, 8, 4}, {64, 14, 4}, {256, 4, 4},  {32, 18, 5},
+                                       {32, 16, 5}, {32, 20, 5}};
 constexpr uint32_t kPassConfigCount = sizeof(kPassConfigs) / sizeof(kPassConfigs[0]);
 
 template <int P>
@@ -415,6 +418,10 @@ void launch_pass(uint32_t config, uint32_t cc, cudaStream_t st, const DevSolver 
 {
     const uint32_t t = kPassConfigs[config].threads;
     const uint32_t grid = (cc + t - 1) / t;
+    if (kPassConfigs[config].staged == 5u) { // a colour at a time: the plain kernel
+        k_pass<P, 128, 4><<<(cc + 127u) / 128u, 128, 0, st>>>(S, cfirst, cc, K);
+        return;
+    }
     if (kPassConfigs[config].staged == 4u) {
         if (P == kWarm) {
             const uint32_t pair_grid = (2u * cc + t - 1) / t;
@@ -495,6 +502,233 @@ __global__ void k_overflow(DevSolver S, uint32_t cfirst, uint32_t ccount, uint32
     }
     for (uint32_t g = 0; g < ccount; ++g) {
         contact_op<P>(S, cfirst + g, K);
+    }
+}
+
+// ---------------------------------------------------------------------------------------
+// Dependency-driven passes
+// ---------------------------------------------------------------------------------------
+//
+// One launch runs a whole warm start, solve or relax pass over every colour, in place of a
+// launch per colour (whose start and tail leave SMs idle, and whose last colours hold a few
+// constraints each). Warps take tickets in order; a ticket is 32 consecutive constraints of one
+// kind (joints or contacts) of one colour, the ranges in colour order, a colour's joints before
+// its contacts. A constraint of colour c waits until, on each body it writes, every constraint
+// of an earlier colour that writes the body has finished this pass. A body has at most one
+// constraint of each colour (the colouring's rule), so that count, the constraint's rank on the
+// body, is the number of earlier colours in the body's colour mask; prepare stores the ranks
+// (k_colour_ranks). Each finished constraint adds one to the counters of the bodies it wrote,
+// with release semantics after its velocity stores; a waiting constraint reads them with
+// acquire semantics, and only then reads the velocities, so by the PTX memory model it sees
+// the released rows. Every body thus takes its constraints in colour order, as with a launch
+// per colour, and every result has the same bits. A ticket waits only on lower tickets, held by
+// warps that are running, so every wait ends; each is bounded all the same: a wait that gives
+// up sets kErrWait (the call then fails) and the pass goes on without it, and once one has
+// given up the others give up at once.
+
+struct FlowTable {
+    uint32_t ranges;                           // ranges in use
+    uint32_t tickets;                          // tickets of all ranges
+    uint32_t ticket[2 * NPH_GPU_COLORS];       // each range's first ticket
+    uint32_t first[2 * NPH_GPU_COLORS];        // each range's first constraint
+    uint32_t count[2 * NPH_GPU_COLORS];        // each range's constraints
+    uint32_t colour_kind[2 * NPH_GPU_COLORS];  // the range's colour, | kFlowJoints for joints
+};
+constexpr uint32_t kFlowJoints = 0x100u;
+constexpr uint32_t kFlowPolls = 1u << 20; // about a second of polls, 64 ns of sleep apart
+
+NPH_D uint32_t ld_acquire_gpu(const uint32_t *p)
+{
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+NPH_D void red_release_gpu_add(uint32_t *p, uint32_t v)
+{
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
+}
+
+// Waits until `need` constraints that write `body` have finished this pass.
+NPH_D void flow_wait(uint32_t *done, uint32_t body, uint32_t need, uint32_t *err)
+{
+    if (need == 0u) {
+        return;
+    }
+    for (uint32_t i = 0; i < kFlowPolls; ++i) {
+        if (ld_acquire_gpu(&done[body]) >= need) {
+            return;
+        }
+        if (i >= 8u) {
+            if ((i & 1023u) == 0u && (*(const volatile uint32_t *)err & kErrWait) != 0u) {
+                return;
+            }
+            __nanosleep(64);
+        }
+    }
+    atomicOr(err, kErrWait);
+}
+
+// The wait of a manifold of a dependency-driven pass: its ranks are in hdr.w.
+struct FlowGate {
+    uint32_t *done;
+    uint32_t *err;
+    NPH_D void operator()(uint4 hdr) const
+    {
+        if ((hdr.z & kHdrWriteA) != 0u) {
+            flow_wait(done, hdr.x, hdr.w & kRankMask, err);
+        }
+        if ((hdr.z & kHdrWriteB) != 0u) {
+            flow_wait(done, hdr.y, (hdr.w >> kRankBits) & kRankMask, err);
+        }
+    }
+};
+
+// The bodies a constraint writes: contacts 0..m-1, then joints.
+NPH_D void written_bodies(const DevSolver &S, bool joint, uint32_t k, uint32_t &a, uint32_t &b, bool &wa,
+                          bool &wb)
+{
+    if (joint) {
+        uint32_t flags;
+        joint_head(S, k, a, b, flags);
+        wa = (flags & kJWriteA) != 0u;
+        wb = (flags & kJWriteB) != 0u;
+    } else {
+        const uint4 hdr = S.hdr[k];
+        a = hdr.x;
+        b = hdr.y;
+        wa = (hdr.z & kHdrWriteA) != 0u && (hdr.z & kHdrPointsMask) != 0u;
+        wb = (hdr.z & kHdrWriteB) != 0u && (hdr.z & kHdrPointsMask) != 0u;
+    }
+}
+
+// A joint of a dependency-driven pass, out of line: the joints' registers stay out of the
+// contacts' path.
+template <int P> __device__ __noinline__ void flow_joint(const DevSolver &S, uint32_t j, const StepConsts &K)
+{
+    joint_op<P>(S, j, K);
+}
+
+template <int P, int kMinBlocks>
+__global__ void __launch_bounds__(32, kMinBlocks)
+k_pass_flow(DevSolver S, FlowTable F, StepConsts K, uint32_t *ticket, uint32_t *err)
+{
+    extern __shared__ float4 tile[];
+    const uint32_t lane = threadIdx.x;
+    const Tile<32> T{tile, lane};
+    const FlowGate gate{S.done, err};
+    // The next ticket is taken while the current one runs.
+    uint32_t t = 0u;
+    if (lane == 0u) {
+        t = atomicAdd(ticket, 1u);
+    }
+    t = __shfl_sync(0xFFFFFFFFu, t, 0);
+    while (t < F.tickets) {
+        uint32_t next = 0u;
+        if (lane == 0u) {
+            next = atomicAdd(ticket, 1u);
+        }
+        uint32_t r = 0u;
+        while (r + 1u < F.ranges && F.ticket[r + 1u] <= t) {
+            ++r;
+        }
+        const uint32_t ck = F.colour_kind[r];
+        const uint32_t idx = (t - F.ticket[r]) * 32u + lane;
+        if (idx < F.count[r]) {
+            const uint32_t i = F.first[r] + idx;
+            const bool joint = (ck & kFlowJoints) != 0u;
+            if (joint) {
+                uint32_t a, b, flags;
+                joint_head(S, i, a, b, flags);
+                const uint32_t rank = S.jrank[i];
+                if ((flags & kJWriteA) != 0u) {
+                    flow_wait(S.done, a, rank & kRankMask, err);
+                }
+                if ((flags & kJWriteB) != 0u) {
+                    flow_wait(S.done, b, (rank >> kRankBits) & kRankMask, err);
+                }
+                flow_joint<P>(S, i, K);
+            } else if (P == kWarm) {
+                warm_manifold(S, i, gate);
+            } else {
+                solve_manifold_staged<P == kSolve, 32, false, false>(S, i, K, T, gate);
+            }
+            // The header again (the pass kept none of it live): the bodies written, released.
+            uint32_t a, b;
+            bool wa, wb;
+            written_bodies(S, joint, i, a, b, wa, wb);
+            if (wa) {
+                red_release_gpu_add(&S.done[a], 1u);
+            }
+            if (wb) {
+                red_release_gpu_add(&S.done[b], 1u);
+            }
+        }
+        t = __shfl_sync(0xFFFFFFFFu, next, 0);
+    }
+}
+
+// The colour of constraint k of a kind, from its colour table (NPH_GPU_COLORS: the overflow).
+NPH_D uint32_t colour_of(const ColorTable &tab, uint32_t k)
+{
+    uint32_t colour = NPH_GPU_COLORS;
+    for (uint32_t c = 0; c < NPH_GPU_COLORS; ++c) {
+        if (k >= tab.cfirst[c] && k - tab.cfirst[c] < tab.ccount[c]) {
+            colour = c;
+        }
+    }
+    return colour;
+}
+
+// The colours whose constraints write each body slot (bit c of cmask).
+__global__ void __launch_bounds__(kBlock) k_colour_masks(DevSolver S, uint32_t m, uint32_t nj, ColorTable C,
+                                                         ColorTable J)
+{
+    const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
+    if (i >= m + nj) {
+        return;
+    }
+    const bool joint = i >= m;
+    const uint32_t k = joint ? i - m : i;
+    const uint32_t colour = colour_of(joint ? J : C, k);
+    if (colour == NPH_GPU_COLORS) {
+        return; // the overflow runs before the pass
+    }
+    uint32_t a, b;
+    bool wa, wb;
+    written_bodies(S, joint, k, a, b, wa, wb);
+    uint32_t *mask = const_cast<uint32_t *>(S.cmask);
+    if (wa) {
+        atomicOr(&mask[a], 1u << colour);
+    }
+    if (wb) {
+        atomicOr(&mask[b], 1u << colour);
+    }
+}
+
+// Each constraint's ranks on the bodies it writes (the earlier colours in their masks): a
+// manifold's into hdr.w, a joint's into jrank.
+__global__ void __launch_bounds__(kBlock) k_colour_ranks(DevSolver S, uint32_t m, uint32_t nj, ColorTable C,
+                                                         ColorTable J)
+{
+    const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
+    if (i >= m + nj) {
+        return;
+    }
+    const bool joint = i >= m;
+    const uint32_t k = joint ? i - m : i;
+    const uint32_t colour = colour_of(joint ? J : C, k);
+    uint32_t a, b;
+    bool wa, wb;
+    written_bodies(S, joint, k, a, b, wa, wb);
+    const uint32_t below = colour < NPH_GPU_COLORS ? (1u << colour) - 1u : 0u;
+    const uint32_t ra = wa ? (uint32_t)__popc(S.cmask[a] & below) : 0u;
+    const uint32_t rb = wb ? (uint32_t)__popc(S.cmask[b] & below) : 0u;
+    const uint32_t rank = ra | (rb << kRankBits);
+    if (joint) {
+        S.jrank[k] = rank;
+    } else {
+        S.hdr[k].w = rank;
     }
 }
 
@@ -994,6 +1228,10 @@ struct NphGpuSolver {
     float *rest = nullptr;
     float4 *pa = nullptr, *pb = nullptr, *pt = nullptr, *pi = nullptr;
     float4 *jw = nullptr;
+    // The dependency-driven passes: per body slot the colours that write it and the finished
+    // constraints of the current pass; done[n + 1] the pass's next warp ticket.
+    uint32_t *cmask = nullptr, *done = nullptr;
+    uint32_t *jrank = nullptr; // per joint: its ranks on its bodies
     uint32_t *d_err = nullptr;     // [0] error bits, [1..25] points per colour slot
     uint32_t *h_err = nullptr;     // pinned copy of the same 26 words
     // Per-launch timing of a profiled step.
@@ -1069,10 +1307,11 @@ void drop_graph(NphGpuSolver *s)
 // Device bytes of the record and row arrays at these capacities.
 uint64_t array_bytes(uint64_t bcap, uint64_t fcap, uint64_t mcap, uint64_t jcap)
 {
-    return bcap * (sizeof(NphGpuBody) + 13u * sizeof(float4)) + fcap * sizeof(NphGpuBody) +
+    return bcap * (sizeof(NphGpuBody) + 13u * sizeof(float4) + 2u * sizeof(uint32_t)) + 2u * sizeof(uint32_t) +
+           fcap * sizeof(NphGpuBody) +
            mcap * (sizeof(NphGpuContact) + sizeof(uint4) + sizeof(float4) + sizeof(float) +
                    16u * sizeof(float4)) +
-           jcap * (sizeof(NphGpuJoint) + (uint64_t)kJointRows * sizeof(float4));
+           jcap * (sizeof(NphGpuJoint) + (uint64_t)kJointRows * sizeof(float4) + sizeof(uint32_t));
 }
 
 // Device bytes of the packed drop-in's arrays at these capacities.
@@ -1124,7 +1363,7 @@ NphGpuResult ensure_capacity(NphGpuSolver *s, uint32_t n, uint32_t nf, uint32_t 
         const uint32_t cap = n + 1u + (n + 1u) / 8u;
         // vel, pos and prm in one allocation: the body rows the constraint passes gather.
         ok = ok && dalloc(s->d_bodies, cap) && dalloc(s->body_rows, 7ull * cap) &&
-             dalloc(s->itg, 6ull * cap);
+             dalloc(s->itg, 6ull * cap) && dalloc(s->cmask, cap) && dalloc(s->done, cap + 2ull);
         if (ok) {
             s->vel = s->body_rows;
             s->pos = s->body_rows + 2ull * cap;
@@ -1146,7 +1385,7 @@ NphGpuResult ensure_capacity(NphGpuSolver *s, uint32_t n, uint32_t nf, uint32_t 
     }
     if (ok && nj > s->jcap) {
         const uint32_t cap = nj + nj / 8u + 1u;
-        ok = dalloc(s->d_joints, cap) && dalloc(s->jw, (size_t)kJointRows * cap);
+        ok = dalloc(s->d_joints, cap) && dalloc(s->jw, (size_t)kJointRows * cap) && dalloc(s->jrank, cap);
         s->jcap = ok ? cap : 0;
     }
     if (!ok) {
@@ -1174,6 +1413,9 @@ DevSolver dev_solver(const NphGpuSolver *s)
     S.mcap = s->mcap;
     S.jw = s->jw;
     S.jcap = s->jcap;
+    S.cmask = s->cmask;
+    S.done = s->done;
+    S.jrank = s->jrank;
     return S;
 }
 
@@ -1255,6 +1497,56 @@ template <int P> void enqueue_pass(NphGpuSolver *s, const StepConsts &K)
         mark_end(s);
         s->launches++;
     }
+    const uint32_t cfg = s->pass_config[P];
+    if constexpr (P != kRestitution) {
+    if (kPassConfigs[cfg].staged == 5u) {
+        // Every colour in one dependency-driven launch (k_pass_flow).
+        FlowTable F{};
+        uint32_t tickets = 0, ranges = 0;
+        uint64_t units = 0;
+        double flow_bytes = 0.0;
+        for (uint32_t c = 0; c < NPH_GPU_COLORS; ++c) {
+            for (uint32_t half = 0; half < 2u; ++half) { // the colour's joints, then its contacts
+                const bool joint = half == 0u;
+                const uint32_t count = joint ? s->jcount[c] : s->ccount[c];
+                if (count > 0u) {
+                    F.ticket[ranges] = tickets;
+                    F.first[ranges] = joint ? s->jfirst[c] : s->cfirst[c];
+                    F.count[ranges] = count;
+                    F.colour_kind[ranges] = c | (joint ? kFlowJoints : 0u);
+                    tickets += (count + 31u) / 32u;
+                    ranges += 1u;
+                }
+            }
+            units += (uint64_t)s->ccount[c] + s->jcount[c];
+            flow_bytes += bytes(c, s->jcount[c]);
+        }
+        F.ranges = ranges;
+        F.tickets = tickets;
+        if (tickets == 0u) {
+            return;
+        }
+        static const uint32_t sms = [] {
+            int dev = 0, n = 148;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+            return (uint32_t)n;
+        }();
+        const uint32_t grid = std::min<uint32_t>(tickets, sms * kPassConfigs[cfg].min_blocks);
+        const size_t smem = P == kWarm ? 0 : (size_t)kPointSlots * 32u * sizeof(float4);
+        uint32_t *ticket = s->done + s->n + 1u;
+        cudaMemsetAsync(s->done, 0, (s->n + 2ull) * sizeof(uint32_t), s->stream);
+        mark_begin(s, kind, units, flow_bytes);
+        switch (kPassConfigs[cfg].min_blocks) {
+        case 16: k_pass_flow<P, 16><<<grid, 32, smem, s->stream>>>(S, F, K, ticket, s->d_err); break;
+        case 20: k_pass_flow<P, 20><<<grid, 32, smem, s->stream>>>(S, F, K, ticket, s->d_err); break;
+        default: k_pass_flow<P, 18><<<grid, 32, smem, s->stream>>>(S, F, K, ticket, s->d_err); break;
+        }
+        mark_end(s);
+        s->launches++;
+        return;
+    }
+    }
     for (uint32_t c = 0; c < NPH_GPU_COLORS; ++c) {
         const uint32_t jc = P == kRestitution ? 0u : s->jcount[c];
         const uint32_t cc = s->ccount[c];
@@ -1323,6 +1615,22 @@ void enqueue_prepare(NphGpuSolver *s, const StepConsts &K)
             S, s->d_contacts, s->d_fixed, s->n, s->nf, s->m, T, s->d_err, s->d_err + 1);
         mark_end(s);
         s->launches++;
+    }
+    bool flow = false;
+    for (uint32_t p = kWarm; p <= kRelax; ++p) {
+        flow = flow || kPassConfigs[s->pass_config[p]].staged == 5u;
+    }
+    if (flow && s->m + s->nj > 0u) {
+        // The colours that write each body, for the dependency-driven passes.
+        ColorTable J;
+        std::memcpy(J.cfirst, s->jfirst, sizeof J.cfirst);
+        std::memcpy(J.ccount, s->jcount, sizeof J.ccount);
+        cudaMemsetAsync(s->cmask, 0, (s->n + 1ull) * sizeof(uint32_t), s->stream);
+        mark_begin(s, kKPrepareConstraints, (uint64_t)s->m + s->nj, 56.0 * (s->m + s->nj));
+        k_colour_masks<<<blocks_for((uint64_t)s->m + s->nj), kBlock, 0, s->stream>>>(S, s->m, s->nj, T, J);
+        k_colour_ranks<<<blocks_for((uint64_t)s->m + s->nj), kBlock, 0, s->stream>>>(S, s->m, s->nj, T, J);
+        mark_end(s);
+        s->launches += 2u;
     }
 }
 
@@ -1661,6 +1969,9 @@ NphGpuResult read_error(NphGpuSolver *s)
         return r;
     }
     s->stats.error_word = *s->h_err;
+    if ((*s->h_err & kErrWait) != 0u) {
+        return NPH_GPU_DEVICE_LOST;
+    }
     return *s->h_err != 0u ? NPH_GPU_INVALID_ARGUMENT : NPH_GPU_OK;
 }
 
@@ -1927,6 +2238,9 @@ NPH_GPU_API void nph_gpu_solver_destroy(NphGpuSolver *s)
     dfree(s->body_rows);
     s->vel = s->pos = s->prm = nullptr;
     dfree(s->itg);
+    dfree(s->cmask);
+    dfree(s->done);
+    dfree(s->jrank);
     dfree(s->hdr);
     dfree(s->nrm);
     dfree(s->rest);

@@ -65,6 +65,8 @@ def lib() -> ctypes.CDLL:
         "nph_gpu_mlp_train": (ctypes.c_int32, [_vp, _vp, _vp, ctypes.c_uint64, _u32, _u32,
                                                ctypes.c_float, ctypes.c_uint64,
                                                P(ctypes.c_float)]),
+        "nph_gpu_mlp_time_kernels": (ctypes.c_int32, [_vp, ctypes.c_uint64, _u32, P(ctypes.c_float),
+                                                      P(ctypes.c_float)]),
         "nph_gpu_world_features": (ctypes.c_int32, [_vp, P(abi.WorldParams), ctypes.c_float, _vp,
                                                     _vp, _vp, ctypes.c_uint64]),
         "nph_gpu_solver_set_warm_start_model": (ctypes.c_int32, [_vp, _vp]),
@@ -362,6 +364,14 @@ class Mlp:
                                             g.ctypes.data, ctypes.byref(loss)),
                "nph_gpu_mlp_gradients")
         return g, float(loss.value)
+
+    def time_kernels(self, count: int, reps: int = 5) -> dict:
+        """nph_gpu_mlp_time_kernels: device milliseconds of one forward and one gradient
+        launch over `count` device-resident synthetic rows."""
+        f, g = ctypes.c_float(), ctypes.c_float()
+        _check(self.L.nph_gpu_mlp_time_kernels(self._h, count, reps, ctypes.byref(f), ctypes.byref(g)),
+               "nph_gpu_mlp_time_kernels")
+        return {"forward_ms": float(f.value), "gradients_ms": float(g.value)}
 
     def train(self, x: np.ndarray, t: np.ndarray, epochs: int, batch: int, lr: float,
               seed: int = 0) -> float:

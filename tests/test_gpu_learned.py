@@ -206,12 +206,15 @@ def gated_against_plain_and_learned(solver, net, view, params, tol=1e-4, max_pas
 
 
 def test_gated_start_falls_back_to_the_plain_start(solver):
-    """A network whose starts push every new contact far too hard (an untrained network with
-    its weights scaled up): the gate sees the larger residual and the plain start runs."""
+    """A network whose starts push every new contact far too hard (an untrained network whose
+    normal output's bias, the last layer's first bias, is set to 50 impulse scales): the gate
+    sees the larger residual and the plain start runs."""
     from nepheline_b200.solver import Mlp
     params = abi.WorldParams.default()
     net = Mlp(seed=11)
-    net.set_weights(net.get_weights() * 8.0)
+    w = net.get_weights()
+    w[-abi.MLP_OUTPUTS] = 50.0
+    net.set_weights(w)
     try:
         assert not gated_against_plain_and_learned(solver, net, moving_world(seed=8), params)
     finally:
