@@ -300,13 +300,27 @@ def reference_sample(dims, steps: int, warmup: int, workers: int, params) -> dic
             "manifolds": manifolds, "bodies": len(sc.bodies), "dims": tuple(dims)}
 
 
-# The solve pass's DRAM bytes per launch on the 128 x 128 x 64 lattice: an ncu capture of the
-# same kernel (dram__bytes_read.sum + dram__bytes_write.sum) on the 96 x 96 x 64 lattice, scaled
-# to this workload's launches by their manifolds (profiles/solve_traffic_lattice.md).
-SOLVE_TRAFFIC_PER_LAUNCH = 149_700_000
-SOLVE_TRAFFIC_SOURCE = ("ncu capture of the solve pass on the 96x96x64 lattice scaled by "
-                        "manifolds to this workload's launches; a constant, not measured in "
-                        "this run")
+# DRAM bytes per constraint of the pass kernels (dram__bytes_read.sum + dram__bytes_write.sum
+# of one ncu capture on the 96 x 96 x 64 lattice, over the constraints that launch ran), by pass
+# kind and configuration form; the bench scales them by the units of its own launches. ncu
+# flushes the caches before a capture, so these are upper figures for the bench's warm L2.
+# Lean staged, a colour a launch: 145.8 and 146.3 MB over a colour of 248,672 manifolds
+# (profiles/pass_staged_lean_lattice_96x96x64.md); dependency-driven, a pass a launch: 1,067.5 MB
+# over 1,747,968 manifolds and 174,797 joints (profiles/pass_flow_lattice_96x96x64.md).
+TRAFFIC_PER_UNIT = {("relax", "lean"): 586.3, ("solve", "lean"): 588.3, ("relax", "flow"): 555.2}
+TRAFFIC_SOURCE = ("ncu DRAM bytes per constraint of the same kernel on the 96x96x64 lattice x "
+                  "this launch's constraints; a constant of the build, not measured in this run")
+LEAN_CONFIGS, FLOW_CONFIGS = range(10, 15), range(19, 22)
+
+
+def pass_form(config: int):
+    """The configuration form whose traffic was captured, or None."""
+    if config in LEAN_CONFIGS:
+        return "lean"
+    if config in FLOW_CONFIGS:
+        return "flow"
+    return None
+
 
 def _out_fields(view) -> dict:
     """The outputs phys_solve writes, per field (contact points within each manifold's count)."""
@@ -857,7 +871,7 @@ def run_learned(args):
                    "bodies": int(held.n), "eval_steps": eval_steps, "max_passes": args.max_passes,
                    "training": dict(fit, world_steps=args.pile_worlds * args.train_steps,
                                     world_steps_asked=50000, steps=args.train_steps,
-                                    samples=sampled, data_s=data_s, plain_step_s=step_s,
+                                    sample_steps=sampled, data_s=data_s, plain_step_s=step_s,
                                     train_s=train_s, epochs=args.epochs)},
         "plain": plain if plain is not None else args.max_passes * len(evals),
         "plain_reached": plain is not None,
@@ -1018,10 +1032,12 @@ def main():
     # DRAM bytes per launch of the dominant kernel cannot be counted inside this run (that
     # takes a profiler): the figure is this build's ncu capture of the same kernel, scaled to
     # this workload's launches, and the line says so.
-    traffic = SOLVE_TRAFFIC_PER_LAUNCH if top[0] == "solve" and tuple(dims) == (128, 128, 64) else None
+    kind_index = {"warm_start": 0, "solve": 1, "relax": 2, "restitution": 3}.get(top[0])
+    per_unit = TRAFFIC_PER_UNIT.get((top[0], pass_form(tuned[kind_index]))) if kind_index is not None else None
+    traffic = per_unit * top[1]["units"] / top[1]["launches"] if per_unit else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
                 "frac": achieved / pk["hbm_gbs"], "traffic": traffic,
-                "traffic_source": SOLVE_TRAFFIC_SOURCE if traffic else None, "kernel": top[0],
+                "traffic_source": TRAFFIC_SOURCE if traffic else None, "kernel": top[0],
                 "peak_source": pk["source"], "launches_per_step": top[1]["launches"] // 3,
                 "ms_per_launch": per_launch_ms, "algorithmic_bytes_per_launch": per_launch_bytes,
                 "kernel_share": top[1]["total_ms"] / sum(v["total_ms"] for v in kinds.values())}

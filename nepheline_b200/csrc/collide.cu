@@ -134,7 +134,10 @@ __global__ void __launch_bounds__(256) k_scatter(const uint32_t *counts, const u
 
 // Four blocks an SM (64 registers): 0.5 % faster on the mixed pairs than three (80 registers),
 // which were 5 % faster than two.
-__global__ void __launch_bounds__(256, 4) k_collide_sorted(const NphGpuShape *a, const NphGpuPose *pa,
+#ifndef NPH_COLLIDE_BLOCKS_PER_SM
+#define NPH_COLLIDE_BLOCKS_PER_SM 4
+#endif
+__global__ void __launch_bounds__(256, NPH_COLLIDE_BLOCKS_PER_SM) k_collide_sorted(const NphGpuShape *a, const NphGpuPose *pa,
                                                         const NphGpuShape *b, const NphGpuPose *pb,
                                                         const float *spec, uint32_t count, const uint32_t *order,
                                                         NphGpuManifold *out, uint32_t *bad)
