@@ -132,10 +132,12 @@ __global__ void __launch_bounds__(256) k_scatter(const uint32_t *counts, const u
     }
 }
 
-// Four blocks an SM (64 registers): 0.5 % faster on the mixed pairs than three (80 registers),
-// which were 5 % faster than two.
+// Three blocks an SM (80 registers): on the 4,194,304 mixed pairs 3.72 ms against 3.70 for four
+// (64 registers) and 3.91 for two (109); DRAM bytes a launch 24 % fewer than with four, 39 %
+// more than with two: each thread's clip polygons, candidates and corners live in local
+// memory, and fewer resident threads keep more of those lines in L2.
 #ifndef NPH_COLLIDE_BLOCKS_PER_SM
-#define NPH_COLLIDE_BLOCKS_PER_SM 4
+#define NPH_COLLIDE_BLOCKS_PER_SM 3
 #endif
 __global__ void __launch_bounds__(256, NPH_COLLIDE_BLOCKS_PER_SM) k_collide_sorted(const NphGpuShape *a, const NphGpuPose *pa,
                                                         const NphGpuShape *b, const NphGpuPose *pb,
