@@ -306,8 +306,10 @@ def reference_sample(dims, steps: int, warmup: int, workers: int, params) -> dic
 # flushes the caches before a capture, so these are upper figures for the bench's warm L2.
 # Lean staged, a colour a launch: 145.8 and 146.3 MB over a colour of 248,672 manifolds
 # (profiles/pass_staged_lean_lattice_96x96x64.md); dependency-driven, a pass a launch: 1,067.5 MB
-# over 1,747,968 manifolds and 174,797 joints (profiles/pass_flow_lattice_96x96x64.md).
-TRAFFIC_PER_UNIT = {("relax", "lean"): 586.3, ("solve", "lean"): 588.3, ("relax", "flow"): 555.2}
+# (relax) and 1,097.6 MB (solve) over 1,747,968 manifolds and 174,797 joints
+# (profiles/pass_flow_lattice_96x96x64.md).
+TRAFFIC_PER_UNIT = {("relax", "lean"): 586.3, ("solve", "lean"): 588.3, ("relax", "flow"): 555.2,
+                    ("solve", "flow"): 570.9}
 TRAFFIC_SOURCE = ("ncu DRAM bytes per constraint of the same kernel on the 96x96x64 lattice x "
                   "this launch's constraints; a constant of the build, not measured in this run")
 LEAN_CONFIGS, FLOW_CONFIGS = range(10, 15), range(19, 22)
