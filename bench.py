@@ -312,14 +312,12 @@ TRAFFIC_PER_UNIT = {("relax", "lean"): 586.3, ("solve", "lean"): 588.3, ("relax"
                     ("solve", "flow"): 570.9}
 TRAFFIC_SOURCE = ("ncu DRAM bytes per constraint of the same kernel on the 96x96x64 lattice x "
                   "this launch's constraints; a constant of the build, not measured in this run")
-LEAN_CONFIGS, FLOW_CONFIGS = range(10, 15), range(19, 22)
-
-
 def pass_form(config: int):
     """The configuration form whose traffic was captured, or None."""
-    if config in LEAN_CONFIGS:
+    from nepheline_b200 import abi
+    if config in abi.PASS_CONFIGS_LEAN:
         return "lean"
-    if config in FLOW_CONFIGS:
+    if config in abi.PASS_CONFIGS_FLOW:
         return "flow"
     return None
 

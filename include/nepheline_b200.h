@@ -501,6 +501,11 @@ NPH_GPU_API void *nph_gpu_solver_stream(const NphGpuSolver *solver);
 NPH_GPU_API NphGpuResult nph_gpu_solver_set_memory_limit(NphGpuSolver *solver, uint64_t bytes);
 /* The bytes the solver's record and row arrays hold now (the figure the budget limits). */
 NPH_GPU_API uint64_t nph_gpu_solver_memory(const NphGpuSolver *solver);
+/* Failure injection for the dependency-driven passes (a test hook; 0, the default: off). Every
+ * constraint then waits for `extra` more finished constraints on its bodies than will come, so
+ * its waits give up after about a second: the call returns NPH_GPU_DEVICE_LOST with nothing
+ * written back, and the solver (and its device context) takes the next call as usual. */
+NPH_GPU_API NphGpuResult nph_gpu_solver_set_wait_injection(NphGpuSolver *solver, uint32_t extra);
 
 /* One kind of kernel in a profiled step. */
 typedef struct NphGpuKernelTime {

@@ -231,6 +231,10 @@ class KernelTime(ctypes.Structure):
 BATCH_SHARED_NONE, BATCH_SHARED_SMALL, BATCH_SHARED_LARGE = 0, 1, 2
 BATCH_PERSISTENT, BATCH_MERGED = 0, 1
 START_PLAIN, START_LEARNED, START_GATED = 0, 1, 2
+# Pass configurations (csrc/solver.cu kPassConfigs) of the lean staged form, a colour a launch,
+# and of the dependency-driven form, a pass a launch.
+PASS_CONFIGS_LEAN = range(10, 15)
+PASS_CONFIGS_FLOW = range(19, 22)
 
 # The learned warm start's network and point slots (nepheline_b200.h).
 MLP_INPUTS, MLP_HIDDEN, MLP_OUTPUTS = 16, 64, 3

@@ -709,7 +709,7 @@ __global__ void __launch_bounds__(kBlock) k_colour_masks(DevSolver S, uint32_t m
 // Each constraint's ranks on the bodies it writes (the earlier colours in their masks): a
 // manifold's into hdr.w, a joint's into jrank.
 __global__ void __launch_bounds__(kBlock) k_colour_ranks(DevSolver S, uint32_t m, uint32_t nj, ColorTable C,
-                                                         ColorTable J)
+                                                         ColorTable J, uint32_t extra)
 {
     const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
     if (i >= m + nj) {
@@ -722,8 +722,8 @@ __global__ void __launch_bounds__(kBlock) k_colour_ranks(DevSolver S, uint32_t m
     bool wa, wb;
     written_bodies(S, joint, k, a, b, wa, wb);
     const uint32_t below = colour < NPH_GPU_COLORS ? (1u << colour) - 1u : 0u;
-    const uint32_t ra = wa ? (uint32_t)__popc(S.cmask[a] & below) : 0u;
-    const uint32_t rb = wb ? (uint32_t)__popc(S.cmask[b] & below) : 0u;
+    const uint32_t ra = wa ? (uint32_t)__popc(S.cmask[a] & below) + extra : 0u;
+    const uint32_t rb = wb ? (uint32_t)__popc(S.cmask[b] & below) + extra : 0u;
     const uint32_t rank = ra | (rb << kRankBits);
     if (joint) {
         S.jrank[k] = rank;
@@ -1208,6 +1208,7 @@ struct NphGpuSolver {
     // Capacities of the device arrays.
     uint32_t bcap = 0, fcap = 0, mcap = 0, jcap = 0;
     uint64_t memory_limit = 0; // bytes the record and row arrays may take (0: no limit)
+    uint32_t wait_injection = 0; // added to every dependency count (a test hook)
     // The packed drop-in's device arrays (allocated by its first call).
     NphGpuBodyInput *in_bodies = nullptr;
     NphGpuContactInput *in_contacts = nullptr;
@@ -1628,7 +1629,8 @@ void enqueue_prepare(NphGpuSolver *s, const StepConsts &K)
         cudaMemsetAsync(s->cmask, 0, (s->n + 1ull) * sizeof(uint32_t), s->stream);
         mark_begin(s, kKPrepareConstraints, (uint64_t)s->m + s->nj, 56.0 * (s->m + s->nj));
         k_colour_masks<<<blocks_for((uint64_t)s->m + s->nj), kBlock, 0, s->stream>>>(S, s->m, s->nj, T, J);
-        k_colour_ranks<<<blocks_for((uint64_t)s->m + s->nj), kBlock, 0, s->stream>>>(S, s->m, s->nj, T, J);
+        k_colour_ranks<<<blocks_for((uint64_t)s->m + s->nj), kBlock, 0, s->stream>>>(S, s->m, s->nj, T, J,
+                                                                                     s->wait_injection);
         mark_end(s);
         s->launches += 2u;
     }
@@ -2615,6 +2617,18 @@ NPH_GPU_API NphGpuResult nph_gpu_solver_set_memory_limit(NphGpuSolver *s, uint64
 NPH_GPU_API uint64_t nph_gpu_solver_memory(const NphGpuSolver *s)
 {
     return s != nullptr ? array_bytes(s->bcap, s->fcap, s->mcap, s->jcap) : 0u;
+}
+
+NPH_GPU_API NphGpuResult nph_gpu_solver_set_wait_injection(NphGpuSolver *s, uint32_t extra)
+{
+    if (s == nullptr || extra > 64u) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    if (s->wait_injection != extra) {
+        s->wait_injection = extra;
+        drop_graph(s);
+    }
+    return NPH_GPU_OK;
 }
 
 } // extern "C"

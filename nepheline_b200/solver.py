@@ -49,6 +49,7 @@ def lib() -> ctypes.CDLL:
         "nph_gpu_solver_stats": (ctypes.c_int32, [_vp, P(abi.StepStats)]),
         "nph_gpu_solver_stream": (_vp, [_vp]),
         "nph_gpu_solver_set_memory_limit": (ctypes.c_int32, [_vp, ctypes.c_uint64]),
+        "nph_gpu_solver_set_wait_injection": (ctypes.c_int32, [_vp, _u32]),
         "nph_gpu_solver_memory": (ctypes.c_uint64, [_vp]),
         "nph_gpu_graph_color": (ctypes.c_int32, [_vp, _vp, _vp, _vp, _u32, _u32, _vp, _vp]),
         "nph_gpu_version": (ctypes.c_char_p, []),
@@ -197,6 +198,12 @@ class Solver:
     def memory(self) -> int:
         """Bytes the record and row arrays hold now."""
         return int(self.L.nph_gpu_solver_memory(self._h))
+
+    def set_wait_injection(self, extra: int) -> None:
+        """Test hook: the dependency-driven passes' waits ask for `extra` more finished
+        constraints than will come, so they give up (0: off)."""
+        _check(self.L.nph_gpu_solver_set_wait_injection(self._h, int(extra)),
+               "nph_gpu_solver_set_wait_injection")
 
     def stats(self) -> abi.StepStats:
         st = abi.StepStats()

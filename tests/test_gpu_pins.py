@@ -9,6 +9,9 @@
   (test_sensor.c:342-392): a device-array growth beyond the solver's memory budget returns
   OUT_OF_MEMORY and leaves the view untouched (world.h:163-165: the step did not happen); a body
   with a non-finite value is refused with INVALID_ARGUMENT before anything is written back.
+* A device wait that runs out, without a fault: the dependency-driven passes' waits are given
+  counts that never come; each gives up after about a second, the call returns DEVICE_LOST with
+  the view untouched, and the same solver then steps the view as the restatement does.
 """
 from __future__ import annotations
 
@@ -111,3 +114,30 @@ def test_a_body_with_a_non_finite_value_is_refused(solver, ref_lib, field, index
     v = good.copy()
     solver.phys_solve(v, params, DT)
     assert not helpers.mismatches(v, port32(good, params, DT))
+
+
+def test_a_wait_that_runs_out_fails_the_call_and_the_next_call_works(ref_lib):
+    import time
+
+    from nepheline_b200.solver import Solver, SolverError
+    from oracle.refworld import port32
+    params = abi.WorldParams.default()
+    good = lattice_view(5, seed=4)
+    s = Solver(device=0)
+    try:
+        for kind in (1, 2):  # solve and relax, dependency-driven
+            s.set_pass_config(kind, abi.PASS_CONFIGS_FLOW[0])
+        s.set_wait_injection(1)
+        v = good.copy()
+        t0 = time.perf_counter()
+        with pytest.raises(SolverError) as err:
+            s.phys_solve(v, params, DT)
+        assert err.value.code == abi.DEVICE_LOST
+        assert time.perf_counter() - t0 < 60.0
+        for name in ("bodies", "contacts", "joints"):
+            assert getattr(v, name).tobytes() == getattr(good, name).tobytes(), name
+        s.set_wait_injection(0)
+        s.phys_solve(v, params, DT)
+        assert not helpers.mismatches(v, port32(good, params, DT))
+    finally:
+        s.close()
