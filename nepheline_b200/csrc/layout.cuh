@@ -33,9 +33,12 @@
 namespace nph {
 
 // A constraint's rank on a body it writes, in hdr.w for a manifold (A in bits 0-7, B in bits
-// 8-15): how many constraints of earlier colours write that body (at most the colours).
+// 8-15): how many constraints of earlier colours write that body (at most the colours); bits
+// 16 and 17: a constraint of a later colour writes A, B (only then is its finishing counted).
 constexpr uint32_t kRankBits = 8u;
 constexpr uint32_t kRankMask = 0xFFu;
+constexpr uint32_t kRankLaterA = 1u << 16;
+constexpr uint32_t kRankLaterB = 1u << 17;
 
 // Manifold header bits (hdr.z).
 constexpr uint32_t kHdrPointsMask = 7u;        // the manifold's own point count, 0..4

@@ -617,16 +617,32 @@ k_pass_flow(DevSolver S, FlowTable F, StepConsts K, uint32_t *ticket, uint32_t *
     const uint32_t lane = threadIdx.x;
     const Tile<32> T{tile, lane};
     const FlowGate gate{S.done, err};
-    // The next ticket is taken while the current one runs.
-    uint32_t t = 0u;
+    // Tickets two deep: while ticket t runs, the next one is known (its constraint's header
+    // fetched into L1 ahead of it) and the one after is being taken.
+    uint32_t t = 0u, t1 = 0u;
     if (lane == 0u) {
         t = atomicAdd(ticket, 1u);
+        t1 = atomicAdd(ticket, 1u);
     }
     t = __shfl_sync(0xFFFFFFFFu, t, 0);
+    t1 = __shfl_sync(0xFFFFFFFFu, t1, 0);
     while (t < F.tickets) {
         uint32_t next = 0u;
         if (lane == 0u) {
             next = atomicAdd(ticket, 1u);
+        }
+        if (t1 < F.tickets) {
+            uint32_t r1 = 0u;
+            while (r1 + 1u < F.ranges && F.ticket[r1 + 1u] <= t1) {
+                ++r1;
+            }
+            const uint32_t idx1 = (t1 - F.ticket[r1]) * 32u + lane;
+            if (idx1 < F.count[r1]) {
+                const uint32_t i1 = F.first[r1] + idx1;
+                const void *row = (F.colour_kind[r1] & kFlowJoints) != 0u ? (const void *)&S.jw[kJrHead * S.jcap + i1]
+                                                                          : (const void *)&S.hdr[i1];
+                asm volatile("prefetch.global.L1 [%0];\n" ::"l"(row));
+            }
         }
         uint32_t r = 0u;
         while (r + 1u < F.ranges && F.ticket[r + 1u] <= t) {
@@ -653,18 +669,21 @@ k_pass_flow(DevSolver S, FlowTable F, StepConsts K, uint32_t *ticket, uint32_t *
             } else {
                 solve_manifold_staged<P == kSolve, 32, false, false>(S, i, K, T, gate);
             }
-            // The header again (the pass kept none of it live): the bodies written, released.
+            // The header again (the pass kept none of it live): the bodies written, released
+            // where a constraint of a later colour waits on them.
             uint32_t a, b;
             bool wa, wb;
             written_bodies(S, joint, i, a, b, wa, wb);
-            if (wa) {
+            const uint32_t rank = joint ? S.jrank[i] : S.hdr[i].w;
+            if (wa && (rank & kRankLaterA) != 0u) {
                 red_release_gpu_add(&S.done[a], 1u);
             }
-            if (wb) {
+            if (wb && (rank & kRankLaterB) != 0u) {
                 red_release_gpu_add(&S.done[b], 1u);
             }
         }
-        t = __shfl_sync(0xFFFFFFFFu, next, 0);
+        t = t1;
+        t1 = __shfl_sync(0xFFFFFFFFu, next, 0);
     }
 }
 
@@ -722,9 +741,12 @@ __global__ void __launch_bounds__(kBlock) k_colour_ranks(DevSolver S, uint32_t m
     bool wa, wb;
     written_bodies(S, joint, k, a, b, wa, wb);
     const uint32_t below = colour < NPH_GPU_COLORS ? (1u << colour) - 1u : 0u;
-    const uint32_t ra = wa ? (uint32_t)__popc(S.cmask[a] & below) + extra : 0u;
-    const uint32_t rb = wb ? (uint32_t)__popc(S.cmask[b] & below) + extra : 0u;
-    const uint32_t rank = ra | (rb << kRankBits);
+    const uint32_t above = colour < NPH_GPU_COLORS ? ~((2u << colour) - 1u) : 0u;
+    const uint32_t ma = wa ? S.cmask[a] : 0u, mb = wb ? S.cmask[b] : 0u;
+    const uint32_t ra = wa ? (uint32_t)__popc(ma & below) + extra : 0u;
+    const uint32_t rb = wb ? (uint32_t)__popc(mb & below) + extra : 0u;
+    const uint32_t rank = ra | (rb << kRankBits) | ((ma & above) != 0u ? kRankLaterA : 0u) |
+                          ((mb & above) != 0u ? kRankLaterB : 0u);
     if (joint) {
         S.jrank[k] = rank;
     } else {
