@@ -632,6 +632,9 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_set_config(NphGpuBatch *batch,
  * step and download calls do not use them. */
 #define NPH_GPU_BATCH_MAX_PARTS 16u
 NPH_GPU_API NphGpuResult nph_gpu_batch_set_pipeline(NphGpuBatch *batch, uint32_t parts);
+/* The merged packing's pass configuration per pass kind, as nph_gpu_solver_set_pass_config
+ * (the autotuner sets them too). Results do not depend on it. */
+NPH_GPU_API NphGpuResult nph_gpu_batch_set_pass_config(NphGpuBatch *batch, uint32_t pass, uint32_t config);
 NPH_GPU_API uint32_t nph_gpu_batch_config_count(void);
 /* The batch autotuner: times every configuration on the uploaded worlds (`rounds` timed steps
  * each after an untimed one; the worlds advance) and keeps the fastest. */

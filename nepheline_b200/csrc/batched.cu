@@ -495,6 +495,8 @@ StepConsts make_step_consts(const NphGpuWorldParams &p, float dt);
 
 using namespace nph;
 
+constexpr uint32_t kNoPassConfig = 0xFFFFFFFFu; // the merged solver's own pass configuration
+
 struct NphGpuBatch {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -512,6 +514,7 @@ struct NphGpuBatch {
     // state lives in the solver (true after a merged step, until the next upload).
     uint32_t packing = NPH_GPU_BATCH_PERSISTENT;
     NphGpuSolver *merged = nullptr;
+    uint32_t merged_pass[4] = {kNoPassConfig, kNoPassConfig, kNoPassConfig, kNoPassConfig}; // set ones
     uint32_t *d_cmap = nullptr, *d_cworld = nullptr, *d_jmap = nullptr, *d_jworld = nullptr;
     uint64_t cap_cmap = 0, cap_jmap = 0;
     bool maps_valid = false;
@@ -934,6 +937,14 @@ NphGpuResult merged_setup(NphGpuBatch *b, bool sync = true)
         r = nph_gpu_solver_create(&d, &b->merged);
         if (r != NPH_GPU_OK) {
             b->merged = nullptr;
+            return r;
+        }
+        for (uint32_t p = 0; p < 4u && r == NPH_GPU_OK; ++p) {
+            if (b->merged_pass[p] != kNoPassConfig) {
+                r = nph_gpu_solver_set_pass_config(b->merged, p, b->merged_pass[p]);
+            }
+        }
+        if (r != NPH_GPU_OK) {
             return r;
         }
     }
@@ -1707,6 +1718,18 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_set_pipeline(NphGpuBatch *b, uint32_t par
     b->pipeline_parts = parts;
     if (parts == 1u) {
         return ensure_parts(b, 0u); // the parts' arrays released
+    }
+    return NPH_GPU_OK;
+}
+
+NPH_GPU_API NphGpuResult nph_gpu_batch_set_pass_config(NphGpuBatch *b, uint32_t pass, uint32_t config)
+{
+    if (b == nullptr || pass >= 4u || config >= nph_gpu_pass_config_count()) {
+        return NPH_GPU_INVALID_ARGUMENT;
+    }
+    b->merged_pass[pass] = config;
+    if (b->merged != nullptr) {
+        return nph_gpu_solver_set_pass_config(b->merged, pass, config);
     }
     return NPH_GPU_OK;
 }

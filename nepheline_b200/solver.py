@@ -50,6 +50,7 @@ def lib() -> ctypes.CDLL:
         "nph_gpu_solver_stream": (_vp, [_vp]),
         "nph_gpu_solver_set_memory_limit": (ctypes.c_int32, [_vp, ctypes.c_uint64]),
         "nph_gpu_solver_set_wait_injection": (ctypes.c_int32, [_vp, _u32]),
+        "nph_gpu_batch_set_pass_config": (ctypes.c_int32, [_vp, _u32, _u32]),
         "nph_gpu_solver_memory": (ctypes.c_uint64, [_vp]),
         "nph_gpu_graph_color": (ctypes.c_int32, [_vp, _vp, _vp, _vp, _u32, _u32, _vp, _vp]),
         "nph_gpu_version": (ctypes.c_char_p, []),
@@ -472,6 +473,13 @@ class Batch:
         _check(self.L.nph_gpu_batch_hit_events(self._h, threshold, out.ctypes.data, cap, ctypes.byref(count)),
                "nph_gpu_batch_hit_events")
         return out[:min(int(count.value), cap)]
+
+    def set_merged_pass_configs(self, configs) -> None:
+        """The merged packing's pass configuration per pass kind (warm start, solve, relax,
+        restitution), as Solver.set_pass_config."""
+        for kind, config in enumerate(configs):
+            _check(self.L.nph_gpu_batch_set_pass_config(self._h, kind, int(config)),
+                   "nph_gpu_batch_set_pass_config")
 
     def set_pipeline(self, parts: int) -> None:
         """phys_solve_worlds in `parts` consecutive runs of worlds, each on its own stream, so
