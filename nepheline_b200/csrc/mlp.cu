@@ -309,8 +309,51 @@ __device__ __forceinline__ void store_a(__nv_bfloat16 (*dst)[kHidRow], const uin
     }
 }
 
+// The block's FP32 gradient in shared memory: each weight matrix's rows kAccPad floats longer
+// than the matrix is wide, so that a warp's 32 atomic adds of one tensor-core tile (eight rows,
+// four column pairs) fall in distinct banks but for pairs (the rows 64 floats apart put them in
+// four banks), then the biases.
+constexpr int kAccPad = 4;
+constexpr int kAccW1 = 0;
+constexpr int kAccW2 = kAccW1 + kHid * (kIn + kAccPad);
+constexpr int kAccW3 = kAccW2 + kHid * (kHid + kAccPad);
+constexpr int kAccW4 = kAccW3 + kHid * (kHid + kAccPad);
+constexpr int kAccB1 = kAccW4 + kOut * (kHid + kAccPad);
+constexpr int kAccB2 = kAccB1 + kHid;
+constexpr int kAccB3 = kAccB2 + kHid;
+constexpr int kAccB4 = kAccB3 + kHid;
+constexpr int kAcc = kAccB4 + kOut;
+
+// The accumulator slot of parameter p.
+__device__ __forceinline__ int acc_index(int p)
+{
+    if (p < kB1) {
+        return kAccW1 + (p - kW1) / kIn * (kIn + kAccPad) + (p - kW1) % kIn;
+    }
+    if (p < kW2) {
+        return kAccB1 + p - kB1;
+    }
+    if (p < kB2) {
+        return kAccW2 + (p - kW2) / kHid * (kHid + kAccPad) + (p - kW2) % kHid;
+    }
+    if (p < kW3) {
+        return kAccB2 + p - kB2;
+    }
+    if (p < kB3) {
+        return kAccW3 + (p - kW3) / kHid * (kHid + kAccPad) + (p - kW3) % kHid;
+    }
+    if (p < kW4) {
+        return kAccB3 + p - kB3;
+    }
+    if (p < kB4) {
+        return kAccW4 + (p - kW4) / kHid * (kHid + kAccPad) + (p - kW4) % kHid;
+    }
+    return kAccB4 + p - kB4;
+}
+
 // grad[o][i] += sum over the tile's 16 samples of dz[s][o] h[s][i], for O outputs x I inputs,
-// on the tensor cores (A = dz^T, B = h), accumulated into fp32 shared memory.
+// on the tensor cores (A = dz^T, B = h), accumulated into fp32 shared memory (rows I + kAccPad
+// floats apart).
 template <int O, int I>
 __device__ void weight_grad(const __nv_bfloat16 (*dz)[kHidRow], const __nv_bfloat16 (*h)[kHidRow], float *grad,
                             int g, int t)
@@ -333,13 +376,14 @@ __device__ void weight_grad(const __nv_bfloat16 (*dz)[kHidRow], const __nv_bfloa
             const uint32_t b1 = pair2(h[2 * t + 8][i], h[2 * t + 9][i]);
             mma(d, a, b0, b1);
             const int c = nt * 8 + 2 * t;
+            constexpr int kRow = I + kAccPad;
             if (o0 < O) {
-                atomicAdd(&grad[o0 * I + c], d[0]);
-                atomicAdd(&grad[o0 * I + c + 1], d[1]);
+                atomicAdd(&grad[o0 * kRow + c], d[0]);
+                atomicAdd(&grad[o0 * kRow + c + 1], d[1]);
             }
             if (o1 < O) {
-                atomicAdd(&grad[o1 * I + c], d[2]);
-                atomicAdd(&grad[o1 * I + c + 1], d[3]);
+                atomicAdd(&grad[o1 * kRow + c], d[2]);
+                atomicAdd(&grad[o1 * kRow + c + 1], d[3]);
             }
         }
     }
@@ -383,7 +427,7 @@ __device__ __forceinline__ void mask_to_a(float d[8][4], const bool m[8][4], uin
 struct GradSmem {
     SmemWeights W;
     SmemTile T[kWarps];
-    float acc[kParams];
+    float acc[kAcc];
 };
 
 // Forward, loss and gradients of the mean squared error over `count` samples; the gradient
@@ -397,7 +441,7 @@ k_mlp_gradients(const float *x, const float *target, uint32_t count, float norm,
     GradSmem &G = *reinterpret_cast<GradSmem *>(smem_raw);
     SmemWeights &W = G.W;
     float *acc = G.acc;
-    for (int i = threadIdx.x; i < kParams; i += blockDim.x) {
+    for (int i = threadIdx.x; i < kAcc; i += blockDim.x) {
         acc[i] = 0.0f;
     }
     load_weights(W, wb, master);
@@ -435,12 +479,12 @@ k_mlp_gradients(const float *x, const float *target, uint32_t count, float norm,
         S.dz[g + 8][c + 1] = __float2bfloat16(dy[3]);
         store_a(S.h, F.a3, g, t);
         __syncwarp();
-        weight_grad<kOut, kHid>(S.dz, S.h, acc + kW4, g, t);
+        weight_grad<kOut, kHid>(S.dz, S.h, acc + kAccW4, g, t);
         if (c < kOut) {
-            atomicAdd(&acc[kB4 + c], dy[0] + dy[2]);
+            atomicAdd(&acc[kAccB4 + c], dy[0] + dy[2]);
         }
         if (c + 1 < kOut) {
-            atomicAdd(&acc[kB4 + c + 1], dy[1] + dy[3]);
+            atomicAdd(&acc[kAccB4 + c + 1], dy[1] + dy[3]);
         }
         uint32_t dz_out[4];
         dz_out[0] = pack_bf16(dy[0], dy[1]);
@@ -462,11 +506,11 @@ k_mlp_gradients(const float *x, const float *target, uint32_t count, float norm,
         store_tile(S.dz, d, g, t);
         store_a(S.h, F.a2, g, t);
         __syncwarp();
-        weight_grad<kHid, kHid>(S.dz, S.h, acc + kW3, g, t);
+        weight_grad<kHid, kHid>(S.dz, S.h, acc + kAccW3, g, t);
 #pragma unroll
         for (int nt = 0; nt < 8; ++nt) {
-            atomicAdd(&acc[kB3 + nt * 8 + c], d[nt][0] + d[nt][2]);
-            atomicAdd(&acc[kB3 + nt * 8 + c + 1], d[nt][1] + d[nt][3]);
+            atomicAdd(&acc[kAccB3 + nt * 8 + c], d[nt][0] + d[nt][2]);
+            atomicAdd(&acc[kAccB3 + nt * 8 + c + 1], d[nt][1] + d[nt][3]);
         }
         back_mm(dz3, W.w3t, g, t, d);
         // Layer 2.
@@ -476,11 +520,11 @@ k_mlp_gradients(const float *x, const float *target, uint32_t count, float norm,
         store_tile(S.dz, d, g, t);
         store_a(S.h, F.a1, g, t);
         __syncwarp();
-        weight_grad<kHid, kHid>(S.dz, S.h, acc + kW2, g, t);
+        weight_grad<kHid, kHid>(S.dz, S.h, acc + kAccW2, g, t);
 #pragma unroll
         for (int nt = 0; nt < 8; ++nt) {
-            atomicAdd(&acc[kB2 + nt * 8 + c], d[nt][0] + d[nt][2]);
-            atomicAdd(&acc[kB2 + nt * 8 + c + 1], d[nt][1] + d[nt][3]);
+            atomicAdd(&acc[kAccB2 + nt * 8 + c], d[nt][0] + d[nt][2]);
+            atomicAdd(&acc[kAccB2 + nt * 8 + c + 1], d[nt][1] + d[nt][3]);
         }
         back_mm(dz2, W.w2t, g, t, d);
         // Layer 1: dZ1 = dH1 * relu'(z1); dW1 = dZ1^T x.
@@ -497,11 +541,11 @@ k_mlp_gradients(const float *x, const float *target, uint32_t count, float norm,
         *reinterpret_cast<uint32_t *>(&S.h[g][2 * t + 8]) = F.a0[2];
         *reinterpret_cast<uint32_t *>(&S.h[g + 8][2 * t + 8]) = F.a0[3];
         __syncwarp();
-        weight_grad<kHid, kIn>(S.dz, S.h, acc + kW1, g, t);
+        weight_grad<kHid, kIn>(S.dz, S.h, acc + kAccW1, g, t);
 #pragma unroll
         for (int nt = 0; nt < 8; ++nt) {
-            atomicAdd(&acc[kB1 + nt * 8 + c], d[nt][0] + d[nt][2]);
-            atomicAdd(&acc[kB1 + nt * 8 + c + 1], d[nt][1] + d[nt][3]);
+            atomicAdd(&acc[kAccB1 + nt * 8 + c], d[nt][0] + d[nt][2]);
+            atomicAdd(&acc[kAccB1 + nt * 8 + c + 1], d[nt][1] + d[nt][3]);
         }
         (void)dz1;
     }
@@ -516,8 +560,9 @@ k_mlp_gradients(const float *x, const float *target, uint32_t count, float norm,
     }
     __syncthreads();
     for (int i = threadIdx.x; i < kParams; i += blockDim.x) {
-        if (acc[i] != 0.0f) {
-            atomicAdd(&grad[i], acc[i]);
+        const float v = acc[acc_index(i)];
+        if (v != 0.0f) {
+            atomicAdd(&grad[i], v);
         }
     }
 }
