@@ -11,8 +11,9 @@
 // columns (2t, 2t+1) of rows g and g+8 is exactly what the A fragment needs, so only a bias,
 // a ReLU and a conversion to bf16 sit between layers. The network is 64 units wide: a
 // 16-sample warp tile keeps a whole forward and backward pass in registers, which a
-// 128-row tcgen05 tile with its TMEM round trips would not improve at this width (the kernels
-// are bound by reading their feature rows, not by the tensor pipe).
+// 128-row tcgen05 tile with its TMEM round trips would not improve at this width (measured, the
+// forward kernel is bound by instruction issue and the gradient kernel by its shared-memory
+// adds of the weight gradients, neither by the tensor pipe).
 //
 // Training: mean squared error on the three outputs; the backward pass propagates through
 // the same fragments (dH = dZ W on the tensor cores with the transposed weights), and the
