@@ -537,8 +537,11 @@ NPH_GPU_API NphGpuResult nph_gpu_solver_set_pass_config(NphGpuSolver *solver, ui
 NPH_GPU_API uint32_t nph_gpu_pass_config_count(void);
 
 /* The autotuner: times every pass configuration on the uploaded world (`rounds` timed steps
- * each, after one untimed step) and keeps the fastest per pass kind, written to chosen[4]
- * when not NULL. Each timed step is a real step: the world advances. */
+ * each, after one untimed step, launch by launch) and keeps the fastest per pass kind, written
+ * to chosen[4] when not NULL. With a step graph, the solve and relax passes' best
+ * dependency-driven configuration is then weighed against the choice over whole graph steps
+ * (rounds + 1 each), where a colour's joints run beside its contacts. Each timed step is a
+ * real step: the world advances. */
 NPH_GPU_API NphGpuResult nph_gpu_solver_autotune(NphGpuSolver *solver,
                                                  const NphGpuWorldParams *params, float dt,
                                                  uint32_t rounds, uint32_t *chosen);

@@ -2567,6 +2567,12 @@ NPH_GPU_API NphGpuResult nph_gpu_solver_autotune(NphGpuSolver *s, const NphGpuWo
         best[p] = s->pass_config[p];
     }
     rounds = rounds == 0u ? 1u : rounds;
+    double flow_ms[4];
+    uint32_t flow[4];
+    for (uint32_t p = 0; p < 4; ++p) {
+        flow_ms[p] = 1e300;
+        flow[p] = kPassConfigCount;
+    }
     for (uint32_t c = 0; c < kPassConfigCount; ++c) {
         for (uint32_t p = 0; p < 4; ++p) {
             s->pass_config[p] = c;
@@ -2601,6 +2607,56 @@ NPH_GPU_API NphGpuResult nph_gpu_solver_autotune(NphGpuSolver *s, const NphGpuWo
                 best_ms[p] = ms[p];
                 best[p] = c;
             }
+            if (kPassConfigs[c].staged == 5u && ms[p] < flow_ms[p]) {
+                flow_ms[p] = ms[p];
+                flow[p] = c;
+            }
+        }
+    }
+    // Launch by launch, a dependency-driven pass counts its colours' joints and a colour a
+    // launch does not (its joints are a kind of their own, beside it in the step's graph), so
+    // the two forms are compared once more over whole steps of the graph: the chosen set
+    // against the same with solve and relax dependency-driven.
+    if (s->use_graph && flow[kSolve] < kPassConfigCount && flow[kRelax] < kPassConfigCount &&
+        (best[kSolve] != flow[kSolve] || best[kRelax] != flow[kRelax])) {
+        auto step_ms = [&](const uint32_t cfg[4], double &out) -> NphGpuResult {
+            std::memcpy(s->pass_config, cfg, 4 * sizeof(uint32_t));
+            drop_graph(s);
+            NphGpuResult q = launch_step(s, K, params->substeps); // captures and warms
+            cudaEvent_t e0 = nullptr, e1 = nullptr;
+            cudaEventCreate(&e0);
+            cudaEventCreate(&e1);
+            cudaEventRecord(e0, s->stream);
+            for (uint32_t i = 0; i < rounds + 1u && q == NPH_GPU_OK; ++i) {
+                q = launch_step(s, K, params->substeps);
+            }
+            cudaEventRecord(e1, s->stream);
+            if (q == NPH_GPU_OK) {
+                q = check_cuda(cudaEventSynchronize(e1));
+            }
+            float t = 0.0f;
+            if (q == NPH_GPU_OK) {
+                cudaEventElapsedTime(&t, e0, e1);
+            }
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            out = t;
+            return q;
+        };
+        uint32_t with_flow[4];
+        std::memcpy(with_flow, best, sizeof with_flow);
+        with_flow[kSolve] = flow[kSolve];
+        with_flow[kRelax] = flow[kRelax];
+        double plain_ms = 0.0, flow_step_ms = 0.0;
+        r = step_ms(best, plain_ms);
+        if (r == NPH_GPU_OK) {
+            r = step_ms(with_flow, flow_step_ms);
+        }
+        if (r != NPH_GPU_OK) {
+            return r;
+        }
+        if (flow_step_ms < plain_ms) {
+            std::memcpy(best, with_flow, sizeof best);
         }
     }
     for (uint32_t p = 0; p < 4; ++p) {
