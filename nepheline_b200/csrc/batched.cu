@@ -1396,6 +1396,45 @@ NphGpuResult batch_finish(NphGpuBatch *b)
 // Every record the device would refuse (check_world's and prepare's checks: a joint's or a
 // manifold's body outside its world, a manifold without points or with more than four), on
 // the host, so that a pipelined call refuses a batch before any of it is written back.
+// check_world over every world, on up to 16 host threads; the result of the first world (in
+// order) that fails, as a loop over the worlds would return it.
+NphGpuResult check_worlds(const NphGpuWorldView *worlds, uint32_t count)
+{
+    const uint32_t threads = std::max(1u, std::min({16u, std::thread::hardware_concurrency(), count / 64u}));
+    std::vector<uint32_t> first_bad(threads, count);
+    std::vector<NphGpuResult> code(threads, NPH_GPU_OK);
+    auto scan = [&](uint32_t t, uint32_t first, uint32_t end) {
+        for (uint32_t w = first; w < end; ++w) {
+            const NphGpuResult r = check_world(worlds[w]);
+            if (r != NPH_GPU_OK) {
+                first_bad[t] = w;
+                code[t] = r;
+                return;
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (uint32_t t = 1; t < threads; ++t) {
+        const uint32_t first = (uint32_t)((uint64_t)count * t / threads);
+        const uint32_t end = (uint32_t)((uint64_t)count * (t + 1) / threads);
+        try {
+            pool.emplace_back(scan, t, first, end);
+        } catch (...) { // no thread to be had: this one scans the run
+            scan(t, first, end);
+        }
+    }
+    scan(0u, 0u, (uint32_t)((uint64_t)count / threads));
+    for (std::thread &th : pool) {
+        th.join();
+    }
+    for (uint32_t t = 0; t < threads; ++t) { // the runs are in world order
+        if (first_bad[t] < count) {
+            return code[t];
+        }
+    }
+    return NPH_GPU_OK;
+}
+
 NphGpuResult check_records(const NphGpuWorldView *worlds, uint32_t count)
 {
     std::atomic<uint32_t> bad{0};
@@ -1417,7 +1456,7 @@ NphGpuResult check_records(const NphGpuWorldView *worlds, uint32_t count)
             }
         }
     };
-    const uint32_t threads = std::max(1u, std::min({8u, std::thread::hardware_concurrency(), count / 64u}));
+    const uint32_t threads = std::max(1u, std::min({16u, std::thread::hardware_concurrency(), count / 64u}));
     std::vector<std::thread> pool;
     for (uint32_t t = 1; t < threads; ++t) {
         const uint32_t first = (uint32_t)((uint64_t)count * t / threads);
@@ -1559,8 +1598,8 @@ NPH_GPU_API NphGpuResult nph_gpu_batch_upload(NphGpuBatch *b, const NphGpuWorldV
     if (b == nullptr || (count > 0 && worlds == nullptr)) {
         return NPH_GPU_INVALID_ARGUMENT;
     }
-    for (uint32_t w = 0; w < count; ++w) {
-        const NphGpuResult r = check_world(worlds[w]);
+    {
+        const NphGpuResult r = check_worlds(worlds, count);
         if (r != NPH_GPU_OK) {
             return r;
         }
@@ -1624,11 +1663,9 @@ NPH_GPU_API NphGpuResult nph_gpu_phys_solve_worlds(NphGpuBatch *b, const NphGpuW
             params->enable_continuous != 0u) {
             return NPH_GPU_UNSUPPORTED;
         }
-        for (uint32_t w = 0; w < count; ++w) {
-            const NphGpuResult r = check_world(worlds[w]);
-            if (r != NPH_GPU_OK) {
-                return r;
-            }
+        const NphGpuResult r = check_worlds(worlds, count);
+        if (r != NPH_GPU_OK) {
+            return r;
         }
         return solve_in_parts(b, params, dt, worlds, count);
     }
