@@ -1262,17 +1262,43 @@ NphGpuResult upload_begin(NphGpuBatch *b, const NphGpuWorldView *worlds, uint32_
             cf += s.ccount[c];
             jf += s.jcount[c];
         }
-        for (uint32_t j = 0; j < v.joint_count; ++j) {
-            const NphGpuJoint &jr = v.joints[j];
-            s.driven += nph_joint_is_driven(&jr) ? 1u : 0u;
-            s.row_joints += (nph_joint_has_axes(jr.type) || jr.type == NPH_GPU_JOINT_DISTANCE) ? 1u : 0u;
-        }
         bodies += v.body_count;
         slots += v.body_count + 1u;
         fixed += v.fixed_count;
         contacts += v.contact_count;
         joints += v.joint_count;
         max_slots = std::max<uint64_t>(max_slots, v.body_count + 1u);
+    }
+    // Each world's driven and row-type joints: a read of every joint record, on host threads.
+    {
+        const uint32_t threads = std::max(1u, std::min({16u, std::thread::hardware_concurrency(), count / 64u}));
+        auto scan = [&](uint32_t first, uint32_t end) {
+            for (uint32_t w = first; w < end; ++w) {
+                const NphGpuWorldView &v = worlds[w];
+                uint32_t driven = 0, rows = 0;
+                for (uint32_t j = 0; j < v.joint_count; ++j) {
+                    const NphGpuJoint &jr = v.joints[j];
+                    driven += nph_joint_is_driven(&jr) ? 1u : 0u;
+                    rows += (nph_joint_has_axes(jr.type) || jr.type == NPH_GPU_JOINT_DISTANCE) ? 1u : 0u;
+                }
+                slices[w].driven = driven;
+                slices[w].row_joints = rows;
+            }
+        };
+        std::vector<std::thread> pool;
+        for (uint32_t t = 1; t < threads; ++t) {
+            const uint32_t first = (uint32_t)((uint64_t)count * t / threads);
+            const uint32_t end = (uint32_t)((uint64_t)count * (t + 1) / threads);
+            try {
+                pool.emplace_back(scan, first, end);
+            } catch (...) { // no thread to be had: this one scans the run
+                scan(first, end);
+            }
+        }
+        scan(0u, (uint32_t)((uint64_t)count / threads));
+        for (std::thread &th : pool) {
+            th.join();
+        }
     }
     if (slots >= 0xFFFFFFF0ull || contacts >= 0xFFFFFFF0ull || joints >= 0xFFFFFFF0ull ||
         4ull * contacts >= 0xFFFFFFF0ull || (uint64_t)kJointRows * joints >= 0xFFFFFFF0ull) {
