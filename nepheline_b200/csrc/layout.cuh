@@ -11,7 +11,7 @@
 //               all zero unless dynamic (PhysSolverParams, prepare_group's dyn ? .. : 0)
 //     itg[6i..] what integration reads (PhysSolverParams, world_internal.h:403-417)
 //   manifolds (colour order; capacity `mcap`), one lane each:
-//     hdr       solver indices of A and B, and the manifold's bits (kHdr*)
+//     hdr       solver indices of A and B, the manifold's bits (kHdr*), its ranks (kRank*)
 //     nrm       normal.xyz, friction              rest  restitution
 //     per point k, row k*mcap + g:
 //       pa      anchor_a.xyz, adjusted separation
